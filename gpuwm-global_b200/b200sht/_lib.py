@@ -1,0 +1,95 @@
+"""ctypes binding of ``libb200sht.so`` (the C ABI in ``include/b200sht.h``).
+
+There is no CPU fallback: if the library is missing or fails to load, every
+call raises.  Loading does not touch the GPU; the first plan does.
+"""
+from __future__ import annotations
+
+import ctypes
+from pathlib import Path
+
+LIB_PATH = Path(__file__).resolve().parents[1] / "lib" / "libb200sht.so"
+
+SHT_ABI_VERSION = 1
+SHT_PREC_F64 = 0
+SHT_PREC_F32 = 1
+SHT_PREC_SPLIT16 = 2
+SHT_OK = 0
+SHT_ERR_ARG = 1
+SHT_ERR_CUDA = 2
+SHT_ERR_DEVICE = 3
+SHT_ERR_STATE = 4
+
+#: Every symbol ``include/b200sht.h`` declares, with its ctypes signature.
+_P = ctypes.c_void_p
+_I64 = ctypes.c_int64
+_D = ctypes.c_double
+_DP = ctypes.POINTER(ctypes.c_double)
+SIGNATURES = {
+    "sht_abi_version": (ctypes.c_int, []),
+    "sht_last_error": (ctypes.c_char_p, []),
+    "sht_plan_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, _D, ctypes.c_int,
+                                       ctypes.c_int, ctypes.POINTER(_P)]),
+    "sht_plan_destroy": (ctypes.c_int, [_P]),
+    "sht_plan_reserve": (ctypes.c_int, [_P, _I64]),
+    "sht_plan_geometry": (ctypes.c_int, [_P, _DP, _DP, _DP]),
+    "sht_plan_check": (ctypes.c_int, [_P]),
+    "sht_forward": (ctypes.c_int, [_P, _P, _I64, _P, _P]),
+    "sht_inverse": (ctypes.c_int, [_P, _P, _I64, _P, _P]),
+    "sht_inverse_meridional_derivative": (ctypes.c_int, [_P, _P, _I64, _P, _P]),
+    "sht_inverse_zonal_derivative": (ctypes.c_int, [_P, _P, _I64, _P, _P]),
+    "sht_gradient": (ctypes.c_int, [_P, _P, _I64, _P, _P, _P]),
+    "sht_wind_from_vordiv": (ctypes.c_int, [_P, _P, _P, _I64, _P, _P, _P]),
+    "sht_vordiv_from_wind": (ctypes.c_int, [_P, _P, _P, _I64, _P, _P, _P]),
+    "sht_project": (ctypes.c_int, [_P, _P, _I64, _P, _P]),
+    "sht_laplacian": (ctypes.c_int, [_P, _P, _I64, _P, _P]),
+    "sht_inverse_laplacian": (ctypes.c_int, [_P, _P, _I64, _P, _P]),
+    "sht_helmholtz_solve": (ctypes.c_int, [_P, ctypes.c_int, _DP, _DP, _DP, _DP, _DP, _D,
+                                           _P, _P, _P, _P, _P, _P, _P]),
+}
+
+_lib = None
+
+
+class ShtError(RuntimeError):
+    """A failing library call (status and message from ``sht_last_error``)."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(message)
+        self.status = status
+
+
+def load(path: Path | None = None):
+    """Load the library once and bind every declared symbol."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    p = Path(path) if path else LIB_PATH
+    if not p.exists():
+        raise ImportError(
+            f"b200sht CUDA library not built ({p}); run "
+            "`python gpuwm-global_b200/b200sht/build.py` or __graft_entry__.build()")
+    lib = ctypes.CDLL(str(p))
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    if lib.sht_abi_version() != SHT_ABI_VERSION:
+        raise ImportError(f"{p}: ABI version {lib.sht_abi_version()} != {SHT_ABI_VERSION}")
+    _lib = lib
+    return lib
+
+
+def check(status: int) -> None:
+    """Raise for a non-zero status: ValueError for argument errors (the
+    reference raises ValueError for bad shapes), ShtError otherwise."""
+    if status == SHT_OK:
+        return
+    msg = (load().sht_last_error() or b"").decode()
+    if status == SHT_ERR_ARG:
+        raise ValueError(msg)
+    raise ShtError(status, msg)
+
+
+def call(name: str, *args) -> None:
+    check(getattr(load(), name)(*args))

@@ -1,0 +1,320 @@
+"""Triangular spherical-harmonic transform pair on a Gaussian grid, on a B200.
+
+Drop-in for the reference's ``SphericalHarmonicTransform``
+(src/arwen_global/spectral/transform.py:632-1863): the same ``create``
+signature, entry points, coefficient layout ``(*lead, T+1, T+1)`` indexed
+``[n, m]`` (zero above the triangle, real at ``m = 0``), grid layout
+``(*lead, nlat, nlon)`` with row 0 southernmost, and the same error messages
+for shape mismatches.  Each call is one C-ABI call into ``libb200sht.so`` on
+the current torch stream; arrays are torch CUDA tensors (numpy inputs are
+copied to the device).
+
+Precision: ``"float64"`` (FP64 SIMT contractions; the parity path),
+``"float32"`` (plain FP32 FFMA contractions) and ``"split16"`` (FP16 hi/lo
+split contractions on tcgen05 tensor cores with FP32 accumulation).  The
+reference's ``tensor_core_contractions=True`` (its TF32 opt-in) selects
+``"split16"`` on a float32 transform.
+
+The reference's memory-layout knobs (``legendre_band``, ``streaming``,
+``latitude_bands``) are accepted and validated but change nothing here: the
+tables are resident in HBM and the contraction walks the triangle directly.
+``order_partition`` (the multi-card order axis) is out of scope and refused.
+"""
+from __future__ import annotations
+
+import ctypes
+import hashlib
+import json
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+import torch
+
+from . import _lib
+from .backend import Backend, get_backend
+from .grid import EARTH_RADIUS_M, GaussianGrid, shape_for
+
+_PREC_CODE = {"float64": _lib.SHT_PREC_F64, "float32": _lib.SHT_PREC_F32,
+              "split16": _lib.SHT_PREC_SPLIT16}
+
+
+class Plan:
+    """Owns one ``sht_plan`` handle."""
+
+    def __init__(self, truncation, nlat, nlon, radius_m, precision):
+        self._lib = _lib.load()
+        handle = ctypes.c_void_p()
+        _lib.check(self._lib.sht_plan_create(int(truncation), int(nlat), int(nlon),
+                                             float(radius_m), _PREC_CODE[precision], 0,
+                                             ctypes.byref(handle)))
+        self.handle = handle
+
+    def geometry(self, nlat):
+        mu, w, cl = (np.zeros(nlat) for _ in range(3))
+        dp = ctypes.POINTER(ctypes.c_double)
+        _lib.check(self._lib.sht_plan_geometry(self.handle, mu.ctypes.data_as(dp),
+                                               w.ctypes.data_as(dp), cl.ctypes.data_as(dp)))
+        return mu, w, cl
+
+    def reserve(self, planes):
+        _lib.check(self._lib.sht_plan_reserve(self.handle, int(planes)))
+
+    def check(self):
+        _lib.check(self._lib.sht_plan_check(self.handle))
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h is not None and h.value:
+            try:
+                self._lib.sht_plan_destroy(h)
+            except Exception:
+                pass
+            self.handle = None
+
+
+def _ptr(t: torch.Tensor):
+    return ctypes.c_void_p(t.data_ptr())
+
+
+def _stream():
+    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+@dataclass
+class SphericalHarmonicTransform:
+    grid: GaussianGrid
+    backend: Backend
+    plan: Plan = field(repr=False)
+    tensor_core_contractions: bool = False
+    legendre_band: int = 32
+    streaming: bool = False
+    latitude_bands: int = 1
+    #: Number of Legendre contractions issued (the reference's census seam,
+    #: tools/arwen_global_transform_census.py counts ``_batched_contract``).
+    contraction_count: int = 0
+
+    @classmethod
+    def create(cls, truncation, *, nlat=None, nlon=None, dealias_factor=1.5, radius_m=None,
+               grid=None, backend="b200", precision="float32",
+               tensor_core_contractions=False, legendre_band=32, streaming=False,
+               latitude_bands=1, order_partition=(), device=None):
+        if tuple(order_partition or ()):
+            raise ValueError("order_partition (the multi-card order axis) is not built by the "
+                             "B200 engine: the whole table is resident on one GPU")
+        if int(legendre_band) < 1:
+            raise ValueError(f"legendre_band must be >= 1, got {legendre_band}")
+        if int(latitude_bands) < 1:
+            raise ValueError(f"latitude_bands must be >= 1, got {latitude_bands}")
+        prec = str(precision).strip().lower()
+        if tensor_core_contractions:
+            if prec not in ("float32", "split16"):
+                raise ValueError("tensor_core_contractions=True requires precision='float32'")
+            prec = "split16"
+        be = get_backend(backend, prec, device)
+        if grid is not None:
+            if nlat is not None or nlon is not None or radius_m is not None or dealias_factor != 1.5:
+                raise ValueError("grid= carries its own shape and radius: nlat, nlon, "
+                                 "dealias_factor and radius_m cannot be combined with it")
+            g = grid.truncated_to(truncation)
+            nl, no, rad = g.nlat, g.nlon, g.radius_m
+            t = int(truncation)
+        else:
+            nl, no = shape_for(truncation, nlat=nlat, nlon=nlon, dealias_factor=dealias_factor)
+            rad = EARTH_RADIUS_M if radius_m is None else float(radius_m)
+            if not math.isfinite(rad) or rad <= 0:
+                raise ValueError("radius_m must be finite and positive")
+            t = int(truncation)
+        with torch.cuda.device(be.device):
+            plan = Plan(t, nl, no, rad, prec)
+            mu, w, cl = plan.geometry(nl)
+        g = GaussianGrid.from_geometry(t, nl, no, mu, w, cl, rad)
+        return cls(g, be, plan, bool(tensor_core_contractions or prec == "split16"),
+                   int(legendre_band), bool(streaming), int(latitude_bands))
+
+    # ------------------------------------------------------------- shape
+    @property
+    def truncation(self) -> int:
+        return self.grid.truncation
+
+    @property
+    def spectral_shape(self):
+        n = self.truncation + 1
+        return n, n
+
+    @property
+    def precision(self) -> str:
+        return self.backend.precision
+
+    @property
+    def geometry_identity(self) -> dict:
+        return {
+            "truncation": int(self.truncation),
+            "nlat": int(self.grid.nlat),
+            "nlon": int(self.grid.nlon),
+            "radius_m": float(self.grid.radius_m),
+            "normalization": "complex-orthonormal-condon-shortley",
+            "latitude_grid": "gauss-legendre-in-sin-latitude",
+        }
+
+    @property
+    def geometry_hash(self) -> str:
+        raw = json.dumps(self.geometry_identity, sort_keys=True, separators=(",", ":")).encode()
+        return hashlib.sha256(raw).hexdigest()
+
+    @property
+    def identity(self) -> dict:
+        payload = {
+            **self.geometry_identity,
+            "backend": self.backend.name,
+            "float_dtype": str(self.backend.float_dtype).replace("torch.", ""),
+        }
+        if self.precision == "split16":
+            # Different arithmetic from the float32 path: never share its hash.
+            payload["tensor_core_contractions"] = "split-fp16-tcgen05"
+        return payload
+
+    @property
+    def identity_hash(self) -> str:
+        raw = json.dumps(self.identity, sort_keys=True, separators=(",", ":")).encode()
+        return hashlib.sha256(raw).hexdigest()
+
+    def zeros(self, *leading):
+        return torch.zeros((*leading, *self.spectral_shape), dtype=self.backend.complex_dtype,
+                           device=self.backend.device)
+
+    # --------------------------------------------------------- validation
+    def _validate_grid(self, f) -> None:
+        if tuple(f.shape[-2:]) != self.grid.shape:
+            raise ValueError(
+                f"grid field has trailing shape {tuple(f.shape[-2:])}, expected {self.grid.shape}")
+
+    def _validate_spectral(self, c) -> None:
+        if tuple(c.shape[-2:]) != self.spectral_shape:
+            raise ValueError(
+                f"spectral field has trailing shape {tuple(c.shape[-2:])}, "
+                f"expected {self.spectral_shape}")
+
+    def _grid_in(self, field):
+        f = self.backend.asarray(field, dtype=self.backend.float_dtype)
+        self._validate_grid(f)
+        return f.contiguous()
+
+    def _spec_in(self, coeff):
+        c = self.backend.asarray(coeff, dtype=self.backend.complex_dtype)
+        self._validate_spectral(c)
+        return c.contiguous()
+
+    @staticmethod
+    def _planes(t: torch.Tensor) -> int:
+        return int(np.prod(t.shape[:-2], dtype=np.int64)) if t.dim() > 2 else 1
+
+    def _empty_grid(self, lead):
+        return torch.empty((*lead, *self.grid.shape), dtype=self.backend.float_dtype,
+                           device=self.backend.device)
+
+    def _empty_spec(self, lead):
+        return torch.empty((*lead, *self.spectral_shape), dtype=self.backend.complex_dtype,
+                           device=self.backend.device)
+
+    # ---------------------------------------------------------- transforms
+    def forward(self, field):
+        """grid -> spectral (transform.py:1486)."""
+        f = self._grid_in(field)
+        out = self._empty_spec(f.shape[:-2])
+        self.contraction_count += 1
+        _lib.call("sht_forward", self.plan.handle, _ptr(f), self._planes(f), _ptr(out), _stream())
+        return out
+
+    def _synth(self, name, coeff):
+        c = self._spec_in(coeff)
+        out = self._empty_grid(c.shape[:-2])
+        self.contraction_count += 1
+        _lib.call(name, self.plan.handle, _ptr(c), self._planes(c), _ptr(out), _stream())
+        return out
+
+    def inverse(self, coeff):
+        """spectral -> grid (transform.py:1742)."""
+        return self._synth("sht_inverse", coeff)
+
+    def inverse_meridional_derivative(self, coeff):
+        """d field / d latitude in grid space (transform.py:1748)."""
+        return self._synth("sht_inverse_meridional_derivative", coeff)
+
+    def inverse_zonal_derivative(self, coeff):
+        """d field / d longitude in grid space (transform.py:1752)."""
+        return self._synth("sht_inverse_zonal_derivative", coeff)
+
+    def gradient(self, coeff):
+        """Physical (east, north) derivatives per metre (transform.py:1762)."""
+        c = self._spec_in(coeff)
+        east = self._empty_grid(c.shape[:-2])
+        north = self._empty_grid(c.shape[:-2])
+        self.contraction_count += 2
+        _lib.call("sht_gradient", self.plan.handle, _ptr(c), self._planes(c), _ptr(east),
+                  _ptr(north), _stream())
+        return east, north
+
+    def _elementwise(self, name, coeff):
+        c = self._spec_in(coeff)
+        out = self._empty_spec(c.shape[:-2])
+        _lib.call(name, self.plan.handle, _ptr(c), self._planes(c), _ptr(out), _stream())
+        return out
+
+    def project(self, coeff):
+        """Triangle mask and real m = 0 column (transform.py:1124-1144)."""
+        return self._elementwise("sht_project", coeff)
+
+    def laplacian(self, coeff):
+        return self._elementwise("sht_laplacian", coeff)
+
+    def inverse_laplacian(self, coeff):
+        return self._elementwise("sht_inverse_laplacian", coeff)
+
+    # ---------------------------------------------------------- diagnostics
+    def spectral_mean_square(self, coeff) -> float:
+        c = self.backend.to_numpy(coeff)
+        self._validate_spectral(c)
+        weight = np.ones(self.truncation + 1)
+        weight[1:] = 2.0
+        total = np.sum(np.abs(c) ** 2 * weight[None, :], axis=(-2, -1))
+        return float(np.asarray(total).mean() / (4.0 * np.pi))
+
+    def power_by_degree(self, coeff) -> np.ndarray:
+        c = self.backend.to_numpy(coeff)
+        weight = np.ones(self.truncation + 1)
+        weight[1:] = 2.0
+        return np.sum(np.abs(c) ** 2 * weight[None, :], axis=-1)
+
+    def constant_coeff(self, value: float):
+        out = self.zeros()
+        out[0, 0] = float(value) * math.sqrt(4.0 * math.pi)
+        return out
+
+    def add_grid_constant(self, coeff, value: float):
+        out = self.backend.asarray(coeff).clone()
+        out[..., 0, 0] += float(value) * math.sqrt(4.0 * math.pi)
+        return out
+
+    def transform_check(self, *, seed: int = 0, max_degree=None) -> dict:
+        """Round trip and Parseval KAT (transform.py:1837-1863)."""
+        rng = np.random.default_rng(seed)
+        t = self.truncation if max_degree is None else min(self.truncation, int(max_degree))
+        coeff = np.zeros(self.spectral_shape, dtype=np.complex128)
+        for n in range(t + 1):
+            for m in range(n + 1):
+                coeff[n, m] = rng.normal() + (0.0j if m == 0 else 1j * rng.normal())
+        grid = self.inverse(coeff)
+        back = self.backend.to_numpy(self.forward(grid))
+        scale = max(1.0, float(np.max(np.abs(coeff))))
+        error = float(np.max(np.abs(back - coeff)) / scale)
+        spatial_ms = self.grid.global_mean(self.backend.to_numpy(grid) ** 2)
+        spectral_ms = float(np.sum(np.abs(coeff) ** 2 * np.where(
+            np.arange(self.truncation + 1)[None, :] == 0, 1.0, 2.0)) / (4.0 * np.pi))
+        parseval = abs(spatial_ms - spectral_ms) / max(1.0, abs(spectral_ms))
+        return {"truncation": self.truncation, "nlat": self.grid.nlat, "nlon": self.grid.nlon,
+                "roundtrip_relative_linf": error, "parseval_relative_error": float(parseval)}
+
+    def check_device(self) -> None:
+        """Raise if a kernel of this plan reported a device error word."""
+        self.plan.check()

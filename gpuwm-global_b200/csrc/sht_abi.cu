@@ -1,0 +1,430 @@
+// C ABI of the b200sht library: plan lifecycle, scratch, and the transform
+// entry points declared in include/b200sht.h.  Each entry point validates its
+// arguments, enqueues kernels on the caller's stream and returns a status; a
+// failure leaves a thread-local message (sht_last_error).
+#include <cstdio>
+#include <exception>
+#include <mutex>
+
+#include "sht_plan.h"
+
+namespace sht {
+
+static thread_local std::string g_error;
+void set_error(const std::string& msg) { g_error = msg; }
+void clear_error() { g_error.clear(); }
+
+namespace {
+
+template <class F>
+int guarded(F&& f) {
+  try {
+    clear_error();
+    f();
+    return SHT_OK;
+  } catch (const Error& e) {
+    set_error(e.msg);
+    return e.code;
+  } catch (const std::exception& e) {
+    set_error(e.what());
+    return SHT_ERR_STATE;
+  }
+}
+
+enum TableKind { kBasis = 0, kDBasis = 1, kAnalysis = 2, kRot = 3, kShear = 4 };
+
+const void* table_ptr(const sht_plan* p, int kind) {
+  switch (kind) {
+    case kBasis: return p->basis;
+    case kDBasis: return p->dbasis;
+    case kAnalysis: return p->analysis;
+    case kRot: return p->rot;
+    default: return p->shear;
+  }
+}
+int table_flip(int kind) { return (kind == kDBasis || kind == kShear) ? 1 : 0; }
+int table_dir(int kind) { return (kind == kBasis || kind == kDBasis) ? 0 : 1; }
+
+void check_plan(const sht_plan* p) {
+  SHT_REQUIRE(p != nullptr, "plan is NULL");
+  SHT_REQUIRE(p->geometry_only || p->basis != nullptr, "plan was not built");
+}
+
+void check_transform_plan(const sht_plan* p) {
+  check_plan(p);
+  SHT_REQUIRE(!p->geometry_only, "geometry-only plan cannot transform");
+}
+
+void check_ptr(const void* ptr, const char* name) {
+  if (ptr == nullptr) throw Error{SHT_ERR_ARG, std::string(name) + " is NULL"};
+}
+
+void ensure_scratch(sht_plan* p, int64_t R) {
+  if (R <= p->scratch_rows) return;
+  SHT_CUDA_OR_THROW(cudaDeviceSynchronize());  // nothing may still read the old buffers
+  for (int i = 0; i < 2; ++i) {
+    if (p->wfold[i]) cudaFree(p->wfold[i]);
+    if (p->cfold[i]) cudaFree(p->cfold[i]);
+    p->wfold[i] = p->cfold[i] = nullptr;
+  }
+  p->scratch_rows = 0;
+  for (int i = 0; i < 2; ++i) {
+    SHT_CUDA_OR_THROW(cudaMalloc(&p->wfold[i], p->elem() * std::max<int64_t>(p->wfold_elems(R), 1)));
+    SHT_CUDA_OR_THROW(cudaMalloc(&p->cfold[i], p->elem() * std::max<int64_t>(p->cfold_elems(R), 1)));
+  }
+  p->scratch_rows = R;
+}
+
+template <typename T>
+void contract(sht_plan* p, int kind, const T* data, T* out, int64_t R, cudaStream_t s) {
+  const int dir = table_dir(kind), flip = table_flip(kind);
+  if constexpr (sizeof(T) == 4) {
+    if (p->prec == SHT_PREC_SPLIT16 && p->tc != nullptr) {
+      launch_gemm_tc(p, dir, flip, kind, data, out, R, s);
+      return;
+    }
+  }
+  launch_gemm_simt<T>(p, dir, flip, static_cast<const T*>(table_ptr(p, kind)), data, out, R, s);
+}
+
+template <typename T>
+void do_forward(sht_plan* p, const T* grid, int64_t planes, T* coeff, cudaStream_t s) {
+  const int64_t R = 2 * planes;
+  ensure_scratch(p, R);
+  T* w = static_cast<T*>(p->wfold[0]);
+  T* c = static_cast<T*>(p->cfold[0]);
+  launch_forward_fold<T>(p, grid, nullptr, planes, w, s);
+  contract<T>(p, kAnalysis, w, c, R, s);
+  launch_unpack<T>(p, kUnpackScalar, c, nullptr, planes, coeff, nullptr, s);
+}
+
+template <typename T>
+void do_synthesis(sht_plan* p, int kind, int mode, const T* coeff, int64_t planes, T* grid,
+                  cudaStream_t s) {
+  const int64_t R = 2 * planes;
+  ensure_scratch(p, R);
+  T* w = static_cast<T*>(p->wfold[0]);
+  T* c = static_cast<T*>(p->cfold[0]);
+  launch_pack<T>(p, coeff, nullptr, planes, kPackPlain, c, s);
+  contract<T>(p, kind, c, w, R, s);
+  launch_inverse_unfold<T>(p, mode, w, nullptr, planes, grid, nullptr, s);
+}
+
+template <typename T>
+void do_gradient(sht_plan* p, const T* coeff, int64_t planes, T* east, T* north,
+                 cudaStream_t s) {
+  const int64_t R = 2 * planes;
+  ensure_scratch(p, R);
+  T* c = static_cast<T*>(p->cfold[0]);
+  T* w0 = static_cast<T*>(p->wfold[0]);
+  T* w1 = static_cast<T*>(p->wfold[1]);
+  launch_pack<T>(p, coeff, nullptr, planes, kPackPlain, c, s);
+  contract<T>(p, kBasis, c, w0, R, s);
+  contract<T>(p, kDBasis, c, w1, R, s);
+  launch_inverse_unfold<T>(p, kUnfoldGradient, w0, w1, planes, east, north, s);
+}
+
+template <typename T>
+void do_wind(sht_plan* p, const T* vort, const T* div, int64_t planes, T* u, T* v,
+             cudaStream_t s) {
+  const int64_t R = 4 * planes;
+  ensure_scratch(p, R);
+  T* c = static_cast<T*>(p->cfold[0]);
+  T* w0 = static_cast<T*>(p->wfold[0]);
+  T* w1 = static_cast<T*>(p->wfold[1]);
+  launch_pack<T>(p, vort, div, planes, kPackInvLap, c, s);
+  contract<T>(p, kBasis, c, w0, R, s);
+  contract<T>(p, kDBasis, c, w1, R, s);
+  launch_inverse_unfold<T>(p, kUnfoldWind, w0, w1, planes, u, v, s);
+}
+
+template <typename T>
+void do_vordiv(sht_plan* p, const T* u, const T* v, int64_t planes, T* vort, T* div,
+               cudaStream_t s) {
+  const int64_t R = 4 * planes;
+  ensure_scratch(p, R);
+  T* w = static_cast<T*>(p->wfold[0]);
+  T* c0 = static_cast<T*>(p->cfold[0]);
+  T* c1 = static_cast<T*>(p->cfold[1]);
+  launch_forward_fold<T>(p, u, v, planes, w, s);
+  contract<T>(p, kRot, w, c0, R, s);
+  contract<T>(p, kShear, w, c1, R, s);
+  launch_unpack<T>(p, kUnpackVorDiv, c0, c1, planes, vort, div, s);
+}
+
+void destroy(sht_plan* p) {
+  if (!p) return;
+  destroy_tc_tables(p);
+  void* ptrs[] = {p->d_mu, p->d_w, p->d_coslat, p->basis, p->dbasis, p->analysis, p->rot,
+                  p->shear, p->tw_l, p->tw_n, p->d_radices, p->d_items[0], p->d_items[1],
+                  p->d_desc[0][0], p->d_desc[0][1], p->d_desc[1][0], p->d_desc[1][1],
+                  p->wfold[0], p->wfold[1], p->cfold[0], p->cfold[1], p->d_err};
+  for (void* q : ptrs)
+    if (q) cudaFree(q);
+  delete p;
+}
+
+#define DISPATCH(p, FN, ...)                       \
+  do {                                             \
+    if ((p)->prec == SHT_PREC_F64)                 \
+      FN<double>(__VA_ARGS__);                     \
+    else                                           \
+      FN<float>(__VA_ARGS__);                      \
+  } while (0)
+
+}  // namespace
+}  // namespace sht
+
+using namespace sht;
+
+extern "C" {
+
+int sht_abi_version(void) { return SHT_ABI_VERSION; }
+
+const char* sht_last_error(void) { return g_error.c_str(); }
+
+int sht_plan_create(int truncation, int nlat, int nlon, double radius_m, int precision,
+                    int flags, sht_plan** out_plan) {
+  return guarded([&] {
+    SHT_REQUIRE(out_plan != nullptr, "out_plan is NULL");
+    *out_plan = nullptr;
+    SHT_REQUIRE(truncation >= 1, "truncation must be >= 1");
+    SHT_REQUIRE(nlat >= truncation + 1, "nlat must be >= truncation + 1");
+    SHT_REQUIRE(nlon % 2 == 0, "nlon must be even");
+    SHT_REQUIRE(nlon >= 2 * truncation + 2, "nlon must be >= 2 * truncation + 2");
+    SHT_REQUIRE(radius_m > 0, "radius_m must be positive");
+    SHT_REQUIRE(precision == SHT_PREC_F64 || precision == SHT_PREC_F32 ||
+                    precision == SHT_PREC_SPLIT16,
+                "precision must be SHT_PREC_F64, SHT_PREC_F32 or SHT_PREC_SPLIT16");
+    SHT_REQUIRE(flags == 0 || flags == SHT_FLAG_GEOMETRY_ONLY,
+                "flags must be 0 or SHT_FLAG_GEOMETRY_ONLY");
+    sht_plan* p = new sht_plan();
+    p->T = truncation;
+    p->nlat = nlat;
+    p->nlon = nlon;
+    p->radius = radius_m;
+    p->prec = precision;
+    cudaStream_t s = nullptr;
+    try {
+      SHT_CUDA_OR_THROW(cudaGetDevice(&p->device));
+      SHT_CUDA_OR_THROW(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+      SHT_CUDA_OR_THROW(cudaMalloc(&p->d_err, sizeof(unsigned) * 4));
+      SHT_CUDA_OR_THROW(cudaMemsetAsync(p->d_err, 0, sizeof(unsigned) * 4, s));
+      p->geometry_only = (flags & SHT_FLAG_GEOMETRY_ONLY) != 0;
+      build_geometry_and_tables(p, s);
+      if (!p->geometry_only) {
+        build_fft(p, s);
+        build_gemm_items(p);
+      }
+      SHT_CUDA_OR_THROW(cudaStreamSynchronize(s));
+      SHT_CUDA_OR_THROW(cudaStreamDestroy(s));
+    } catch (...) {
+      if (s) cudaStreamDestroy(s);
+      destroy(p);
+      throw;
+    }
+    *out_plan = p;
+  });
+}
+
+int sht_plan_destroy(sht_plan* plan) {
+  return guarded([&] {
+    if (plan) cudaDeviceSynchronize();
+    destroy(plan);
+  });
+}
+
+int sht_plan_reserve(sht_plan* plan, int64_t planes) {
+  return guarded([&] {
+    check_transform_plan(plan);
+    SHT_REQUIRE(planes >= 0, "planes must be >= 0");
+    ensure_scratch(plan, 4 * planes);
+  });
+}
+
+int sht_plan_geometry(const sht_plan* plan, double* mu, double* weights, double* coslat) {
+  return guarded([&] {
+    check_plan(plan);
+    size_t n = plan->nlat;
+    if (mu) std::copy(plan->h_mu.begin(), plan->h_mu.begin() + n, mu);
+    if (weights) std::copy(plan->h_w.begin(), plan->h_w.begin() + n, weights);
+    if (coslat) std::copy(plan->h_coslat.begin(), plan->h_coslat.begin() + n, coslat);
+  });
+}
+
+int sht_plan_check(sht_plan* plan) {
+  return guarded([&] {
+    check_plan(plan);
+    SHT_CUDA_OR_THROW(cudaDeviceSynchronize());
+    unsigned h[4] = {0, 0, 0, 0};
+    SHT_CUDA_OR_THROW(cudaMemcpy(h, plan->d_err, sizeof(h), cudaMemcpyDeviceToHost));
+    SHT_CUDA_OR_THROW(cudaMemset(plan->d_err, 0, sizeof(h)));
+    if (h[0] != 0) {
+      char buf[256];
+      snprintf(buf, sizeof(buf),
+               "device error word 0x%x: a kernel gave up on a bounded wait "
+               "(tile %u, stage %u)",
+               h[0], h[1], h[2]);
+      throw Error{SHT_ERR_DEVICE, buf};
+    }
+  });
+}
+
+#define SHT_CHECK_CALL(plan, planes)                                   \
+  check_transform_plan(plan);                                          \
+  SHT_REQUIRE((planes) >= 0, "planes must be >= 0");                   \
+  if ((planes) == 0) return;                                           \
+  cudaStream_t s = static_cast<cudaStream_t>(stream);                  \
+  plan->last_stream = s
+
+#define SHT_TYPED(plan, CALL)                                          \
+  do {                                                                 \
+    if ((plan)->prec == SHT_PREC_F64) {                                \
+      using T = double;                                                \
+      CALL;                                                            \
+    } else {                                                           \
+      using T = float;                                                 \
+      CALL;                                                            \
+    }                                                                  \
+  } while (0)
+
+#define CP(x) static_cast<const T*>(x)
+#define MP(x) static_cast<T*>(x)
+
+int sht_forward(sht_plan* plan, const void* grid, int64_t planes, void* coeff, void* stream) {
+  return guarded([&] {
+    SHT_CHECK_CALL(plan, planes);
+    check_ptr(grid, "grid");
+    check_ptr(coeff, "coeff");
+    SHT_TYPED(plan, do_forward<T>(plan, CP(grid), planes, MP(coeff), s));
+  });
+}
+
+int sht_inverse(sht_plan* plan, const void* coeff, int64_t planes, void* grid, void* stream) {
+  return guarded([&] {
+    SHT_CHECK_CALL(plan, planes);
+    check_ptr(coeff, "coeff");
+    check_ptr(grid, "grid");
+    SHT_TYPED(plan, do_synthesis<T>(plan, kBasis, kUnfoldScalar, CP(coeff), planes, MP(grid), s));
+  });
+}
+
+int sht_inverse_meridional_derivative(sht_plan* plan, const void* coeff, int64_t planes,
+                                      void* grid, void* stream) {
+  return guarded([&] {
+    SHT_CHECK_CALL(plan, planes);
+    check_ptr(coeff, "coeff");
+    check_ptr(grid, "grid");
+    SHT_TYPED(plan, do_synthesis<T>(plan, kDBasis, kUnfoldMeridional, CP(coeff), planes,
+                                    MP(grid), s));
+  });
+}
+
+int sht_inverse_zonal_derivative(sht_plan* plan, const void* coeff, int64_t planes, void* grid,
+                                 void* stream) {
+  return guarded([&] {
+    SHT_CHECK_CALL(plan, planes);
+    check_ptr(coeff, "coeff");
+    check_ptr(grid, "grid");
+    SHT_TYPED(plan, do_synthesis<T>(plan, kBasis, kUnfoldZonal, CP(coeff), planes, MP(grid), s));
+  });
+}
+
+int sht_gradient(sht_plan* plan, const void* coeff, int64_t planes, void* east, void* north,
+                 void* stream) {
+  return guarded([&] {
+    SHT_CHECK_CALL(plan, planes);
+    check_ptr(coeff, "coeff");
+    check_ptr(east, "east");
+    check_ptr(north, "north");
+    SHT_TYPED(plan, do_gradient<T>(plan, CP(coeff), planes, MP(east), MP(north), s));
+  });
+}
+
+int sht_wind_from_vordiv(sht_plan* plan, const void* vorticity, const void* divergence,
+                         int64_t planes, void* u, void* v, void* stream) {
+  return guarded([&] {
+    SHT_CHECK_CALL(plan, planes);
+    check_ptr(vorticity, "vorticity");
+    check_ptr(divergence, "divergence");
+    check_ptr(u, "u");
+    check_ptr(v, "v");
+    SHT_TYPED(plan, do_wind<T>(plan, CP(vorticity), CP(divergence), planes, MP(u), MP(v), s));
+  });
+}
+
+int sht_vordiv_from_wind(sht_plan* plan, const void* u, const void* v, int64_t planes,
+                         void* vorticity, void* divergence, void* stream) {
+  return guarded([&] {
+    SHT_CHECK_CALL(plan, planes);
+    check_ptr(u, "u");
+    check_ptr(v, "v");
+    check_ptr(vorticity, "vorticity");
+    check_ptr(divergence, "divergence");
+    SHT_TYPED(plan, do_vordiv<T>(plan, CP(u), CP(v), planes, MP(vorticity), MP(divergence), s));
+  });
+}
+
+static int elementwise_entry(sht_plan* plan, int mode, const void* in, int64_t planes, void* out,
+                             void* stream) {
+  return guarded([&] {
+    SHT_CHECK_CALL(plan, planes);
+    check_ptr(in, "in");
+    check_ptr(out, "out");
+    SHT_TYPED(plan, launch_elementwise<T>(plan, mode, CP(in), planes, MP(out), s));
+  });
+}
+
+int sht_project(sht_plan* plan, const void* in, int64_t planes, void* out, void* stream) {
+  return elementwise_entry(plan, kElemProject, in, planes, out, stream);
+}
+int sht_laplacian(sht_plan* plan, const void* in, int64_t planes, void* out, void* stream) {
+  return elementwise_entry(plan, kElemLaplacian, in, planes, out, stream);
+}
+int sht_inverse_laplacian(sht_plan* plan, const void* in, int64_t planes, void* out,
+                          void* stream) {
+  return elementwise_entry(plan, kElemInvLaplacian, in, planes, out, stream);
+}
+
+int sht_helmholtz_solve(sht_plan* plan, int nlev, const double* b, const double* c,
+                        const double* eigvec, const double* eigvec_inv,
+                        const double* eigenvalues, double tau_w, const void* divergence,
+                        const void* theta, const void* lnps, void* out_divergence,
+                        void* out_theta, void* out_lnps, void* stream) {
+  return guarded([&] {
+    check_transform_plan(plan);
+    SHT_REQUIRE(nlev >= 1 && nlev <= 96, "nlev must be in [1, 96]");
+    for (const void* q : {(const void*)b, (const void*)c, (const void*)eigvec,
+                          (const void*)eigvec_inv, (const void*)eigenvalues, divergence, theta,
+                          lnps, (const void*)out_divergence, (const void*)out_theta,
+                          (const void*)out_lnps})
+      check_ptr(q, "helmholtz argument");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    plan->last_stream = s;
+    const int L1 = nlev + 1;
+    const size_t nm = (size_t)nlev * L1 * 2 + (size_t)nlev * nlev * 2 + nlev;
+    std::vector<double> host(nm);
+    size_t o = 0;
+    std::copy(b, b + nlev * L1, host.begin() + o);
+    o += nlev * L1;
+    std::copy(c, c + L1 * nlev, host.begin() + o);
+    o += L1 * nlev;
+    std::copy(eigvec, eigvec + nlev * nlev, host.begin() + o);
+    o += nlev * nlev;
+    std::copy(eigvec_inv, eigvec_inv + nlev * nlev, host.begin() + o);
+    o += nlev * nlev;
+    std::copy(eigenvalues, eigenvalues + nlev, host.begin() + o);
+    SHT_TYPED(plan, {
+      std::vector<T> conv(host.begin(), host.end());
+      T* dm = nullptr;
+      SHT_CUDA_OR_THROW(cudaMallocAsync(&dm, sizeof(T) * nm, s));
+      SHT_CUDA_OR_THROW(cudaMemcpyAsync(dm, conv.data(), sizeof(T) * nm, cudaMemcpyHostToDevice, s));
+      launch_helmholtz<T>(plan, nlev, dm, tau_w, CP(divergence), CP(theta), CP(lnps),
+                          MP(out_divergence), MP(out_theta), MP(out_lnps), s);
+      SHT_CUDA_OR_THROW(cudaFreeAsync(dm, s));
+      SHT_CUDA_OR_THROW(cudaStreamSynchronize(s));  // the host staging buffer dies here
+    });
+  });
+}
+
+}  // extern "C"

@@ -1,0 +1,192 @@
+// Spectral-side layout kernels.
+//
+// pack:   coefficients (planes, T+1, T+1) [n, m] -> the synthesis operand
+//         Cfold, rows (m, q, i) with n = m + q + 2i and the (plane, field,
+//         re/im) columns innermost; optional per-degree factor (the inverse
+//         Laplacian of the vector synthesis, transform.py:1804-1811).
+// unpack: the analysis output Cfold -> coefficients, zero above the
+//         triangle and Imag(c[n,0]) = 0 (transform.py:1435-1452); the vector
+//         mode combines the rotational and shear contractions into
+//         (vorticity, divergence) with the i*m factor and projects
+//         (vector.py:113-134).
+// Both go through a 32 x 32 shared tile so the [n, m] side is read/written
+// along m and the folded side along the plane index.
+#include "sht_plan.h"
+
+namespace sht {
+namespace {
+
+template <typename T> using V2 = typename Vec2<T>::type;
+
+// Row of (m, q, i) in the folded operand: orders below m fill
+// sum_{m' < m} (T + 1 - m') rows; parity 1 follows the parity-0 block.
+__device__ __forceinline__ int64_t cf_row(int T, int m, int q, int i) {
+  int64_t base = (int64_t)m * (T + 1) - (int64_t)m * (m - 1) / 2;
+  return base + (q ? parity_count(T, m, 0) : 0) + i;
+}
+
+template <typename T>
+__global__ void pack_kernel(int Tn, double radius, int mode, const V2<T>* __restrict__ c0,
+                            const V2<T>* __restrict__ c1, int64_t planes, int F,
+                            V2<T>* __restrict__ cf) {
+  __shared__ V2<T> tile[32][33];
+  const int m0 = blockIdx.x * 32;
+  const int n = blockIdx.y;
+  if (m0 > n) return;
+  const int f = blockIdx.z % F;
+  const int64_t p0 = (int64_t)(blockIdx.z / F) * 32;
+  const V2<T>* src = f ? c1 : c0;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int64_t t1 = Tn + 1;
+  const T eig = T(-((double)n * ((double)n + 1.0)) / (radius * radius));
+  for (int pp = ty; pp < 32; pp += 8) {
+    int64_t p = p0 + pp;
+    int m = m0 + tx;
+    V2<T> v = mk2<T>(T(0), T(0));
+    if (p < planes && m <= n) v = src[(p * t1 + n) * t1 + m];
+    tile[pp][tx] = v;
+  }
+  __syncthreads();
+  const int64_t Rc = planes * F;
+  for (int mm = ty; mm < 32; mm += 8) {
+    int m = m0 + mm;
+    if (m > n) break;
+    int q = (n - m) & 1, i = (n - m) >> 1;
+    int64_t row = cf_row(Tn, m, q, i);
+    int64_t p = p0 + tx;
+    if (p < planes) {
+      V2<T> v = tile[tx][mm];
+      if (mode == kPackInvLap) {
+        // c / eig (complex by real), zero at degree 0
+        v = n == 0 ? mk2<T>(T(0), T(0)) : mk2<T>(v.x / eig, v.y / eig);
+        if (m == 0) v.y = T(0);  // project() inside inverse_laplacian
+      }
+      cf[row * Rc + p * F + f] = v;
+    }
+  }
+}
+
+template <typename T>
+__global__ void unpack_kernel(int Tn, int mode, const V2<T>* __restrict__ cf0,
+                              const V2<T>* __restrict__ cf1, int64_t planes,
+                              V2<T>* __restrict__ o0, V2<T>* __restrict__ o1) {
+  __shared__ V2<T> tile[2][32][33];
+  const int m0 = blockIdx.x * 32;
+  const int n = blockIdx.y;
+  const int64_t p0 = (int64_t)blockIdx.z * 32;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int64_t t1 = Tn + 1;
+  const int F = mode == kUnpackVorDiv ? 2 : 1;
+  const int64_t Rc = planes * F;
+  if (m0 <= n) {
+    for (int mm = ty; mm < 32; mm += 8) {
+      int m = m0 + mm;
+      int64_t p = p0 + tx;
+      V2<T> a = mk2<T>(T(0), T(0)), b = a;
+      if (m <= n && p < planes) {
+        int q = (n - m) & 1, i = (n - m) >> 1;
+        int64_t row = cf_row(Tn, m, q, i);
+        if (mode == kUnpackScalar) {
+          a = cf0[row * Rc + p];
+        } else {
+          // rot/shear rows hold (u, v) per plane: columns 2p (u), 2p+1 (v).
+          V2<T> ru = cf0[row * Rc + 2 * p], rv = cf0[row * Rc + 2 * p + 1];
+          V2<T> su = cf1[row * Rc + 2 * p], sv = cf1[row * Rc + 2 * p + 1];
+          T mf = T(m);
+          // zeta = i m rot[v] + shear[u];  D = i m rot[u] - shear[v]
+          a = mk2<T>(-mf * rv.y + su.x, mf * rv.x + su.y);
+          b = mk2<T>(-mf * ru.y - sv.x, mf * ru.x - sv.y);
+        }
+        if (m == 0) {
+          a.y = T(0);
+          b.y = T(0);
+        }
+      }
+      tile[0][tx][mm] = a;
+      tile[1][tx][mm] = b;
+    }
+  }
+  __syncthreads();
+  for (int pp = ty; pp < 32; pp += 8) {
+    int64_t p = p0 + pp;
+    int m = m0 + tx;
+    if (p >= planes || m > Tn) continue;
+    int64_t off = (p * t1 + n) * t1 + m;
+    V2<T> a = mk2<T>(T(0), T(0)), b = a;
+    if (m <= n) {
+      a = tile[0][pp][tx];
+      b = tile[1][pp][tx];
+    }
+    o0[off] = a;
+    if (mode == kUnpackVorDiv) o1[off] = b;
+  }
+}
+
+template <typename T>
+__global__ void elementwise_kernel(int Tn, double radius, int mode, const V2<T>* __restrict__ in,
+                                   int64_t total, V2<T>* __restrict__ out) {
+  const int64_t t1 = Tn + 1;
+  for (int64_t idx = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; idx < total;
+       idx += (int64_t)gridDim.x * blockDim.x) {
+    int m = (int)(idx % t1);
+    int n = (int)((idx / t1) % t1);
+    V2<T> v = in[idx];
+    T eig = T(-((double)n * ((double)n + 1.0)) / (radius * radius));
+    if (mode == kElemLaplacian) {
+      v = mk2<T>(v.x * eig, v.y * eig);
+    } else {
+      if (mode == kElemInvLaplacian) v = n == 0 ? mk2<T>(T(0), T(0)) : mk2<T>(v.x / eig, v.y / eig);
+      if (m > n) v = mk2<T>(T(0), T(0));
+      if (m == 0) v.y = T(0);
+    }
+    out[idx] = v;
+  }
+}
+
+}  // namespace
+
+template <typename T>
+void launch_pack(const sht_plan* p, const T* coeff0, const T* coeff1, int64_t planes, int mode,
+                 T* cfold, cudaStream_t s) {
+  if (planes == 0) return;
+  int F = coeff1 ? 2 : 1;
+  dim3 grid((unsigned)div_up(p->T + 1, 32), (unsigned)(p->T + 1), (unsigned)(div_up(planes, 32) * F));
+  SHT_REQUIRE(grid.z <= 65535, "too many planes for one pack launch");
+  pack_kernel<T><<<grid, dim3(32, 8), 0, s>>>(p->T, p->radius, mode, (const V2<T>*)coeff0,
+                                              (const V2<T>*)coeff1, planes, F, (V2<T>*)cfold);
+  SHT_CUDA_OR_THROW(cudaGetLastError());
+}
+
+template <typename T>
+void launch_unpack(const sht_plan* p, int mode, const T* cf0, const T* cf1, int64_t planes,
+                   T* out0, T* out1, cudaStream_t s) {
+  if (planes == 0) return;
+  dim3 grid((unsigned)div_up(p->T + 1, 32), (unsigned)(p->T + 1), (unsigned)div_up(planes, 32));
+  SHT_REQUIRE(grid.z <= 65535, "too many planes for one unpack launch");
+  unpack_kernel<T><<<grid, dim3(32, 8), 0, s>>>(p->T, mode, (const V2<T>*)cf0, (const V2<T>*)cf1,
+                                                planes, (V2<T>*)out0, (V2<T>*)out1);
+  SHT_CUDA_OR_THROW(cudaGetLastError());
+}
+
+template <typename T>
+void launch_elementwise(const sht_plan* p, int mode, const T* in, int64_t planes, T* out,
+                        cudaStream_t s) {
+  int64_t total = planes * (int64_t)(p->T + 1) * (p->T + 1);
+  if (total == 0) return;
+  int blocks = (int)std::min<int64_t>(div_up(total, 256), 148 * 16);
+  elementwise_kernel<T><<<blocks, 256, 0, s>>>(p->T, p->radius, mode, (const V2<T>*)in, total,
+                                               (V2<T>*)out);
+  SHT_CUDA_OR_THROW(cudaGetLastError());
+}
+
+#define INST(T)                                                                                  \
+  template void launch_pack<T>(const sht_plan*, const T*, const T*, int64_t, int, T*,          \
+                               cudaStream_t);                                                   \
+  template void launch_unpack<T>(const sht_plan*, int, const T*, const T*, int64_t, T*, T*,    \
+                                 cudaStream_t);                                                 \
+  template void launch_elementwise<T>(const sht_plan*, int, const T*, int64_t, T*, cudaStream_t);
+INST(float)
+INST(double)
+#undef INST
+
+}  // namespace sht

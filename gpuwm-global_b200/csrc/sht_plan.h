@@ -1,0 +1,136 @@
+// Internal plan object and the per-(order, parity) bookkeeping shared by the
+// kernels.  Not part of the public ABI.
+#pragma once
+
+#include "sht_common.cuh"
+
+// One (order m, degree-parity q) block of a Legendre contraction, the unit of
+// work of every GEMM launch.  Offsets are element offsets into the table and
+// ROW offsets into the data/output (multiplied by the call's row count R in
+// the kernel).  C[x][r] = sum_k Tab[k][x] * D[k][r].
+struct ShtGemmDesc {
+  int64_t t_off;  // element offset of the table block
+  int64_t d_row;  // row offset of the data block (k = 0)
+  int64_t c_row;  // row offset of the output block (x = 0)
+  int X;          // output extent (x)
+  int K;          // contraction extent (k)
+  int ldt;        // table leading dimension (padded x extent)
+  int m;          // order (for epilogues)
+};
+
+// A tile of a GEMM launch: problem index and first x.
+struct ShtGemmItem {
+  int problem;
+  int x0;
+};
+
+struct ShtTc16;  // split-precision tensor-core tables (sht_gemm_tc.cu)
+
+struct sht_plan {
+  int T = 0, nlat = 0, nlon = 0, H = 0, L = 0, prec = 0;
+  int Hx = 0;         // H padded to a multiple of 4 (synthesis tables)
+  bool nlat_odd = false;
+  double radius = 0;
+  int device = 0;
+  bool geometry_only = false;
+
+  // FP64 geometry on the device and a host copy.
+  double* d_mu = nullptr;
+  double* d_w = nullptr;
+  double* d_coslat = nullptr;
+  std::vector<double> h_mu, h_w, h_coslat;
+
+  // Per (m, q) bookkeeping, index m*2+q.
+  std::vector<int> e, ex;                        // count and padded count
+  std::vector<int64_t> syn_off, ana_off, cf_row;  // table offsets, Cfold row offsets
+  int64_t syn_total = 0, ana_total = 0, cf_rows = 0;
+
+  // Tables in the plan's element type (double for F64, float otherwise).
+  // Synthesis layout [m][q][i][h] (ld Hx); analysis layout [m][q][h][i] (ld ex).
+  void* basis = nullptr;     // P_nm
+  void* dbasis = nullptr;    // dP_nm / dphi
+  void* analysis = nullptr;  // Gram-corrected 2 pi w P
+  void* rot = nullptr;       // 2 pi w P / (a cos phi)
+  void* shear = nullptr;     // 2 pi w dP / a
+
+  ShtTc16* tc = nullptr;     // SPLIT16 tiles
+
+  // FFT: twiddles exp(-2 pi i k / L), k < L, and exp(-2 pi i k / N), k <= L.
+  void* tw_l = nullptr;
+  void* tw_n = nullptr;
+  std::vector<int> radices;
+  int* d_radices = nullptr;
+
+  // GEMM descriptors: [direction][flip] (direction 0 synthesis, 1 analysis).
+  ShtGemmDesc* d_desc[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+  std::vector<ShtGemmDesc> h_desc[2][2];
+  ShtGemmItem* d_items[2] = {nullptr, nullptr};
+  int n_items[2] = {0, 0};
+  int n_problems = 0;
+  int gemm_bx = 0;  // x tile of the SIMT kernel the item lists were built for
+
+  // Scratch (grown on demand): two waists and two Cfold buffers.
+  void* wfold[2] = {nullptr, nullptr};
+  void* cfold[2] = {nullptr, nullptr};
+  int64_t scratch_rows = 0;  // R capacity (rows = 2 * planes * fields)
+
+  unsigned* d_err = nullptr;
+  cudaStream_t last_stream = nullptr;
+
+  size_t elem() const { return prec == SHT_PREC_F64 ? 8 : 4; }
+  int64_t wfold_elems(int64_t R) const { return int64_t(T + 1) * 2 * H * R; }
+  int64_t cfold_elems(int64_t R) const { return cf_rows * R; }
+};
+
+namespace sht {
+
+// Geometry and tables (sht_geometry.cu).
+void build_geometry_and_tables(sht_plan* p, cudaStream_t s);
+
+// FFT (sht_fft.cu).
+void build_fft(sht_plan* p, cudaStream_t s);
+template <typename T>
+void launch_forward_fold(const sht_plan* p, const T* g0, const T* g1, int64_t planes,
+                         T* wfold, cudaStream_t s);
+// Inverse modes.
+enum UnfoldMode { kUnfoldScalar = 0, kUnfoldZonal = 1, kUnfoldGradient = 2, kUnfoldWind = 3,
+                  kUnfoldMeridional = 4 };
+template <typename T>
+void launch_inverse_unfold(const sht_plan* p, int mode, const T* wP, const T* wD,
+                           int64_t planes, T* out0, T* out1, cudaStream_t s);
+
+// SIMT Legendre GEMM (sht_gemm_simt.cu).
+void build_gemm_items(sht_plan* p);
+template <typename T>
+void launch_gemm_simt(const sht_plan* p, int direction, int flip, const T* table,
+                      const T* data, T* out, int64_t R, cudaStream_t s);
+
+// Pack / unpack / elementwise (sht_pack.cu).
+enum PackMode { kPackPlain = 0, kPackInvLap = 1 };
+template <typename T>
+void launch_pack(const sht_plan* p, const T* coeff0, const T* coeff1, int64_t planes,
+                 int mode, T* cfold, cudaStream_t s);
+enum UnpackMode { kUnpackScalar = 0, kUnpackVorDiv = 1 };
+template <typename T>
+void launch_unpack(const sht_plan* p, int mode, const T* cf0, const T* cf1, int64_t planes,
+                   T* out0, T* out1, cudaStream_t s);
+enum ElemMode { kElemProject = 0, kElemLaplacian = 1, kElemInvLaplacian = 2 };
+template <typename T>
+void launch_elementwise(const sht_plan* p, int mode, const T* in, int64_t planes, T* out,
+                        cudaStream_t s);
+
+// Helmholtz (sht_helmholtz.cu).
+template <typename T>
+void launch_helmholtz(const sht_plan* p, int nlev, const T* mats, double tau_w,
+                      const T* div, const T* theta, const T* lnps, T* odiv, T* otheta,
+                      T* olnps, cudaStream_t s);
+
+// Split-precision tensor-core path (sht_gemm_tc.cu).
+void build_tc_tables(sht_plan* p, const double* basis64, const double* dbasis64,
+                     const double* analysis64, const double* rot64, const double* shear64,
+                     cudaStream_t s);
+void destroy_tc_tables(sht_plan* p);
+void launch_gemm_tc(const sht_plan* p, int direction, int flip, int table_kind,
+                    const float* data, float* out, int64_t R, cudaStream_t s);
+
+}  // namespace sht

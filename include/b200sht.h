@@ -1,0 +1,139 @@
+/*
+ * b200sht: spherical-harmonic transform pair on a Gaussian grid, B200 (sm_100a).
+ *
+ * C ABI for the transform calls of the ArWen Global sl_si dycore
+ * (FahrenheitResearch/gpuwm-global).  Every entry point returns an int status
+ * (0 = ok) and leaves a thread-local message readable with sht_last_error(),
+ * the convention of rust/global-render-kernels/src/lib.rs:1-40 in the
+ * reference.  Device buffers are owned by the caller and passed as plain
+ * device pointers; the plan owns its Legendre tables, FFT twiddles and
+ * scratch.  Work is stream-ordered on the caller's stream (a cudaStream_t
+ * passed as void*, NULL = legacy default stream) with no implicit host sync.
+ *
+ * Layouts (the reference's, src/arwen_global/spectral/transform.py:1051-1144):
+ *   grid     (planes, nlat, nlon) real, C-contiguous, row 0 southernmost
+ *   spectral (planes, T+1, T+1) complex interleaved (re, im), indexed [n, m],
+ *            zero above the triangle (m > n), Imag(c[n,0]) = 0 on output.
+ * Element type: double/complex128 for SHT_PREC_F64 plans, float/complex64
+ * for SHT_PREC_F32 and SHT_PREC_SPLIT16 plans.
+ */
+#ifndef B200SHT_H
+#define B200SHT_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SHT_ABI_VERSION 1
+
+/* Arithmetic of the Legendre contractions. */
+#define SHT_PREC_F64 0     /* FP64 SIMT: the parity path (1e-12 vs FP64 reference) */
+#define SHT_PREC_F32 1     /* plain FP32 FFMA path */
+#define SHT_PREC_SPLIT16 2 /* FP16 hi+lo split on tcgen05 tensor cores, FP32 accumulate */
+
+/* sht_plan_create flags. */
+#define SHT_FLAG_GEOMETRY_ONLY 1
+
+/* Status codes. */
+#define SHT_OK 0
+#define SHT_ERR_ARG 1      /* invalid argument (shape, pointer, precision) */
+#define SHT_ERR_CUDA 2     /* a CUDA runtime call failed */
+#define SHT_ERR_DEVICE 3   /* a kernel reported an error word (bounded wait expired) */
+#define SHT_ERR_STATE 4    /* plan in an unusable state */
+
+typedef struct sht_plan sht_plan;
+
+/* ABI version of the loaded library (SHT_ABI_VERSION). */
+int sht_abi_version(void);
+
+/* Message of the last failing call on this thread ("" if none). */
+const char* sht_last_error(void);
+
+/* Build a plan on the current device: FP64 Gauss nodes/weights by Newton
+ * iteration, the normalised P_nm recurrence, dP/dphi, the Gram-corrected
+ * analysis rows and the vector-analysis tables, all computed on the GPU, then
+ * cast (F32) or split into FP16 hi/lo tiles (SPLIT16).  Replaces
+ * SphericalHarmonicTransform.__post_init__/_build_tables
+ * (src/arwen_global/spectral/transform.py:753-899) and GaussianGrid.create
+ * (src/arwen_global/spectral/grid.py:97-126).  nlat/nlon are taken as given
+ * (the Python layer applies the reference's shape rule, grid.py:26-94).
+ * flags: 0, or SHT_FLAG_GEOMETRY_ONLY to compute only the Gauss nodes and
+ * weights (sht_plan_geometry works; transform calls fail). */
+int sht_plan_create(int truncation, int nlat, int nlon, double radius_m,
+                    int precision, int flags, sht_plan** out_plan);
+int sht_plan_destroy(sht_plan* plan);
+
+/* Grow the plan's scratch for calls of up to `planes` planes (optional; calls
+ * grow it on demand, which allocates and is therefore not capturable). */
+int sht_plan_reserve(sht_plan* plan, int64_t planes);
+
+/* Copy the FP64 geometry to host arrays of nlat doubles (any may be NULL). */
+int sht_plan_geometry(const sht_plan* plan, double* mu, double* weights, double* coslat);
+
+/* Read and clear the plan's device error word (synchronises the plan's last
+ * stream).  Returns SHT_ERR_DEVICE with a message if a kernel gave up on a
+ * bounded wait. */
+int sht_plan_check(sht_plan* plan);
+
+/* grid -> spectral.  SphericalHarmonicTransform.forward (transform.py:1486). */
+int sht_forward(sht_plan* plan, const void* grid, int64_t planes, void* coeff, void* stream);
+
+/* spectral -> grid.  SphericalHarmonicTransform.inverse (transform.py:1742). */
+int sht_inverse(sht_plan* plan, const void* coeff, int64_t planes, void* grid, void* stream);
+
+/* d/dphi synthesis.  inverse_meridional_derivative (transform.py:1748). */
+int sht_inverse_meridional_derivative(sht_plan* plan, const void* coeff, int64_t planes,
+                                      void* grid, void* stream);
+
+/* d/dlambda synthesis.  inverse_zonal_derivative (transform.py:1752). */
+int sht_inverse_zonal_derivative(sht_plan* plan, const void* coeff, int64_t planes,
+                                 void* grid, void* stream);
+
+/* (east, north) physical gradient per metre.  gradient (transform.py:1762). */
+int sht_gradient(sht_plan* plan, const void* coeff, int64_t planes, void* east,
+                 void* north, void* stream);
+
+/* vorticity/divergence -> (u, v).
+ * VorticityDivergenceOperator.wind_from_vordiv (src/arwen_global/spectral/vector.py:36-52). */
+int sht_wind_from_vordiv(sht_plan* plan, const void* vorticity, const void* divergence,
+                         int64_t planes, void* u, void* v, void* stream);
+
+/* (u, v) -> vorticity/divergence by integration by parts.
+ * VorticityDivergenceOperator.vordiv_from_wind (vector.py:54-73). */
+int sht_vordiv_from_wind(sht_plan* plan, const void* u, const void* v, int64_t planes,
+                         void* vorticity, void* divergence, void* stream);
+
+/* Triangle mask and Imag(c[n,0]) = 0.  project (transform.py:1124-1144).
+ * in and out may alias. */
+int sht_project(sht_plan* plan, const void* in, int64_t planes, void* out, void* stream);
+
+/* Multiply by -n(n+1)/a^2.  laplacian (transform.py:1798). */
+int sht_laplacian(sht_plan* plan, const void* in, int64_t planes, void* out, void* stream);
+
+/* Divide by -n(n+1)/a^2, zero degree 0, project.  inverse_laplacian (transform.py:1804). */
+int sht_inverse_laplacian(sht_plan* plan, const void* in, int64_t planes, void* out,
+                          void* stream);
+
+/* Semi-implicit stage solve (I - tau_w L) y = r per total degree in the
+ * vertical-mode basis.  VerticalModeSemiImplicit.solve_shifted
+ * (src/arwen_global/semi_implicit.py:921-953) with helmholtz_inverse
+ * (semi_implicit.py:585-609) applied as V diag(1/(1 + tau_w^2 k_n^2 lambda_j)) V^-1.
+ * Host matrices (row-major float64): b (nlev x nlev+1), c (nlev+1 x nlev),
+ * eigvec V (nlev x nlev), eigvec_inv V^-1 (nlev x nlev), eigenvalues (nlev).
+ * Device arrays in the plan's complex type: divergence/theta (nlev, T+1, T+1),
+ * lnps (T+1, T+1); results go to the out_* arrays (which may alias the inputs).
+ * Degree zero passes through; outputs are projected. */
+int sht_helmholtz_solve(sht_plan* plan, int nlev, const double* b, const double* c,
+                        const double* eigvec, const double* eigvec_inv,
+                        const double* eigenvalues, double tau_w,
+                        const void* divergence, const void* theta, const void* lnps,
+                        void* out_divergence, void* out_theta, void* out_lnps,
+                        void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* B200SHT_H */

@@ -166,6 +166,40 @@ def record_ynm(ref_root: Path) -> None:
     print("wrote ynm_reference.json")
 
 
+def record_gauss_exact() -> None:
+    """Gauss-Legendre nodes/weights to 40 digits (mpmath Newton on P_n),
+    rounded to float64: the accuracy yardstick for the device geometry."""
+    import mpmath
+
+    mpmath.mp.dps = 40
+    out = {}
+    for n in (15, 33, 50, 94, 768):
+        xs, ws = [], []
+        for k in range(n // 2):
+            x = mpmath.cos(mpmath.pi * (k + mpmath.mpf("0.75")) / (n + mpmath.mpf("0.5")))
+            for _ in range(60):
+                p = mpmath.legendre(n, x)
+                dp = n * (x * p - mpmath.legendre(n - 1, x)) / (x * x - 1)
+                step = p / dp
+                x -= step
+                if abs(step) < mpmath.mpf(10) ** -38:
+                    break
+            dp = n * (x * mpmath.legendre(n, x) - mpmath.legendre(n - 1, x)) / (x * x - 1)
+            xs.append(float(x))
+            ws.append(float(2 / ((1 - x * x) * dp * dp)))
+        mu = np.array([-v for v in xs] + ([0.0] if n % 2 else []) + xs[::-1])
+        w_mid = []
+        if n % 2:
+            x = mpmath.mpf(0)
+            dp = n * (x * mpmath.legendre(n, x) - mpmath.legendre(n - 1, x)) / (x * x - 1)
+            w_mid = [float(2 / dp ** 2)]
+        w = np.array(ws + w_mid + ws[::-1])
+        out[f"mu_{n}"] = mu
+        out[f"w_{n}"] = w
+    np.savez_compressed(HERE / "gauss_exact.npz", **out)
+    print("wrote gauss_exact.npz")
+
+
 def main() -> None:
     ref_root = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
     os.environ.setdefault("ARWEN_GLOBAL_LEGENDRE_CACHE", "off")
@@ -173,6 +207,7 @@ def main() -> None:
     record_transforms(ref_root)
     record_helmholtz()
     record_ynm(ref_root)
+    record_gauss_exact()
 
 
 if __name__ == "__main__":
