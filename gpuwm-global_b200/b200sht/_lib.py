@@ -19,6 +19,9 @@ SHT_ERR_ARG = 1
 SHT_ERR_CUDA = 2
 SHT_ERR_DEVICE = 3
 SHT_ERR_STATE = 4
+#: Kernel kinds of sht_plan_read_timing, in order.
+KERNEL_KINDS = ("fft_forward", "fft_inverse", "legendre_analysis", "legendre_synthesis", "pack",
+                "unpack", "elementwise", "helmholtz")
 
 #: Every symbol ``include/b200sht.h`` declares, with its ctypes signature.
 _P = ctypes.c_void_p
@@ -34,6 +37,9 @@ SIGNATURES = {
     "sht_plan_reserve": (ctypes.c_int, [_P, _I64]),
     "sht_plan_geometry": (ctypes.c_int, [_P, _DP, _DP, _DP]),
     "sht_plan_check": (ctypes.c_int, [_P]),
+    "sht_plan_set_timing": (ctypes.c_int, [_P, ctypes.c_int]),
+    "sht_plan_read_timing": (ctypes.c_int, [_P, _DP, ctypes.POINTER(_I64), ctypes.POINTER(_I64),
+                                            ctypes.c_int, ctypes.c_int]),
     "sht_forward": (ctypes.c_int, [_P, _P, _I64, _P, _P]),
     "sht_inverse": (ctypes.c_int, [_P, _P, _I64, _P, _P]),
     "sht_inverse_meridional_derivative": (ctypes.c_int, [_P, _P, _I64, _P, _P]),

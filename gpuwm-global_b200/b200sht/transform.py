@@ -63,6 +63,20 @@ class Plan:
     def check(self):
         _lib.check(self._lib.sht_plan_check(self.handle))
 
+    def set_timing(self, enable: bool):
+        _lib.check(self._lib.sht_plan_set_timing(self.handle, 1 if enable else 0))
+
+    def read_timing(self, reset: bool = False) -> dict:
+        """``{kind: {"ms": total, "launches": n, "timed": n}}`` per kernel kind."""
+        k = len(_lib.KERNEL_KINDS)
+        ms = (ctypes.c_double * k)()
+        launches = (ctypes.c_int64 * k)()
+        timed = (ctypes.c_int64 * k)()
+        _lib.check(self._lib.sht_plan_read_timing(self.handle, ms, launches, timed, k,
+                                                  1 if reset else 0))
+        return {name: {"ms": ms[i], "launches": launches[i], "timed": timed[i]}
+                for i, name in enumerate(_lib.KERNEL_KINDS)}
+
     def __del__(self):
         h = getattr(self, "handle", None)
         if h is not None and h.value:

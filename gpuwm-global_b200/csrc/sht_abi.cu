@@ -33,6 +33,45 @@ int guarded(F&& f) {
 
 enum TableKind { kBasis = 0, kDBasis = 1, kAnalysis = 2, kRot = 3, kShear = 4 };
 
+cudaEvent_t pool_event(sht_plan* p) {
+  if (!p->event_pool.empty()) {
+    cudaEvent_t e = p->event_pool.back();
+    p->event_pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e = nullptr;
+  SHT_CUDA_OR_THROW(cudaEventCreate(&e));
+  return e;
+}
+
+// Counts a launch of `kind` and, with timing on, brackets it with events.
+class KernelScope {
+ public:
+  KernelScope(sht_plan* p, int kind, cudaStream_t s) : p_(p), kind_(kind), s_(s) {
+    p_->launches[kind_]++;
+    if (p_->timing) {
+      start_ = pool_event(p_);
+      SHT_CUDA_OR_THROW(cudaEventRecord(start_, s_));
+    }
+  }
+  ~KernelScope() {
+    if (start_ == nullptr) return;
+    cudaEvent_t stop = nullptr;
+    try {
+      stop = pool_event(p_);
+    } catch (...) {
+      return;
+    }
+    if (cudaEventRecord(stop, s_) == cudaSuccess) p_->timing_recs.push_back({kind_, start_, stop});
+  }
+
+ private:
+  sht_plan* p_;
+  int kind_;
+  cudaStream_t s_;
+  cudaEvent_t start_ = nullptr;
+};
+
 const void* table_ptr(const sht_plan* p, int kind) {
   switch (kind) {
     case kBasis: return p->basis;
@@ -78,6 +117,7 @@ void ensure_scratch(sht_plan* p, int64_t R) {
 template <typename T>
 void contract(sht_plan* p, int kind, const T* data, T* out, int64_t R, cudaStream_t s) {
   const int dir = table_dir(kind), flip = table_flip(kind);
+  KernelScope scope(p, dir == 0 ? SHT_KIND_LEGENDRE_SYNTHESIS : SHT_KIND_LEGENDRE_ANALYSIS, s);
   if constexpr (sizeof(T) == 4) {
     if (p->prec == SHT_PREC_SPLIT16 && p->tc != nullptr) {
       launch_gemm_tc(p, dir, flip, kind, data, out, R, s);
@@ -93,9 +133,15 @@ void do_forward(sht_plan* p, const T* grid, int64_t planes, T* coeff, cudaStream
   ensure_scratch(p, R);
   T* w = static_cast<T*>(p->wfold[0]);
   T* c = static_cast<T*>(p->cfold[0]);
-  launch_forward_fold<T>(p, grid, nullptr, planes, w, s);
+  {
+    KernelScope k(p, SHT_KIND_FFT_FORWARD, s);
+    launch_forward_fold<T>(p, grid, nullptr, planes, w, s);
+  }
   contract<T>(p, kAnalysis, w, c, R, s);
-  launch_unpack<T>(p, kUnpackScalar, c, nullptr, planes, coeff, nullptr, s);
+  {
+    KernelScope k(p, SHT_KIND_UNPACK, s);
+    launch_unpack<T>(p, kUnpackScalar, c, nullptr, planes, coeff, nullptr, s);
+  }
 }
 
 template <typename T>
@@ -105,9 +151,15 @@ void do_synthesis(sht_plan* p, int kind, int mode, const T* coeff, int64_t plane
   ensure_scratch(p, R);
   T* w = static_cast<T*>(p->wfold[0]);
   T* c = static_cast<T*>(p->cfold[0]);
-  launch_pack<T>(p, coeff, nullptr, planes, kPackPlain, c, s);
+  {
+    KernelScope k(p, SHT_KIND_PACK, s);
+    launch_pack<T>(p, coeff, nullptr, planes, kPackPlain, c, s);
+  }
   contract<T>(p, kind, c, w, R, s);
-  launch_inverse_unfold<T>(p, mode, w, nullptr, planes, grid, nullptr, s);
+  {
+    KernelScope k(p, SHT_KIND_FFT_INVERSE, s);
+    launch_inverse_unfold<T>(p, mode, w, nullptr, planes, grid, nullptr, s);
+  }
 }
 
 template <typename T>
@@ -118,10 +170,16 @@ void do_gradient(sht_plan* p, const T* coeff, int64_t planes, T* east, T* north,
   T* c = static_cast<T*>(p->cfold[0]);
   T* w0 = static_cast<T*>(p->wfold[0]);
   T* w1 = static_cast<T*>(p->wfold[1]);
-  launch_pack<T>(p, coeff, nullptr, planes, kPackPlain, c, s);
+  {
+    KernelScope k(p, SHT_KIND_PACK, s);
+    launch_pack<T>(p, coeff, nullptr, planes, kPackPlain, c, s);
+  }
   contract<T>(p, kBasis, c, w0, R, s);
   contract<T>(p, kDBasis, c, w1, R, s);
-  launch_inverse_unfold<T>(p, kUnfoldGradient, w0, w1, planes, east, north, s);
+  {
+    KernelScope k(p, SHT_KIND_FFT_INVERSE, s);
+    launch_inverse_unfold<T>(p, kUnfoldGradient, w0, w1, planes, east, north, s);
+  }
 }
 
 template <typename T>
@@ -132,10 +190,16 @@ void do_wind(sht_plan* p, const T* vort, const T* div, int64_t planes, T* u, T* 
   T* c = static_cast<T*>(p->cfold[0]);
   T* w0 = static_cast<T*>(p->wfold[0]);
   T* w1 = static_cast<T*>(p->wfold[1]);
-  launch_pack<T>(p, vort, div, planes, kPackInvLap, c, s);
+  {
+    KernelScope k(p, SHT_KIND_PACK, s);
+    launch_pack<T>(p, vort, div, planes, kPackInvLap, c, s);
+  }
   contract<T>(p, kBasis, c, w0, R, s);
   contract<T>(p, kDBasis, c, w1, R, s);
-  launch_inverse_unfold<T>(p, kUnfoldWind, w0, w1, planes, u, v, s);
+  {
+    KernelScope k(p, SHT_KIND_FFT_INVERSE, s);
+    launch_inverse_unfold<T>(p, kUnfoldWind, w0, w1, planes, u, v, s);
+  }
 }
 
 template <typename T>
@@ -146,15 +210,26 @@ void do_vordiv(sht_plan* p, const T* u, const T* v, int64_t planes, T* vort, T* 
   T* w = static_cast<T*>(p->wfold[0]);
   T* c0 = static_cast<T*>(p->cfold[0]);
   T* c1 = static_cast<T*>(p->cfold[1]);
-  launch_forward_fold<T>(p, u, v, planes, w, s);
+  {
+    KernelScope k(p, SHT_KIND_FFT_FORWARD, s);
+    launch_forward_fold<T>(p, u, v, planes, w, s);
+  }
   contract<T>(p, kRot, w, c0, R, s);
   contract<T>(p, kShear, w, c1, R, s);
-  launch_unpack<T>(p, kUnpackVorDiv, c0, c1, planes, vort, div, s);
+  {
+    KernelScope k(p, SHT_KIND_UNPACK, s);
+    launch_unpack<T>(p, kUnpackVorDiv, c0, c1, planes, vort, div, s);
+  }
 }
 
 void destroy(sht_plan* p) {
   if (!p) return;
   destroy_tc_tables(p);
+  for (auto& r : p->timing_recs) {
+    cudaEventDestroy(r.start);
+    cudaEventDestroy(r.stop);
+  }
+  for (cudaEvent_t e : p->event_pool) cudaEventDestroy(e);
   void* ptrs[] = {p->d_mu, p->d_w, p->d_coslat, p->basis, p->dbasis, p->analysis, p->rot,
                   p->shear, p->tw_l, p->tw_n, p->d_radices, p->d_items[0], p->d_items[1],
                   p->d_desc[0][0], p->d_desc[0][1], p->d_desc[1][0], p->d_desc[1][1],
@@ -249,6 +324,38 @@ int sht_plan_geometry(const sht_plan* plan, double* mu, double* weights, double*
     if (mu) std::copy(plan->h_mu.begin(), plan->h_mu.begin() + n, mu);
     if (weights) std::copy(plan->h_w.begin(), plan->h_w.begin() + n, weights);
     if (coslat) std::copy(plan->h_coslat.begin(), plan->h_coslat.begin() + n, coslat);
+  });
+}
+
+int sht_plan_set_timing(sht_plan* plan, int enable) {
+  return guarded([&] {
+    check_plan(plan);
+    plan->timing = enable != 0;
+  });
+}
+
+int sht_plan_read_timing(sht_plan* plan, double* ms, int64_t* launches, int64_t* timed, int n,
+                         int reset) {
+  return guarded([&] {
+    check_plan(plan);
+    SHT_REQUIRE(n >= 0 && n <= SHT_KIND_COUNT, "n must be in [0, SHT_KIND_COUNT]");
+    for (auto& r : plan->timing_recs) {
+      SHT_CUDA_OR_THROW(cudaEventSynchronize(r.stop));
+      float e = 0.f;
+      SHT_CUDA_OR_THROW(cudaEventElapsedTime(&e, r.start, r.stop));
+      plan->ms[r.kind] += e;
+      plan->timed[r.kind]++;
+      plan->event_pool.push_back(r.start);
+      plan->event_pool.push_back(r.stop);
+    }
+    plan->timing_recs.clear();
+    for (int i = 0; i < n; ++i) {
+      if (ms) ms[i] = plan->ms[i];
+      if (launches) launches[i] = plan->launches[i];
+      if (timed) timed[i] = plan->timed[i];
+    }
+    if (reset)
+      for (int i = 0; i < SHT_KIND_COUNT; ++i) plan->ms[i] = 0, plan->launches[i] = 0, plan->timed[i] = 0;
   });
 }
 
@@ -371,6 +478,7 @@ static int elementwise_entry(sht_plan* plan, int mode, const void* in, int64_t p
     SHT_CHECK_CALL(plan, planes);
     check_ptr(in, "in");
     check_ptr(out, "out");
+    KernelScope k(plan, SHT_KIND_ELEMENTWISE, s);
     SHT_TYPED(plan, launch_elementwise<T>(plan, mode, CP(in), planes, MP(out), s));
   });
 }
@@ -419,6 +527,7 @@ int sht_helmholtz_solve(sht_plan* plan, int nlev, const double* b, const double*
       T* dm = nullptr;
       SHT_CUDA_OR_THROW(cudaMallocAsync(&dm, sizeof(T) * nm, s));
       SHT_CUDA_OR_THROW(cudaMemcpyAsync(dm, conv.data(), sizeof(T) * nm, cudaMemcpyHostToDevice, s));
+      KernelScope k(plan, SHT_KIND_HELMHOLTZ, s);
       launch_helmholtz<T>(plan, nlev, dm, tau_w, CP(divergence), CP(theta), CP(lnps),
                           MP(out_divergence), MP(out_theta), MP(out_lnps), s);
       SHT_CUDA_OR_THROW(cudaFreeAsync(dm, s));

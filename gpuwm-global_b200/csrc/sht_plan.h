@@ -77,6 +77,18 @@ struct sht_plan {
   unsigned* d_err = nullptr;
   cudaStream_t last_stream = nullptr;
 
+  // Per-kernel timing (sht_plan_set_timing / sht_plan_read_timing).
+  struct TimingRec {
+    int kind;
+    cudaEvent_t start, stop;
+  };
+  bool timing = false;
+  std::vector<TimingRec> timing_recs;
+  std::vector<cudaEvent_t> event_pool;
+  int64_t launches[SHT_KIND_COUNT] = {};
+  int64_t timed[SHT_KIND_COUNT] = {};
+  double ms[SHT_KIND_COUNT] = {};
+
   size_t elem() const { return prec == SHT_PREC_F64 ? 8 : 4; }
   int64_t wfold_elems(int64_t R) const { return int64_t(T + 1) * 2 * H * R; }
   int64_t cfold_elems(int64_t R) const { return cf_rows * R; }

@@ -77,6 +77,29 @@ int sht_plan_geometry(const sht_plan* plan, double* mu, double* weights, double*
  * bounded wait. */
 int sht_plan_check(sht_plan* plan);
 
+/* Kernel kinds of the per-kernel timing counters. */
+#define SHT_KIND_FFT_FORWARD 0   /* grid -> folded waist */
+#define SHT_KIND_FFT_INVERSE 1   /* folded waist -> grid */
+#define SHT_KIND_LEGENDRE_ANALYSIS 2
+#define SHT_KIND_LEGENDRE_SYNTHESIS 3
+#define SHT_KIND_PACK 4          /* spectral -> synthesis operand */
+#define SHT_KIND_UNPACK 5        /* analysis output -> spectral */
+#define SHT_KIND_ELEMENTWISE 6   /* project / Laplacian */
+#define SHT_KIND_HELMHOLTZ 7
+#define SHT_KIND_COUNT 8
+
+/* Per-kernel device timing, the engine's counterpart of the reference's
+ * StepProfiler (src/arwen_global/profile.py:1-50): when enabled, every kernel
+ * launch of the plan is bracketed by CUDA events on its stream.  Launch
+ * counters run always.  Not for use while a stream is being captured. */
+int sht_plan_set_timing(sht_plan* plan, int enable);
+
+/* Accumulated device milliseconds, launches and timed launches per kind
+ * (arrays of n <= SHT_KIND_COUNT entries, any may be NULL); synchronises on
+ * the recorded events; reset != 0 clears the counters. */
+int sht_plan_read_timing(sht_plan* plan, double* ms, int64_t* launches, int64_t* timed,
+                         int n, int reset);
+
 /* grid -> spectral.  SphericalHarmonicTransform.forward (transform.py:1486). */
 int sht_forward(sht_plan* plan, const void* grid, int64_t planes, void* coeff, void* stream);
 
