@@ -14,6 +14,8 @@ SHT_ABI_VERSION = 1
 SHT_PREC_F64 = 0
 SHT_PREC_F32 = 1
 SHT_PREC_SPLIT16 = 2
+SHT_FLAG_GEOMETRY_ONLY = 1
+SHT_FLAG_GENERIC_FFT = 2
 SHT_OK = 0
 SHT_ERR_ARG = 1
 SHT_ERR_CUDA = 2

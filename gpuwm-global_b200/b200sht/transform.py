@@ -42,11 +42,11 @@ _PREC_CODE = {"float64": _lib.SHT_PREC_F64, "float32": _lib.SHT_PREC_F32,
 class Plan:
     """Owns one ``sht_plan`` handle."""
 
-    def __init__(self, truncation, nlat, nlon, radius_m, precision):
+    def __init__(self, truncation, nlat, nlon, radius_m, precision, flags=0):
         self._lib = _lib.load()
         handle = ctypes.c_void_p()
         _lib.check(self._lib.sht_plan_create(int(truncation), int(nlat), int(nlon),
-                                             float(radius_m), _PREC_CODE[precision], 0,
+                                             float(radius_m), _PREC_CODE[precision], int(flags),
                                              ctypes.byref(handle)))
         self.handle = handle
 
@@ -112,7 +112,7 @@ class SphericalHarmonicTransform:
     def create(cls, truncation, *, nlat=None, nlon=None, dealias_factor=1.5, radius_m=None,
                grid=None, backend="b200", precision="float32",
                tensor_core_contractions=False, legendre_band=32, streaming=False,
-               latitude_bands=1, order_partition=(), device=None):
+               latitude_bands=1, order_partition=(), device=None, plan_flags=0):
         if tuple(order_partition or ()):
             raise ValueError("order_partition (the multi-card order axis) is not built by the "
                              "B200 engine: the whole table is resident on one GPU")
@@ -140,7 +140,7 @@ class SphericalHarmonicTransform:
                 raise ValueError("radius_m must be finite and positive")
             t = int(truncation)
         with torch.cuda.device(be.device):
-            plan = Plan(t, nl, no, rad, prec)
+            plan = Plan(t, nl, no, rad, prec, plan_flags)
             mu, w, cl = plan.geometry(nl)
         g = GaussianGrid.from_geometry(t, nl, no, mu, w, cl, rad)
         return cls(g, be, plan, bool(tensor_core_contractions or prec == "split16"),

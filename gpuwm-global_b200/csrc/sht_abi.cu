@@ -271,8 +271,8 @@ int sht_plan_create(int truncation, int nlat, int nlon, double radius_m, int pre
     SHT_REQUIRE(precision == SHT_PREC_F64 || precision == SHT_PREC_F32 ||
                     precision == SHT_PREC_SPLIT16,
                 "precision must be SHT_PREC_F64, SHT_PREC_F32 or SHT_PREC_SPLIT16");
-    SHT_REQUIRE(flags == 0 || flags == SHT_FLAG_GEOMETRY_ONLY,
-                "flags must be 0 or SHT_FLAG_GEOMETRY_ONLY");
+    SHT_REQUIRE((flags & ~(SHT_FLAG_GEOMETRY_ONLY | SHT_FLAG_GENERIC_FFT)) == 0,
+                "flags must be a combination of SHT_FLAG_GEOMETRY_ONLY and SHT_FLAG_GENERIC_FFT");
     sht_plan* p = new sht_plan();
     p->T = truncation;
     p->nlat = nlat;
@@ -286,6 +286,7 @@ int sht_plan_create(int truncation, int nlat, int nlon, double radius_m, int pre
       SHT_CUDA_OR_THROW(cudaMalloc(&p->d_err, sizeof(unsigned) * 4));
       SHT_CUDA_OR_THROW(cudaMemsetAsync(p->d_err, 0, sizeof(unsigned) * 4, s));
       p->geometry_only = (flags & SHT_FLAG_GEOMETRY_ONLY) != 0;
+      p->force_generic_fft = (flags & SHT_FLAG_GENERIC_FFT) != 0;
       build_geometry_and_tables(p, s);
       if (!p->geometry_only) {
         build_fft(p, s);

@@ -494,6 +494,8 @@ void build_fft(sht_plan* p, cudaStream_t s) {
     while (r % q == 0) { rad.push_back(q); r /= q; }
   SHT_REQUIRE(rad.size() <= 24, "nlon has too many prime factors");
   p->radices = rad;
+  p->fast_fft = fast_fft_supported(p) && !p->force_generic_fft;
+  if (p->fast_fft) fast_fft_init_constants(s);
 
   double2 *tl = nullptr, *tn = nullptr;
   SHT_CUDA_OR_THROW(cudaMalloc(&tl, sizeof(double2) * L));
@@ -520,6 +522,12 @@ void build_fft(sht_plan* p, cudaStream_t s) {
 template <typename T>
 void launch_forward_fold(const sht_plan* p, const T* g0, const T* g1, int64_t planes,
                          T* wfold, cudaStream_t s) {
+  if constexpr (sizeof(T) == 4) {
+    if (p->fast_fft) {
+      fast_forward_fold(p, g0, g1, planes, wfold, s);
+      return;
+    }
+  }
   // g0 (and g1 for a stacked (u, v) pair) are (planes, nlat, nlon) grids.
   const int fields = g1 ? 2 : 1;
   FoldArgs a{};
@@ -544,6 +552,12 @@ void launch_forward_fold(const sht_plan* p, const T* g0, const T* g1, int64_t pl
 template <typename T>
 void launch_inverse_unfold(const sht_plan* p, int mode, const T* wP, const T* wD,
                            int64_t planes, T* out0, T* out1, cudaStream_t s) {
+  if constexpr (sizeof(T) == 4) {
+    if (p->fast_fft) {
+      fast_inverse_unfold(p, mode, wP, wD, planes, out0, out1, s);
+      return;
+    }
+  }
   UnfoldArgs a{};
   a.f = make_shape(p);
   a.nlat = p->nlat;

@@ -1,0 +1,441 @@
+// Register-resident longitude FFTs for the grid sizes of the ArWen configs
+// (nlon = 64 F with F in {2, 3, 4, 6, 8, 12, 16, 24}: 192, 384, 768 and 1536
+// longitudes among them), FP32.
+//
+// One warp owns one grid row.  The complex length L = nlon/2 = 32 F is split
+// four-step style as L = F x 32: lane l loads the F samples z[l + 32 j] with F
+// independent 8-byte loads issued back to back (the memory-level parallelism
+// the shared-memory Stockham kernel lacked), does an F-point DFT in
+// registers, applies exp(-+2 pi i l k1 / L), and one padded shared-memory
+// transpose hands each of F lanes a 32-point DFT, also in registers.  The
+// real-input untangling, 1/nlon scaling and the equator fold (forward) or the
+// unfold and the mode combinations (inverse) run in the CTA epilogue /
+// prologue, so grid and waist are each touched exactly once.
+#include "sht_plan.h"
+
+namespace sht {
+namespace {
+
+// exp(-2 pi i k / 24), exp(-2 pi i k / 32) and exp(-2 pi i k / 16).
+__constant__ float2 c_w24[24];
+__constant__ float2 c_w32[32];
+__constant__ float2 c_w16[16];
+
+__device__ __forceinline__ float2 cmulf(float2 a, float2 b) {
+  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ float2 cconjf(float2 a) { return make_float2(a.x, -a.y); }
+__device__ __forceinline__ float2 caddf(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 csubf(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+template <bool INV>
+__device__ __forceinline__ float2 rot90f(float2 a) {
+  return INV ? make_float2(-a.y, a.x) : make_float2(a.y, -a.x);
+}
+template <bool INV>
+__device__ __forceinline__ float2 tw(float2 w) { return INV ? cconjf(w) : w; }
+
+template <bool INV>
+__device__ __forceinline__ void d2(float2& a, float2& b) {
+  float2 t = a;
+  a = caddf(t, b);
+  b = csubf(t, b);
+}
+template <bool INV>
+__device__ __forceinline__ void d3(float2& a, float2& b, float2& c) {
+  const float s1 = INV ? 0.86602540378443864676f : -0.86602540378443864676f;
+  float2 t1 = caddf(b, c), t2 = csubf(b, c);
+  float2 m1 = make_float2(a.x - 0.5f * t1.x, a.y - 0.5f * t1.y);
+  float2 m2 = make_float2(-s1 * t2.y, s1 * t2.x);
+  a = caddf(a, t1);
+  b = caddf(m1, m2);
+  c = csubf(m1, m2);
+}
+template <bool INV>
+__device__ __forceinline__ void d4(float2* v) {
+  float2 a0 = caddf(v[0], v[2]), a1 = csubf(v[0], v[2]);
+  float2 b0 = caddf(v[1], v[3]), b1 = rot90f<INV>(csubf(v[1], v[3]));
+  v[0] = caddf(a0, b0);
+  v[2] = csubf(a0, b0);
+  v[1] = caddf(a1, b1);
+  v[3] = csubf(a1, b1);
+}
+template <bool INV>
+__device__ __forceinline__ void d8(float2* v) {
+  float2 e[4] = {v[0], v[2], v[4], v[6]}, o[4] = {v[1], v[3], v[5], v[7]};
+  d4<INV>(e);
+  d4<INV>(o);
+  const float r = 0.70710678118654752440f;
+  o[1] = cmulf(o[1], make_float2(r, INV ? r : -r));
+  o[2] = rot90f<INV>(o[2]);
+  o[3] = cmulf(o[3], make_float2(-r, INV ? r : -r));
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    v[k] = caddf(e[k], o[k]);
+    v[k + 4] = csubf(e[k], o[k]);
+  }
+}
+// Four-step in registers: N = N1 * N2, n = N2 n1 + n2, k = k1 + N1 k2.
+template <int N1, bool INV>
+__device__ __forceinline__ void dpow2(float2* v) {
+  if constexpr (N1 == 1) {
+  } else if constexpr (N1 == 2) {
+    d2<INV>(v[0], v[1]);
+  } else if constexpr (N1 == 4) {
+    d4<INV>(v);
+  } else if constexpr (N1 == 8) {
+    d8<INV>(v);
+  } else {  // 16 = 4 x 4
+    float2 a[4][4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+#pragma unroll
+      for (int j = 0; j < 4; ++j) a[i][j] = v[j * 4 + i];
+      d4<INV>(a[i]);
+    }
+#pragma unroll
+    for (int i = 1; i < 4; ++i)
+#pragma unroll
+      for (int j = 1; j < 4; ++j) a[i][j] = cmulf(a[i][j], tw<INV>(c_w16[i * j]));
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      float2 b[4] = {a[0][j], a[1][j], a[2][j], a[3][j]};
+      d4<INV>(b);
+#pragma unroll
+      for (int i = 0; i < 4; ++i) v[i * 4 + j] = b[i];
+    }
+  }
+}
+
+// F-point DFT, F = P2 (power of two) or 3 * P2.
+template <int F, bool INV>
+__device__ __forceinline__ void dftF(float2* v) {
+  if constexpr (F % 3 != 0) {
+    dpow2<F, INV>(v);
+  } else {
+    constexpr int N1 = F / 3;
+    float2 a[3][N1];
+#pragma unroll
+    for (int n2 = 0; n2 < 3; ++n2) {
+#pragma unroll
+      for (int n1 = 0; n1 < N1; ++n1) a[n2][n1] = v[3 * n1 + n2];
+      dpow2<N1, INV>(a[n2]);
+    }
+#pragma unroll
+    for (int n2 = 1; n2 < 3; ++n2)
+#pragma unroll
+      for (int k1 = 1; k1 < N1; ++k1) a[n2][k1] = cmulf(a[n2][k1], tw<INV>(c_w24[(n2 * k1 * (24 / F)) % 24]));
+#pragma unroll
+    for (int k1 = 0; k1 < N1; ++k1) {
+      d3<INV>(a[0][k1], a[1][k1], a[2][k1]);
+#pragma unroll
+      for (int k2 = 0; k2 < 3; ++k2) v[k1 + N1 * k2] = a[k2][k1];
+    }
+  }
+}
+
+// 32-point DFT = 8 x 4.
+template <bool INV>
+__device__ __forceinline__ void dft32(float2* v) {
+  float2 a[4][8];
+#pragma unroll
+  for (int n2 = 0; n2 < 4; ++n2) {
+#pragma unroll
+    for (int n1 = 0; n1 < 8; ++n1) a[n2][n1] = v[4 * n1 + n2];
+    d8<INV>(a[n2]);
+  }
+#pragma unroll
+  for (int n2 = 1; n2 < 4; ++n2)
+#pragma unroll
+    for (int k1 = 1; k1 < 8; ++k1) a[n2][k1] = cmulf(a[n2][k1], tw<INV>(c_w32[n2 * k1]));
+#pragma unroll
+  for (int k1 = 0; k1 < 8; ++k1) {
+    float2 b[4] = {a[0][k1], a[1][k1], a[2][k1], a[3][k1]};
+    d4<INV>(b);
+#pragma unroll
+    for (int k2 = 0; k2 < 4; ++k2) v[k1 + 8 * k2] = b[k2];
+  }
+}
+
+// Per-warp shared region: F rows of 33 (the transpose), reused as the
+// natural-order spectrum of L = 32 F entries.
+template <int F> struct WarpSmem {
+  static constexpr int kStride = 33;
+  static constexpr int kFloats2 = F * kStride;
+};
+
+// The L-point complex FFT of one warp's row: in registers z[j] = x[l + 32 j]
+// (lane l); out: the natural-order spectrum written to `reg` (length L).
+template <int F, bool INV>
+__device__ __forceinline__ void warp_fft(float2 (&z)[F], float2* reg, const float2* __restrict__ twL,
+                                         int lane) {
+  constexpr int L = 32 * F;
+  dftF<F, INV>(z);
+  // exp(-+2 pi i lane k1 / L)
+#pragma unroll
+  for (int k1 = 1; k1 < F; ++k1) z[k1] = cmulf(z[k1], tw<INV>(twL[(lane * k1) % L]));
+#pragma unroll
+  for (int k1 = 0; k1 < F; ++k1) reg[k1 * WarpSmem<F>::kStride + lane] = z[k1];
+  __syncwarp();
+  float2 y[32];
+  if (lane < F) {
+#pragma unroll
+    for (int l = 0; l < 32; ++l) y[l] = reg[lane * WarpSmem<F>::kStride + l];
+  }
+  __syncwarp();
+  if (lane < F) {
+    dft32<INV>(y);
+    // output index k = lane + F k2 (natural order)
+#pragma unroll
+    for (int k2 = 0; k2 < 32; ++k2) reg[lane + F * k2] = y[k2];
+  }
+  __syncwarp();
+}
+
+struct FastFoldArgs {
+  int nlat, nlon, T, H, nlat_odd, F, G;  // F: fields per plane; G: planes per CTA
+  int64_t planes;
+};
+
+// grid -> waist [m][s][h][r], r = (p*F + f)*2 + c.  8 warps: warp w handles
+// (pf = w >> 1, side = w & 1) with pf = gp*F + f.
+template <int FF>
+__global__ void __launch_bounds__(256) fast_forward_fold(FastFoldArgs a, const float* __restrict__ g0,
+                                                         const float* __restrict__ g1,
+                                                         const float2* __restrict__ twL,
+                                                         const float2* __restrict__ twN,
+                                                         float2* __restrict__ wfold) {
+  constexpr int L = 32 * FF;
+  extern __shared__ float2 smem_dyn[];
+  auto smem = [&](int w) { return smem_dyn + w * WarpSmem<FF>::kFloats2; };
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int h = blockIdx.x;
+  const int64_t p0 = (int64_t)blockIdx.y * a.G;
+  const bool eq = a.nlat_odd && h == a.H - 1;
+  const int pf = warp >> 1, side = warp & 1;
+  const int nper = a.G * a.F;
+  const int f = pf % a.F, gp = pf / a.F;
+  const int64_t plane = p0 + gp;
+  const bool active = pf < nper && plane < a.planes && !(eq && side == 1);
+  float2* reg = smem(warp);
+  if (active) {
+    const int j = side ? (a.nlat - 1 - h) : h;
+    const float2* src =
+        reinterpret_cast<const float2*>((f ? g1 : g0) + (plane * a.nlat + j) * (int64_t)a.nlon);
+    float2 z[FF];
+#pragma unroll
+    for (int i = 0; i < FF; ++i) z[i] = __ldg(src + lane + 32 * i);
+    warp_fft<FF, false>(z, reg, twL, lane);
+  }
+  __syncthreads();
+  // Untangle, scale, fold, write: thread -> (m, pf) with pf fastest.
+  const float inv_n = 1.0f / (float)a.nlon;
+  const int64_t Rc = a.planes * a.F;  // complex columns per waist row
+  for (int t = threadIdx.x; t < (a.T + 1) * nper; t += blockDim.x) {
+    int m = t / nper, q = t - m * nper;
+    int gq = q / a.F;
+    if (p0 + gq >= a.planes) continue;
+    float2 w = twN[m];
+    float2 X[2];
+#pragma unroll
+    for (int sd = 0; sd < 2; ++sd) {
+      if (sd == 1 && eq) {
+        X[1] = make_float2(0.f, 0.f);
+        continue;
+      }
+      const float2* zr = smem(q * 2 + sd);
+      float2 zk = zr[m];
+      float2 zc = cconjf(zr[m == 0 ? 0 : L - m]);
+      float2 ev = caddf(zk, zc), od = csubf(zk, zc);
+      float2 t1 = cmulf(w, od);
+      X[sd] = make_float2(0.5f * (ev.x + t1.y) * inv_n, 0.5f * (ev.y - t1.x) * inv_n);
+    }
+    float2 S = eq ? X[0] : caddf(X[0], X[1]);
+    float2 D = eq ? make_float2(0.f, 0.f) : csubf(X[0], X[1]);
+    int64_t col = p0 * a.F + q;
+    wfold[((int64_t)(m * 2 + 0) * a.H + h) * Rc + col] = S;
+    wfold[((int64_t)(m * 2 + 1) * a.H + h) * Rc + col] = D;
+  }
+}
+
+struct FastUnfoldArgs {
+  int nlat, nlon, T, H, nlat_odd, mode, G;
+  int64_t planes;
+  float radius;
+};
+
+// waist(s) -> grid.  8 warps: warp w handles (row pair index po = w >> 1,
+// side = w & 1) with po = gp*NO + o (o: output field).
+template <int FF>
+__global__ void __launch_bounds__(256) fast_inverse_unfold(FastUnfoldArgs a, const float2* __restrict__ wP,
+                                                           const float2* __restrict__ wD,
+                                                           const double* __restrict__ coslat,
+                                                           const float2* __restrict__ twL,
+                                                           const float2* __restrict__ twN,
+                                                           float* __restrict__ out0,
+                                                           float* __restrict__ out1) {
+  constexpr int L = 32 * FF;
+  extern __shared__ float2 smem_dyn[];
+  auto smem = [&](int w) { return smem_dyn + w * WarpSmem<FF>::kFloats2; };
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int h = blockIdx.x;
+  const int64_t p0 = (int64_t)blockIdx.y * a.G;
+  const bool eq = a.nlat_odd && h == a.H - 1;
+  const int NO = (a.mode == kUnfoldGradient || a.mode == kUnfoldWind) ? 2 : 1;
+  const int FW = a.mode == kUnfoldWind ? 2 : 1;
+  const int64_t Rc = a.planes * FW;
+  const float inv_a = 1.0f / a.radius;
+  const int jrow[2] = {h, a.nlat - 1 - h};
+
+  // Stage 1: Fourier coefficients of every output row into smem[row][m].
+  for (int t = threadIdx.x; t < (a.T + 1) * a.G; t += blockDim.x) {
+    int m = t / a.G, gp = t - m * a.G;
+    int64_t plane = p0 + gp;
+    if (plane >= a.planes) continue;
+#pragma unroll
+    for (int sd = 0; sd < 2; ++sd) {
+      if (sd == 1 && eq) continue;
+      float sgn = sd ? -1.f : 1.f;
+      float im_over = (float)m / (a.radius * (float)coslat[jrow[sd]]);
+      auto fetch = [&](const float2* w, int fld) {
+        int64_t c0 = ((int64_t)(m * 2 + 0) * a.H + h) * Rc + plane * FW + fld;
+        int64_t c1 = ((int64_t)(m * 2 + 1) * a.H + h) * Rc + plane * FW + fld;
+        float2 s = w[c0], d = w[c1];
+        return make_float2(s.x + sgn * d.x, s.y + sgn * d.y);
+      };
+      float2 o0, o1 = make_float2(0.f, 0.f);
+      if (a.mode == kUnfoldScalar || a.mode == kUnfoldMeridional) {
+        o0 = fetch(wP, 0);
+      } else if (a.mode == kUnfoldZonal) {
+        float2 x = fetch(wP, 0);
+        o0 = make_float2(-(float)m * x.y, (float)m * x.x);
+      } else if (a.mode == kUnfoldGradient) {
+        float2 x = fetch(wP, 0);
+        o0 = make_float2(-(float)m * x.y, (float)m * x.x);
+        o1 = fetch(wD, 0);
+      } else {
+        float2 xp = fetch(wP, 0), xc = fetch(wP, 1);
+        float2 dp = fetch(wD, 0), dc = fetch(wD, 1);
+        o0 = make_float2(-dp.x * inv_a - im_over * xc.y, -dp.y * inv_a + im_over * xc.x);
+        o1 = make_float2(-im_over * xp.y + dc.x * inv_a, im_over * xp.x + dc.y * inv_a);
+      }
+      smem((gp * NO + 0) * 2 + sd)[m] = o0;
+      if (NO == 2) smem((gp * NO + 1) * 2 + sd)[m] = o1;
+    }
+  }
+  __syncthreads();
+  const int po = warp >> 1, side = warp & 1;
+  const int o = po % NO, gp = po / NO;
+  const int64_t plane = p0 + gp;
+  if (po >= a.G * NO || plane >= a.planes || (eq && side == 1)) return;
+  float2* reg = smem(warp);
+  // Stage 2: entangle z[k] for k = lane + 32 j straight into registers.
+  float2 z[FF];
+#pragma unroll
+  for (int i = 0; i < FF; ++i) {
+    int k = lane + 32 * i;
+    float2 xk = k <= a.T ? reg[k] : make_float2(0.f, 0.f);
+    int kc = L - k;
+    float2 xc = (k > 0 && kc <= a.T) ? cconjf(reg[kc]) : make_float2(0.f, 0.f);
+    if (k == 0) xk.y = 0.f;
+    float2 s = caddf(xk, xc), d = csubf(xk, xc);
+    float2 wd = cmulf(cconjf(twN[k]), d);
+    z[i] = make_float2(s.x - wd.y, s.y + wd.x);
+  }
+  __syncwarp();
+  warp_fft<FF, true>(z, reg, twL, lane);
+  // Stage 3: natural-order z[n] -> x[2n], x[2n+1] with the row scaling.
+  const int j = jrow[side];
+  // The gradient divides the grid by (a cos phi) and by a, as the reference does.
+  const bool divide = a.mode == kUnfoldGradient;
+  const float den = o == 0 ? a.radius * (float)coslat[j] : a.radius;
+  float2* dst = reinterpret_cast<float2*>((o ? out1 : out0) + (plane * a.nlat + j) * (int64_t)a.nlon);
+#pragma unroll 4
+  for (int i = 0; i < FF; ++i) {
+    float2 v = reg[lane + 32 * i];
+    if (divide) v = make_float2(v.x / den, v.y / den);
+    dst[lane + 32 * i] = v;
+  }
+}
+
+template <int FF>
+void launch_fwd(const sht_plan* p, const float* g0, const float* g1, int64_t planes, float* wfold,
+                cudaStream_t s) {
+  FastFoldArgs a{p->nlat, p->nlon, p->T, p->H, p->nlat_odd ? 1 : 0, g1 ? 2 : 1, 0, planes};
+  a.G = 4 / a.F;
+  dim3 grid((unsigned)p->H, (unsigned)div_up(planes, a.G));
+  const size_t sm = sizeof(float2) * 8 * WarpSmem<FF>::kFloats2;
+  SHT_CUDA_OR_THROW(cudaFuncSetAttribute(fast_forward_fold<FF>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  fast_forward_fold<FF><<<grid, 256, sm, s>>>(a, g0, g1 ? g1 : g0, (const float2*)p->tw_l,
+                                             (const float2*)p->tw_n, (float2*)wfold);
+  SHT_CUDA_OR_THROW(cudaGetLastError());
+}
+
+template <int FF>
+void launch_inv(const sht_plan* p, int mode, const float* wP, const float* wD, int64_t planes,
+                float* out0, float* out1, cudaStream_t s) {
+  int NO = (mode == kUnfoldGradient || mode == kUnfoldWind) ? 2 : 1;
+  FastUnfoldArgs a{p->nlat, p->nlon, p->T, p->H, p->nlat_odd ? 1 : 0, mode, 4 / NO, planes,
+                   (float)p->radius};
+  dim3 grid((unsigned)p->H, (unsigned)div_up(planes, a.G));
+  const size_t sm = sizeof(float2) * 8 * WarpSmem<FF>::kFloats2;
+  SHT_CUDA_OR_THROW(cudaFuncSetAttribute(fast_inverse_unfold<FF>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  fast_inverse_unfold<FF><<<grid, 256, sm, s>>>(a, (const float2*)wP, (const float2*)(wD ? wD : wP),
+                                               p->d_coslat, (const float2*)p->tw_l,
+                                               (const float2*)p->tw_n, out0, out1 ? out1 : out0);
+  SHT_CUDA_OR_THROW(cudaGetLastError());
+}
+
+}  // namespace
+
+bool fast_fft_supported(const sht_plan* p) {
+  if (p->prec == SHT_PREC_F64 || p->L % 32 != 0) return false;
+  switch (p->L / 32) {
+    case 2: case 3: case 4: case 6: case 8: case 12: case 16: case 24: return true;
+    default: return false;
+  }
+}
+
+void fast_fft_init_constants(cudaStream_t s) {
+  float2 w24[24], w32[32], w16[16];
+  for (int k = 0; k < 24; ++k) w24[k] = make_float2((float)cos(-2 * kPi * k / 24), (float)sin(-2 * kPi * k / 24));
+  for (int k = 0; k < 32; ++k) w32[k] = make_float2((float)cos(-2 * kPi * k / 32), (float)sin(-2 * kPi * k / 32));
+  for (int k = 0; k < 16; ++k) w16[k] = make_float2((float)cos(-2 * kPi * k / 16), (float)sin(-2 * kPi * k / 16));
+  SHT_CUDA_OR_THROW(cudaMemcpyToSymbolAsync(c_w24, w24, sizeof(w24), 0, cudaMemcpyHostToDevice, s));
+  SHT_CUDA_OR_THROW(cudaMemcpyToSymbolAsync(c_w32, w32, sizeof(w32), 0, cudaMemcpyHostToDevice, s));
+  SHT_CUDA_OR_THROW(cudaMemcpyToSymbolAsync(c_w16, w16, sizeof(w16), 0, cudaMemcpyHostToDevice, s));
+  SHT_CUDA_OR_THROW(cudaStreamSynchronize(s));
+}
+
+void fast_forward_fold(const sht_plan* p, const float* g0, const float* g1, int64_t planes,
+                       float* wfold, cudaStream_t s) {
+  switch (p->L / 32) {
+    case 2: launch_fwd<2>(p, g0, g1, planes, wfold, s); break;
+    case 3: launch_fwd<3>(p, g0, g1, planes, wfold, s); break;
+    case 4: launch_fwd<4>(p, g0, g1, planes, wfold, s); break;
+    case 6: launch_fwd<6>(p, g0, g1, planes, wfold, s); break;
+    case 8: launch_fwd<8>(p, g0, g1, planes, wfold, s); break;
+    case 12: launch_fwd<12>(p, g0, g1, planes, wfold, s); break;
+    case 16: launch_fwd<16>(p, g0, g1, planes, wfold, s); break;
+    case 24: launch_fwd<24>(p, g0, g1, planes, wfold, s); break;
+    default: throw Error{SHT_ERR_STATE, "fast FFT: unsupported length"};
+  }
+}
+
+void fast_inverse_unfold(const sht_plan* p, int mode, const float* wP, const float* wD,
+                         int64_t planes, float* out0, float* out1, cudaStream_t s) {
+  switch (p->L / 32) {
+    case 2: launch_inv<2>(p, mode, wP, wD, planes, out0, out1, s); break;
+    case 3: launch_inv<3>(p, mode, wP, wD, planes, out0, out1, s); break;
+    case 4: launch_inv<4>(p, mode, wP, wD, planes, out0, out1, s); break;
+    case 6: launch_inv<6>(p, mode, wP, wD, planes, out0, out1, s); break;
+    case 8: launch_inv<8>(p, mode, wP, wD, planes, out0, out1, s); break;
+    case 12: launch_inv<12>(p, mode, wP, wD, planes, out0, out1, s); break;
+    case 16: launch_inv<16>(p, mode, wP, wD, planes, out0, out1, s); break;
+    case 24: launch_inv<24>(p, mode, wP, wD, planes, out0, out1, s); break;
+    default: throw Error{SHT_ERR_STATE, "fast FFT: unsupported length"};
+  }
+}
+
+}  // namespace sht

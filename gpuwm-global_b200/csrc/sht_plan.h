@@ -60,6 +60,8 @@ struct sht_plan {
   void* tw_n = nullptr;
   std::vector<int> radices;
   int* d_radices = nullptr;
+  bool fast_fft = false;           // register-resident kernels (sht_fft_fast.cu)
+  bool force_generic_fft = false;  // SHT_FLAG_GENERIC_FFT
 
   // GEMM descriptors: [direction][flip] (direction 0 synthesis, 1 analysis).
   ShtGemmDesc* d_desc[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
@@ -110,6 +112,15 @@ enum UnfoldMode { kUnfoldScalar = 0, kUnfoldZonal = 1, kUnfoldGradient = 2, kUnf
 template <typename T>
 void launch_inverse_unfold(const sht_plan* p, int mode, const T* wP, const T* wD,
                            int64_t planes, T* out0, T* out1, cudaStream_t s);
+
+// Register-resident FP32 FFTs for nlon = 64 F, F in {2,3,4,6,8,12,16,24}
+// (sht_fft_fast.cu).
+bool fast_fft_supported(const sht_plan* p);
+void fast_fft_init_constants(cudaStream_t s);
+void fast_forward_fold(const sht_plan* p, const float* g0, const float* g1, int64_t planes,
+                       float* wfold, cudaStream_t s);
+void fast_inverse_unfold(const sht_plan* p, int mode, const float* wP, const float* wD,
+                         int64_t planes, float* out0, float* out1, cudaStream_t s);
 
 // SIMT Legendre GEMM (sht_gemm_simt.cu).
 void build_gemm_items(sht_plan* p);

@@ -33,8 +33,10 @@ extern "C" {
 #define SHT_PREC_F32 1     /* plain FP32 FFMA path */
 #define SHT_PREC_SPLIT16 2 /* FP16 hi+lo split on tcgen05 tensor cores, FP32 accumulate */
 
-/* sht_plan_create flags. */
-#define SHT_FLAG_GEOMETRY_ONLY 1
+/* sht_plan_create flags (bitwise or). */
+#define SHT_FLAG_GEOMETRY_ONLY 1 /* Gauss nodes and weights only */
+#define SHT_FLAG_GENERIC_FFT 2   /* shared-memory Stockham FFTs even where the
+                                    register-resident kernels apply (testing) */
 
 /* Status codes. */
 #define SHT_OK 0
@@ -59,8 +61,9 @@ const char* sht_last_error(void);
  * (src/arwen_global/spectral/transform.py:753-899) and GaussianGrid.create
  * (src/arwen_global/spectral/grid.py:97-126).  nlat/nlon are taken as given
  * (the Python layer applies the reference's shape rule, grid.py:26-94).
- * flags: 0, or SHT_FLAG_GEOMETRY_ONLY to compute only the Gauss nodes and
- * weights (sht_plan_geometry works; transform calls fail). */
+ * flags: SHT_FLAG_GEOMETRY_ONLY computes only the Gauss nodes and weights
+ * (sht_plan_geometry works; transform calls fail); SHT_FLAG_GENERIC_FFT
+ * selects the generic FFT kernels. */
 int sht_plan_create(int truncation, int nlat, int nlon, double radius_m,
                     int precision, int flags, sht_plan** out_plan);
 int sht_plan_destroy(sht_plan* plan);

@@ -200,6 +200,40 @@ def record_gauss_exact() -> None:
     print("wrote gauss_exact.npz")
 
 
+def record_fp32_errors() -> None:
+    """The reference's own float32 accuracy on the config grids: relative
+    spectral L2 of vordiv_from_wind (float32 inputs) and of forward against
+    its float64 path, on the seeded red-spectrum inputs the GPU tests use.
+    The integration-by-parts vector analysis loses digits to cancellation
+    in float32, so its bar is set from the reference rather than 2e-6."""
+    from arwen_global.spectral.transform import SphericalHarmonicTransform
+    from arwen_global.spectral.vector import VorticityDivergenceOperator
+
+    sys.path.insert(0, str(HERE.parents[1] / "gpuwm-global_b200"))
+    from b200sht.synthetic import red_spectrum
+
+    def rel_l2(a, b):
+        w = np.where(np.arange(a.shape[-1]) == 0, 1.0, 2.0)[None, :]
+        return float(np.sqrt(np.sum(w * np.abs(a - b) ** 2) / np.sum(w * np.abs(b) ** 2)))
+
+    out = {}
+    for t, kw in [(62, {"nlat": 94, "nlon": 192, "dealias_factor": 1.49}),
+                  (126, {"nlat": 192, "nlon": 384}), (255, {}), (511, {})]:
+        r64 = SphericalHarmonicTransform.create(t, precision="float64", **kw)
+        r32 = SphericalHarmonicTransform.create(t, precision="float32", **kw)
+        v64, v32 = VorticityDivergenceOperator(r64), VorticityDivergenceOperator(r32)
+        c = red_spectrum(t, 3)
+        u, v = v64.wind_from_vordiv(c, c[::-1].copy())
+        z, d = v64.vordiv_from_wind(u, v)
+        z2, d2 = v32.vordiv_from_wind(u.astype(np.float32), v.astype(np.float32))
+        g = r64.inverse(c)
+        f2 = r32.forward(g.astype(np.float32))
+        out[str(t)] = {"vordiv": max(rel_l2(z2, z), rel_l2(d2, d)),
+                       "forward": rel_l2(f2, r64.forward(g))}
+        print("fp32 errors", t, out[str(t)], flush=True)
+    (HERE / "reference_fp32_errors.json").write_text(json.dumps(out, indent=1, sort_keys=True))
+
+
 def main() -> None:
     ref_root = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
     os.environ.setdefault("ARWEN_GLOBAL_LEGENDRE_CACHE", "off")
@@ -208,6 +242,7 @@ def main() -> None:
     record_helmholtz()
     record_ynm(ref_root)
     record_gauss_exact()
+    record_fp32_errors()
 
 
 if __name__ == "__main__":

@@ -48,7 +48,7 @@ def test_plan_create_validates_before_cuda(lib):
         (10, 16, 20, 1.0, 0, 0),     # nlon < 2T+2
         (10, 16, 32, -1.0, 0, 0),    # radius
         (10, 16, 32, 1.0, 7, 0),     # precision
-        (10, 16, 32, 1.0, 0, 5),     # flags
+        (10, 16, 32, 1.0, 0, 8),     # flags
     ]
     for args in cases:
         st = lib.sht_plan_create(*args, ctypes.byref(h))

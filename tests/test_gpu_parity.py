@@ -235,3 +235,80 @@ def test_leading_shapes_and_empty_batches():
         assert rel_max(c, ora.forward(f)) < 1e-12
     empty = sht.forward(np.zeros((0, sht.grid.nlat, sht.grid.nlon)))
     assert tuple(empty.shape) == (0, 22, 22)
+
+
+CONFIG_GRIDS = [(62, 94, 192, 1.49), (126, 192, 384, 1.5), (255, 384, 768, 1.5),
+                (511, 768, 1536, 1.5)]
+
+
+@pytest.mark.parametrize("t,nlat,nlon,df", CONFIG_GRIDS)
+def test_fp32_and_split_against_fp64_at_config_grids(t, nlat, nlon, df):
+    """Every transform of the FP32 and split paths, with the register-resident
+    FFT and with the generic FFT, against the GPU FP64 path (itself pinned to
+    the reference above and to the oracle below)."""
+    import torch
+
+    from b200sht import SphericalHarmonicTransform, VorticityDivergenceOperator
+    from b200sht._lib import SHT_FLAG_GENERIC_FFT
+    from b200sht.synthetic import red_spectrum
+
+    import json
+
+    from conftest import GOLDEN
+
+    kw = dict(nlat=nlat, nlon=nlon, dealias_factor=df)
+    # The reference's own float32 vector analysis loses digits to the
+    # i m rot + shear cancellation (1.9e-6 at T62 to 1.2e-5 at T511): the
+    # vorticity/divergence bar is 1.5x the reference float32 error.
+    ref_err = json.loads((GOLDEN / "reference_fp32_errors.json").read_text())[str(t)]
+    vordiv_tol = max(2e-6, 1.5 * ref_err["vordiv"])
+    coeff = red_spectrum(t, 3)
+    f64 = SphericalHarmonicTransform.create(t, precision="float64", **kw)
+    vec64 = VorticityDivergenceOperator(f64)
+    np_ = f64.backend.to_numpy
+    g64 = f64.inverse(coeff)
+    c64 = np_(f64.forward(g64))
+    e64, n64 = (np_(x) for x in f64.gradient(coeff))
+    u64, v64 = (np_(x) for x in vec64.wind_from_vordiv(coeff, coeff[::-1].copy()))
+    z64, d64 = (np_(x) for x in vec64.vordiv_from_wind(u64, v64))
+    for precision in ("float32", "split16"):
+        for flags in (0, SHT_FLAG_GENERIC_FFT):
+            sht = SphericalHarmonicTransform.create(t, precision=precision, plan_flags=flags, **kw)
+            vec = VorticityDivergenceOperator(sht)
+            g32 = g64.to(torch.float32)
+            assert rel_l2(np_(sht.forward(g32)), c64) < 2e-6, (precision, flags)
+            assert rel_max(np_(sht.inverse(coeff)), np_(g64)) < 2e-6, (precision, flags)
+            e, n = sht.gradient(coeff)
+            assert rel_max(np_(e), e64) < 2e-6 and rel_max(np_(n), n64) < 2e-6
+            u, v = vec.wind_from_vordiv(coeff, coeff[::-1].copy())
+            assert rel_max(np_(u), u64) < 2e-6 and rel_max(np_(v), v64) < 2e-6
+            z, d = vec.vordiv_from_wind(u64, v64)
+            assert rel_l2(np_(z), z64) < vordiv_tol and rel_l2(np_(d), d64) < vordiv_tol
+            sht.check_device()
+
+
+def test_fp64_against_oracle_t255():
+    from b200sht import SphericalHarmonicTransform
+    from b200sht.synthetic import red_spectrum
+    from oracle.dense_sht import DenseSHT
+
+    ora = DenseSHT(255)
+    sht = SphericalHarmonicTransform.create(255, precision="float64")
+    coeff = red_spectrum(255, 2, seed=5)
+    g = sht.backend.to_numpy(sht.inverse(coeff))
+    assert rel_max(g, ora.inverse(coeff)) < 1e-12
+    rng = np.random.default_rng(1)
+    f = g + 0.01 * rng.standard_normal(g.shape)
+    assert rel_max(sht.backend.to_numpy(sht.forward(f)), ora.forward(f)) < 1e-12
+
+
+def test_fp64_roundtrip_t511():
+    """forward(inverse(c)) = c at full size (the Gram-corrected analysis)."""
+    from b200sht import SphericalHarmonicTransform
+    from b200sht.synthetic import red_spectrum
+
+    sht = SphericalHarmonicTransform.create(511, precision="float64")
+    coeff = red_spectrum(511, 2, seed=9)
+    back = sht.backend.to_numpy(sht.forward(sht.inverse(coeff)))
+    assert rel_l2(back, coeff) < 1e-12
+    assert rel_max(back, coeff) < 1e-11
