@@ -106,12 +106,25 @@ void ensure_scratch(sht_plan* p, int64_t R) {
     if (p->cfold[i]) cudaFree(p->cfold[i]);
     p->wfold[i] = p->cfold[i] = nullptr;
   }
+  if (p->rowmax) cudaFree(p->rowmax);
+  p->rowmax = nullptr;
   p->scratch_rows = 0;
   for (int i = 0; i < 2; ++i) {
     SHT_CUDA_OR_THROW(cudaMalloc(&p->wfold[i], p->elem() * std::max<int64_t>(p->wfold_elems(R), 1)));
     SHT_CUDA_OR_THROW(cudaMalloc(&p->cfold[i], p->elem() * std::max<int64_t>(p->cfold_elems(R), 1)));
   }
+  SHT_CUDA_OR_THROW(cudaMalloc(&p->rowmax, sizeof(float) * std::max<int64_t>(R, 1)));
   p->scratch_rows = R;
+}
+
+bool uses_tc(const sht_plan* p) { return p->prec == SHT_PREC_SPLIT16 && p->tc != nullptr; }
+
+// The row-max buffer the producer of a split-precision operand fills
+// (zeroed first), or nullptr on the FP32/FP64 paths.
+float* rowmax_for(sht_plan* p, int64_t R, cudaStream_t s) {
+  if (!uses_tc(p)) return nullptr;
+  SHT_CUDA_OR_THROW(cudaMemsetAsync(p->rowmax, 0, sizeof(float) * R, s));
+  return p->rowmax;
 }
 
 template <typename T>
@@ -119,8 +132,8 @@ void contract(sht_plan* p, int kind, const T* data, T* out, int64_t R, cudaStrea
   const int dir = table_dir(kind), flip = table_flip(kind);
   KernelScope scope(p, dir == 0 ? SHT_KIND_LEGENDRE_SYNTHESIS : SHT_KIND_LEGENDRE_ANALYSIS, s);
   if constexpr (sizeof(T) == 4) {
-    if (p->prec == SHT_PREC_SPLIT16 && p->tc != nullptr) {
-      launch_gemm_tc(p, dir, flip, kind, data, out, R, s);
+    if (uses_tc(p)) {
+      launch_gemm_tc(p, dir, flip, kind, data, p->rowmax, out, R, s);
       return;
     }
   }
@@ -134,8 +147,9 @@ void do_forward(sht_plan* p, const T* grid, int64_t planes, T* coeff, cudaStream
   T* w = static_cast<T*>(p->wfold[0]);
   T* c = static_cast<T*>(p->cfold[0]);
   {
+    float* rm = rowmax_for(p, R, s);
     KernelScope k(p, SHT_KIND_FFT_FORWARD, s);
-    launch_forward_fold<T>(p, grid, nullptr, planes, w, s);
+    launch_forward_fold<T>(p, grid, nullptr, planes, w, s, rm);
   }
   contract<T>(p, kAnalysis, w, c, R, s);
   {
@@ -152,8 +166,9 @@ void do_synthesis(sht_plan* p, int kind, int mode, const T* coeff, int64_t plane
   T* w = static_cast<T*>(p->wfold[0]);
   T* c = static_cast<T*>(p->cfold[0]);
   {
+    float* rm = rowmax_for(p, R, s);
     KernelScope k(p, SHT_KIND_PACK, s);
-    launch_pack<T>(p, coeff, nullptr, planes, kPackPlain, c, s);
+    launch_pack<T>(p, coeff, nullptr, planes, kPackPlain, c, s, rm);
   }
   contract<T>(p, kind, c, w, R, s);
   {
@@ -171,8 +186,9 @@ void do_gradient(sht_plan* p, const T* coeff, int64_t planes, T* east, T* north,
   T* w0 = static_cast<T*>(p->wfold[0]);
   T* w1 = static_cast<T*>(p->wfold[1]);
   {
+    float* rm = rowmax_for(p, R, s);
     KernelScope k(p, SHT_KIND_PACK, s);
-    launch_pack<T>(p, coeff, nullptr, planes, kPackPlain, c, s);
+    launch_pack<T>(p, coeff, nullptr, planes, kPackPlain, c, s, rm);
   }
   contract<T>(p, kBasis, c, w0, R, s);
   contract<T>(p, kDBasis, c, w1, R, s);
@@ -191,8 +207,9 @@ void do_wind(sht_plan* p, const T* vort, const T* div, int64_t planes, T* u, T* 
   T* w0 = static_cast<T*>(p->wfold[0]);
   T* w1 = static_cast<T*>(p->wfold[1]);
   {
+    float* rm = rowmax_for(p, R, s);
     KernelScope k(p, SHT_KIND_PACK, s);
-    launch_pack<T>(p, vort, div, planes, kPackInvLap, c, s);
+    launch_pack<T>(p, vort, div, planes, kPackInvLap, c, s, rm);
   }
   contract<T>(p, kBasis, c, w0, R, s);
   contract<T>(p, kDBasis, c, w1, R, s);
@@ -211,8 +228,9 @@ void do_vordiv(sht_plan* p, const T* u, const T* v, int64_t planes, T* vort, T* 
   T* c0 = static_cast<T*>(p->cfold[0]);
   T* c1 = static_cast<T*>(p->cfold[1]);
   {
+    float* rm = rowmax_for(p, R, s);
     KernelScope k(p, SHT_KIND_FFT_FORWARD, s);
-    launch_forward_fold<T>(p, u, v, planes, w, s);
+    launch_forward_fold<T>(p, u, v, planes, w, s, rm);
   }
   contract<T>(p, kRot, w, c0, R, s);
   contract<T>(p, kShear, w, c1, R, s);
@@ -233,7 +251,7 @@ void destroy(sht_plan* p) {
   void* ptrs[] = {p->d_mu, p->d_w, p->d_coslat, p->basis, p->dbasis, p->analysis, p->rot,
                   p->shear, p->tw_l, p->tw_n, p->d_radices, p->d_items[0], p->d_items[1],
                   p->d_desc[0][0], p->d_desc[0][1], p->d_desc[1][0], p->d_desc[1][1],
-                  p->wfold[0], p->wfold[1], p->cfold[0], p->cfold[1], p->d_err};
+                  p->wfold[0], p->wfold[1], p->cfold[0], p->cfold[1], p->rowmax, p->d_err};
   for (void* q : ptrs)
     if (q) cudaFree(q);
   delete p;

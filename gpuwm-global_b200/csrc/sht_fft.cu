@@ -247,7 +247,8 @@ __device__ void load_w16(V2<T>* w16, const V2<T>* tw, int L) {
 template <typename T>
 __global__ void forward_fold_kernel(FoldArgs a, const T* __restrict__ g0,
                                     const T* __restrict__ g1, const V2<T>* __restrict__ tw_l,
-                                    const V2<T>* __restrict__ tw_n, T* __restrict__ wfold) {
+                                    const V2<T>* __restrict__ tw_n, T* __restrict__ wfold,
+                                    float* __restrict__ rowmax) {
   extern __shared__ unsigned char smem_raw[];
   V2<T>* bufA = reinterpret_cast<V2<T>*>(smem_raw);
   const int h = blockIdx.x;
@@ -283,6 +284,7 @@ __global__ void forward_fold_kernel(FoldArgs a, const T* __restrict__ g0,
   const int64_t R = a.planes * a.F * 2;
   const T inv_n = T(1) / T(a.nlon);
   V2<T>* out = reinterpret_cast<V2<T>*>(wfold);
+  float mre = 0.f, mim = 0.f;  // this thread's column maxima (pf = tid % nper)
   for (int t = threadIdx.x; t < (a.T + 1) * nper; t += blockDim.x) {
     int m = t / nper, pf = t - m * nper;
     int gp = pf / a.F;
@@ -313,6 +315,12 @@ __global__ void forward_fold_kernel(FoldArgs a, const T* __restrict__ g0,
     int64_t base1 = ((int64_t)(m * 2 + 1) * a.H + h) * (R / 2) + rr;
     out[base0] = S;
     out[base1] = D;
+    mre = fmaxf(mre, (float)fmax(fabs(S.x), fabs(D.x)));
+    mim = fmaxf(mim, (float)fmax(fabs(S.y), fabs(D.y)));
+  }
+  if (rowmax != nullptr) {
+    const int pf = threadIdx.x % nper;  // fixed per thread: blockDim % nper == 0
+    rowmax_merge(rowmax, p0 * a.F + pf, p0 + pf / a.F < a.planes, mre, mim, nper);
   }
 }
 
@@ -521,10 +529,10 @@ void build_fft(sht_plan* p, cudaStream_t s) {
 
 template <typename T>
 void launch_forward_fold(const sht_plan* p, const T* g0, const T* g1, int64_t planes,
-                         T* wfold, cudaStream_t s) {
+                         T* wfold, cudaStream_t s, float* rowmax) {
   if constexpr (sizeof(T) == 4) {
     if (p->fast_fft) {
-      fast_forward_fold(p, g0, g1, planes, wfold, s);
+      fast_forward_fold(p, g0, g1, planes, wfold, s, rowmax);
       return;
     }
   }
@@ -544,8 +552,9 @@ void launch_forward_fold(const sht_plan* p, const T* g0, const T* g1, int64_t pl
   size_t sm = smem_bytes<T>(p, rows);
   allow_smem(forward_fold_kernel<T>, sm);
   dim3 grid_dim((unsigned)p->H, (unsigned)div_up(planes, a.G));
+  SHT_REQUIRE(rowmax == nullptr || 256 % (a.G * a.F) == 0, "row maxima need 256 % (G F) == 0");
   forward_fold_kernel<T><<<grid_dim, 256, sm, s>>>(a, g0, g1 ? g1 : g0, (const V2<T>*)p->tw_l,
-                                                   (const V2<T>*)p->tw_n, wfold);
+                                                   (const V2<T>*)p->tw_n, wfold, rowmax);
   SHT_CUDA_OR_THROW(cudaGetLastError());
 }
 
@@ -581,9 +590,9 @@ void launch_inverse_unfold(const sht_plan* p, int mode, const T* wP, const T* wD
 }
 
 template void launch_forward_fold<float>(const sht_plan*, const float*, const float*, int64_t,
-                                         float*, cudaStream_t);
+                                         float*, cudaStream_t, float*);
 template void launch_forward_fold<double>(const sht_plan*, const double*, const double*, int64_t,
-                                          double*, cudaStream_t);
+                                          double*, cudaStream_t, float*);
 template void launch_inverse_unfold<float>(const sht_plan*, int, const float*, const float*,
                                            int64_t, float*, float*, cudaStream_t);
 template void launch_inverse_unfold<double>(const sht_plan*, int, const double*, const double*,

@@ -203,7 +203,8 @@ __global__ void __launch_bounds__(256) fast_forward_fold(FastFoldArgs a, const f
                                                          const float* __restrict__ g1,
                                                          const float2* __restrict__ twL,
                                                          const float2* __restrict__ twN,
-                                                         float2* __restrict__ wfold) {
+                                                         float2* __restrict__ wfold,
+                                                         float* __restrict__ rowmax) {
   constexpr int L = 32 * FF;
   extern __shared__ float2 smem_dyn[];
   auto smem = [&](int w) { return smem_dyn + w * WarpSmem<FF>::kFloats2; };
@@ -230,6 +231,7 @@ __global__ void __launch_bounds__(256) fast_forward_fold(FastFoldArgs a, const f
   // Untangle, scale, fold, write: thread -> (m, pf) with pf fastest.
   const float inv_n = 1.0f / (float)a.nlon;
   const int64_t Rc = a.planes * a.F;  // complex columns per waist row
+  float mre = 0.f, mim = 0.f;         // this thread's column maxima (q = tid % nper)
   for (int t = threadIdx.x; t < (a.T + 1) * nper; t += blockDim.x) {
     int m = t / nper, q = t - m * nper;
     int gq = q / a.F;
@@ -254,6 +256,12 @@ __global__ void __launch_bounds__(256) fast_forward_fold(FastFoldArgs a, const f
     int64_t col = p0 * a.F + q;
     wfold[((int64_t)(m * 2 + 0) * a.H + h) * Rc + col] = S;
     wfold[((int64_t)(m * 2 + 1) * a.H + h) * Rc + col] = D;
+    mre = fmaxf(mre, fmaxf(fabsf(S.x), fabsf(D.x)));
+    mim = fmaxf(mim, fmaxf(fabsf(S.y), fabsf(D.y)));
+  }
+  if (rowmax != nullptr) {
+    const int q = threadIdx.x % nper;  // fixed per thread: blockDim % nper == 0
+    rowmax_merge(rowmax, p0 * a.F + q, p0 + q / a.F < a.planes, mre, mim, nper);
   }
 }
 
@@ -359,7 +367,7 @@ __global__ void __launch_bounds__(256) fast_inverse_unfold(FastUnfoldArgs a, con
 
 template <int FF>
 void launch_fwd(const sht_plan* p, const float* g0, const float* g1, int64_t planes, float* wfold,
-                cudaStream_t s) {
+                cudaStream_t s, float* rowmax) {
   FastFoldArgs a{p->nlat, p->nlon, p->T, p->H, p->nlat_odd ? 1 : 0, g1 ? 2 : 1, 0, planes};
   a.G = 4 / a.F;
   dim3 grid((unsigned)p->H, (unsigned)div_up(planes, a.G));
@@ -367,7 +375,7 @@ void launch_fwd(const sht_plan* p, const float* g0, const float* g1, int64_t pla
   SHT_CUDA_OR_THROW(cudaFuncSetAttribute(fast_forward_fold<FF>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
   fast_forward_fold<FF><<<grid, 256, sm, s>>>(a, g0, g1 ? g1 : g0, (const float2*)p->tw_l,
-                                             (const float2*)p->tw_n, (float2*)wfold);
+                                             (const float2*)p->tw_n, (float2*)wfold, rowmax);
   SHT_CUDA_OR_THROW(cudaGetLastError());
 }
 
@@ -409,16 +417,16 @@ void fast_fft_init_constants(cudaStream_t s) {
 }
 
 void fast_forward_fold(const sht_plan* p, const float* g0, const float* g1, int64_t planes,
-                       float* wfold, cudaStream_t s) {
+                       float* wfold, cudaStream_t s, float* rowmax) {
   switch (p->L / 32) {
-    case 2: launch_fwd<2>(p, g0, g1, planes, wfold, s); break;
-    case 3: launch_fwd<3>(p, g0, g1, planes, wfold, s); break;
-    case 4: launch_fwd<4>(p, g0, g1, planes, wfold, s); break;
-    case 6: launch_fwd<6>(p, g0, g1, planes, wfold, s); break;
-    case 8: launch_fwd<8>(p, g0, g1, planes, wfold, s); break;
-    case 12: launch_fwd<12>(p, g0, g1, planes, wfold, s); break;
-    case 16: launch_fwd<16>(p, g0, g1, planes, wfold, s); break;
-    case 24: launch_fwd<24>(p, g0, g1, planes, wfold, s); break;
+    case 2: launch_fwd<2>(p, g0, g1, planes, wfold, s, rowmax); break;
+    case 3: launch_fwd<3>(p, g0, g1, planes, wfold, s, rowmax); break;
+    case 4: launch_fwd<4>(p, g0, g1, planes, wfold, s, rowmax); break;
+    case 6: launch_fwd<6>(p, g0, g1, planes, wfold, s, rowmax); break;
+    case 8: launch_fwd<8>(p, g0, g1, planes, wfold, s, rowmax); break;
+    case 12: launch_fwd<12>(p, g0, g1, planes, wfold, s, rowmax); break;
+    case 16: launch_fwd<16>(p, g0, g1, planes, wfold, s, rowmax); break;
+    case 24: launch_fwd<24>(p, g0, g1, planes, wfold, s, rowmax); break;
     default: throw Error{SHT_ERR_STATE, "fast FFT: unsupported length"};
   }
 }

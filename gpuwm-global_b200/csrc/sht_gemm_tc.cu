@@ -6,28 +6,36 @@
 //   M = 128 data rows r (plane x re/im), N = a tile of the table's x extent
 //   (<= 256, multiple of 16), K = the contraction (latitude pairs for the
 //   analysis, degrees for the synthesis).
-// Both operands are split into FP16 hi + lo halves after a power-of-two
-// scaling that puts each operand row/column maximum in [2^14, 2^15):
-//   A ~ (hi_a + lo_a) / s_r,  B ~ (hi_b + lo_b) / s_x,
-//   C = (hi_a hi_b + hi_a lo_b + lo_a hi_b) / (s_r s_x)      (lo*lo dropped)
-// accumulated in FP32 in tensor memory.  The table halves and their column
-// scales are built once per plan from the FP64 tables and stored in global
-// memory as the exact shared-memory image of each (tile, K-stage), so one
-// bulk copy per half moves a stage.  The data rows are split on the fly by
-// converter warps: a first pass over the tile's K extent finds each row's
-// maximum (the per-row, per-order scale), a second converts and stores the
-// halves into shared memory.
+// Both operands are split into two FP16 parts after a power-of-two scaling
+// that puts each data row / table column maximum in [2^14, 2^15):
+//   a s_r = a1 + a2,  b s_x = b1 + b2            (11 significant bits each)
+//   C = (a1 b1 + [a1 b2 + a2 b1]) / (s_r s_x)
+// The main product a1 b1 and the two correction products accumulate in two
+// separate TMEM accumulators and are added in FP32 in the epilogue.  The
+// separation is what makes the result as accurate as an FP32 contraction:
+// the tensor core's FP32 accumulate truncates, and with all three products
+// in one accumulator every correction step adds another truncation of the
+// full-size sum (1.3e-6 relative spectral L2 at T255 against 2.4e-7 with the
+// accumulators separated, in an emulation of the pipeline; the plain FP32
+// path measures 2.9e-7 at T511).  The table parts and the column scales are
+// built once per plan from the FP64 tables and stored as the exact
+// shared-memory image of each (tile, K-stage), so one bulk copy per part
+// moves a stage.  The data rows are split on the fly by converter warps;
+// their row scales come from the row maxima the producing kernel (the
+// longitude FFT or the pack kernel) merged while writing the operand.
 //
 // Roles (448 threads, one CTA per SM, persistent over a cost-sorted tile list):
 //   warp 0      bulk-copy loader for the table stages; owns TMEM alloc/free
 //   warp 1      MMA issuer (one thread)
 //   warps 2-5   epilogue: tcgen05.ld of the accumulator, unscale, store
 //   warps 6-13  converters for the data operand
-// Pipelines: STAGES shared-memory stages (full/empty mbarriers), two TMEM
-// accumulators of 256 columns (full/empty mbarriers), four row-scale slots.
-// Every mbarrier wait is bounded by a clock budget; on expiry the thread
-// raises the plan's error word, sets a CTA abort flag and every role drains
-// and exits, so a fault in the pipeline logic cannot hang the GPU.
+// Pipelines: STAGES shared-memory stages (full/empty mbarriers) and one TMEM
+// accumulator pair (main and correction, 256 columns each; full/empty
+// mbarriers).  Every mbarrier wait is bounded by a clock budget; on expiry the
+// waiting thread raises the plan's error word and a CTA abort flag, and each
+// epilogue warp decides to stop as a whole (__any_sync) before the
+// warp-collective TMEM loads, so a fault in the pipeline logic cannot hang
+// the GPU.
 //
 // Operand layouts are the canonical no-swizzle MN-major UMMA layouts: a core
 // matrix is 8 K-rows of 8 contiguous M (or N) elements (16 bytes each row,
@@ -71,26 +79,26 @@ namespace sht {
 namespace {
 
 constexpr int BM = 128;
-constexpr int BK = 64;
-constexpr int STAGES = 2;
+constexpr int BK = 32;
+constexpr int STAGES = 4;
+constexpr int NPARTS = 2;
 constexpr int NMAX = 256;
 constexpr int kThreads = 448;
 constexpr int kConvThreads = 256;
 constexpr int kConvWarp0 = 6;
-constexpr int kEpiWarp0 = 2;
 constexpr long long kWaitBudget = 4000000000LL;  // clock cycles (~2 s)
 
 // Shared-memory plan (bytes).
-constexpr int kAStage = BM * BK * 2;     // one half of the A stage: 16 KB
-constexpr int kBStage = NMAX * BK * 2;   // one half of the B stage: 32 KB
-constexpr int kOffA = 0;                                  // [STAGES][2][kAStage]
-constexpr int kOffB = kOffA + STAGES * 2 * kAStage;       // [STAGES][2][kBStage]
-constexpr int kOffRS = kOffB + STAGES * 2 * kBStage;      // float rowscale[4][128]
-constexpr int kOffRed = kOffRS + 4 * BM * 4;              // float red[8][128]
-constexpr int kOffBar = kOffRed + 8 * BM * 4;             // mbarriers (8 B each)
-constexpr int kNumBars = 3 * STAGES + 4 + 4 + 4 + 1;
-constexpr int kOffMisc = kOffBar + kNumBars * 8;          // tmem base, abort flag
-constexpr int kSmemBytes = kOffMisc + 16 + 1024;          // + alignment slack
+constexpr int kAPart = BM * BK * 2;      // one FP16 part of the A stage: 8 KB
+constexpr int kBPart = NMAX * BK * 2;    // one FP16 part of the B stage: 16 KB
+constexpr int kALbo = (BM / 8) * 128;    // A: K-group stride (16 M-groups of 128 B)
+constexpr int kOffA = 0;                                   // [STAGES][NPARTS][kAPart]
+constexpr int kOffB = kOffA + STAGES * NPARTS * kAPart;    // [STAGES][NPARTS][kBPart]
+constexpr int kOffBar = kOffB + STAGES * NPARTS * kBPart;  // mbarriers (8 B each)
+constexpr int kNumBars = 3 * STAGES + 2 + 1;
+constexpr int kOffMisc = kOffBar + kNumBars * 8;           // tmem base, abort flag
+constexpr int kSmemBytes = kOffMisc + 16 + 1024;           // + alignment slack
+static_assert(kSmemBytes <= 227 * 1024, "shared memory plan exceeds 227 KB");
 
 // ---------------------------------------------------------------- PTX
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -205,6 +213,7 @@ struct TcArgs {
   const float* colscale;
   const int64_t* cs_off;   // per problem
   const float* data;
+  const float* rowmax;  // per data row: max |value| (from the producer kernel)
   float* out;
   int64_t R;
   unsigned* err;
@@ -216,24 +225,9 @@ struct Pipe {
   uint64_t* empty;
   uint64_t* acc_full;
   uint64_t* acc_empty;
-  uint64_t* rs_free;  // [4]
-  uint64_t* rs_full;  // [4]
   uint64_t* done;
   volatile int* abort;
 };
-
-// Named-barrier reduction: every thread of the group gets the OR of `v`
-// (bar.red also orders shared memory like bar.sync).
-__device__ __forceinline__ bool group_any(bool v, int id, int count) {
-  uint32_t out;
-  asm volatile(
-      "{\n\t.reg .pred pi, po;\n\tsetp.ne.u32 pi, %1, 0;\n\t"
-      "bar.red.or.pred po, %2, %3, pi;\n\tselp.u32 %0, 1, 0, po;\n\t}"
-      : "=r"(out)
-      : "r"((uint32_t)v), "r"(id), "r"(count)
-      : "memory");
-  return out != 0;
-}
 
 // Bounded wait: returns false (and raises the abort flag) when the clock
 // budget runs out or another role has aborted.
@@ -257,13 +251,11 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(TcArgs a) {
   unsigned char* smem = smem_raw + ((1024 - (smem_u32(smem_raw) & 1023)) & 1023);
   unsigned char* sA = smem + kOffA;
   unsigned char* sB = smem + kOffB;
-  float* rowscale = reinterpret_cast<float*>(smem + kOffRS);
-  float* red = reinterpret_cast<float*>(smem + kOffRed);
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem + kOffBar);
   uint32_t* tmem_base_smem = reinterpret_cast<uint32_t*>(smem + kOffMisc);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(smem + kOffMisc + 4);
-  Pipe pp{bars, bars + STAGES, bars + 2 * STAGES, bars + 3 * STAGES, bars + 3 * STAGES + 2,
-          bars + 3 * STAGES + 4, bars + 3 * STAGES + 8, bars + 3 * STAGES + 12, abort_flag};
+  Pipe pp{bars, bars + STAGES, bars + 2 * STAGES, bars + 3 * STAGES, bars + 3 * STAGES + 1,
+          bars + 3 * STAGES + 2, abort_flag};
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (threadIdx.x == 0) {
@@ -272,14 +264,8 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(TcArgs a) {
       mbar_init(&pp.full_b[s], 1);
       mbar_init(&pp.empty[s], 1);
     }
-    for (int b = 0; b < 2; ++b) {
-      mbar_init(&pp.acc_full[b], 1);
-      mbar_init(&pp.acc_empty[b], 128);
-    }
-    for (int b = 0; b < 4; ++b) {
-      mbar_init(&pp.rs_free[b], 128);
-      mbar_init(&pp.rs_full[b], 128);
-    }
+    mbar_init(pp.acc_full, 1);
+    mbar_init(pp.acc_empty, 128);
     mbar_init(pp.done, 1);
     *abort_flag = 0;
     fence_barrier_init();
@@ -304,7 +290,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(TcArgs a) {
       for (int s = 0; s < STAGES; ++s) armed[s] = -1;
       for (int t = blockIdx.x; t < a.n_tiles && !*abort_flag; t += gridDim.x) {
         const ShtTcTile tl = a.tiles[t];
-        const int half = tl.nsize * BK * 2;
+        const int part = tl.nsize * BK * 2;  // bytes of one FP16 part of one stage
         const unsigned char* src = a.img + a.img_off[tl.img];
         bool ok = true;
         for (int ks = 0; ks < tl.kst; ++ks) {
@@ -312,10 +298,12 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(TcArgs a) {
             ok = false;
             break;
           }
-          mbar_arrive_expect_tx(&pp.full_b[stage], 2 * half);
-          unsigned char* dst = sB + stage * 2 * kBStage;
-          bulk_g2s(dst, src + (int64_t)ks * 2 * half, half, &pp.full_b[stage]);
-          bulk_g2s(dst + kBStage, src + (int64_t)ks * 2 * half + half, half, &pp.full_b[stage]);
+          mbar_arrive_expect_tx(&pp.full_b[stage], NPARTS * part);
+          unsigned char* dst = sB + stage * NPARTS * kBPart;
+#pragma unroll
+          for (int pt = 0; pt < NPARTS; ++pt)
+            bulk_g2s(dst + pt * kBPart, src + ((int64_t)ks * NPARTS + pt) * part, part,
+                     &pp.full_b[stage]);
           armed[stage] = (int)phase;
           if (++stage == STAGES) { stage = 0; phase ^= 1; }
         }
@@ -336,15 +324,15 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(TcArgs a) {
     if (lane == 0) {
       int stage = 0;
       uint32_t phase = 0;
-      int acc = 0;
       uint32_t acc_phase = 0;
       bool issued = false;
+      const uint32_t d_main = tmem_base;           // columns [0, 256)
+      const uint32_t d_corr = tmem_base + NMAX;    // columns [256, 512)
       for (int t = blockIdx.x; t < a.n_tiles && !*abort_flag; t += gridDim.x) {
         const ShtTcTile tl = a.tiles[t];
         if (tl.kst == 0) continue;
-        if (!wait_bar(&pp.acc_empty[acc], acc_phase ^ 1, pp, a.err, 2)) break;
+        if (!wait_bar(pp.acc_empty, acc_phase ^ 1, pp, a.err, 2)) break;
         tc_fence_after();
-        const uint32_t d_tmem = tmem_base + (uint32_t)(acc * NMAX);
         const uint32_t idesc = instr_desc(tl.nsize);
         const uint32_t lbo_b = (uint32_t)tl.nsize * 16;
         bool ok = true;
@@ -355,29 +343,27 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(TcArgs a) {
             break;
           }
           tc_fence_after();
-          const uint32_t a_hi = smem_u32(sA + stage * 2 * kAStage);
-          const uint32_t a_lo = a_hi + kAStage;
-          const uint32_t b_hi = smem_u32(sB + stage * 2 * kBStage);
-          const uint32_t b_lo = b_hi + kBStage;
+          const uint32_t a0 = smem_u32(sA + stage * NPARTS * kAPart);
+          const uint32_t b0 = smem_u32(sB + stage * NPARTS * kBPart);
 #pragma unroll
           for (int j = 0; j < BK / 16; ++j) {
             // one K step of 16 = two K groups of 8
-            const uint64_t dah = smem_desc(a_hi + j * 2 * 2048, 2048, 128);
-            const uint64_t dal = smem_desc(a_lo + j * 2 * 2048, 2048, 128);
-            const uint64_t dbh = smem_desc(b_hi + j * 2 * lbo_b, lbo_b, 128);
-            const uint64_t dbl = smem_desc(b_lo + j * 2 * lbo_b, lbo_b, 128);
+            const uint64_t da1 = smem_desc(a0 + j * 2 * kALbo, kALbo, 128);
+            const uint64_t da2 = smem_desc(a0 + kAPart + j * 2 * kALbo, kALbo, 128);
+            const uint64_t db1 = smem_desc(b0 + j * 2 * lbo_b, lbo_b, 128);
+            const uint64_t db2 = smem_desc(b0 + kBPart + j * 2 * lbo_b, lbo_b, 128);
             const uint32_t accum = (ks > 0 || j > 0) ? 1u : 0u;
-            mma_f16(d_tmem, dah, dbh, idesc, accum);
-            mma_f16(d_tmem, dah, dbl, idesc, 1u);
-            mma_f16(d_tmem, dal, dbh, idesc, 1u);
+            mma_f16(d_main, da1, db1, idesc, accum);  // a1 b1
+            mma_f16(d_corr, da1, db2, idesc, accum);  // a1 b2
+            mma_f16(d_corr, da2, db1, idesc, 1u);     // a2 b1
           }
           issued = true;
           mma_commit(&pp.empty[stage]);  // frees the stage when these MMAs finish
           if (++stage == STAGES) { stage = 0; phase ^= 1; }
         }
         if (!ok) break;
-        mma_commit(&pp.acc_full[acc]);
-        if (++acc == 2) { acc = 0; acc_phase ^= 1; }
+        mma_commit(pp.acc_full);
+        acc_phase ^= 1;
       }
       if (issued) {
         // All issued MMAs complete before TMEM is released.
@@ -391,13 +377,9 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(TcArgs a) {
     // ----------------------------------------------------------- epilogue
     const int eg = warp & 3;  // TMEM lane group accessible to this warp
     const int row = eg * 32 + lane;
-    const int et = threadIdx.x - kEpiWarp0 * 32;  // 0..127
-    int acc = 0;
     uint32_t acc_phase = 0;
-    int ti = 0;  // non-empty tiles seen (row-scale slot = ti & 3)
-    // Decisions that gate tcgen05.ld.sync.aligned and the named barriers are
-    // made by one elected thread and shared with group_any, so the 128
-    // epilogue threads always take the same path.
+    // The wait outcome is made warp-uniform (__any_sync) before the
+    // warp-collective tcgen05.ld.
     for (int t = blockIdx.x; t < a.n_tiles; t += gridDim.x) {
       const ShtTcTile tl = a.tiles[t];
       const ShtGemmDesc d = a.descs[tl.problem];
@@ -409,131 +391,95 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(TcArgs a) {
           for (int x = tl.n0; x < min(tl.n0 + tl.nsize, d.X); ++x) outb[(int64_t)x * R + r] = 0.f;
         continue;
       }
-      bool failed = false;
-      if (et == 0)
-        failed = !wait_bar(&pp.acc_full[acc], acc_phase, pp, a.err, 5) ||
-                 !wait_bar(&pp.rs_full[ti & 3], (ti >> 2) & 1, pp, a.err, 8);
-      if (group_any(failed, 2, 128)) break;
+      const bool failed = !wait_bar(pp.acc_full, acc_phase, pp, a.err, 5);
+      if (__any_sync(0xffffffffu, failed)) break;
       tc_fence_after();
-      const float rs = rowscale[(ti & 3) * BM + row];
-      mbar_arrive(&pp.rs_free[ti & 3]);
+      const float rs = r < R ? 1.f / pow2_scale(a.rowmax[r]) : 0.f;
       const float* cs = a.colscale + a.cs_off[tl.problem];
-      const uint32_t taddr = tmem_base + ((uint32_t)(eg * 32) << 16) + (uint32_t)(acc * NMAX);
+      const uint32_t lane_off = (uint32_t)(eg * 32) << 16;
       for (int c0 = 0; c0 < tl.nsize; c0 += 16) {
-        float v[16];
-        tmem_ld16(taddr + (uint32_t)c0, v);
+        float vm[16], vc[16];
+        tmem_ld16(tmem_base + lane_off + (uint32_t)c0, vm);
+        tmem_ld16(tmem_base + lane_off + (uint32_t)(NMAX + c0), vc);
         if (r < R) {
 #pragma unroll
           for (int i = 0; i < 16; ++i) {
             const int x = tl.n0 + c0 + i;
-            if (x < d.X) outb[(int64_t)x * R + r] = v[i] * rs * cs[x];
+            if (x < d.X) outb[(int64_t)x * R + r] = (vm[i] + vc[i]) * rs * cs[x];
           }
         }
       }
       tc_fence_before();
-      mbar_arrive(&pp.acc_empty[acc]);
-      if (++acc == 2) { acc = 0; acc_phase ^= 1; }
-      ++ti;
+      mbar_arrive(pp.acc_empty);
+      acc_phase ^= 1;
     }
   } else {
     // --------------------------------------------------------- converters
+    // Thread -> (kk = ct % 8, 8-row group mg = (ct/8) % 16), K groups
+    // kg = ct/128 + 2j (j < BK/16): each store is one 16-byte core-matrix row,
+    // and a warp's 32 stores cover 512 contiguous bytes (no bank conflicts).
     const int ct = threadIdx.x - kConvWarp0 * 32;  // 0..255
+    const int kk = ct & 7, mg = (ct >> 3) & 15, kgs = ct >> 7;
     int stage = 0;
     uint32_t phase = 0;
-    int ti = 0;  // non-empty tiles seen (row-scale slot = ti & 3)
     for (int t = blockIdx.x; t < a.n_tiles; t += gridDim.x) {
       const ShtTcTile tl = a.tiles[t];
       if (tl.kst == 0) continue;
       const ShtGemmDesc d = a.descs[tl.problem];
       const float* Db = a.data + d.d_row * R;
-      // Row-scale slot ti & 3 must be free (its epilogue has read it).  One
-      // elected thread waits; the group-wide reduction is also the barrier
-      // that keeps this tile's writes of red[] behind every converter's read
-      // of the previous tile's scales.
-      bool failed = false;
-      if (ct == 0) failed = !wait_bar(&pp.rs_free[ti & 3], ((ti >> 2) & 1) ^ 1, pp, a.err, 6);
-      if (group_any(failed, 1, kConvThreads)) break;
-      {
-        const int rq = (ct & 31) * 4;
-        const int kg = ct >> 5;
-        float mx[4] = {0.f, 0.f, 0.f, 0.f};
-        const int64_t rr = tl.r0 + rq;
-        for (int k = kg; k < d.K; k += 8) {
-          const float* p = Db + (int64_t)k * R + rr;
-#pragma unroll
-          for (int i = 0; i < 4; ++i)
-            if (rr + i < R) mx[i] = fmaxf(mx[i], fabsf(__ldg(p + i)));
-        }
-#pragma unroll
-        for (int i = 0; i < 4; ++i) red[kg * BM + rq + i] = mx[i];
-        asm volatile("bar.sync 1, %0;" ::"n"(kConvThreads));
-        if (ct < BM) {
-          float m = 0.f;
-#pragma unroll
-          for (int g = 0; g < 8; ++g) m = fmaxf(m, red[g * BM + ct]);
-          const float s = pow2_scale(m);
-          rowscale[(ti & 3) * BM + ct] = 1.f / s;  // the epilogue multiplies by 1/s_r
-          red[ct] = s;                             // the converters multiply by s_r
-          mbar_arrive(&pp.rs_full[ti & 3]);        // publishes the slot to the epilogue
-        }
-        asm volatile("bar.sync 1, %0;" ::"n"(kConvThreads));
-      }
-      // Pass 2: convert K stages. Thread: (kk = ct % 8, 8-row group mg = (ct/8) % 16),
-      // K groups kg = ct/128 + 2j.
-      const int kk = ct & 7, mg = (ct >> 3) & 15, kgs = ct >> 7;
+      const int64_t rbase = tl.r0 + mg * 8;
       float sc[8];
 #pragma unroll
-      for (int i = 0; i < 8; ++i) sc[i] = red[mg * 8 + i];
-      const int64_t rbase = tl.r0 + mg * 8;
+      for (int i = 0; i < 8; ++i) sc[i] = rbase + i < R ? pow2_scale(a.rowmax[rbase + i]) : 1.f;
       const bool full_rows = rbase + 8 <= R && (R % 4) == 0;
       bool ok = true;
       for (int ks = 0; ks < tl.kst; ++ks) {
-        bool f = false;
-        if (ct == 0) f = !wait_bar(&pp.empty[stage], phase ^ 1, pp, a.err, 7);
-        if (group_any(f, 1, kConvThreads)) {
-          ok = false;
-          break;
-        }
-        unsigned char* dhi = sA + stage * 2 * kAStage;
-        unsigned char* dlo = dhi + kAStage;
+        // Loads first (independent of the stage being free), then wait.
+        float v[BK / 16][8];
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
-          const int kg = kgs + 2 * j;
-          const int k = ks * BK + kg * 8 + kk;
-          float v[8];
+        for (int j = 0; j < BK / 16; ++j) {
+          const int k = ks * BK + (kgs + 2 * j) * 8 + kk;
           if (k < d.K) {
             const float* p = Db + (int64_t)k * R + rbase;
             if (full_rows) {
               const float4 u0 = __ldg(reinterpret_cast<const float4*>(p));
               const float4 u1 = __ldg(reinterpret_cast<const float4*>(p + 4));
-              v[0] = u0.x; v[1] = u0.y; v[2] = u0.z; v[3] = u0.w;
-              v[4] = u1.x; v[5] = u1.y; v[6] = u1.z; v[7] = u1.w;
+              v[j][0] = u0.x; v[j][1] = u0.y; v[j][2] = u0.z; v[j][3] = u0.w;
+              v[j][4] = u1.x; v[j][5] = u1.y; v[j][6] = u1.z; v[j][7] = u1.w;
             } else {
 #pragma unroll
-              for (int i = 0; i < 8; ++i) v[i] = (rbase + i < R) ? __ldg(p + i) : 0.f;
+              for (int i = 0; i < 8; ++i) v[j][i] = (rbase + i < R) ? __ldg(p + i) : 0.f;
             }
           } else {
 #pragma unroll
-            for (int i = 0; i < 8; ++i) v[i] = 0.f;
+            for (int i = 0; i < 8; ++i) v[j][i] = 0.f;
           }
-          __align__(16) __half hi[8];
-          __align__(16) __half lo[8];
+        }
+        if (!wait_bar(&pp.empty[stage], phase ^ 1, pp, a.err, 7)) {
+          ok = false;
+          break;
+        }
+        unsigned char* dst = sA + stage * NPARTS * kAPart;
+#pragma unroll
+        for (int j = 0; j < BK / 16; ++j) {
+          const int kg = kgs + 2 * j;
+          __align__(16) __half h1[8];
+          __align__(16) __half h2[8];
 #pragma unroll
           for (int i = 0; i < 8; ++i) {
-            const float x = v[i] * sc[i];
-            hi[i] = __float2half_rn(x);
-            lo[i] = __float2half_rn(x - __half2float(hi[i]));
+            const float x = v[j][i] * sc[i];
+            h1[i] = __float2half_rn(x);
+            h2[i] = __float2half_rn(x - __half2float(h1[i]));
           }
-          const int off = kg * 2048 + mg * 128 + kk * 16;
-          *reinterpret_cast<uint4*>(dhi + off) = *reinterpret_cast<const uint4*>(hi);
-          *reinterpret_cast<uint4*>(dlo + off) = *reinterpret_cast<const uint4*>(lo);
+          const int off = kg * kALbo + mg * 128 + kk * 16;
+          *reinterpret_cast<uint4*>(dst + off) = *reinterpret_cast<const uint4*>(h1);
+          *reinterpret_cast<uint4*>(dst + kAPart + off) = *reinterpret_cast<const uint4*>(h2);
         }
         fence_proxy_async();
         mbar_arrive(&pp.full_a[stage]);
         if (++stage == STAGES) { stage = 0; phase ^= 1; }
       }
       if (!ok) break;
-      ++ti;
     }
   }
 
@@ -582,19 +528,20 @@ struct BlockInfo {
 };
 
 // One thread per image element of one (problem, n-tile) block; the image is
-// [k-stage][hi|lo][kg 8][ng nsize/8][kk 8][nn 8] halves.
+// [k-stage][part 2][kg BK/8][ng nsize/8][kk 8][nn 8] halves, the parts being
+// the two FP16 terms (hi, lo) of the scaled FP64 value.
 __global__ void image_kernel(ImgArgs a, const BlockInfo* blocks, int nblocks, unsigned char* img) {
   const int b = blockIdx.y;
   if (b >= nblocks) return;
   const BlockInfo bi = blocks[b];
   const ShtGemmDesc d = a.descs[bi.problem];
-  const int64_t per_stage = (int64_t)bi.nsize * BK;  // halves per half-image
-  const int64_t total = per_stage * bi.kst;
+  const int64_t per_part = (int64_t)bi.nsize * BK;  // halves per part per stage
+  const int64_t total = per_part * bi.kst;
   __half* base = reinterpret_cast<__half*>(img + bi.off);
   for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total;
        e += (int64_t)gridDim.x * blockDim.x) {
-    const int ks = (int)(e / per_stage);
-    int rem = (int)(e % per_stage);
+    const int ks = (int)(e / per_part);
+    int rem = (int)(e % per_part);
     const int nn = rem & 7;
     rem >>= 3;
     const int kk = rem & 7;
@@ -603,16 +550,16 @@ __global__ void image_kernel(ImgArgs a, const BlockInfo* blocks, int nblocks, un
     const int kg = rem / (bi.nsize / 8);
     const int x = bi.n0 + ng * 8 + nn;
     const int k = ks * BK + kg * 8 + kk;
-    float hi = 0.f, lo = 0.f;
+    __half p1 = __float2half_rn(0.f), p2 = p1;
     if (x < d.X && k < d.K) {
       const double v = a.tab[d.t_off + (int64_t)k * d.ldt + x] * (double)a.colmul[a.cs_off[bi.problem] + x];
-      const __half h = __float2half_rn((float)v);
-      hi = __half2float(h);
-      lo = (float)(v - (double)hi);
+      p1 = __float2half_rn((float)v);
+      p2 = __float2half_rn((float)(v - (double)__half2float(p1)));
     }
     const int64_t pos = ((int64_t)(kg * (bi.nsize / 8) + ng) * 8 + kk) * 8 + nn;
-    base[(int64_t)ks * 2 * per_stage + pos] = __float2half_rn(hi);
-    base[(int64_t)ks * 2 * per_stage + per_stage + pos] = __float2half_rn(lo);
+    __half* st = base + (int64_t)ks * NPARTS * per_part;
+    st[pos] = p1;
+    st[per_part + pos] = p2;
   }
 }
 
@@ -677,7 +624,7 @@ void build_tc_tables(sht_plan* p, const double* basis64, const double* dbasis64,
         for (int j = 0; j < nt; ++j) {
           tc->img_off[dir].push_back(off);
           if (d.X > 0 && kst > 0) blocks[dir].push_back({i, j * ns, ns, kst, off});
-          off += (int64_t)kst * 2 * ns * BK * 2;
+          off += (int64_t)kst * NPARTS * ns * BK * 2;
         }
       }
       tc->img_bytes[dir] = off;
@@ -748,7 +695,7 @@ void destroy_tc_tables(sht_plan* p) {
 }
 
 void launch_gemm_tc(const sht_plan* p, int direction, int flip, int table_kind, const float* data,
-                    float* out, int64_t R, cudaStream_t s) {
+                    const float* rowmax, float* out, int64_t R, cudaStream_t s) {
   ShtTc16* tc = p->tc;
   SHT_REQUIRE(tc != nullptr, "tensor-core tables not built");
   if (R == 0) return;
@@ -788,6 +735,7 @@ void launch_gemm_tc(const sht_plan* p, int direction, int flip, int table_kind, 
   a.colscale = tc->colscale[table_kind];
   a.cs_off = tc->d_cs_off[dir];
   a.data = data;
+  a.rowmax = rowmax;
   a.out = out;
   a.R = R;
   a.err = p->d_err;

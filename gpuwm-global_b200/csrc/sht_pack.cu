@@ -28,8 +28,9 @@ __device__ __forceinline__ int64_t cf_row(int T, int m, int q, int i) {
 template <typename T>
 __global__ void pack_kernel(int Tn, double radius, int mode, const V2<T>* __restrict__ c0,
                             const V2<T>* __restrict__ c1, int64_t planes, int F,
-                            V2<T>* __restrict__ cf) {
+                            V2<T>* __restrict__ cf, float* __restrict__ rowmax) {
   __shared__ V2<T> tile[32][33];
+  __shared__ float red[2][8][32];
   const int m0 = blockIdx.x * 32;
   const int n = blockIdx.y;
   if (m0 > n) return;
@@ -48,6 +49,7 @@ __global__ void pack_kernel(int Tn, double radius, int mode, const V2<T>* __rest
   }
   __syncthreads();
   const int64_t Rc = planes * F;
+  float mre = 0.f, mim = 0.f;
   for (int mm = ty; mm < 32; mm += 8) {
     int m = m0 + mm;
     if (m > n) break;
@@ -62,6 +64,24 @@ __global__ void pack_kernel(int Tn, double radius, int mode, const V2<T>* __rest
         if (m == 0) v.y = T(0);  // project() inside inverse_laplacian
       }
       cf[row * Rc + p * F + f] = v;
+      mre = fmaxf(mre, (float)fabs(v.x));
+      mim = fmaxf(mim, (float)fabs(v.y));
+    }
+  }
+  if (rowmax != nullptr) {
+    // Row maxima of this CTA's 32 columns: reduce the 8 ty groups, publish once.
+    red[0][ty][tx] = mre;
+    red[1][ty][tx] = mim;
+    __syncthreads();
+    if (ty == 0 && p0 + tx < planes) {
+      float a = 0.f, b = 0.f;
+      for (int k = 0; k < 8; ++k) {
+        a = fmaxf(a, red[0][k][tx]);
+        b = fmaxf(b, red[1][k][tx]);
+      }
+      const int64_t col = (p0 + tx) * F + f;
+      atomicMax(reinterpret_cast<int*>(rowmax + 2 * col), __float_as_int(a));
+      atomicMax(reinterpret_cast<int*>(rowmax + 2 * col + 1), __float_as_int(b));
     }
   }
 }
@@ -147,13 +167,14 @@ __global__ void elementwise_kernel(int Tn, double radius, int mode, const V2<T>*
 
 template <typename T>
 void launch_pack(const sht_plan* p, const T* coeff0, const T* coeff1, int64_t planes, int mode,
-                 T* cfold, cudaStream_t s) {
+                 T* cfold, cudaStream_t s, float* rowmax) {
   if (planes == 0) return;
   int F = coeff1 ? 2 : 1;
   dim3 grid((unsigned)div_up(p->T + 1, 32), (unsigned)(p->T + 1), (unsigned)(div_up(planes, 32) * F));
   SHT_REQUIRE(grid.z <= 65535, "too many planes for one pack launch");
   pack_kernel<T><<<grid, dim3(32, 8), 0, s>>>(p->T, p->radius, mode, (const V2<T>*)coeff0,
-                                              (const V2<T>*)coeff1, planes, F, (V2<T>*)cfold);
+                                              (const V2<T>*)coeff1, planes, F, (V2<T>*)cfold,
+                                              rowmax);
   SHT_CUDA_OR_THROW(cudaGetLastError());
 }
 
@@ -181,7 +202,7 @@ void launch_elementwise(const sht_plan* p, int mode, const T* in, int64_t planes
 
 #define INST(T)                                                                                  \
   template void launch_pack<T>(const sht_plan*, const T*, const T*, int64_t, int, T*,          \
-                               cudaStream_t);                                                   \
+                               cudaStream_t, float*);                                           \
   template void launch_unpack<T>(const sht_plan*, int, const T*, const T*, int64_t, T*, T*,    \
                                  cudaStream_t);                                                 \
   template void launch_elementwise<T>(const sht_plan*, int, const T*, int64_t, T*, cudaStream_t);

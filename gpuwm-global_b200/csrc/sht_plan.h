@@ -74,6 +74,7 @@ struct sht_plan {
   // Scratch (grown on demand): two waists and two Cfold buffers.
   void* wfold[2] = {nullptr, nullptr};
   void* cfold[2] = {nullptr, nullptr};
+  float* rowmax = nullptr;   // per data row max |value| (split-precision row scales)
   int64_t scratch_rows = 0;  // R capacity (rows = 2 * planes * fields)
 
   unsigned* d_err = nullptr;
@@ -103,9 +104,12 @@ void build_geometry_and_tables(sht_plan* p, cudaStream_t s);
 
 // FFT (sht_fft.cu).
 void build_fft(sht_plan* p, cudaStream_t s);
+// rowmax (optional): per data row r (plane/field/re-im), the running maximum
+// of |value| over everything the kernel writes, merged with atomicMax on the
+// float bits (the row scales of the split-precision contraction).
 template <typename T>
 void launch_forward_fold(const sht_plan* p, const T* g0, const T* g1, int64_t planes,
-                         T* wfold, cudaStream_t s);
+                         T* wfold, cudaStream_t s, float* rowmax = nullptr);
 // Inverse modes.
 enum UnfoldMode { kUnfoldScalar = 0, kUnfoldZonal = 1, kUnfoldGradient = 2, kUnfoldWind = 3,
                   kUnfoldMeridional = 4 };
@@ -118,7 +122,7 @@ void launch_inverse_unfold(const sht_plan* p, int mode, const T* wP, const T* wD
 bool fast_fft_supported(const sht_plan* p);
 void fast_fft_init_constants(cudaStream_t s);
 void fast_forward_fold(const sht_plan* p, const float* g0, const float* g1, int64_t planes,
-                       float* wfold, cudaStream_t s);
+                       float* wfold, cudaStream_t s, float* rowmax = nullptr);
 void fast_inverse_unfold(const sht_plan* p, int mode, const float* wP, const float* wD,
                          int64_t planes, float* out0, float* out1, cudaStream_t s);
 
@@ -132,7 +136,22 @@ void launch_gemm_simt(const sht_plan* p, int direction, int flip, const T* table
 enum PackMode { kPackPlain = 0, kPackInvLap = 1 };
 template <typename T>
 void launch_pack(const sht_plan* p, const T* coeff0, const T* coeff1, int64_t planes,
-                 int mode, T* cfold, cudaStream_t s);
+                 int mode, T* cfold, cudaStream_t s, float* rowmax = nullptr);
+
+// Warp-level merge of per-thread row maxima: lanes with equal lane % nper
+// hold the same column (complex index col); lanes < nper publish.
+__device__ __forceinline__ void rowmax_merge(float* rowmax, int64_t col, bool valid, float mre,
+                                             float mim, int nper) {
+  const int lane = threadIdx.x & 31;
+  for (int off = nper; off < 32; off <<= 1) {
+    mre = fmaxf(mre, __shfl_xor_sync(0xffffffffu, mre, off));
+    mim = fmaxf(mim, __shfl_xor_sync(0xffffffffu, mim, off));
+  }
+  if (lane < nper && valid) {
+    atomicMax(reinterpret_cast<int*>(rowmax + 2 * col), __float_as_int(mre));
+    atomicMax(reinterpret_cast<int*>(rowmax + 2 * col + 1), __float_as_int(mim));
+  }
+}
 enum UnpackMode { kUnpackScalar = 0, kUnpackVorDiv = 1 };
 template <typename T>
 void launch_unpack(const sht_plan* p, int mode, const T* cf0, const T* cf1, int64_t planes,
@@ -154,6 +173,7 @@ void build_tc_tables(sht_plan* p, const double* basis64, const double* dbasis64,
                      cudaStream_t s);
 void destroy_tc_tables(sht_plan* p);
 void launch_gemm_tc(const sht_plan* p, int direction, int flip, int table_kind,
-                    const float* data, float* out, int64_t R, cudaStream_t s);
+                    const float* data, const float* rowmax, float* out, int64_t R,
+                    cudaStream_t s);
 
 }  // namespace sht
