@@ -43,6 +43,7 @@ SIGNATURES = {
     "sht_plan_read_timing": (ctypes.c_int, [_P, _DP, ctypes.POINTER(_I64), ctypes.POINTER(_I64),
                                             ctypes.c_int, ctypes.c_int]),
     "sht_forward": (ctypes.c_int, [_P, _P, _I64, _P, _P]),
+    "sht_forward_static_scratch": (ctypes.c_int, [_P, _P, _I64, _P, _P]),
     "sht_inverse": (ctypes.c_int, [_P, _P, _I64, _P, _P]),
     "sht_inverse_meridional_derivative": (ctypes.c_int, [_P, _P, _I64, _P, _P]),
     "sht_inverse_zonal_derivative": (ctypes.c_int, [_P, _P, _I64, _P, _P]),

@@ -106,6 +106,23 @@ int sht_plan_read_timing(sht_plan* plan, double* ms, int64_t* launches, int64_t*
 /* grid -> spectral.  SphericalHarmonicTransform.forward (transform.py:1486). */
 int sht_forward(sht_plan* plan, const void* grid, int64_t planes, void* coeff, void* stream);
 
+/* Size of the device buffer compiled into the library for
+ * sht_forward_static_scratch (32 MiB, held on every GPU that loads it). */
+#define SHT_STATIC_SCRATCH_BYTES (32u << 20)
+
+/* grid -> spectral, like sht_forward, for callers that cannot allocate device
+ * memory when they transform (a host callback, an allocator hook, a process
+ * whose device budget belongs to an external memory manager).  It has no
+ * counterpart in the reference.  Its scratch is the fixed
+ * SHT_STATIC_SCRATCH_BYTES buffer above instead of the plan's on-demand
+ * scratch, and it allocates nothing; a call that needs more (too many
+ * planes) is rejected with SHT_ERR_ARG and the per-call plane limit in the
+ * message.  FP32 and FP64 plans only.  The first call on a device looks the
+ * buffer's address up (make it before any stream capture); every call shares
+ * the buffer, so calls that overlap on the GPU race on it. */
+int sht_forward_static_scratch(sht_plan* plan, const void* grid, int64_t planes, void* coeff,
+                               void* stream);
+
 /* spectral -> grid.  SphericalHarmonicTransform.inverse (transform.py:1742). */
 int sht_inverse(sht_plan* plan, const void* coeff, int64_t planes, void* grid, void* stream);
 
