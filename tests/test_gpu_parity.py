@@ -259,9 +259,12 @@ def test_fp32_and_split_against_fp64_at_config_grids(t, nlat, nlon, df):
     kw = dict(nlat=nlat, nlon=nlon, dealias_factor=df)
     # The reference's own float32 vector analysis loses digits to the
     # i m rot + shear cancellation (1.9e-6 at T62 to 1.2e-5 at T511): the
-    # vorticity/divergence bar is 1.5x the reference float32 error.
+    # vorticity/divergence bar is 1.5x the reference float32 error for the
+    # FP32 path and 2x for the split path (whose two FP16 terms per operand
+    # carry 22 bits, one fewer than FP32).
     ref_err = json.loads((GOLDEN / "reference_fp32_errors.json").read_text())[str(t)]
-    vordiv_tol = max(2e-6, 1.5 * ref_err["vordiv"])
+    vordiv_tol = {"float32": max(2e-6, 1.5 * ref_err["vordiv"]),
+                  "split16": max(2e-6, 2.0 * ref_err["vordiv"])}
     coeff = red_spectrum(t, 3)
     f64 = SphericalHarmonicTransform.create(t, precision="float64", **kw)
     vec64 = VorticityDivergenceOperator(f64)
@@ -275,15 +278,21 @@ def test_fp32_and_split_against_fp64_at_config_grids(t, nlat, nlon, df):
         for flags in (0, SHT_FLAG_GENERIC_FFT):
             sht = SphericalHarmonicTransform.create(t, precision=precision, plan_flags=flags, **kw)
             vec = VorticityDivergenceOperator(sht)
+            tag = (precision, flags)
             g32 = g64.to(torch.float32)
-            assert rel_l2(np_(sht.forward(g32)), c64) < 2e-6, (precision, flags)
-            assert rel_max(np_(sht.inverse(coeff)), np_(g64)) < 2e-6, (precision, flags)
+            err = rel_l2(np_(sht.forward(g32)), c64)
+            assert err < 2e-6, (tag, "forward", err)
+            err = rel_max(np_(sht.inverse(coeff)), np_(g64))
+            assert err < 2e-6, (tag, "inverse", err)
             e, n = sht.gradient(coeff)
-            assert rel_max(np_(e), e64) < 2e-6 and rel_max(np_(n), n64) < 2e-6
+            err = max(rel_max(np_(e), e64), rel_max(np_(n), n64))
+            assert err < 2e-6, (tag, "gradient", err)
             u, v = vec.wind_from_vordiv(coeff, coeff[::-1].copy())
-            assert rel_max(np_(u), u64) < 2e-6 and rel_max(np_(v), v64) < 2e-6
+            err = max(rel_max(np_(u), u64), rel_max(np_(v), v64))
+            assert err < 2e-6, (tag, "wind", err)
             z, d = vec.vordiv_from_wind(u64, v64)
-            assert rel_l2(np_(z), z64) < vordiv_tol and rel_l2(np_(d), d64) < vordiv_tol
+            err = max(rel_l2(np_(z), z64), rel_l2(np_(d), d64))
+            assert err < vordiv_tol[precision], (tag, "vordiv", err)
             sht.check_device()
 
 
