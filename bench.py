@@ -51,6 +51,12 @@ def parse():
     ap.add_argument("--profile-only", action="store_true",
                     help="one plan, warmup + steps of the pair, no checks (small ncu case)")
     ap.add_argument("--precision", default="split16", choices=["split16", "float32", "float64"])
+    ap.add_argument("--workload", default="pair", choices=["pair", "ensemble", "step"],
+                    help="pair: the T511 L40 transform pair (default); ensemble: 32 members "
+                         "at T126 + the T255 control as one batch; step: the full T511 "
+                         "dycore-step transform set as one CUDA graph, with the "
+                         "Rossby-Haurwitz wave's energy drift over --drift-steps steps")
+    ap.add_argument("--drift-steps", type=int, default=100)
     return ap.parse_args()
 
 
@@ -204,6 +210,11 @@ def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+        return
+    if args.workload != "pair":
+        from b200sht.workloads import run_workload
+
+        print(json.dumps(run_workload(args, ClockSampler)), flush=True)
         return
     import torch
     import torch.distributed as dist

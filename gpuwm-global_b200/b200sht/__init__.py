@@ -10,6 +10,8 @@ from .grid import GaussianGrid, shape_for
 from .transform import SphericalHarmonicTransform
 from .vector import VorticityDivergenceOperator
 from .semi_implicit import SpectralState, VerticalModeOperator, VerticalModeSemiImplicit
+from .batch import TransformBatch
+from .step import DycoreTransformStep
 
 __all__ = [
     "GaussianGrid",
@@ -19,4 +21,6 @@ __all__ = [
     "SpectralState",
     "VerticalModeOperator",
     "VerticalModeSemiImplicit",
+    "TransformBatch",
+    "DycoreTransformStep",
 ]

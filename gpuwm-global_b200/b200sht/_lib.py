@@ -55,6 +55,15 @@ SIGNATURES = {
     "sht_inverse_laplacian": (ctypes.c_int, [_P, _P, _I64, _P, _P]),
     "sht_helmholtz_solve": (ctypes.c_int, [_P, ctypes.c_int, _DP, _DP, _DP, _DP, _DP, _D,
                                            _P, _P, _P, _P, _P, _P, _P]),
+    "sht_vertical_create": (ctypes.c_int, [_P, ctypes.c_int, _DP, _DP, _DP, _DP, _DP,
+                                           ctypes.POINTER(_P)]),
+    "sht_vertical_destroy": (ctypes.c_int, [_P]),
+    "sht_helmholtz_apply": (ctypes.c_int, [_P, _P, _D, _P, _P, _P, _P, _P, _P, _P]),
+    "sht_batch_create": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(_P), ctypes.POINTER(_I64),
+                                        ctypes.POINTER(_P)]),
+    "sht_batch_destroy": (ctypes.c_int, [_P]),
+    "sht_batch_forward": (ctypes.c_int, [_P, ctypes.POINTER(_P), ctypes.POINTER(_P), _P]),
+    "sht_batch_inverse": (ctypes.c_int, [_P, ctypes.POINTER(_P), ctypes.POINTER(_P), _P]),
 }
 
 _lib = None

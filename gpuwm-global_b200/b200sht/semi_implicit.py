@@ -17,6 +17,7 @@ import math
 from dataclasses import dataclass
 
 import numpy as np
+import torch
 
 from . import _lib
 from .transform import SphericalHarmonicTransform, _ptr, _stream
@@ -54,6 +55,43 @@ class VerticalModeOperator:
     def nlev(self) -> int:
         return int(self.b_matrix.shape[0])
 
+    def device_handle(self, transform: SphericalHarmonicTransform) -> "DeviceVerticalOperator":
+        """The operator uploaded for ``transform``'s device and precision
+        (created on first use and kept, like the reference's per-run
+        ``VerticalStructureOperator``)."""
+        key = (str(transform.backend.device), transform.precision)
+        cache = self.__dict__.setdefault("_device_handles", {})
+        if key not in cache:
+            cache[key] = DeviceVerticalOperator(transform, self)
+        return cache[key]
+
+
+class DeviceVerticalOperator:
+    """One ``sht_vertical`` handle: B, C and the modal basis resident on the
+    device, so that ``sht_helmholtz_apply`` copies and allocates nothing."""
+
+    def __init__(self, transform: SphericalHarmonicTransform, op: VerticalModeOperator):
+        self._lib = _lib.load()
+        dp = ctypes.POINTER(ctypes.c_double)
+        handle = ctypes.c_void_p()
+        with torch.cuda.device(transform.backend.device):
+            _lib.check(self._lib.sht_vertical_create(
+                transform.plan.handle, op.nlev, op.b_matrix.ctypes.data_as(dp),
+                op.c_matrix.ctypes.data_as(dp), op.eigenvectors.ctypes.data_as(dp),
+                op.eigenvectors_inv.ctypes.data_as(dp), op.eigenvalues.ctypes.data_as(dp),
+                ctypes.byref(handle)))
+        self.handle = handle
+        self.nlev = op.nlev
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h is not None and h.value:
+            try:
+                self._lib.sht_vertical_destroy(h)
+            except Exception:
+                pass
+            self.handle = None
+
 
 @dataclass
 class SpectralState:
@@ -89,15 +127,20 @@ class VerticalModeSemiImplicit:
         nlev = operator.nlev
         if d.shape[0] != nlev or th.shape[0] != nlev or d.dim() != 3 or th.dim() != 3 or lp.dim() != 2:
             raise ValueError("divergence/theta must be (nlev, T+1, T+1) and lnps (T+1, T+1)")
-        od, oth, olp = d.clone(), th.clone(), lp.clone()
-        dp = ctypes.POINTER(ctypes.c_double)
-        op = operator
-        _lib.call("sht_helmholtz_solve", t.plan.handle, nlev,
-                  op.b_matrix.ctypes.data_as(dp), op.c_matrix.ctypes.data_as(dp),
-                  op.eigenvectors.ctypes.data_as(dp), op.eigenvectors_inv.ctypes.data_as(dp),
-                  op.eigenvalues.ctypes.data_as(dp), float(tau_s) * self.divergence_weight,
-                  _ptr(d), _ptr(th), _ptr(lp), _ptr(od), _ptr(oth), _ptr(olp), _stream())
+        od, oth, olp = torch.empty_like(d), torch.empty_like(th), torch.empty_like(lp)
+        self.solve_into(t, operator, tau_s, d, th, lp, od, oth, olp)
         return od, oth, olp
+
+    def solve_into(self, transform, operator, tau_s, divergence, theta, lnps, out_divergence,
+                   out_theta, out_lnps) -> None:
+        """``solve_arrays`` on caller-owned device arrays (outputs may alias
+        inputs): one ``sht_helmholtz_apply`` with the operator kept on the
+        device, so no allocation, host copy or synchronisation happens here
+        once the operator has been uploaded."""
+        handle = operator.device_handle(transform)
+        _lib.call("sht_helmholtz_apply", transform.plan.handle, handle.handle,
+                  float(tau_s) * self.divergence_weight, _ptr(divergence), _ptr(theta),
+                  _ptr(lnps), _ptr(out_divergence), _ptr(out_theta), _ptr(out_lnps), _stream())
 
     def solve_shifted(self, state, transform, operator, tau_s):
         """The IMEX stage solve (semi_implicit.py:921-953); inactive: identity."""

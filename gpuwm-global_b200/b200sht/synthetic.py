@@ -48,3 +48,32 @@ def rossby_haurwitz_wind(mu: np.ndarray, nlon: int, *, omega=7.848e-6, k=7.848e-
     u = a * omega * c + a * k * c ** (r - 1) * (r * s * s - c * c) * np.cos(r * lon)
     v = -a * k * r * c ** (r - 1) * s * np.sin(r * lon)
     return u, v
+
+
+def seeded_vertical_operator(nlev: int = 40, seed: int = CONTROL_SEED):
+    """Seeded ``B`` (nlev x nlev+1) and ``C`` (nlev+1 x nlev) whose structure
+    matrix ``M = -B C`` is symmetric and strictly diagonally dominant with a
+    positive diagonal, so its modes are real and its eigenvalues positive.
+
+    The diagonal holds gravity-wave speeds squared from 340 m/s (deepest
+    mode) down to 8 m/s; each off-diagonal entry is a seeded fraction of the
+    geometric mean of its two diagonal entries, scaled so every row's
+    off-diagonal sum stays below half its diagonal.  ``C = [I; w^T]`` carries a
+    seeded surface-pressure row ``w`` and ``B = [-M - b w^T | b]`` a seeded
+    surface column ``b``, so ``-B C = M`` exactly.
+    """
+    rng = np.random.default_rng(seed + 40)
+    speeds = np.geomspace(340.0, 8.0, int(nlev))
+    diag = speeds ** 2
+    off = rng.uniform(-1.0, 1.0, (nlev, nlev))
+    off = 0.5 * (off + off.T)
+    np.fill_diagonal(off, 0.0)
+    off *= np.sqrt(np.outer(diag, diag))
+    row = np.abs(off).sum(axis=1)
+    scale = np.min(0.5 * diag / np.maximum(row, 1e-300))
+    m = np.diag(diag) + off * min(1.0, scale)
+    w = rng.uniform(0.5, 1.5, nlev) / nlev
+    b = rng.uniform(-1.0, 1.0, nlev) * 1e-2
+    b_matrix = np.concatenate([-m - np.outer(b, w), b[:, None]], axis=1)
+    c_matrix = np.concatenate([np.eye(nlev), w[None, :]], axis=0)
+    return b_matrix, c_matrix

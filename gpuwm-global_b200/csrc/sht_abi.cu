@@ -8,6 +8,24 @@
 
 #include "sht_plan.h"
 
+// Plans run together (sht_batch_create).  The batch borrows its plans; its
+// own tile cache holds the merged tensor-core tile lists.
+struct sht_batch {
+  std::vector<sht_plan*> plans;
+  std::vector<int64_t> planes;
+  sht::TcTileCache* cache = nullptr;
+};
+
+// A vertical structure operator resident on the plan's device: B, C, the
+// modal basis and its inverse, and the eigenvalues, packed in the plan's
+// arithmetic type in the order launch_helmholtz reads them.
+struct sht_vertical {
+  int device = 0;
+  int prec = 0;
+  int nlev = 0;
+  void* mats = nullptr;
+};
+
 namespace sht {
 
 static thread_local std::string g_error;
@@ -140,6 +158,27 @@ void contract(sht_plan* p, int kind, const T* data, T* out, int64_t R, cudaStrea
   launch_gemm_simt<T>(p, dir, flip, static_cast<const T*>(table_ptr(p, kind)), data, out, R, s);
 }
 
+// Two contractions of the same data (P and dP/dphi tables of a gradient or
+// wind synthesis; rotational and shear tables of a vordiv analysis): one
+// tensor-core launch over the merged tiles on the split path.
+template <typename T>
+void contract2(sht_plan* p, int kind0, T* out0, int kind1, T* out1, const T* data, int64_t R,
+               cudaStream_t s) {
+  if constexpr (sizeof(T) == 4) {
+    if (uses_tc(p)) {
+      const int dir = table_dir(kind0);
+      KernelScope scope(p, dir == 0 ? SHT_KIND_LEGENDRE_SYNTHESIS : SHT_KIND_LEGENDRE_ANALYSIS, s);
+      TcGroupSpec g[2] = {
+          {p, dir, table_flip(kind0), kind0, data, p->rowmax, out0, R},
+          {p, table_dir(kind1), table_flip(kind1), kind1, data, p->rowmax, out1, R}};
+      launch_gemm_tc_groups(g, 2, tc_plan_cache(p), s);
+      return;
+    }
+  }
+  contract<T>(p, kind0, data, out0, R, s);
+  contract<T>(p, kind1, data, out1, R, s);
+}
+
 template <typename T>
 void do_forward(sht_plan* p, const T* grid, int64_t planes, T* coeff, cudaStream_t s) {
   const int64_t R = 2 * planes;
@@ -190,8 +229,7 @@ void do_gradient(sht_plan* p, const T* coeff, int64_t planes, T* east, T* north,
     KernelScope k(p, SHT_KIND_PACK, s);
     launch_pack<T>(p, coeff, nullptr, planes, kPackPlain, c, s, rm);
   }
-  contract<T>(p, kBasis, c, w0, R, s);
-  contract<T>(p, kDBasis, c, w1, R, s);
+  contract2<T>(p, kBasis, w0, kDBasis, w1, c, R, s);
   {
     KernelScope k(p, SHT_KIND_FFT_INVERSE, s);
     launch_inverse_unfold<T>(p, kUnfoldGradient, w0, w1, planes, east, north, s);
@@ -211,8 +249,7 @@ void do_wind(sht_plan* p, const T* vort, const T* div, int64_t planes, T* u, T* 
     KernelScope k(p, SHT_KIND_PACK, s);
     launch_pack<T>(p, vort, div, planes, kPackInvLap, c, s, rm);
   }
-  contract<T>(p, kBasis, c, w0, R, s);
-  contract<T>(p, kDBasis, c, w1, R, s);
+  contract2<T>(p, kBasis, w0, kDBasis, w1, c, R, s);
   {
     KernelScope k(p, SHT_KIND_FFT_INVERSE, s);
     launch_inverse_unfold<T>(p, kUnfoldWind, w0, w1, planes, u, v, s);
@@ -232,12 +269,133 @@ void do_vordiv(sht_plan* p, const T* u, const T* v, int64_t planes, T* vort, T* 
     KernelScope k(p, SHT_KIND_FFT_FORWARD, s);
     launch_forward_fold<T>(p, u, v, planes, w, s, rm);
   }
-  contract<T>(p, kRot, w, c0, R, s);
-  contract<T>(p, kShear, w, c1, R, s);
+  contract2<T>(p, kRot, c0, kShear, c1, w, R, s);
   {
     KernelScope k(p, SHT_KIND_UNPACK, s);
     launch_unpack<T>(p, kUnpackVorDiv, c0, c1, planes, vort, div, s);
   }
+}
+
+// ------------------------------------------------------------------ batches
+// A batch of plans (different truncations, or the same truncation under
+// separate plans) run as one transform: per-plan FFT, pack and unpack
+// launches around ONE Legendre launch per direction.  On the split path that
+// launch is the persistent tensor-core kernel over the merged, cost-sorted
+// tiles of every plan, so the large low-order tiles of the biggest
+// truncation start first and the small tiles of all plans fill the tail.
+template <typename T>
+void contract_batch(sht_batch* b, int kind, T* const* data, T* const* out, cudaStream_t s) {
+  const int n = (int)b->plans.size();
+  if constexpr (sizeof(T) == 4) {
+    if (uses_tc(b->plans[0])) {
+      const int dir = table_dir(kind);
+      KernelScope scope(b->plans[0],
+                        dir == 0 ? SHT_KIND_LEGENDRE_SYNTHESIS : SHT_KIND_LEGENDRE_ANALYSIS, s);
+      TcGroupSpec g[kMaxTcGroups];
+      for (int i = 0; i < n; ++i)
+        g[i] = {b->plans[i], dir, table_flip(kind), kind, data[i], b->plans[i]->rowmax, out[i],
+                2 * b->planes[i]};
+      launch_gemm_tc_groups(g, n, b->cache, s);
+      return;
+    }
+  }
+  for (int i = 0; i < n; ++i) contract<T>(b->plans[i], kind, data[i], out[i], 2 * b->planes[i], s);
+}
+
+template <typename T>
+void do_batch_forward(sht_batch* b, const void* const* grids, void* const* coeffs, cudaStream_t s) {
+  const int n = (int)b->plans.size();
+  T* w[kMaxTcGroups];
+  T* c[kMaxTcGroups];
+  for (int i = 0; i < n; ++i) {
+    sht_plan* p = b->plans[i];
+    const int64_t planes = b->planes[i], R = 2 * planes;
+    ensure_scratch(p, R);
+    w[i] = static_cast<T*>(p->wfold[0]);
+    c[i] = static_cast<T*>(p->cfold[0]);
+    float* rm = rowmax_for(p, R, s);
+    KernelScope k(p, SHT_KIND_FFT_FORWARD, s);
+    launch_forward_fold<T>(p, static_cast<const T*>(grids[i]), nullptr, planes, w[i], s, rm);
+  }
+  contract_batch<T>(b, kAnalysis, w, c, s);
+  for (int i = 0; i < n; ++i) {
+    KernelScope k(b->plans[i], SHT_KIND_UNPACK, s);
+    launch_unpack<T>(b->plans[i], kUnpackScalar, c[i], nullptr, b->planes[i],
+                     static_cast<T*>(coeffs[i]), nullptr, s);
+  }
+}
+
+template <typename T>
+void do_batch_inverse(sht_batch* b, const void* const* coeffs, void* const* grids, cudaStream_t s) {
+  const int n = (int)b->plans.size();
+  T* w[kMaxTcGroups];
+  T* c[kMaxTcGroups];
+  for (int i = 0; i < n; ++i) {
+    sht_plan* p = b->plans[i];
+    const int64_t planes = b->planes[i], R = 2 * planes;
+    ensure_scratch(p, R);
+    w[i] = static_cast<T*>(p->wfold[0]);
+    c[i] = static_cast<T*>(p->cfold[0]);
+    float* rm = rowmax_for(p, R, s);
+    KernelScope k(p, SHT_KIND_PACK, s);
+    launch_pack<T>(p, static_cast<const T*>(coeffs[i]), nullptr, planes, kPackPlain, c[i], s, rm);
+  }
+  contract_batch<T>(b, kBasis, c, w, s);
+  for (int i = 0; i < n; ++i) {
+    KernelScope k(b->plans[i], SHT_KIND_FFT_INVERSE, s);
+    launch_inverse_unfold<T>(b->plans[i], kUnfoldScalar, w[i], nullptr, b->planes[i],
+                             static_cast<T*>(grids[i]), nullptr, s);
+  }
+}
+
+// ------------------------------------------------------- vertical operators
+sht_vertical* vertical_upload(const sht_plan* plan, int nlev, const double* b, const double* c,
+                              const double* eigvec, const double* eigvec_inv,
+                              const double* eigenvalues) {
+  SHT_REQUIRE(nlev >= 1 && nlev <= 96, "nlev must be in [1, 96]");
+  for (const void* q : {(const void*)b, (const void*)c, (const void*)eigvec,
+                        (const void*)eigvec_inv, (const void*)eigenvalues})
+    check_ptr(q, "vertical operator matrix");
+  const int L1 = nlev + 1;
+  const size_t nm = (size_t)nlev * L1 * 2 + (size_t)nlev * nlev * 2 + nlev;
+  std::vector<double> host(nm);
+  size_t o = 0;
+  std::copy(b, b + nlev * L1, host.begin() + o);
+  o += nlev * L1;
+  std::copy(c, c + L1 * nlev, host.begin() + o);
+  o += L1 * nlev;
+  std::copy(eigvec, eigvec + nlev * nlev, host.begin() + o);
+  o += nlev * nlev;
+  std::copy(eigvec_inv, eigvec_inv + nlev * nlev, host.begin() + o);
+  o += nlev * nlev;
+  std::copy(eigenvalues, eigenvalues + nlev, host.begin() + o);
+  auto* op = new sht_vertical;
+  op->device = plan->device;
+  op->prec = plan->prec;
+  op->nlev = nlev;
+  try {
+    if (plan->prec == SHT_PREC_F64) {
+      SHT_CUDA_OR_THROW(cudaMalloc(&op->mats, sizeof(double) * nm));
+      SHT_CUDA_OR_THROW(cudaMemcpy(op->mats, host.data(), sizeof(double) * nm,
+                                   cudaMemcpyHostToDevice));
+    } else {
+      std::vector<float> conv(host.begin(), host.end());
+      SHT_CUDA_OR_THROW(cudaMalloc(&op->mats, sizeof(float) * nm));
+      SHT_CUDA_OR_THROW(cudaMemcpy(op->mats, conv.data(), sizeof(float) * nm,
+                                   cudaMemcpyHostToDevice));
+    }
+  } catch (...) {
+    if (op->mats) cudaFree(op->mats);
+    delete op;
+    throw;
+  }
+  return op;
+}
+
+void vertical_free(sht_vertical* op) {
+  if (!op) return;
+  if (op->mats) cudaFree(op->mats);
+  delete op;
 }
 
 void destroy(sht_plan* p) {
@@ -513,6 +671,20 @@ int sht_inverse_laplacian(sht_plan* plan, const void* in, int64_t planes, void* 
   return elementwise_entry(plan, kElemInvLaplacian, in, planes, out, stream);
 }
 
+static void vertical_apply(sht_plan* plan, const sht_vertical* op, double tau_w,
+                           const void* divergence, const void* theta, const void* lnps,
+                           void* out_divergence, void* out_theta, void* out_lnps,
+                           cudaStream_t s) {
+  for (const void* q : {divergence, theta, lnps, (const void*)out_divergence,
+                        (const void*)out_theta, (const void*)out_lnps})
+    check_ptr(q, "helmholtz argument");
+  plan->last_stream = s;
+  KernelScope k(plan, SHT_KIND_HELMHOLTZ, s);
+  SHT_TYPED(plan, launch_helmholtz<T>(plan, op->nlev, static_cast<const T*>(op->mats), tau_w,
+                                      CP(divergence), CP(theta), CP(lnps), MP(out_divergence),
+                                      MP(out_theta), MP(out_lnps), s));
+}
+
 int sht_helmholtz_solve(sht_plan* plan, int nlev, const double* b, const double* c,
                         const double* eigvec, const double* eigvec_inv,
                         const double* eigenvalues, double tau_w, const void* divergence,
@@ -520,38 +692,119 @@ int sht_helmholtz_solve(sht_plan* plan, int nlev, const double* b, const double*
                         void* out_theta, void* out_lnps, void* stream) {
   return guarded([&] {
     check_transform_plan(plan);
-    SHT_REQUIRE(nlev >= 1 && nlev <= 96, "nlev must be in [1, 96]");
-    for (const void* q : {(const void*)b, (const void*)c, (const void*)eigvec,
-                          (const void*)eigvec_inv, (const void*)eigenvalues, divergence, theta,
-                          lnps, (const void*)out_divergence, (const void*)out_theta,
-                          (const void*)out_lnps})
-      check_ptr(q, "helmholtz argument");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    plan->last_stream = s;
-    const int L1 = nlev + 1;
-    const size_t nm = (size_t)nlev * L1 * 2 + (size_t)nlev * nlev * 2 + nlev;
-    std::vector<double> host(nm);
-    size_t o = 0;
-    std::copy(b, b + nlev * L1, host.begin() + o);
-    o += nlev * L1;
-    std::copy(c, c + L1 * nlev, host.begin() + o);
-    o += L1 * nlev;
-    std::copy(eigvec, eigvec + nlev * nlev, host.begin() + o);
-    o += nlev * nlev;
-    std::copy(eigvec_inv, eigvec_inv + nlev * nlev, host.begin() + o);
-    o += nlev * nlev;
-    std::copy(eigenvalues, eigenvalues + nlev, host.begin() + o);
-    SHT_TYPED(plan, {
-      std::vector<T> conv(host.begin(), host.end());
-      T* dm = nullptr;
-      SHT_CUDA_OR_THROW(cudaMallocAsync(&dm, sizeof(T) * nm, s));
-      SHT_CUDA_OR_THROW(cudaMemcpyAsync(dm, conv.data(), sizeof(T) * nm, cudaMemcpyHostToDevice, s));
-      KernelScope k(plan, SHT_KIND_HELMHOLTZ, s);
-      launch_helmholtz<T>(plan, nlev, dm, tau_w, CP(divergence), CP(theta), CP(lnps),
-                          MP(out_divergence), MP(out_theta), MP(out_lnps), s);
-      SHT_CUDA_OR_THROW(cudaFreeAsync(dm, s));
-      SHT_CUDA_OR_THROW(cudaStreamSynchronize(s));  // the host staging buffer dies here
-    });
+    // One-shot form: upload, solve, and free once the solve has finished.
+    sht_vertical* op = vertical_upload(plan, nlev, b, c, eigvec, eigvec_inv, eigenvalues);
+    try {
+      vertical_apply(plan, op, tau_w, divergence, theta, lnps, out_divergence, out_theta,
+                     out_lnps, s);
+      SHT_CUDA_OR_THROW(cudaStreamSynchronize(s));
+    } catch (...) {
+      vertical_free(op);
+      throw;
+    }
+    vertical_free(op);
+  });
+}
+
+int sht_vertical_create(sht_plan* plan, int nlev, const double* b, const double* c,
+                        const double* eigvec, const double* eigvec_inv,
+                        const double* eigenvalues, sht_vertical** out) {
+  return guarded([&] {
+    check_ptr(out, "out");
+    *out = nullptr;
+    check_transform_plan(plan);
+    int device = 0;
+    SHT_CUDA_OR_THROW(cudaGetDevice(&device));
+    SHT_REQUIRE(device == plan->device, "the current device is not the plan's device");
+    *out = vertical_upload(plan, nlev, b, c, eigvec, eigvec_inv, eigenvalues);
+  });
+}
+
+int sht_vertical_destroy(sht_vertical* op) {
+  return guarded([&] { vertical_free(op); });
+}
+
+int sht_helmholtz_apply(sht_plan* plan, const sht_vertical* op, double tau_w,
+                        const void* divergence, const void* theta, const void* lnps,
+                        void* out_divergence, void* out_theta, void* out_lnps, void* stream) {
+  return guarded([&] {
+    check_transform_plan(plan);
+    check_ptr(op, "vertical operator");
+    SHT_REQUIRE(op->device == plan->device && op->prec == plan->prec,
+                "the vertical operator was created for another plan's device or precision");
+    vertical_apply(plan, op, tau_w, divergence, theta, lnps, out_divergence, out_theta, out_lnps,
+                   static_cast<cudaStream_t>(stream));
+  });
+}
+
+int sht_batch_create(int nplans, sht_plan* const* plans, const int64_t* planes,
+                     sht_batch** out) {
+  return guarded([&] {
+    check_ptr(out, "out");
+    *out = nullptr;
+    SHT_REQUIRE(nplans >= 1 && nplans <= kMaxTcGroups, "a batch holds 1 to 4 plans");
+    check_ptr(plans, "plans");
+    check_ptr(planes, "planes");
+    for (int i = 0; i < nplans; ++i) {
+      check_transform_plan(plans[i]);
+      SHT_REQUIRE(planes[i] >= 1, "every plan of a batch needs planes >= 1");
+      SHT_REQUIRE(plans[i]->prec == plans[0]->prec, "the plans of a batch share one precision");
+      SHT_REQUIRE(plans[i]->device == plans[0]->device, "the plans of a batch share one device");
+      for (int j = 0; j < i; ++j)
+        SHT_REQUIRE(plans[j] != plans[i],
+                    "a plan appears twice in a batch (its scratch would be shared)");
+    }
+    auto* b = new sht_batch;
+    b->plans.assign(plans, plans + nplans);
+    b->planes.assign(planes, planes + nplans);
+    b->cache = tc_cache_create();
+    *out = b;
+  });
+}
+
+int sht_batch_destroy(sht_batch* batch) {
+  return guarded([&] {
+    if (!batch) return;
+    tc_cache_destroy(batch->cache);
+    delete batch;
+  });
+}
+
+static void check_batch_call(sht_batch* b, const void* const* in, void* const* out) {
+  check_ptr(b, "batch");
+  check_ptr(in, "input array list");
+  check_ptr(out, "output array list");
+  for (size_t i = 0; i < b->plans.size(); ++i) {
+    check_transform_plan(b->plans[i]);
+    check_ptr(in[i], "batch input");
+    check_ptr(out[i], "batch output");
+  }
+}
+
+int sht_batch_forward(sht_batch* batch, const void* const* grids, void* const* coeffs,
+                      void* stream) {
+  return guarded([&] {
+    check_batch_call(batch, grids, coeffs);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    for (sht_plan* p : batch->plans) p->last_stream = s;
+    if (batch->plans[0]->prec == SHT_PREC_F64)
+      do_batch_forward<double>(batch, grids, coeffs, s);
+    else
+      do_batch_forward<float>(batch, grids, coeffs, s);
+  });
+}
+
+int sht_batch_inverse(sht_batch* batch, const void* const* coeffs, void* const* grids,
+                      void* stream) {
+  return guarded([&] {
+    check_batch_call(batch, coeffs, grids);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    for (sht_plan* p : batch->plans) p->last_stream = s;
+    if (batch->plans[0]->prec == SHT_PREC_F64)
+      do_batch_inverse<double>(batch, coeffs, grids, s);
+    else
+      do_batch_inverse<float>(batch, coeffs, grids, s);
   });
 }
 

@@ -191,20 +191,34 @@ __device__ __forceinline__ void warp_fft(float2 (&z)[F], float2* reg, const floa
   __syncwarp();
 }
 
+// A CTA runs kWarps warps, one grid row each: G planes x NF fields x the two
+// hemisphere rows (8 rows).
+constexpr int kWarps = 8;
+
+// An opaque copy of a pointer.  The FFT kernels read their twiddles through
+// it, so the compiler cannot hoist a whole row of twiddle loads into
+// registers ahead of the butterflies (which costs ~20 registers per thread,
+// one resident CTA per SM).
+__device__ __forceinline__ const float2* opaque(const float2* p) {
+  asm volatile("" : "+l"(p));
+  return p;
+}
+
 struct FastFoldArgs {
   int nlat, nlon, T, H, nlat_odd, F, G;  // F: fields per plane; G: planes per CTA
   int64_t planes;
 };
 
-// grid -> waist [m][s][h][r], r = (p*F + f)*2 + c.  8 warps: warp w handles
+// grid -> waist [m][s][h][r], r = (p*F + f)*2 + c.  Warp w handles
 // (pf = w >> 1, side = w & 1) with pf = gp*F + f.
 template <int FF>
-__global__ void __launch_bounds__(256) fast_forward_fold(FastFoldArgs a, const float* __restrict__ g0,
-                                                         const float* __restrict__ g1,
-                                                         const float2* __restrict__ twL,
-                                                         const float2* __restrict__ twN,
-                                                         float2* __restrict__ wfold,
-                                                         float* __restrict__ rowmax) {
+__global__ void __launch_bounds__(kWarps * 32) fast_forward_fold(FastFoldArgs a,
+                                                                 const float* __restrict__ g0,
+                                                                 const float* __restrict__ g1,
+                                                                 const float2* __restrict__ twL,
+                                                                 const float2* __restrict__ twN,
+                                                                 float2* __restrict__ wfold,
+                                                                 float* __restrict__ rowmax) {
   constexpr int L = 32 * FF;
   extern __shared__ float2 smem_dyn[];
   auto smem = [&](int w) { return smem_dyn + w * WarpSmem<FF>::kFloats2; };
@@ -225,7 +239,7 @@ __global__ void __launch_bounds__(256) fast_forward_fold(FastFoldArgs a, const f
     float2 z[FF];
 #pragma unroll
     for (int i = 0; i < FF; ++i) z[i] = __ldg(src + lane + 32 * i);
-    warp_fft<FF, false>(z, reg, twL, lane);
+    warp_fft<FF, false>(z, reg, opaque(twL), lane);
   }
   __syncthreads();
   // Untangle, scale, fold, write: thread -> (m, pf) with pf fastest.
@@ -271,63 +285,84 @@ struct FastUnfoldArgs {
   float radius;
 };
 
-// waist(s) -> grid.  8 warps: warp w handles (row pair index po = w >> 1,
-// side = w & 1) with po = gp*NO + o (o: output field).
-template <int FF>
-__global__ void __launch_bounds__(256) fast_inverse_unfold(FastUnfoldArgs a, const float2* __restrict__ wP,
-                                                           const float2* __restrict__ wD,
-                                                           const double* __restrict__ coslat,
-                                                           const float2* __restrict__ twL,
-                                                           const float2* __restrict__ twN,
-                                                           float* __restrict__ out0,
-                                                           float* __restrict__ out1) {
+// waist(s) -> grid.  Warp w handles (row pair index po = w >> 1, side = w & 1)
+// with po = gp*NO + o (o: output field).  NF waist columns feed each
+// (m, plane): 1 (scalar, zonal, meridional), 2 (gradient: the P and dP
+// syntheses of one field), 4 (wind: P and dP of psi and chi).
+template <int FF, int NF>
+__global__ void __launch_bounds__(kWarps * 32) fast_inverse_unfold(FastUnfoldArgs a,
+                                                                   const float2* __restrict__ wP,
+                                                                   const float2* __restrict__ wD,
+                                                                   const double* __restrict__ coslat,
+                                                                   const float2* __restrict__ twL,
+                                                                   const float2* __restrict__ twN,
+                                                                   float* __restrict__ out0,
+                                                                   float* __restrict__ out1) {
   constexpr int L = 32 * FF;
+  constexpr int NO = NF == 1 ? 1 : 2;
   extern __shared__ float2 smem_dyn[];
   auto smem = [&](int w) { return smem_dyn + w * WarpSmem<FF>::kFloats2; };
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int h = blockIdx.x;
   const int64_t p0 = (int64_t)blockIdx.y * a.G;
   const bool eq = a.nlat_odd && h == a.H - 1;
-  const int NO = (a.mode == kUnfoldGradient || a.mode == kUnfoldWind) ? 2 : 1;
-  const int FW = a.mode == kUnfoldWind ? 2 : 1;
-  const int64_t Rc = a.planes * FW;
+  const int64_t Rc = a.planes * (NF == 4 ? 2 : 1);
   const float inv_a = 1.0f / a.radius;
   const int jrow[2] = {h, a.nlat - 1 - h};
 
   // Stage 1: Fourier coefficients of every output row into smem[row][m].
-  for (int t = threadIdx.x; t < (a.T + 1) * a.G; t += blockDim.x) {
-    int m = t / a.G, gp = t - m * a.G;
-    int64_t plane = p0 + gp;
-    if (plane >= a.planes) continue;
+  // Each thread first issues the waist loads of kBatch items (NF symmetric /
+  // antisymmetric pairs each), then combines them: the loads of a batch are
+  // in flight together instead of one dependent round trip per item.
+  constexpr int kBatch = 4;
+  const int total = (a.T + 1) * a.G;
+  for (int base = threadIdx.x; base < total; base += kBatch * blockDim.x) {
+    float2 S[kBatch][NF], D[kBatch][NF];
 #pragma unroll
-    for (int sd = 0; sd < 2; ++sd) {
-      if (sd == 1 && eq) continue;
-      float sgn = sd ? -1.f : 1.f;
-      float im_over = (float)m / (a.radius * (float)coslat[jrow[sd]]);
-      auto fetch = [&](const float2* w, int fld) {
-        int64_t c0 = ((int64_t)(m * 2 + 0) * a.H + h) * Rc + plane * FW + fld;
-        int64_t c1 = ((int64_t)(m * 2 + 1) * a.H + h) * Rc + plane * FW + fld;
-        float2 s = w[c0], d = w[c1];
-        return make_float2(s.x + sgn * d.x, s.y + sgn * d.y);
-      };
-      float2 o0, o1 = make_float2(0.f, 0.f);
-      if (a.mode == kUnfoldScalar || a.mode == kUnfoldMeridional) {
-        o0 = fetch(wP, 0);
-      } else if (a.mode == kUnfoldZonal) {
-        float2 x = fetch(wP, 0);
-        o0 = make_float2(-(float)m * x.y, (float)m * x.x);
-      } else if (a.mode == kUnfoldGradient) {
-        float2 x = fetch(wP, 0);
-        o0 = make_float2(-(float)m * x.y, (float)m * x.x);
-        o1 = fetch(wD, 0);
-      } else {
-        float2 xp = fetch(wP, 0), xc = fetch(wP, 1);
-        float2 dp = fetch(wD, 0), dc = fetch(wD, 1);
-        o0 = make_float2(-dp.x * inv_a - im_over * xc.y, -dp.y * inv_a + im_over * xc.x);
-        o1 = make_float2(-im_over * xp.y + dc.x * inv_a, im_over * xp.x + dc.y * inv_a);
+    for (int u = 0; u < kBatch; ++u) {
+      const int t = base + u * blockDim.x;
+      const int m = t / a.G, gp = t - m * a.G;
+      if (t < total && p0 + gp < a.planes) {
+        const int64_t r = (p0 + gp) * (NF == 4 ? 2 : 1);
+        const int64_t c0 = ((int64_t)(m * 2 + 0) * a.H + h) * Rc + r;
+        const int64_t c1 = ((int64_t)(m * 2 + 1) * a.H + h) * Rc + r;
+#pragma unroll
+        for (int k = 0; k < NF; ++k) {
+          const float2* w = (NF == 1 || k < NF / 2) ? wP : wD;
+          const int fld = NF == 4 ? (k & 1) : 0;
+          S[u][k] = w[c0 + fld];
+          D[u][k] = w[c1 + fld];
+        }
       }
-      smem((gp * NO + 0) * 2 + sd)[m] = o0;
-      if (NO == 2) smem((gp * NO + 1) * 2 + sd)[m] = o1;
+    }
+#pragma unroll
+    for (int u = 0; u < kBatch; ++u) {
+      const int t = base + u * blockDim.x;
+      const int m = t / a.G, gp = t - m * a.G;
+      if (t >= total || p0 + gp >= a.planes) continue;
+#pragma unroll
+      for (int sd = 0; sd < 2; ++sd) {
+        if (sd == 1 && eq) continue;
+        const float sgn = sd ? -1.f : 1.f;
+        float2 x[NF];
+#pragma unroll
+        for (int k = 0; k < NF; ++k)
+          x[k] = make_float2(S[u][k].x + sgn * D[u][k].x, S[u][k].y + sgn * D[u][k].y);
+        float2 o0, o1 = make_float2(0.f, 0.f);
+        if constexpr (NF == 1) {
+          o0 = a.mode == kUnfoldZonal ? make_float2(-(float)m * x[0].y, (float)m * x[0].x) : x[0];
+        } else if constexpr (NF == 2) {
+          o0 = make_float2(-(float)m * x[0].y, (float)m * x[0].x);
+          o1 = x[1];
+        } else {
+          // x = {P psi, P chi, dP psi, dP chi}
+          const float im_over = (float)m / (a.radius * (float)coslat[jrow[sd]]);
+          o0 = make_float2(-x[2].x * inv_a - im_over * x[1].y, -x[2].y * inv_a + im_over * x[1].x);
+          o1 = make_float2(-im_over * x[0].y + x[3].x * inv_a, im_over * x[0].x + x[3].y * inv_a);
+        }
+        smem((gp * NO + 0) * 2 + sd)[m] = o0;
+        if (NO == 2) smem((gp * NO + 1) * 2 + sd)[m] = o1;
+      }
     }
   }
   __syncthreads();
@@ -336,6 +371,7 @@ __global__ void __launch_bounds__(256) fast_inverse_unfold(FastUnfoldArgs a, con
   const int64_t plane = p0 + gp;
   if (po >= a.G * NO || plane >= a.planes || (eq && side == 1)) return;
   float2* reg = smem(warp);
+  const float2* tn = opaque(twN);
   // Stage 2: entangle z[k] for k = lane + 32 j straight into registers.
   float2 z[FF];
 #pragma unroll
@@ -346,15 +382,15 @@ __global__ void __launch_bounds__(256) fast_inverse_unfold(FastUnfoldArgs a, con
     float2 xc = (k > 0 && kc <= a.T) ? cconjf(reg[kc]) : make_float2(0.f, 0.f);
     if (k == 0) xk.y = 0.f;
     float2 s = caddf(xk, xc), d = csubf(xk, xc);
-    float2 wd = cmulf(cconjf(twN[k]), d);
+    float2 wd = cmulf(cconjf(tn[k]), d);
     z[i] = make_float2(s.x - wd.y, s.y + wd.x);
   }
   __syncwarp();
-  warp_fft<FF, true>(z, reg, twL, lane);
+  warp_fft<FF, true>(z, reg, opaque(twL), lane);
   // Stage 3: natural-order z[n] -> x[2n], x[2n+1] with the row scaling.
   const int j = jrow[side];
   // The gradient divides the grid by (a cos phi) and by a, as the reference does.
-  const bool divide = a.mode == kUnfoldGradient;
+  const bool divide = NF == 2;
   const float den = o == 0 ? a.radius * (float)coslat[j] : a.radius;
   float2* dst = reinterpret_cast<float2*>((o ? out1 : out0) + (plane * a.nlat + j) * (int64_t)a.nlon);
 #pragma unroll 4
@@ -369,30 +405,42 @@ template <int FF>
 void launch_fwd(const sht_plan* p, const float* g0, const float* g1, int64_t planes, float* wfold,
                 cudaStream_t s, float* rowmax) {
   FastFoldArgs a{p->nlat, p->nlon, p->T, p->H, p->nlat_odd ? 1 : 0, g1 ? 2 : 1, 0, planes};
-  a.G = 4 / a.F;
+  a.G = kWarps / 2 / a.F;
   dim3 grid((unsigned)p->H, (unsigned)div_up(planes, a.G));
-  const size_t sm = sizeof(float2) * 8 * WarpSmem<FF>::kFloats2;
+  const size_t sm = sizeof(float2) * kWarps * WarpSmem<FF>::kFloats2;
   SHT_CUDA_OR_THROW(cudaFuncSetAttribute(fast_forward_fold<FF>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-  fast_forward_fold<FF><<<grid, 256, sm, s>>>(a, g0, g1 ? g1 : g0, (const float2*)p->tw_l,
-                                             (const float2*)p->tw_n, (float2*)wfold, rowmax);
+  fast_forward_fold<FF><<<grid, kWarps * 32, sm, s>>>(a, g0, g1 ? g1 : g0, (const float2*)p->tw_l,
+                                                      (const float2*)p->tw_n, (float2*)wfold,
+                                                      rowmax);
+  SHT_CUDA_OR_THROW(cudaGetLastError());
+}
+
+template <int FF, int NF>
+void launch_inv_nf(const sht_plan* p, int mode, const float* wP, const float* wD, int64_t planes,
+                   float* out0, float* out1, cudaStream_t s) {
+  constexpr int NO = NF == 1 ? 1 : 2;
+  FastUnfoldArgs a{p->nlat, p->nlon, p->T, p->H, p->nlat_odd ? 1 : 0, mode, kWarps / 2 / NO,
+                   planes, (float)p->radius};
+  dim3 grid((unsigned)p->H, (unsigned)div_up(planes, a.G));
+  const size_t sm = sizeof(float2) * kWarps * WarpSmem<FF>::kFloats2;
+  SHT_CUDA_OR_THROW(cudaFuncSetAttribute(fast_inverse_unfold<FF, NF>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  fast_inverse_unfold<FF, NF><<<grid, kWarps * 32, sm, s>>>(
+      a, (const float2*)wP, (const float2*)(wD ? wD : wP), p->d_coslat, (const float2*)p->tw_l,
+      (const float2*)p->tw_n, out0, out1 ? out1 : out0);
   SHT_CUDA_OR_THROW(cudaGetLastError());
 }
 
 template <int FF>
 void launch_inv(const sht_plan* p, int mode, const float* wP, const float* wD, int64_t planes,
                 float* out0, float* out1, cudaStream_t s) {
-  int NO = (mode == kUnfoldGradient || mode == kUnfoldWind) ? 2 : 1;
-  FastUnfoldArgs a{p->nlat, p->nlon, p->T, p->H, p->nlat_odd ? 1 : 0, mode, 4 / NO, planes,
-                   (float)p->radius};
-  dim3 grid((unsigned)p->H, (unsigned)div_up(planes, a.G));
-  const size_t sm = sizeof(float2) * 8 * WarpSmem<FF>::kFloats2;
-  SHT_CUDA_OR_THROW(cudaFuncSetAttribute(fast_inverse_unfold<FF>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-  fast_inverse_unfold<FF><<<grid, 256, sm, s>>>(a, (const float2*)wP, (const float2*)(wD ? wD : wP),
-                                               p->d_coslat, (const float2*)p->tw_l,
-                                               (const float2*)p->tw_n, out0, out1 ? out1 : out0);
-  SHT_CUDA_OR_THROW(cudaGetLastError());
+  if (mode == kUnfoldWind)
+    launch_inv_nf<FF, 4>(p, mode, wP, wD, planes, out0, out1, s);
+  else if (mode == kUnfoldGradient)
+    launch_inv_nf<FF, 2>(p, mode, wP, wD, planes, out0, out1, s);
+  else
+    launch_inv_nf<FF, 1>(p, mode, wP, wD, planes, out0, out1, s);
 }
 
 }  // namespace

@@ -4,34 +4,36 @@
 // For every (order m, parity q) block: out[x][r] = sum_k Tab[k][x] D[k][r].
 // The MMA sees it as C (M x N) = A (M x K) B^T with
 //   M = 128 data rows r (plane x re/im), N = a tile of the table's x extent
-//   (<= 256, multiple of 16), K = the contraction (latitude pairs for the
+//   (<= 128, multiple of 16), K = the contraction (latitude pairs for the
 //   analysis, degrees for the synthesis).
 // Both operands are split into two FP16 parts after a power-of-two scaling
 // that puts each data row / table column maximum in [2^14, 2^15):
 //   a s_r = a1 + a2,  b s_x = b1 + b2            (11 significant bits each)
 //   C = (a1 b1 + [a1 b2 + a2 b1]) / (s_r s_x)
-// The main product a1 b1 and the two correction products accumulate in two
-// separate TMEM accumulators and are added in FP32 in the epilogue.  The
-// separation is what makes the result as accurate as an FP32 contraction:
-// the tensor core's FP32 accumulate truncates, and with all three products
-// in one accumulator every correction step adds another truncation of the
-// full-size sum (1.3e-6 relative spectral L2 at T255 against 2.4e-7 with the
-// accumulators separated, in an emulation of the pipeline; the plain FP32
-// path measures 2.9e-7 at T511).  The table parts and the column scales are
+// The main product a1 b1 accumulates in NMAIN = 3 TMEM accumulators, one per
+// contiguous third of the K steps, and the two correction products in a
+// fourth; the epilogue adds the four in FP32.  The tensor core's FP32
+// accumulate truncates: with all three products in one accumulator every
+// correction step adds another truncation of the full-size sum (1.3e-6
+// relative spectral L2 at T255, in an emulation of the pipeline), with the
+// correction separated the main sum's own truncations remain (1.2e-6 at
+// T511 measured), and splitting the main sum into three segments cuts their
+// growth (3.6e-7 at T511 measured; the plain FP32 path measures 2.9e-7).  The table parts and the column scales are
 // built once per plan from the FP64 tables and stored as the exact
 // shared-memory image of each (tile, K-stage), so one bulk copy per part
 // moves a stage.  The data rows are split on the fly by converter warps;
 // their row scales come from the row maxima the producing kernel (the
 // longitude FFT or the pack kernel) merged while writing the operand.
 //
-// Roles (448 threads, one CTA per SM, persistent over a cost-sorted tile list):
+// Roles (448 threads, one CTA per SM, persistent over a cost-sorted tile list
+// that may merge several contractions: the P and dP/dphi tables of a
+// gradient or wind synthesis, or the plans of a batch):
 //   warp 0      bulk-copy loader for the table stages; owns TMEM alloc/free
 //   warp 1      MMA issuer (one thread)
 //   warps 2-5   epilogue: tcgen05.ld of the accumulator, unscale, store
 //   warps 6-13  converters for the data operand
-// Pipelines: STAGES shared-memory stages (full/empty mbarriers) and one TMEM
-// accumulator pair (main and correction, 256 columns each; full/empty
-// mbarriers).  Every mbarrier wait is bounded by a clock budget; on expiry the
+// Pipelines: STAGES shared-memory stages (full/empty mbarriers) and one set of
+// four TMEM accumulators of 128 columns (full/empty mbarriers).  Every mbarrier wait is bounded by a clock budget; on expiry the
 // waiting thread raises the plan's error word and a CTA abort flag, and each
 // epilogue warp decides to stop as a whole (__any_sync) before the
 // warp-collective TMEM loads, so a fault in the pipeline logic cannot hang
@@ -43,10 +45,14 @@
 // groups LBO bytes apart.
 #include <algorithm>
 #include <cmath>
+#include <map>
+#include <mutex>
+#include <vector>
 
 #include "sht_plan.h"
 
 struct ShtTcTile {
+  int group;    // index into the launch's group list
   int problem;  // index into the direction's descriptor list
   int n0;       // first x of the tile
   int nsize;    // tile N (multiple of 16, <= 256); 0 for an empty problem
@@ -68,10 +74,8 @@ struct ShtTc16 {
   std::vector<int> nt_of[2], nsize_of[2], kst_of[2], img_base[2];
   int64_t img_bytes[2] = {0, 0};
   int64_t cs_elems[2] = {0, 0};
-  // Tile lists are built per row count R (cached).
-  int64_t tiles_R[2] = {-1, -1};
-  ShtTcTile* d_tiles[2] = {nullptr, nullptr};
-  int n_tiles[2] = {0, 0};
+  // Tile lists of this plan's own launches.
+  sht::TcTileCache* tiles = nullptr;
   int sm_count = 148;
 };
 
@@ -80,9 +84,10 @@ namespace {
 
 constexpr int BM = 128;
 constexpr int BK = 32;
-constexpr int STAGES = 4;
+constexpr int STAGES = 6;
 constexpr int NPARTS = 2;
-constexpr int NMAX = 256;
+constexpr int NMAIN = 3;    // main-product accumulators (contiguous K segments)
+constexpr int NMAX = 128;   // tile N; TMEM: (NMAIN + 1) x NMAX = 512 columns
 constexpr int kThreads = 448;
 constexpr int kConvThreads = 256;
 constexpr int kConvWarp0 = 6;
@@ -171,17 +176,35 @@ __device__ __forceinline__ void mma_commit(uint64_t* bar) {
                    smem_u32(bar))
                : "memory");
 }
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
-  uint32_t r[16];
+// tcgen05.ld of 16 consecutive columns, without the wait: the registers are
+// valid only after tmem_wait16 below.
+__device__ __forceinline__ void tmem_ld16_async(uint32_t taddr, uint32_t (&r)[16]) {
   asm volatile(
       "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
       : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
         "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
         "=r"(r[14]), "=r"(r[15])
       : "r"(taddr));
-  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+// tcgen05.wait::ld (when WAIT) and a register dependency on r, so that no
+// use of r can be scheduled before the wait.
+template <bool WAIT>
+__device__ __forceinline__ void tmem_wait16(uint32_t (&r)[16]) {
+  if constexpr (WAIT) {
+    asm volatile("tcgen05.wait::ld.sync.aligned;"
+                 : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]),
+                   "+r"(r[6]), "+r"(r[7]), "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11]),
+                   "+r"(r[12]), "+r"(r[13]), "+r"(r[14]), "+r"(r[15])
+                 :
+                 : "memory");
+  } else {
+    asm volatile(""
+                 : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]),
+                   "+r"(r[6]), "+r"(r[7]), "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11]),
+                   "+r"(r[12]), "+r"(r[13]), "+r"(r[14]), "+r"(r[15])
+                 :
+                 : "memory");
+  }
 }
 
 // No-swizzle shared-memory matrix descriptor (sm_100 version bits = 1).
@@ -204,18 +227,25 @@ __device__ __forceinline__ float pow2_scale(float mx) {
   return ldexpf(1.f, max(-126, min(126, 15 - e)));
 }
 
-struct TcArgs {
+// One contraction of a launch: a table (one direction of one plan), the data
+// operand with its row maxima, and the output.  A launch runs the merged,
+// cost-sorted tiles of up to kMaxTcGroups of them.
+struct TcGroup {
   const ShtGemmDesc* descs;
-  const ShtTcTile* tiles;
-  int n_tiles;
   const unsigned char* img;
   const int64_t* img_off;  // per (problem, n-tile) block: byte offset of k-stage 0
   const float* colscale;
   const int64_t* cs_off;   // per problem
   const float* data;
-  const float* rowmax;  // per data row: max |value| (from the producer kernel)
+  const float* rowmax;     // per data row: max |value| (from the producer kernel)
   float* out;
   int64_t R;
+};
+
+struct TcArgs {
+  TcGroup g[kMaxTcGroups];
+  const ShtTcTile* tiles;
+  int n_tiles;
   unsigned* err;
 };
 
@@ -245,7 +275,7 @@ __device__ bool wait_bar(uint64_t* bar, uint32_t parity, const Pipe& pp, unsigne
   return true;
 }
 
-__global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(TcArgs a) {
+__global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_constant__ TcArgs a) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   // 1024-byte align the working area.
   unsigned char* smem = smem_raw + ((1024 - (smem_u32(smem_raw) & 1023)) & 1023);
@@ -278,7 +308,6 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(TcArgs a) {
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem_base = *tmem_base_smem;
-  const int64_t R = a.R;
 
   if (warp == 0) {
     // ------------------------------------------------------------ loader
@@ -290,8 +319,9 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(TcArgs a) {
       for (int s = 0; s < STAGES; ++s) armed[s] = -1;
       for (int t = blockIdx.x; t < a.n_tiles && !*abort_flag; t += gridDim.x) {
         const ShtTcTile tl = a.tiles[t];
+        const TcGroup& G = a.g[tl.group];
         const int part = tl.nsize * BK * 2;  // bytes of one FP16 part of one stage
-        const unsigned char* src = a.img + a.img_off[tl.img];
+        const unsigned char* src = G.img + G.img_off[tl.img];
         bool ok = true;
         for (int ks = 0; ks < tl.kst; ++ks) {
           if (!wait_bar(&pp.empty[stage], phase ^ 1, pp, a.err, 1)) {
@@ -326,8 +356,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(TcArgs a) {
       uint32_t phase = 0;
       uint32_t acc_phase = 0;
       bool issued = false;
-      const uint32_t d_main = tmem_base;           // columns [0, 256)
-      const uint32_t d_corr = tmem_base + NMAX;    // columns [256, 512)
+      const uint32_t d_corr = tmem_base + NMAIN * NMAX;  // the last 128 columns
       for (int t = blockIdx.x; t < a.n_tiles && !*abort_flag; t += gridDim.x) {
         const ShtTcTile tl = a.tiles[t];
         if (tl.kst == 0) continue;
@@ -335,6 +364,8 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(TcArgs a) {
         tc_fence_after();
         const uint32_t idesc = instr_desc(tl.nsize);
         const uint32_t lbo_b = (uint32_t)tl.nsize * 16;
+        const int nsteps = tl.kst * (BK / 16);  // K steps of 16 in the tile
+        int seg_prev = -1;
         bool ok = true;
         for (int ks = 0; ks < tl.kst; ++ks) {
           if (!wait_bar(&pp.full_a[stage], phase, pp, a.err, 3) ||
@@ -352,10 +383,14 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(TcArgs a) {
             const uint64_t da2 = smem_desc(a0 + kAPart + j * 2 * kALbo, kALbo, 128);
             const uint64_t db1 = smem_desc(b0 + j * 2 * lbo_b, lbo_b, 128);
             const uint64_t db2 = smem_desc(b0 + kBPart + j * 2 * lbo_b, lbo_b, 128);
-            const uint32_t accum = (ks > 0 || j > 0) ? 1u : 0u;
-            mma_f16(d_main, da1, db1, idesc, accum);  // a1 b1
-            mma_f16(d_corr, da1, db2, idesc, accum);  // a1 b2
-            mma_f16(d_corr, da2, db1, idesc, 1u);     // a2 b1
+            const int step = ks * (BK / 16) + j;
+            const int seg = step * NMAIN / nsteps;  // contiguous thirds of the K steps
+            const uint32_t accum_main = seg == seg_prev ? 1u : 0u;
+            seg_prev = seg;
+            const uint32_t accum_corr = step > 0 ? 1u : 0u;
+            mma_f16(tmem_base + (uint32_t)(seg * NMAX), da1, db1, idesc, accum_main);  // a1 b1
+            mma_f16(d_corr, da1, db2, idesc, accum_corr);                              // a1 b2
+            mma_f16(d_corr, da2, db1, idesc, 1u);                                      // a2 b1
           }
           issued = true;
           mma_commit(&pp.empty[stage]);  // frees the stage when these MMAs finish
@@ -382,9 +417,11 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(TcArgs a) {
     // warp-collective tcgen05.ld.
     for (int t = blockIdx.x; t < a.n_tiles; t += gridDim.x) {
       const ShtTcTile tl = a.tiles[t];
-      const ShtGemmDesc d = a.descs[tl.problem];
+      const TcGroup& G = a.g[tl.group];
+      const ShtGemmDesc d = G.descs[tl.problem];
+      const int64_t R = G.R;
       const int64_t r = tl.r0 + row;
-      float* outb = a.out + d.c_row * R;
+      float* outb = G.out + d.c_row * R;
       if (tl.kst == 0) {
         // empty contraction (K = 0): the output block is zero
         if (r < R)
@@ -394,18 +431,32 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(TcArgs a) {
       const bool failed = !wait_bar(pp.acc_full, acc_phase, pp, a.err, 5);
       if (__any_sync(0xffffffffu, failed)) break;
       tc_fence_after();
-      const float rs = r < R ? 1.f / pow2_scale(a.rowmax[r]) : 0.f;
-      const float* cs = a.colscale + a.cs_off[tl.problem];
+      const float rs = r < R ? 1.f / pow2_scale(G.rowmax[r]) : 0.f;
+      const float* cs = G.colscale + G.cs_off[tl.problem];
       const uint32_t lane_off = (uint32_t)(eg * 32) << 16;
+      // A tile with fewer K steps than NMAIN leaves the last main
+      // accumulators unwritten: only the segments that exist are read.
+      const int nsteps = tl.kst * (BK / 16);
+      const int nseg = nsteps < NMAIN ? nsteps : NMAIN;
       for (int c0 = 0; c0 < tl.nsize; c0 += 16) {
-        float vm[16], vc[16];
-        tmem_ld16(tmem_base + lane_off + (uint32_t)c0, vm);
-        tmem_ld16(tmem_base + lane_off + (uint32_t)(NMAX + c0), vc);
+        // All four accumulators of the chunk are loaded before one wait.
+        uint32_t rc[16], rm[NMAIN][16];
+        tmem_ld16_async(tmem_base + lane_off + (uint32_t)(NMAIN * NMAX + c0), rc);  // corrections
+#pragma unroll
+        for (int g = 0; g < NMAIN; ++g)
+          if (g < nseg) tmem_ld16_async(tmem_base + lane_off + (uint32_t)(g * NMAX + c0), rm[g]);
+        tmem_wait16<true>(rc);
+#pragma unroll
+        for (int g = 0; g < NMAIN; ++g) tmem_wait16<false>(rm[g]);
         if (r < R) {
 #pragma unroll
           for (int i = 0; i < 16; ++i) {
+            float acc = __uint_as_float(rc[i]);
+#pragma unroll
+            for (int g = 0; g < NMAIN; ++g)
+              if (g < nseg) acc += __uint_as_float(rm[g][i]);
             const int x = tl.n0 + c0 + i;
-            if (x < d.X) outb[(int64_t)x * R + r] = (vm[i] + vc[i]) * rs * cs[x];
+            if (x < d.X) outb[(int64_t)x * R + r] = acc * rs * cs[x];
           }
         }
       }
@@ -425,12 +476,14 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(TcArgs a) {
     for (int t = blockIdx.x; t < a.n_tiles; t += gridDim.x) {
       const ShtTcTile tl = a.tiles[t];
       if (tl.kst == 0) continue;
-      const ShtGemmDesc d = a.descs[tl.problem];
-      const float* Db = a.data + d.d_row * R;
+      const TcGroup& G = a.g[tl.group];
+      const ShtGemmDesc d = G.descs[tl.problem];
+      const int64_t R = G.R;
+      const float* Db = G.data + d.d_row * R;
       const int64_t rbase = tl.r0 + mg * 8;
       float sc[8];
 #pragma unroll
-      for (int i = 0; i < 8; ++i) sc[i] = rbase + i < R ? pow2_scale(a.rowmax[rbase + i]) : 1.f;
+      for (int i = 0; i < 8; ++i) sc[i] = rbase + i < R ? pow2_scale(G.rowmax[rbase + i]) : 1.f;
       const bool full_rows = rbase + 8 <= R && (R % 4) == 0;
       bool ok = true;
       for (int ks = 0; ks < tl.kst; ++ks) {
@@ -575,6 +628,7 @@ void build_tc_tables(sht_plan* p, const double* basis64, const double* dbasis64,
                      const double* analysis64, const double* rot64, const double* shear64,
                      cudaStream_t s) {
   ShtTc16* tc = new ShtTc16();
+  tc->tiles = tc_cache_create();
   try {
     int dev = 0;
     SHT_CUDA_OR_THROW(cudaGetDevice(&dev));
@@ -688,60 +742,112 @@ void destroy_tc_tables(sht_plan* p) {
   for (int d = 0; d < 2; ++d) {
     if (tc->d_img_off[d]) cudaFree(tc->d_img_off[d]);
     if (tc->d_cs_off[d]) cudaFree(tc->d_cs_off[d]);
-    if (tc->d_tiles[d]) cudaFree(tc->d_tiles[d]);
   }
+  tc_cache_destroy(tc->tiles);
   delete tc;
   p->tc = nullptr;
 }
 
-void launch_gemm_tc(const sht_plan* p, int direction, int flip, int table_kind, const float* data,
-                    const float* rowmax, float* out, int64_t R, cudaStream_t s) {
-  ShtTc16* tc = p->tc;
-  SHT_REQUIRE(tc != nullptr, "tensor-core tables not built");
-  if (R == 0) return;
-  const int dir = direction;
-  if (tc->tiles_R[dir] != R) {
-    // Tiles: every (problem, n-tile) x every 128-row block, cost-sorted.
-    std::vector<std::pair<int64_t, ShtTcTile>> v;
-    const int np = (int)tc->nt_of[dir].size();
-    for (int i = 0; i < np; ++i) {
-      const int nt = tc->nt_of[dir][i], ns = tc->nsize_of[dir][i], kst = tc->kst_of[dir][i];
-      const int X = p->h_desc[dir][0][i].X;
-      if (X == 0) continue;
-      for (int j = 0; j < nt; ++j)
-        for (int64_t r0 = 0; r0 < R; r0 += BM) {
-          ShtTcTile t{i, j * ns, ns, kst, (int)r0, tc->img_base[dir][i] + j};
-          int64_t cost = (int64_t)ns * kst * BK + 4096;
-          v.push_back({cost, t});
-        }
-    }
-    std::stable_sort(v.begin(), v.end(), [](const auto& a, const auto& b) { return a.first > b.first; });
-    std::vector<ShtTcTile> flat;
-    for (auto& e : v) flat.push_back(e.second);
-    if (tc->d_tiles[dir]) cudaFree(tc->d_tiles[dir]);
-    SHT_CUDA_OR_THROW(cudaMalloc(&tc->d_tiles[dir], sizeof(ShtTcTile) * std::max<size_t>(flat.size(), 1)));
-    SHT_CUDA_OR_THROW(cudaMemcpy(tc->d_tiles[dir], flat.data(), sizeof(ShtTcTile) * flat.size(),
-                                 cudaMemcpyHostToDevice));
-    tc->n_tiles[dir] = (int)flat.size();
-    tc->tiles_R[dir] = R;
+struct TcTileCache {
+  struct List {
+    ShtTcTile* d = nullptr;
+    int n = 0;
+  };
+  // Key: per group (direction, R).  Lists live as long as the cache, so a
+  // launch recorded in a CUDA graph keeps pointing at a live list.
+  std::map<std::vector<int64_t>, List> lists;
+  std::mutex mu;
+};
+
+TcTileCache* tc_cache_create() { return new TcTileCache(); }
+
+void tc_cache_destroy(TcTileCache* c) {
+  if (!c) return;
+  for (auto& e : c->lists) cudaFree(e.second.d);
+  delete c;
+}
+
+TcTileCache* tc_plan_cache(const sht_plan* p) { return p->tc ? p->tc->tiles : nullptr; }
+
+void launch_gemm_tc_groups(const TcGroupSpec* g, int ngroups, TcTileCache* cache, cudaStream_t s) {
+  SHT_REQUIRE(ngroups >= 1 && ngroups <= kMaxTcGroups, "tensor-core launch: 1 to 4 groups");
+  SHT_REQUIRE(cache != nullptr, "tensor-core launch: no tile cache");
+  std::vector<int64_t> key;
+  int64_t rows = 0;
+  for (int i = 0; i < ngroups; ++i) {
+    SHT_REQUIRE(g[i].plan->tc != nullptr, "tensor-core tables not built");
+    key.push_back(g[i].direction);
+    key.push_back(g[i].R);
+    rows += g[i].R;
   }
-  if (tc->n_tiles[dir] == 0) return;
+  if (rows == 0) return;
+  TcTileCache::List list;
+  {
+    std::lock_guard<std::mutex> lock(cache->mu);
+    auto found = cache->lists.find(key);
+    if (found == cache->lists.end()) {
+      // Tiles: every (group, problem, n-tile) x every 128-row block, merged
+      // over the groups and sorted by descending cost.
+      std::vector<std::pair<int64_t, ShtTcTile>> v;
+      for (int gi = 0; gi < ngroups; ++gi) {
+        const sht_plan* p = g[gi].plan;
+        const ShtTc16* tc = p->tc;
+        const int dir = g[gi].direction;
+        const int np = (int)tc->nt_of[dir].size();
+        for (int i = 0; i < np; ++i) {
+          const int nt = tc->nt_of[dir][i], ns = tc->nsize_of[dir][i], kst = tc->kst_of[dir][i];
+          if (p->h_desc[dir][0][i].X == 0) continue;
+          for (int j = 0; j < nt; ++j)
+            for (int64_t r0 = 0; r0 < g[gi].R; r0 += BM) {
+              ShtTcTile t{gi, i, j * ns, ns, kst, (int)r0, tc->img_base[dir][i] + j};
+              v.push_back({(int64_t)ns * kst * BK + 4096, t});
+            }
+        }
+      }
+      std::stable_sort(v.begin(), v.end(),
+                       [](const auto& a, const auto& b) { return a.first > b.first; });
+      std::vector<ShtTcTile> flat;
+      flat.reserve(v.size());
+      for (auto& e : v) flat.push_back(e.second);
+      TcTileCache::List fresh;
+      SHT_CUDA_OR_THROW(cudaMalloc(&fresh.d, sizeof(ShtTcTile) * std::max<size_t>(flat.size(), 1)));
+      SHT_CUDA_OR_THROW(cudaMemcpy(fresh.d, flat.data(), sizeof(ShtTcTile) * flat.size(),
+                                   cudaMemcpyHostToDevice));
+      fresh.n = (int)flat.size();
+      found = cache->lists.emplace(key, fresh).first;
+    }
+    list = found->second;
+  }
+  if (list.n == 0) return;
   TcArgs a{};
-  a.descs = p->d_desc[dir][flip];
-  a.tiles = tc->d_tiles[dir];
-  a.n_tiles = tc->n_tiles[dir];
-  a.img = (const unsigned char*)tc->img[table_kind];
-  a.img_off = tc->d_img_off[dir];
-  a.colscale = tc->colscale[table_kind];
-  a.cs_off = tc->d_cs_off[dir];
-  a.data = data;
-  a.rowmax = rowmax;
-  a.out = out;
-  a.R = R;
-  a.err = p->d_err;
-  const int grid = std::min(tc->n_tiles[dir], tc->sm_count);
+  for (int gi = 0; gi < ngroups; ++gi) {
+    const sht_plan* p = g[gi].plan;
+    const ShtTc16* tc = p->tc;
+    const int dir = g[gi].direction;
+    TcGroup& G = a.g[gi];
+    G.descs = p->d_desc[dir][g[gi].flip];
+    G.img = (const unsigned char*)tc->img[g[gi].table_kind];
+    G.img_off = tc->d_img_off[dir];
+    G.colscale = tc->colscale[g[gi].table_kind];
+    G.cs_off = tc->d_cs_off[dir];
+    G.data = g[gi].data;
+    G.rowmax = g[gi].rowmax;
+    G.out = g[gi].out;
+    G.R = g[gi].R;
+  }
+  a.tiles = list.d;
+  a.n_tiles = list.n;
+  a.err = g[0].plan->d_err;
+  const int grid = std::min(list.n, g[0].plan->tc->sm_count);
   tc_gemm_kernel<<<grid, kThreads, kSmemBytes, s>>>(a);
   SHT_CUDA_OR_THROW(cudaGetLastError());
+}
+
+void launch_gemm_tc(const sht_plan* p, int direction, int flip, int table_kind, const float* data,
+                    const float* rowmax, float* out, int64_t R, cudaStream_t s) {
+  SHT_REQUIRE(p->tc != nullptr, "tensor-core tables not built");
+  TcGroupSpec g{p, direction, flip, table_kind, data, rowmax, out, R};
+  launch_gemm_tc_groups(&g, 1, p->tc->tiles, s);
 }
 
 }  // namespace sht

@@ -176,4 +176,22 @@ void launch_gemm_tc(const sht_plan* p, int direction, int flip, int table_kind,
                     const float* data, const float* rowmax, float* out, int64_t R,
                     cudaStream_t s);
 
+// Several contractions in one persistent tensor-core launch (the two tables
+// of a gradient, wind or vordiv call; the plans of a batch).
+constexpr int kMaxTcGroups = 4;
+struct TcGroupSpec {
+  const sht_plan* plan;
+  int direction, flip, table_kind;
+  const float* data;
+  const float* rowmax;
+  float* out;
+  int64_t R;
+};
+struct TcTileCache;  // merged tile lists, keyed by the groups' (direction, R)
+TcTileCache* tc_cache_create();
+void tc_cache_destroy(TcTileCache* c);
+TcTileCache* tc_plan_cache(const sht_plan* p);  // the plan's own tile lists
+void launch_gemm_tc_groups(const TcGroupSpec* groups, int ngroups, TcTileCache* cache,
+                           cudaStream_t s);
+
 }  // namespace sht

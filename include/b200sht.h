@@ -46,6 +46,8 @@ extern "C" {
 #define SHT_ERR_STATE 4    /* plan in an unusable state */
 
 typedef struct sht_plan sht_plan;
+typedef struct sht_vertical sht_vertical;
+typedef struct sht_batch sht_batch;
 
 /* ABI version of the loaded library (SHT_ABI_VERSION). */
 int sht_abi_version(void);
@@ -174,6 +176,44 @@ int sht_helmholtz_solve(sht_plan* plan, int nlev, const double* b, const double*
                         const void* divergence, const void* theta, const void* lnps,
                         void* out_divergence, void* out_theta, void* out_lnps,
                         void* stream);
+
+/* The same solve with the vertical operator kept on the device.  The
+ * reference builds its VerticalStructureOperator once per run and its
+ * per-(dt, alpha) inverse once per stage weight (semi_implicit.py:585-609,
+ * 887-919); sht_vertical_create uploads B, C, V, V^-1 and the eigenvalues
+ * (same host layout as sht_helmholtz_solve) once, in the plan's arithmetic
+ * type.  sht_helmholtz_apply then does no allocation, no host copy and no
+ * synchronisation, so it can be recorded in a CUDA graph.  An operator
+ * serves plans of the same device and precision as the one it was created
+ * with. */
+int sht_vertical_create(sht_plan* plan, int nlev, const double* b, const double* c,
+                        const double* eigvec, const double* eigvec_inv,
+                        const double* eigenvalues, sht_vertical** out);
+int sht_vertical_destroy(sht_vertical* op);
+int sht_helmholtz_apply(sht_plan* plan, const sht_vertical* op, double tau_w,
+                        const void* divergence, const void* theta, const void* lnps,
+                        void* out_divergence, void* out_theta, void* out_lnps, void* stream);
+
+/* Batches: up to 4 plans (for instance 32 ensemble members at T126 as one
+ * plan of 32 x 200 planes, and the T255 control as another) transformed as
+ * one call.  The reference runs each member and truncation through its own
+ * transform object (src/arwen_global/spectral/transform.py:1435-1490 and
+ * 1629-1746 per call); here the Legendre contractions of all plans run in
+ * ONE launch per direction: on SHT_PREC_SPLIT16 plans the persistent
+ * tensor-core kernel walks the merged work list of every plan sorted by the
+ * triangular per-order cost; F32/F64 plans run one SIMT launch per plan.
+ * The FFT, pack and unpack launches stay per plan.  planes[i] is the plane
+ * count of plan i (fixed for the batch); the arrays of plan i are laid out
+ * as in sht_forward / sht_inverse.  The plans must be distinct, share one
+ * device and one precision, and outlive the batch; a plan must not be used
+ * by another call while a batch call that holds it is in flight. */
+int sht_batch_create(int nplans, sht_plan* const* plans, const int64_t* planes,
+                     sht_batch** out);
+int sht_batch_destroy(sht_batch* batch);
+int sht_batch_forward(sht_batch* batch, const void* const* grids, void* const* coeffs,
+                      void* stream);
+int sht_batch_inverse(sht_batch* batch, const void* const* coeffs, void* const* grids,
+                      void* stream);
 
 #ifdef __cplusplus
 }
