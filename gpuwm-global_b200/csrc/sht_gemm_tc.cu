@@ -102,7 +102,8 @@ constexpr int kOffB = kOffA + STAGES * NPARTS * kAPart;    // [STAGES][NPARTS][k
 constexpr int kOffBar = kOffB + STAGES * NPARTS * kBPart;  // mbarriers (8 B each)
 constexpr int kNumBars = 3 * STAGES + 2 + 1;
 constexpr int kOffMisc = kOffBar + kNumBars * 8;           // tmem base, abort flag
-constexpr int kSmemBytes = kOffMisc + 16 + 1024;           // + alignment slack
+constexpr int kOffCs = kOffMisc + 16;                      // [4 epilogue warps][NMAX] floats
+constexpr int kSmemBytes = kOffCs + 4 * NMAX * 4 + 1024;   // + alignment slack
 static_assert(kSmemBytes <= 227 * 1024, "shared memory plan exceeds 227 KB");
 
 // ---------------------------------------------------------------- PTX
@@ -412,6 +413,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
     // ----------------------------------------------------------- epilogue
     const int eg = warp & 3;  // TMEM lane group accessible to this warp
     const int row = eg * 32 + lane;
+    float* cs_s = reinterpret_cast<float*>(smem + kOffCs) + eg * NMAX;  // this warp's copy
     uint32_t acc_phase = 0;
     // The wait outcome is made warp-uniform (__any_sync) before the
     // warp-collective tcgen05.ld.
@@ -428,11 +430,23 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
           for (int x = tl.n0; x < min(tl.n0 + tl.nsize, d.X); ++x) outb[(int64_t)x * R + r] = 0.f;
         continue;
       }
+      // The tile's row and column scales are fetched while the MMAs run: the
+      // column scales into this warp's shared copy (one L2 round trip per
+      // tile instead of one per 16-column chunk).
+      const float rs = r < R ? 1.f / pow2_scale(G.rowmax[r]) : 0.f;
+      {
+        const float* cs = G.colscale + G.cs_off[tl.problem];
+        __syncwarp();  // the previous tile's reads of cs_s are done
+#pragma unroll
+        for (int j = 0; j < NMAX / 32; ++j) {
+          const int c = j * 32 + lane;
+          cs_s[c] = (c < tl.nsize && tl.n0 + c < d.X) ? cs[tl.n0 + c] : 0.f;
+        }
+        __syncwarp();
+      }
       const bool failed = !wait_bar(pp.acc_full, acc_phase, pp, a.err, 5);
       if (__any_sync(0xffffffffu, failed)) break;
       tc_fence_after();
-      const float rs = r < R ? 1.f / pow2_scale(G.rowmax[r]) : 0.f;
-      const float* cs = G.colscale + G.cs_off[tl.problem];
       const uint32_t lane_off = (uint32_t)(eg * 32) << 16;
       // A tile with fewer K steps than NMAIN leaves the last main
       // accumulators unwritten: only the segments that exist are read.
@@ -456,7 +470,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
             for (int g = 0; g < NMAIN; ++g)
               if (g < nseg) acc += __uint_as_float(rm[g][i]);
             const int x = tl.n0 + c0 + i;
-            if (x < d.X) outb[(int64_t)x * R + r] = acc * rs * cs[x];
+            if (x < d.X) outb[(int64_t)x * R + r] = acc * rs * cs_s[c0 + i];
           }
         }
       }
