@@ -84,7 +84,7 @@ namespace {
 
 constexpr int BM = 128;
 constexpr int BK = 32;
-constexpr int STAGES = 6;
+constexpr int STAGES = 4;
 constexpr int NPARTS = 2;
 constexpr int NMAIN = 3;    // main-product accumulators (contiguous K segments)
 constexpr int NMAX = 128;   // tile N; TMEM: (NMAIN + 1) x NMAX = 512 columns
@@ -103,7 +103,8 @@ constexpr int kOffBar = kOffB + STAGES * NPARTS * kBPart;  // mbarriers (8 B eac
 constexpr int kNumBars = 3 * STAGES + 2 + 1;
 constexpr int kOffMisc = kOffBar + kNumBars * 8;           // tmem base, abort flag
 constexpr int kOffCs = kOffMisc + 16;                      // [4 epilogue warps][NMAX] floats
-constexpr int kSmemBytes = kOffCs + 4 * NMAX * 4 + 1024;   // + alignment slack
+constexpr int kOffStage = (kOffCs + 4 * NMAX * 4 + 127) / 128 * 128;  // staging [NMAX][BM] floats
+constexpr int kSmemBytes = kOffStage + NMAX * BM * 4 + 1024;  // + alignment slack
 static_assert(kSmemBytes <= 227 * 1024, "shared memory plan exceeds 227 KB");
 
 // ---------------------------------------------------------------- PTX
@@ -142,6 +143,33 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
 __device__ __forceinline__ void fence_proxy_async() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
+// Bulk shared -> global store of one staged output row, tracked by the
+// issuing thread's bulk group.
+__device__ __forceinline__ void bulk_s2g(void* dst, const void* src, uint32_t bytes) {
+  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst),
+               "r"(smem_u32(src)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+// The committed bulk stores have finished reading shared memory.
+__device__ __forceinline__ void bulk_wait_read() {
+  asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+}
+// The committed bulk stores have completed.
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+// Named barrier 1 over the four epilogue warps; returns the OR of `pred`
+// over their 128 threads.
+__device__ __forceinline__ bool epi_bar_or(bool pred) {
+  uint32_t out;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\tsetp.ne.u32 q, %1, 0;\n\tbar.red.or.pred p, 1, 128, q;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(out)
+      : "r"((uint32_t)pred)
+      : "memory");
+  return out != 0;
+}
+__device__ __forceinline__ void epi_bar() { asm volatile("bar.sync 1, 128;" ::: "memory"); }
 __device__ __forceinline__ void fence_barrier_init() {
   asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 }
@@ -411,12 +439,19 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
     }
   } else if (warp < kConvWarp0) {
     // ----------------------------------------------------------- epilogue
+    // Per tile: TMEM -> registers -> scaled values in the staging buffer
+    // [column][row].  The accumulator goes back to the MMA warp as soon as the
+    // staging is written; the staged columns (one output row x each, the data
+    // rows r contiguous) then leave as bulk shared->global stores, one per
+    // thread, which run while the next tile's MMAs do.  Every decision that
+    // steers the epilogue's named barrier is reduced over its four warps
+    // (epi_bar_or), so all 128 threads take the same path, and the
+    // warp-collective tcgen05.ld is entered warp-uniformly.
     const int eg = warp & 3;  // TMEM lane group accessible to this warp
     const int row = eg * 32 + lane;
     float* cs_s = reinterpret_cast<float*>(smem + kOffCs) + eg * NMAX;  // this warp's copy
+    float* stage_s = reinterpret_cast<float*>(smem + kOffStage);
     uint32_t acc_phase = 0;
-    // The wait outcome is made warp-uniform (__any_sync) before the
-    // warp-collective tcgen05.ld.
     for (int t = blockIdx.x; t < a.n_tiles; t += gridDim.x) {
       const ShtTcTile tl = a.tiles[t];
       const TcGroup& G = a.g[tl.group];
@@ -445,7 +480,8 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
         __syncwarp();
       }
       const bool failed = !wait_bar(pp.acc_full, acc_phase, pp, a.err, 5);
-      if (__any_sync(0xffffffffu, failed)) break;
+      bulk_wait_read();  // this thread's stores of the previous tile have read the staging
+      if (epi_bar_or(failed)) break;
       tc_fence_after();
       const uint32_t lane_off = (uint32_t)(eg * 32) << 16;
       // A tile with fewer K steps than NMAIN leaves the last main
@@ -462,22 +498,36 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
         tmem_wait16<true>(rc);
 #pragma unroll
         for (int g = 0; g < NMAIN; ++g) tmem_wait16<false>(rm[g]);
-        if (r < R) {
 #pragma unroll
-          for (int i = 0; i < 16; ++i) {
-            float acc = __uint_as_float(rc[i]);
+        for (int i = 0; i < 16; ++i) {
+          float acc = __uint_as_float(rc[i]);
 #pragma unroll
-            for (int g = 0; g < NMAIN; ++g)
-              if (g < nseg) acc += __uint_as_float(rm[g][i]);
-            const int x = tl.n0 + c0 + i;
-            if (x < d.X) outb[(int64_t)x * R + r] = acc * rs * cs_s[c0 + i];
-          }
+          for (int g = 0; g < NMAIN; ++g)
+            if (g < nseg) acc += __uint_as_float(rm[g][i]);
+          stage_s[(c0 + i) * BM + row] = acc * rs * cs_s[c0 + i];
         }
       }
       tc_fence_before();
       mbar_arrive(pp.acc_empty);
       acc_phase ^= 1;
+      fence_proxy_async();  // the staging writes, visible to the bulk-copy proxy
+      epi_bar();
+      const int ncols = min(tl.nsize, d.X - tl.n0);
+      if ((R & 3) == 0) {
+        // 16-byte aligned rows: thread `row` sends staged column `row`.
+        if (row < ncols) {
+          const int64_t nrows = R - tl.r0 < BM ? R - tl.r0 : (int64_t)BM;
+          bulk_s2g(outb + (int64_t)(tl.n0 + row) * R + tl.r0, stage_s + row * BM,
+                   (uint32_t)(nrows * 4));
+        }
+        bulk_commit();
+      } else if (r < R) {
+        // Row lengths that are not a multiple of 4 floats: plain stores of
+        // this thread's own row.
+        for (int c = 0; c < ncols; ++c) outb[(int64_t)(tl.n0 + c) * R + r] = stage_s[c * BM + row];
+      }
     }
+    bulk_wait_all();
   } else {
     // --------------------------------------------------------- converters
     // Thread -> (kk = ct % 8, 8-row group mg = (ct/8) % 16), K groups
