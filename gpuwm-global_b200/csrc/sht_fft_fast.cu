@@ -314,7 +314,7 @@ __global__ void __launch_bounds__(kWarps * 32) fast_inverse_unfold(FastUnfoldArg
   // Each thread first issues the waist loads of kBatch items (NF symmetric /
   // antisymmetric pairs each), then combines them: the loads of a batch are
   // in flight together instead of one dependent round trip per item.
-  constexpr int kBatch = 4;
+  constexpr int kBatch = NF == 4 ? 2 : 4;
   const int total = (a.T + 1) * a.G;
   for (int base = threadIdx.x; base < total; base += kBatch * blockDim.x) {
     float2 S[kBatch][NF], D[kBatch][NF];
