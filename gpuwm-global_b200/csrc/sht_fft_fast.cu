@@ -157,22 +157,35 @@ __device__ __forceinline__ void dft32(float2* v) {
 }
 
 // Per-warp shared region: F rows of 33 (the transpose), reused as the
-// natural-order spectrum of L = 32 F entries.
+// natural-order spectrum of L = 32 F entries.  Regions are padded to 2 float2
+// modulo 8, so that the fold/unfold loops, in which lanes 4j..4j+3 touch the
+// same order m of four different rows, hit four distinct bank groups.
 template <int F> struct WarpSmem {
   static constexpr int kStride = 33;
-  static constexpr int kFloats2 = F * kStride;
+  static constexpr int kFloats2 = F * kStride + ((2 - (F * kStride) % 8) + 8) % 8;
 };
+
+// The four-step twiddles exp(-2 pi i l k1 / L) of every lane l, as a shared
+// table [k1][32]: a warp's read of one k1 is 32 consecutive entries (two
+// wavefronts), where reading them from the length-L table in global memory
+// touched up to F * 8 different cache lines per instruction.
+template <int F>
+__device__ __forceinline__ void load_lane_twiddles(float2* tws, const float2* __restrict__ twL) {
+  constexpr int L = 32 * F;
+  for (int e = threadIdx.x; e < F * 32; e += blockDim.x) {
+    const int k1 = e >> 5, l = e & 31;
+    tws[e] = twL[(l * k1) % L];
+  }
+}
 
 // The L-point complex FFT of one warp's row: in registers z[j] = x[l + 32 j]
 // (lane l); out: the natural-order spectrum written to `reg` (length L).
 template <int F, bool INV>
-__device__ __forceinline__ void warp_fft(float2 (&z)[F], float2* reg, const float2* __restrict__ twL,
-                                         int lane) {
-  constexpr int L = 32 * F;
+__device__ __forceinline__ void warp_fft(float2 (&z)[F], float2* reg, const float2* tws, int lane) {
   dftF<F, INV>(z);
   // exp(-+2 pi i lane k1 / L)
 #pragma unroll
-  for (int k1 = 1; k1 < F; ++k1) z[k1] = cmulf(z[k1], tw<INV>(twL[(lane * k1) % L]));
+  for (int k1 = 1; k1 < F; ++k1) z[k1] = cmulf(z[k1], tw<INV>(tws[k1 * 32 + lane]));
 #pragma unroll
   for (int k1 = 0; k1 < F; ++k1) reg[k1 * WarpSmem<F>::kStride + lane] = z[k1];
   __syncwarp();
@@ -195,10 +208,10 @@ __device__ __forceinline__ void warp_fft(float2 (&z)[F], float2* reg, const floa
 // hemisphere rows (8 rows).
 constexpr int kWarps = 8;
 
-// An opaque copy of a pointer.  The FFT kernels read their twiddles through
-// it, so the compiler cannot hoist a whole row of twiddle loads into
-// registers ahead of the butterflies (which costs ~20 registers per thread,
-// one resident CTA per SM).
+// An opaque copy of a pointer.  The inverse kernel reads its entangling
+// twiddles through it, so the compiler cannot hoist a whole row of them into
+// registers ahead of the butterflies (~20 registers per thread, one resident
+// CTA per SM fewer).
 __device__ __forceinline__ const float2* opaque(const float2* p) {
   asm volatile("" : "+l"(p));
   return p;
@@ -232,6 +245,9 @@ __global__ void __launch_bounds__(kWarps * 32) fast_forward_fold(FastFoldArgs a,
   const int64_t plane = p0 + gp;
   const bool active = pf < nper && plane < a.planes && !(eq && side == 1);
   float2* reg = smem(warp);
+  float2* tws = smem_dyn + kWarps * WarpSmem<FF>::kFloats2;
+  load_lane_twiddles<FF>(tws, twL);
+  __syncthreads();
   if (active) {
     const int j = side ? (a.nlat - 1 - h) : h;
     const float2* src =
@@ -239,7 +255,7 @@ __global__ void __launch_bounds__(kWarps * 32) fast_forward_fold(FastFoldArgs a,
     float2 z[FF];
 #pragma unroll
     for (int i = 0; i < FF; ++i) z[i] = __ldg(src + lane + 32 * i);
-    warp_fft<FF, false>(z, reg, opaque(twL), lane);
+    warp_fft<FF, false>(z, reg, tws, lane);
   }
   __syncthreads();
   // Untangle, scale, fold, write: thread -> (m, pf) with pf fastest.
@@ -310,6 +326,8 @@ __global__ void __launch_bounds__(kWarps * 32) fast_inverse_unfold(FastUnfoldArg
   const float inv_a = 1.0f / a.radius;
   const int jrow[2] = {h, a.nlat - 1 - h};
 
+  float2* tws = smem_dyn + kWarps * WarpSmem<FF>::kFloats2;
+  load_lane_twiddles<FF>(tws, twL);
   // Stage 1: Fourier coefficients of every output row into smem[row][m].
   // Each thread first issues the waist loads of kBatch items (NF symmetric /
   // antisymmetric pairs each), then combines them: the loads of a batch are
@@ -386,7 +404,7 @@ __global__ void __launch_bounds__(kWarps * 32) fast_inverse_unfold(FastUnfoldArg
     z[i] = make_float2(s.x - wd.y, s.y + wd.x);
   }
   __syncwarp();
-  warp_fft<FF, true>(z, reg, opaque(twL), lane);
+  warp_fft<FF, true>(z, reg, tws, lane);
   // Stage 3: natural-order z[n] -> x[2n], x[2n+1] with the row scaling.
   const int j = jrow[side];
   // The gradient divides the grid by (a cos phi) and by a, as the reference does.
@@ -407,7 +425,7 @@ void launch_fwd(const sht_plan* p, const float* g0, const float* g1, int64_t pla
   FastFoldArgs a{p->nlat, p->nlon, p->T, p->H, p->nlat_odd ? 1 : 0, g1 ? 2 : 1, 0, planes};
   a.G = kWarps / 2 / a.F;
   dim3 grid((unsigned)p->H, (unsigned)div_up(planes, a.G));
-  const size_t sm = sizeof(float2) * kWarps * WarpSmem<FF>::kFloats2;
+  const size_t sm = sizeof(float2) * (kWarps * WarpSmem<FF>::kFloats2 + FF * 32);
   SHT_CUDA_OR_THROW(cudaFuncSetAttribute(fast_forward_fold<FF>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
   fast_forward_fold<FF><<<grid, kWarps * 32, sm, s>>>(a, g0, g1 ? g1 : g0, (const float2*)p->tw_l,
@@ -423,7 +441,7 @@ void launch_inv_nf(const sht_plan* p, int mode, const float* wP, const float* wD
   FastUnfoldArgs a{p->nlat, p->nlon, p->T, p->H, p->nlat_odd ? 1 : 0, mode, kWarps / 2 / NO,
                    planes, (float)p->radius};
   dim3 grid((unsigned)p->H, (unsigned)div_up(planes, a.G));
-  const size_t sm = sizeof(float2) * kWarps * WarpSmem<FF>::kFloats2;
+  const size_t sm = sizeof(float2) * (kWarps * WarpSmem<FF>::kFloats2 + FF * 32);
   SHT_CUDA_OR_THROW(cudaFuncSetAttribute(fast_inverse_unfold<FF, NF>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
   fast_inverse_unfold<FF, NF><<<grid, kWarps * 32, sm, s>>>(
