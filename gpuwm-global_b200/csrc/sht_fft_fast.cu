@@ -236,8 +236,10 @@ __global__ void __launch_bounds__(kWarps * 32) fast_forward_fold(FastFoldArgs a,
   extern __shared__ float2 smem_dyn[];
   auto smem = [&](int w) { return smem_dyn + w * WarpSmem<FF>::kFloats2; };
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int h = blockIdx.x;
-  const int64_t p0 = (int64_t)blockIdx.y * a.G;
+  // Plane blocks vary fastest over the grid: CTAs that run together touch
+  // adjacent slices of every waist row.
+  const int h = blockIdx.y;
+  const int64_t p0 = (int64_t)blockIdx.x * a.G;
   const bool eq = a.nlat_odd && h == a.H - 1;
   const int pf = warp >> 1, side = warp & 1;
   const int nper = a.G * a.F;
@@ -254,7 +256,7 @@ __global__ void __launch_bounds__(kWarps * 32) fast_forward_fold(FastFoldArgs a,
         reinterpret_cast<const float2*>((f ? g1 : g0) + (plane * a.nlat + j) * (int64_t)a.nlon);
     float2 z[FF];
 #pragma unroll
-    for (int i = 0; i < FF; ++i) z[i] = __ldg(src + lane + 32 * i);
+    for (int i = 0; i < FF; ++i) z[i] = __ldcs(src + lane + 32 * i);
     warp_fft<FF, false>(z, reg, tws, lane);
   }
   __syncthreads();
@@ -284,8 +286,8 @@ __global__ void __launch_bounds__(kWarps * 32) fast_forward_fold(FastFoldArgs a,
     float2 S = eq ? X[0] : caddf(X[0], X[1]);
     float2 D = eq ? make_float2(0.f, 0.f) : csubf(X[0], X[1]);
     int64_t col = p0 * a.F + q;
-    wfold[((int64_t)(m * 2 + 0) * a.H + h) * Rc + col] = S;
-    wfold[((int64_t)(m * 2 + 1) * a.H + h) * Rc + col] = D;
+    __stcs(&wfold[((int64_t)(m * 2 + 0) * a.H + h) * Rc + col], S);
+    __stcs(&wfold[((int64_t)(m * 2 + 1) * a.H + h) * Rc + col], D);
     mre = fmaxf(mre, fmaxf(fabsf(S.x), fabsf(D.x)));
     mim = fmaxf(mim, fmaxf(fabsf(S.y), fabsf(D.y)));
   }
@@ -319,8 +321,10 @@ __global__ void __launch_bounds__(kWarps * 32) fast_inverse_unfold(FastUnfoldArg
   extern __shared__ float2 smem_dyn[];
   auto smem = [&](int w) { return smem_dyn + w * WarpSmem<FF>::kFloats2; };
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int h = blockIdx.x;
-  const int64_t p0 = (int64_t)blockIdx.y * a.G;
+  // Plane blocks vary fastest over the grid: CTAs that run together touch
+  // adjacent slices of every waist row.
+  const int h = blockIdx.y;
+  const int64_t p0 = (int64_t)blockIdx.x * a.G;
   const bool eq = a.nlat_odd && h == a.H - 1;
   const int64_t Rc = a.planes * (NF == 4 ? 2 : 1);
   const float inv_a = 1.0f / a.radius;
@@ -348,8 +352,8 @@ __global__ void __launch_bounds__(kWarps * 32) fast_inverse_unfold(FastUnfoldArg
         for (int k = 0; k < NF; ++k) {
           const float2* w = (NF == 1 || k < NF / 2) ? wP : wD;
           const int fld = NF == 4 ? (k & 1) : 0;
-          S[u][k] = w[c0 + fld];
-          D[u][k] = w[c1 + fld];
+          S[u][k] = __ldcs(w + c0 + fld);
+          D[u][k] = __ldcs(w + c1 + fld);
         }
       }
     }
@@ -415,7 +419,7 @@ __global__ void __launch_bounds__(kWarps * 32) fast_inverse_unfold(FastUnfoldArg
   for (int i = 0; i < FF; ++i) {
     float2 v = reg[lane + 32 * i];
     if (divide) v = make_float2(v.x / den, v.y / den);
-    dst[lane + 32 * i] = v;
+    __stcs(dst + lane + 32 * i, v);
   }
 }
 
@@ -424,7 +428,7 @@ void launch_fwd(const sht_plan* p, const float* g0, const float* g1, int64_t pla
                 cudaStream_t s, float* rowmax) {
   FastFoldArgs a{p->nlat, p->nlon, p->T, p->H, p->nlat_odd ? 1 : 0, g1 ? 2 : 1, 0, planes};
   a.G = kWarps / 2 / a.F;
-  dim3 grid((unsigned)p->H, (unsigned)div_up(planes, a.G));
+  dim3 grid((unsigned)div_up(planes, a.G), (unsigned)p->H);
   const size_t sm = sizeof(float2) * (kWarps * WarpSmem<FF>::kFloats2 + FF * 32);
   SHT_CUDA_OR_THROW(cudaFuncSetAttribute(fast_forward_fold<FF>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
@@ -440,7 +444,7 @@ void launch_inv_nf(const sht_plan* p, int mode, const float* wP, const float* wD
   constexpr int NO = NF == 1 ? 1 : 2;
   FastUnfoldArgs a{p->nlat, p->nlon, p->T, p->H, p->nlat_odd ? 1 : 0, mode, kWarps / 2 / NO,
                    planes, (float)p->radius};
-  dim3 grid((unsigned)p->H, (unsigned)div_up(planes, a.G));
+  dim3 grid((unsigned)div_up(planes, a.G), (unsigned)p->H);
   const size_t sm = sizeof(float2) * (kWarps * WarpSmem<FF>::kFloats2 + FF * 32);
   SHT_CUDA_OR_THROW(cudaFuncSetAttribute(fast_inverse_unfold<FF, NF>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
