@@ -25,47 +25,66 @@ __device__ __forceinline__ int64_t cf_row(int T, int m, int q, int i) {
   return base + (q ? parity_count(T, m, 0) : 0) + i;
 }
 
+// One CTA: 32 orders x NB degrees x 32 planes.  All NB x 4 loads of a thread
+// are issued before the CTA's one barrier, and the row maxima are merged over
+// the whole block before one atomic per column.
+template <typename T> struct PackCfg { static constexpr int NB = sizeof(T) == 4 ? 4 : 2; };
+
 template <typename T>
-__global__ void pack_kernel(int Tn, double radius, int mode, const V2<T>* __restrict__ c0,
-                            const V2<T>* __restrict__ c1, int64_t planes, int F,
-                            V2<T>* __restrict__ cf, float* __restrict__ rowmax) {
-  __shared__ V2<T> tile[32][33];
+__global__ void __launch_bounds__(256) pack_kernel(int Tn, double radius, int mode,
+                                                   const V2<T>* __restrict__ c0,
+                                                   const V2<T>* __restrict__ c1, int64_t planes,
+                                                   int F, V2<T>* __restrict__ cf,
+                                                   float* __restrict__ rowmax) {
+  constexpr int NB = PackCfg<T>::NB;
+  __shared__ V2<T> tile[NB][32][33];
   __shared__ float red[2][8][32];
   const int m0 = blockIdx.x * 32;
-  const int n = blockIdx.y;
-  if (m0 > n) return;
+  const int n0 = blockIdx.y * NB;
+  if (m0 > n0 + NB - 1 || n0 > Tn) return;  // the whole block is above the triangle
   const int f = blockIdx.z % F;
   const int64_t p0 = (int64_t)(blockIdx.z / F) * 32;
   const V2<T>* src = f ? c1 : c0;
   const int tx = threadIdx.x, ty = threadIdx.y;
   const int64_t t1 = Tn + 1;
-  const T eig = T(-((double)n * ((double)n + 1.0)) / (radius * radius));
-  for (int pp = ty; pp < 32; pp += 8) {
-    int64_t p = p0 + pp;
-    int m = m0 + tx;
-    V2<T> v = mk2<T>(T(0), T(0));
-    if (p < planes && m <= n) v = src[(p * t1 + n) * t1 + m];
-    tile[pp][tx] = v;
+#pragma unroll
+  for (int nb = 0; nb < NB; ++nb) {
+    const int n = n0 + nb;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const int pp = ty + 8 * k;
+      const int64_t p = p0 + pp;
+      const int m = m0 + tx;
+      V2<T> v = mk2<T>(T(0), T(0));
+      if (p < planes && n <= Tn && m <= n) v = __ldcs(src + (p * t1 + n) * t1 + m);
+      tile[nb][pp][tx] = v;
+    }
   }
   __syncthreads();
   const int64_t Rc = planes * F;
+  const int64_t p = p0 + tx;
   float mre = 0.f, mim = 0.f;
-  for (int mm = ty; mm < 32; mm += 8) {
-    int m = m0 + mm;
-    if (m > n) break;
-    int q = (n - m) & 1, i = (n - m) >> 1;
-    int64_t row = cf_row(Tn, m, q, i);
-    int64_t p = p0 + tx;
-    if (p < planes) {
-      V2<T> v = tile[tx][mm];
-      if (mode == kPackInvLap) {
-        // c / eig (complex by real), zero at degree 0
-        v = n == 0 ? mk2<T>(T(0), T(0)) : mk2<T>(v.x / eig, v.y / eig);
-        if (m == 0) v.y = T(0);  // project() inside inverse_laplacian
+  if (p < planes) {
+#pragma unroll
+    for (int nb = 0; nb < NB; ++nb) {
+      const int n = n0 + nb;
+      if (n > Tn) break;
+      const T eig = T(-((double)n * ((double)n + 1.0)) / (radius * radius));
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const int m = m0 + ty + 8 * k;
+        if (m > n) break;
+        const int q = (n - m) & 1, i = (n - m) >> 1;
+        V2<T> v = tile[nb][tx][ty + 8 * k];
+        if (mode == kPackInvLap) {
+          // c / eig (complex by real), zero at degree 0
+          v = n == 0 ? mk2<T>(T(0), T(0)) : mk2<T>(v.x / eig, v.y / eig);
+          if (m == 0) v.y = T(0);  // project() inside inverse_laplacian
+        }
+        cf[cf_row(Tn, m, q, i) * Rc + p * F + f] = v;
+        mre = fmaxf(mre, (float)fabs(v.x));
+        mim = fmaxf(mim, (float)fabs(v.y));
       }
-      cf[row * Rc + p * F + f] = v;
-      mre = fmaxf(mre, (float)fabs(v.x));
-      mim = fmaxf(mim, (float)fabs(v.y));
     }
   }
   if (rowmax != nullptr) {
@@ -73,72 +92,84 @@ __global__ void pack_kernel(int Tn, double radius, int mode, const V2<T>* __rest
     red[0][ty][tx] = mre;
     red[1][ty][tx] = mim;
     __syncthreads();
-    if (ty == 0 && p0 + tx < planes) {
-      float a = 0.f, b = 0.f;
+    if (ty == 0 && p < planes) {
+      float ra = 0.f, rb = 0.f;
       for (int k = 0; k < 8; ++k) {
-        a = fmaxf(a, red[0][k][tx]);
-        b = fmaxf(b, red[1][k][tx]);
+        ra = fmaxf(ra, red[0][k][tx]);
+        rb = fmaxf(rb, red[1][k][tx]);
       }
-      const int64_t col = (p0 + tx) * F + f;
-      atomicMax(reinterpret_cast<int*>(rowmax + 2 * col), __float_as_int(a));
-      atomicMax(reinterpret_cast<int*>(rowmax + 2 * col + 1), __float_as_int(b));
+      const int64_t col = p * F + f;
+      atomicMax(reinterpret_cast<int*>(rowmax + 2 * col), __float_as_int(ra));
+      atomicMax(reinterpret_cast<int*>(rowmax + 2 * col + 1), __float_as_int(rb));
     }
   }
 }
 
+// One CTA: 32 orders x NB degrees x 32 planes, every load issued before the
+// CTA's one barrier.
+template <typename T> struct UnpackCfg { static constexpr int NB = sizeof(T) == 4 ? 2 : 1; };
+
 template <typename T>
-__global__ void unpack_kernel(int Tn, int mode, const V2<T>* __restrict__ cf0,
-                              const V2<T>* __restrict__ cf1, int64_t planes,
-                              V2<T>* __restrict__ o0, V2<T>* __restrict__ o1) {
-  __shared__ V2<T> tile[2][32][33];
+__global__ void __launch_bounds__(256) unpack_kernel(int Tn, int mode, const V2<T>* __restrict__ cf0,
+                                                     const V2<T>* __restrict__ cf1, int64_t planes,
+                                                     V2<T>* __restrict__ o0, V2<T>* __restrict__ o1) {
+  constexpr int NB = UnpackCfg<T>::NB;
+  __shared__ V2<T> tile[2][NB][32][33];
   const int m0 = blockIdx.x * 32;
-  const int n = blockIdx.y;
+  const int n0 = blockIdx.y * NB;
   const int64_t p0 = (int64_t)blockIdx.z * 32;
   const int tx = threadIdx.x, ty = threadIdx.y;
   const int64_t t1 = Tn + 1;
   const int F = mode == kUnpackVorDiv ? 2 : 1;
   const int64_t Rc = planes * F;
-  if (m0 <= n) {
-    for (int mm = ty; mm < 32; mm += 8) {
-      int m = m0 + mm;
-      int64_t p = p0 + tx;
-      V2<T> a = mk2<T>(T(0), T(0)), b = a;
-      if (m <= n && p < planes) {
-        int q = (n - m) & 1, i = (n - m) >> 1;
-        int64_t row = cf_row(Tn, m, q, i);
+  const int64_t p = p0 + tx;
+#pragma unroll
+  for (int nb = 0; nb < NB; ++nb) {
+    const int n = n0 + nb;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const int mm = ty + 8 * k;
+      const int m = m0 + mm;
+      V2<T> va = mk2<T>(T(0), T(0)), vb = va;
+      if (n <= Tn && m <= n && p < planes) {
+        const int q = (n - m) & 1, i = (n - m) >> 1;
+        const int64_t row = cf_row(Tn, m, q, i);
         if (mode == kUnpackScalar) {
-          a = cf0[row * Rc + p];
+          va = __ldcs(cf0 + row * Rc + p);
         } else {
           // rot/shear rows hold (u, v) per plane: columns 2p (u), 2p+1 (v).
-          V2<T> ru = cf0[row * Rc + 2 * p], rv = cf0[row * Rc + 2 * p + 1];
-          V2<T> su = cf1[row * Rc + 2 * p], sv = cf1[row * Rc + 2 * p + 1];
-          T mf = T(m);
+          const V2<T> ru = __ldcs(cf0 + row * Rc + 2 * p), rv = __ldcs(cf0 + row * Rc + 2 * p + 1);
+          const V2<T> su = __ldcs(cf1 + row * Rc + 2 * p), sv = __ldcs(cf1 + row * Rc + 2 * p + 1);
+          const T mf = T(m);
           // zeta = i m rot[v] + shear[u];  D = i m rot[u] - shear[v]
-          a = mk2<T>(-mf * rv.y + su.x, mf * rv.x + su.y);
-          b = mk2<T>(-mf * ru.y - sv.x, mf * ru.x - sv.y);
+          va = mk2<T>(-mf * rv.y + su.x, mf * rv.x + su.y);
+          vb = mk2<T>(-mf * ru.y - sv.x, mf * ru.x - sv.y);
         }
         if (m == 0) {
-          a.y = T(0);
-          b.y = T(0);
+          va.y = T(0);
+          vb.y = T(0);
         }
       }
-      tile[0][tx][mm] = a;
-      tile[1][tx][mm] = b;
+      tile[0][nb][tx][mm] = va;
+      tile[1][nb][tx][mm] = vb;
     }
   }
   __syncthreads();
-  for (int pp = ty; pp < 32; pp += 8) {
-    int64_t p = p0 + pp;
-    int m = m0 + tx;
-    if (p >= planes || m > Tn) continue;
-    int64_t off = (p * t1 + n) * t1 + m;
-    V2<T> a = mk2<T>(T(0), T(0)), b = a;
-    if (m <= n) {
-      a = tile[0][pp][tx];
-      b = tile[1][pp][tx];
+#pragma unroll
+  for (int nb = 0; nb < NB; ++nb) {
+    const int n = n0 + nb;
+    if (n > Tn) break;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const int pp = ty + 8 * k;
+      const int64_t pl = p0 + pp;
+      const int m = m0 + tx;
+      if (pl >= planes || m > Tn) continue;
+      const int64_t off = (pl * t1 + n) * t1 + m;
+      // Above the triangle the tile holds zeros.
+      o0[off] = tile[0][nb][pp][tx];
+      if (mode == kUnpackVorDiv) o1[off] = tile[1][nb][pp][tx];
     }
-    o0[off] = a;
-    if (mode == kUnpackVorDiv) o1[off] = b;
   }
 }
 
@@ -170,7 +201,8 @@ void launch_pack(const sht_plan* p, const T* coeff0, const T* coeff1, int64_t pl
                  T* cfold, cudaStream_t s, float* rowmax) {
   if (planes == 0) return;
   int F = coeff1 ? 2 : 1;
-  dim3 grid((unsigned)div_up(p->T + 1, 32), (unsigned)(p->T + 1), (unsigned)(div_up(planes, 32) * F));
+  dim3 grid((unsigned)div_up(p->T + 1, 32), (unsigned)div_up(p->T + 1, PackCfg<T>::NB),
+            (unsigned)(div_up(planes, 32) * F));
   SHT_REQUIRE(grid.z <= 65535, "too many planes for one pack launch");
   pack_kernel<T><<<grid, dim3(32, 8), 0, s>>>(p->T, p->radius, mode, (const V2<T>*)coeff0,
                                               (const V2<T>*)coeff1, planes, F, (V2<T>*)cfold,
@@ -182,7 +214,8 @@ template <typename T>
 void launch_unpack(const sht_plan* p, int mode, const T* cf0, const T* cf1, int64_t planes,
                    T* out0, T* out1, cudaStream_t s) {
   if (planes == 0) return;
-  dim3 grid((unsigned)div_up(p->T + 1, 32), (unsigned)(p->T + 1), (unsigned)div_up(planes, 32));
+  dim3 grid((unsigned)div_up(p->T + 1, 32), (unsigned)div_up(p->T + 1, UnpackCfg<T>::NB),
+            (unsigned)div_up(planes, 32));
   SHT_REQUIRE(grid.z <= 65535, "too many planes for one unpack launch");
   unpack_kernel<T><<<grid, dim3(32, 8), 0, s>>>(p->T, mode, (const V2<T>*)cf0, (const V2<T>*)cf1,
                                                 planes, (V2<T>*)out0, (V2<T>*)out1);
