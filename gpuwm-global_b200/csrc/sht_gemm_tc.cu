@@ -25,17 +25,19 @@
 // their row scales come from the row maxima the producing kernel (the
 // longitude FFT or the pack kernel) merged while writing the operand.
 //
-// Roles (448 threads, one CTA per SM, persistent over a cost-sorted tile list
+// Roles (576 threads, one CTA per SM, persistent over a cost-sorted tile list
 // that may merge several contractions: the P and dP/dphi tables of a
 // gradient or wind synthesis, or the plans of a batch):
 //   warp 0      bulk-copy loader for the table stages; owns TMEM alloc/free
 //   warp 1      MMA issuer (one thread)
-//   warps 2-5   epilogue: tcgen05.ld of the accumulator, unscale, store
-//   warps 6-13  converters for the data operand
+//   warps 2-9   epilogue: tcgen05.ld of the accumulators, unscale, stage in
+//               shared memory, release the accumulators, bulk-store the tile
+//   warps 10-17 converters for the data operand
 // Pipelines: STAGES shared-memory stages (full/empty mbarriers) and one set of
-// four TMEM accumulators of 128 columns (full/empty mbarriers).  Every mbarrier wait is bounded by a clock budget; on expiry the
-// waiting thread raises the plan's error word and a CTA abort flag, and each
-// epilogue warp decides to stop as a whole (__any_sync) before the
+// four TMEM accumulators of 128 columns (full/empty mbarriers).  Every
+// mbarrier wait is bounded by a clock budget; on expiry the waiting thread
+// raises the plan's error word and a CTA abort flag, and the epilogue warps
+// decide to stop together (a reduction over their named barrier) before the
 // warp-collective TMEM loads, so a fault in the pipeline logic cannot hang
 // the GPU.
 //
@@ -88,9 +90,11 @@ constexpr int STAGES = 4;
 constexpr int NPARTS = 2;
 constexpr int NMAIN = 3;    // main-product accumulators (contiguous K segments)
 constexpr int NMAX = 128;   // tile N; TMEM: (NMAIN + 1) x NMAX = 512 columns
-constexpr int kThreads = 448;
+constexpr int kEpiWarps = 8;                     // two per TMEM lane quarter
+constexpr int kEpiThreads = kEpiWarps * 32;
 constexpr int kConvThreads = 256;
-constexpr int kConvWarp0 = 6;
+constexpr int kConvWarp0 = 2 + kEpiWarps;
+constexpr int kThreads = kConvWarp0 * 32 + kConvThreads;  // 576
 constexpr long long kWaitBudget = 4000000000LL;  // clock cycles (~2 s)
 
 // Shared-memory plan (bytes).
@@ -102,8 +106,8 @@ constexpr int kOffB = kOffA + STAGES * NPARTS * kAPart;    // [STAGES][NPARTS][k
 constexpr int kOffBar = kOffB + STAGES * NPARTS * kBPart;  // mbarriers (8 B each)
 constexpr int kNumBars = 3 * STAGES + 2 + 1;
 constexpr int kOffMisc = kOffBar + kNumBars * 8;           // tmem base, abort flag
-constexpr int kOffCs = kOffMisc + 16;                      // [4 epilogue warps][NMAX] floats
-constexpr int kOffStage = (kOffCs + 4 * NMAX * 4 + 127) / 128 * 128;  // staging [NMAX][BM] floats
+constexpr int kOffCs = kOffMisc + 16;                      // [epilogue warps][NMAX] floats
+constexpr int kOffStage = (kOffCs + kEpiWarps * NMAX * 4 + 127) / 128 * 128;  // staging [NMAX][BM]
 constexpr int kSmemBytes = kOffStage + NMAX * BM * 4 + 1024;  // + alignment slack
 static_assert(kSmemBytes <= 227 * 1024, "shared memory plan exceeds 227 KB");
 
@@ -157,19 +161,19 @@ __device__ __forceinline__ void bulk_wait_read() {
 }
 // The committed bulk stores have completed.
 __device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
-// Named barrier 1 over the four epilogue warps; returns the OR of `pred`
-// over their 128 threads.
+// Named barrier 1 over the eight epilogue warps; returns the OR of `pred`
+// over their 256 threads.
 __device__ __forceinline__ bool epi_bar_or(bool pred) {
   uint32_t out;
   asm volatile(
-      "{\n\t.reg .pred p, q;\n\tsetp.ne.u32 q, %1, 0;\n\tbar.red.or.pred p, 1, 128, q;\n\t"
+      "{\n\t.reg .pred p, q;\n\tsetp.ne.u32 q, %1, 0;\n\tbar.red.or.pred p, 1, 256, q;\n\t"
       "selp.u32 %0, 1, 0, p;\n\t}"
       : "=r"(out)
       : "r"((uint32_t)pred)
       : "memory");
   return out != 0;
 }
-__device__ __forceinline__ void epi_bar() { asm volatile("bar.sync 1, 128;" ::: "memory"); }
+__device__ __forceinline__ void epi_bar() { asm volatile("bar.sync 1, 256;" ::: "memory"); }
 __device__ __forceinline__ void fence_barrier_init() {
   asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 }
@@ -324,7 +328,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
       mbar_init(&pp.empty[s], 1);
     }
     mbar_init(pp.acc_full, 1);
-    mbar_init(pp.acc_empty, 128);
+    mbar_init(pp.acc_empty, kEpiThreads);
     mbar_init(pp.done, 1);
     *abort_flag = 0;
     fence_barrier_init();
@@ -443,13 +447,16 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
     // [column][row].  The accumulator goes back to the MMA warp as soon as the
     // staging is written; the staged columns (one output row x each, the data
     // rows r contiguous) then leave as bulk shared->global stores, one per
-    // thread, which run while the next tile's MMAs do.  Every decision that
-    // steers the epilogue's named barrier is reduced over its four warps
-    // (epi_bar_or), so all 128 threads take the same path, and the
+    // thread, which run while the next tile's MMAs do.  Two warps share each
+    // TMEM lane quarter, one per half of the tile's columns.  Every decision
+    // that steers the epilogue's named barrier is reduced over its eight
+    // warps (epi_bar_or), so all 256 threads take the same path, and the
     // warp-collective tcgen05.ld is entered warp-uniformly.
     const int eg = warp & 3;  // TMEM lane group accessible to this warp
+    const int half = (warp - 2) / 4;
     const int row = eg * 32 + lane;
-    float* cs_s = reinterpret_cast<float*>(smem + kOffCs) + eg * NMAX;  // this warp's copy
+    const int et = threadIdx.x - 64;  // 0 .. kEpiThreads - 1
+    float* cs_s = reinterpret_cast<float*>(smem + kOffCs) + (warp - 2) * NMAX;  // this warp's copy
     float* stage_s = reinterpret_cast<float*>(smem + kOffStage);
     uint32_t acc_phase = 0;
     for (int t = blockIdx.x; t < a.n_tiles; t += gridDim.x) {
@@ -459,10 +466,11 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
       const int64_t R = G.R;
       const int64_t r = tl.r0 + row;
       float* outb = G.out + d.c_row * R;
+      const int cbeg = half * (NMAX / 2), cend = min(tl.nsize, cbeg + NMAX / 2);
       if (tl.kst == 0) {
         // empty contraction (K = 0): the output block is zero
         if (r < R)
-          for (int x = tl.n0; x < min(tl.n0 + tl.nsize, d.X); ++x) outb[(int64_t)x * R + r] = 0.f;
+          for (int x = tl.n0 + cbeg; x < min(tl.n0 + cend, d.X); ++x) outb[(int64_t)x * R + r] = 0.f;
         continue;
       }
       // The tile's row and column scales are fetched while the MMAs run: the
@@ -488,7 +496,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
       // accumulators unwritten: only the segments that exist are read.
       const int nsteps = tl.kst * (BK / 16);
       const int nseg = nsteps < NMAIN ? nsteps : NMAIN;
-      for (int c0 = 0; c0 < tl.nsize; c0 += 16) {
+      for (int c0 = cbeg; c0 < cend; c0 += 16) {
         // All four accumulators of the chunk are loaded before one wait.
         uint32_t rc[16], rm[NMAIN][16];
         tmem_ld16_async(tmem_base + lane_off + (uint32_t)(NMAIN * NMAX + c0), rc);  // corrections
@@ -514,17 +522,18 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
       epi_bar();
       const int ncols = min(tl.nsize, d.X - tl.n0);
       if ((R & 3) == 0) {
-        // 16-byte aligned rows: thread `row` sends staged column `row`.
-        if (row < ncols) {
+        // 16-byte aligned rows: epilogue thread `et` sends staged column `et`.
+        if (et < ncols) {
           const int64_t nrows = R - tl.r0 < BM ? R - tl.r0 : (int64_t)BM;
-          bulk_s2g(outb + (int64_t)(tl.n0 + row) * R + tl.r0, stage_s + row * BM,
+          bulk_s2g(outb + (int64_t)(tl.n0 + et) * R + tl.r0, stage_s + et * BM,
                    (uint32_t)(nrows * 4));
         }
         bulk_commit();
       } else if (r < R) {
         // Row lengths that are not a multiple of 4 floats: plain stores of
-        // this thread's own row.
-        for (int c = 0; c < ncols; ++c) outb[(int64_t)(tl.n0 + c) * R + r] = stage_s[c * BM + row];
+        // this thread's own row, over its half of the columns.
+        for (int c = cbeg; c < min(ncols, cend); ++c)
+          outb[(int64_t)(tl.n0 + c) * R + r] = stage_s[c * BM + row];
       }
     }
     bulk_wait_all();
