@@ -243,16 +243,13 @@ def main():
                                 device_id=dev)
     T, P = args.truncation, args.planes
 
+    from b200sht import replicas
+
     def barrier():
-        if ws > 1:
-            dist.barrier()
+        replicas.barrier(dev)
 
     def max_over_ranks(x):
-        if ws == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return replicas.max_over_ranks(x, dev)
 
     # Inputs: seeded red spectrum; grids are the FP64 synthesis cast to f32.
     coeff64 = torch.as_tensor(red_spectrum(T, P, CONTROL_SEED + rank)).to(dev)
