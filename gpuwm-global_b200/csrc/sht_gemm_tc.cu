@@ -250,6 +250,16 @@ __device__ __forceinline__ uint32_t instr_desc(int n) {
   return (1u << 4) | (1u << 15) | (1u << 16) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
 }
 
+// x rounded to 11 significant bits (the FP16 significand), ties away from
+// zero, by integer arithmetic on the FP32 encoding: the high FP16 part of
+// the split without a float -> half -> float round trip (conversions run at
+// a fraction of the FP32 rate and were the converter warps' bottleneck).
+// Values scaled into FP16's normal range convert to FP16 exactly; below it
+// the FP16 rounding error is under 2^-24 absolute, 2^-38 of the row maximum.
+__device__ __forceinline__ float round_to_11_bits(float x) {
+  return __int_as_float((__float_as_int(x) + 0x1000) & ~0x1FFF);
+}
+
 // Power-of-two scale putting a maximum into [2^14, 2^15).
 __device__ __forceinline__ float pow2_scale(float mx) {
   if (!(mx > 0.f) || !isfinite(mx)) return 1.f;
@@ -308,6 +318,8 @@ __device__ bool wait_bar(uint64_t* bar, uint32_t parity, const Pipe& pp, unsigne
   return true;
 }
 
+// 576 threads = 18 warps, 5 on the busiest of the four SM sub-partitions,
+// whose 16 384 registers cap a thread at 96.
 __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_constant__ TcArgs a) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   // 1024-byte align the working area.
@@ -558,10 +570,9 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
 #pragma unroll
       for (int i = 0; i < 8; ++i) sc[i] = rbase + i < R ? pow2_scale(G.rowmax[rbase + i]) : 1.f;
       const bool full_rows = rbase + 8 <= R && (R % 4) == 0;
-      bool ok = true;
-      for (int ks = 0; ks < tl.kst; ++ks) {
-        // Loads first (independent of the stage being free), then wait.
-        float v[BK / 16][8];
+      // Stage ks + 1 is loaded while stage ks waits for its slot and is
+      // converted (two register buffers, swapped by a 2x unrolled loop).
+      auto load_stage = [&](int ks, float (&v)[BK / 16][8]) {
 #pragma unroll
         for (int j = 0; j < BK / 16; ++j) {
           const int k = ks * BK + (kgs + 2 * j) * 8 + kk;
@@ -581,21 +592,21 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
             for (int i = 0; i < 8; ++i) v[j][i] = 0.f;
           }
         }
-        if (!wait_bar(&pp.empty[stage], phase ^ 1, pp, a.err, 7)) {
-          ok = false;
-          break;
-        }
+      };
+      auto convert_stage = [&](const float (&v)[BK / 16][8]) -> bool {
+        if (!wait_bar(&pp.empty[stage], phase ^ 1, pp, a.err, 7)) return false;
         unsigned char* dst = sA + stage * NPARTS * kAPart;
 #pragma unroll
         for (int j = 0; j < BK / 16; ++j) {
           const int kg = kgs + 2 * j;
-          __align__(16) __half h1[8];
-          __align__(16) __half h2[8];
+          __align__(16) __half2 h1[4];
+          __align__(16) __half2 h2[4];
 #pragma unroll
-          for (int i = 0; i < 8; ++i) {
-            const float x = v[j][i] * sc[i];
-            h1[i] = __float2half_rn(x);
-            h2[i] = __float2half_rn(x - __half2float(h1[i]));
+          for (int i = 0; i < 4; ++i) {
+            const float x0 = v[j][2 * i] * sc[2 * i], x1 = v[j][2 * i + 1] * sc[2 * i + 1];
+            const float a0 = round_to_11_bits(x0), a1 = round_to_11_bits(x1);
+            h1[i] = __floats2half2_rn(a0, a1);           // exact: 11 significant bits
+            h2[i] = __floats2half2_rn(x0 - a0, x1 - a1);  // the remainder, exact in FP32
           }
           const int off = kg * kALbo + mg * 128 + kk * 16;
           *reinterpret_cast<uint4*>(dst + off) = *reinterpret_cast<const uint4*>(h1);
@@ -604,6 +615,17 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
         fence_proxy_async();
         mbar_arrive(&pp.full_a[stage]);
         if (++stage == STAGES) { stage = 0; phase ^= 1; }
+        return true;
+      };
+      bool ok = true;
+      float va[BK / 16][8], vb[BK / 16][8];
+      load_stage(0, va);
+      for (int ks = 0; ks < tl.kst && ok; ks += 2) {
+        if (ks + 1 < tl.kst) load_stage(ks + 1, vb);
+        ok = convert_stage(va);
+        if (!ok || ks + 1 >= tl.kst) break;
+        if (ks + 2 < tl.kst) load_stage(ks + 2, va);
+        ok = convert_stage(vb);
       }
       if (!ok) break;
     }
