@@ -11,6 +11,7 @@ from .transform import SphericalHarmonicTransform
 from .vector import VorticityDivergenceOperator
 from .semi_implicit import SpectralState, VerticalModeOperator, VerticalModeSemiImplicit
 from .batch import TransformBatch
+from .waist import FourierWaist, latitude_band_edges
 from .step import DycoreTransformStep
 
 __all__ = [
@@ -22,5 +23,7 @@ __all__ = [
     "VerticalModeOperator",
     "VerticalModeSemiImplicit",
     "TransformBatch",
+    "FourierWaist",
+    "latitude_band_edges",
     "DycoreTransformStep",
 ]

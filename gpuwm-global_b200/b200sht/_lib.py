@@ -16,6 +16,9 @@ SHT_PREC_F32 = 1
 SHT_PREC_SPLIT16 = 2
 SHT_FLAG_GEOMETRY_ONLY = 1
 SHT_FLAG_GENERIC_FFT = 2
+SHT_WAIST_BASIS = 0
+SHT_WAIST_DBASIS = 1
+SHT_WAIST_ZONAL = 2
 SHT_OK = 0
 SHT_ERR_ARG = 1
 SHT_ERR_CUDA = 2
@@ -59,6 +62,10 @@ SIGNATURES = {
                                            ctypes.POINTER(_P)]),
     "sht_vertical_destroy": (ctypes.c_int, [_P]),
     "sht_helmholtz_apply": (ctypes.c_int, [_P, _P, _D, _P, _P, _P, _P, _P, _P, _P]),
+    "sht_fourier_waist": (ctypes.c_int, [_P, _P, _I64, _P, _P]),
+    "sht_contract_waist": (ctypes.c_int, [_P, _P, _I64, _P, _P]),
+    "sht_contract_to_waist": (ctypes.c_int, [_P, _P, _I64, ctypes.c_int, _P, _P]),
+    "sht_waist_to_grid": (ctypes.c_int, [_P, _P, _I64, _P, _P]),
     "sht_batch_create": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(_P), ctypes.POINTER(_I64),
                                         ctypes.POINTER(_P)]),
     "sht_batch_destroy": (ctypes.c_int, [_P]),

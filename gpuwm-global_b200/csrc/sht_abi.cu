@@ -808,4 +808,91 @@ int sht_batch_inverse(sht_batch* batch, const void* const* coeffs, void* const* 
   });
 }
 
+// ------------------------------------------------------------ Fourier waist
+int sht_fourier_waist(sht_plan* plan, const void* grid, int64_t planes, void* waist,
+                      void* stream) {
+  return guarded([&] {
+    SHT_CHECK_CALL(plan, planes);
+    check_ptr(grid, "grid");
+    check_ptr(waist, "waist");
+    SHT_TYPED(plan, {
+      ensure_scratch(plan, 2 * planes);
+      T* w = static_cast<T*>(plan->wfold[0]);
+      {
+        KernelScope k(plan, SHT_KIND_FFT_FORWARD, s);
+        launch_forward_fold<T>(plan, CP(grid), nullptr, planes, w, s, nullptr);
+      }
+      KernelScope k(plan, SHT_KIND_UNPACK, s);
+      launch_waist_export<T>(plan, w, planes, 0.5, 0, MP(waist), s);
+    });
+  });
+}
+
+int sht_contract_waist(sht_plan* plan, const void* waist, int64_t planes, void* coeff,
+                       void* stream) {
+  return guarded([&] {
+    SHT_CHECK_CALL(plan, planes);
+    check_ptr(waist, "waist");
+    check_ptr(coeff, "coeff");
+    SHT_TYPED(plan, {
+      const int64_t R = 2 * planes;
+      ensure_scratch(plan, R);
+      T* w = static_cast<T*>(plan->wfold[0]);
+      T* c = static_cast<T*>(plan->cfold[0]);
+      {
+        float* rm = rowmax_for(plan, R, s);
+        KernelScope k(plan, SHT_KIND_PACK, s);
+        launch_waist_import<T>(plan, CP(waist), planes, 1.0, w, rm, s);
+      }
+      contract<T>(plan, kAnalysis, w, c, R, s);
+      KernelScope k(plan, SHT_KIND_UNPACK, s);
+      launch_unpack<T>(plan, kUnpackScalar, c, nullptr, planes, MP(coeff), nullptr, s);
+    });
+  });
+}
+
+int sht_contract_to_waist(sht_plan* plan, const void* coeff, int64_t planes, int table,
+                          void* waist, void* stream) {
+  return guarded([&] {
+    SHT_CHECK_CALL(plan, planes);
+    check_ptr(coeff, "coeff");
+    check_ptr(waist, "waist");
+    SHT_REQUIRE(table == SHT_WAIST_BASIS || table == SHT_WAIST_DBASIS || table == SHT_WAIST_ZONAL,
+                "table must be SHT_WAIST_BASIS, SHT_WAIST_DBASIS or SHT_WAIST_ZONAL");
+    SHT_TYPED(plan, {
+      const int64_t R = 2 * planes;
+      ensure_scratch(plan, R);
+      T* w = static_cast<T*>(plan->wfold[0]);
+      T* c = static_cast<T*>(plan->cfold[0]);
+      {
+        float* rm = rowmax_for(plan, R, s);
+        KernelScope k(plan, SHT_KIND_PACK, s);
+        launch_pack<T>(plan, CP(coeff), nullptr, planes, kPackPlain, c, s, rm);
+      }
+      contract<T>(plan, table == SHT_WAIST_DBASIS ? kDBasis : kBasis, c, w, R, s);
+      KernelScope k(plan, SHT_KIND_UNPACK, s);
+      launch_waist_export<T>(plan, w, planes, 1.0, table == SHT_WAIST_ZONAL ? 1 : 0, MP(waist), s);
+    });
+  });
+}
+
+int sht_waist_to_grid(sht_plan* plan, const void* waist, int64_t planes, void* grid,
+                      void* stream) {
+  return guarded([&] {
+    SHT_CHECK_CALL(plan, planes);
+    check_ptr(waist, "waist");
+    check_ptr(grid, "grid");
+    SHT_TYPED(plan, {
+      ensure_scratch(plan, 2 * planes);
+      T* w = static_cast<T*>(plan->wfold[0]);
+      {
+        KernelScope k(plan, SHT_KIND_PACK, s);
+        launch_waist_import<T>(plan, CP(waist), planes, 0.5, w, nullptr, s);
+      }
+      KernelScope k(plan, SHT_KIND_FFT_INVERSE, s);
+      launch_inverse_unfold<T>(plan, kUnfoldScalar, w, nullptr, planes, MP(grid), nullptr, s);
+    });
+  });
+}
+
 }  // extern "C"

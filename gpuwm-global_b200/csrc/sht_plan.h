@@ -167,6 +167,14 @@ void launch_helmholtz(const sht_plan* p, int nlev, const T* mats, double tau_w,
                       const T* div, const T* theta, const T* lnps, T* odiv, T* otheta,
                       T* olnps, cudaStream_t s);
 
+// Reference-layout Fourier waist <-> folded waist (sht_waist.cu).
+template <typename T>
+void launch_waist_export(const sht_plan* p, const T* wfold, int64_t planes, double c, int zonal,
+                         T* waist, cudaStream_t s);
+template <typename T>
+void launch_waist_import(const sht_plan* p, const T* waist, int64_t planes, double c, T* wfold,
+                         float* rowmax, cudaStream_t s);
+
 // Split-precision tensor-core path (sht_gemm_tc.cu).
 void build_tc_tables(sht_plan* p, const double* basis64, const double* dbasis64,
                      const double* analysis64, const double* rot64, const double* shear64,

@@ -194,6 +194,33 @@ int sht_helmholtz_apply(sht_plan* plan, const sht_vertical* op, double tau_w,
                         const void* divergence, const void* theta, const void* lnps,
                         void* out_divergence, void* out_theta, void* out_lnps, void* stream);
 
+/* The Fourier waist in the reference's layout: (planes, nlat, T+1) complex,
+ * the zonal spectrum of each grid row divided by nlon and cut at m = T
+ * (FourierWaist, src/arwen_global/spectral/transform.py:417-629).  The
+ * four calls are the two halves of the transform pair the reference names
+ * so that band pipelines can fill and drain grid space a latitude band at
+ * a time:
+ *   sht_fourier_waist     grid -> waist                (fourier_waist, transform.py:1294-1404)
+ *   sht_contract_waist    waist -> coefficients        (contract_waist / contract_values, 1435-1473)
+ *   sht_contract_to_waist coefficients -> waist        (contract_to_waist, 1629-1650), with the
+ *                         basis, the d/dphi basis, or the basis times i m
+ *                         (gradient_waists' zonal half, 1770-1786)
+ *   sht_waist_to_grid     waist -> grid                (waist_to_grid / waist_band_to_grid, 1704-1735)
+ * sht_contract_waist(sht_fourier_waist(g)) is sht_forward(g) and
+ * sht_waist_to_grid(sht_contract_to_waist(c, SHT_WAIST_BASIS)) is
+ * sht_inverse(c), up to the rounding of the layout conversion. */
+#define SHT_WAIST_BASIS 0
+#define SHT_WAIST_DBASIS 1
+#define SHT_WAIST_ZONAL 2
+int sht_fourier_waist(sht_plan* plan, const void* grid, int64_t planes, void* waist,
+                      void* stream);
+int sht_contract_waist(sht_plan* plan, const void* waist, int64_t planes, void* coeff,
+                       void* stream);
+int sht_contract_to_waist(sht_plan* plan, const void* coeff, int64_t planes, int table,
+                          void* waist, void* stream);
+int sht_waist_to_grid(sht_plan* plan, const void* waist, int64_t planes, void* grid,
+                      void* stream);
+
 /* Batches: up to 4 plans (for instance 32 ensemble members at T126 as one
  * plan of 32 x 200 planes, and the T255 control as another) transformed as
  * one call.  The reference runs each member and truncation through its own

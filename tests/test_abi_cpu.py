@@ -101,3 +101,20 @@ def test_vertical_operator_modes_match_reference_fixture():
         a = op.eigenvectors[:, j] / np.linalg.norm(op.eigenvectors[:, j])
         b = v_ref[:, j] / np.linalg.norm(v_ref[:, j])
         assert abs(abs(a @ b) - 1.0) < 1e-8
+
+
+def test_latitude_band_edges_tile_the_grid():
+    from b200sht import latitude_band_edges
+
+    assert latitude_band_edges(7, 3) == [(0, 2), (2, 4), (4, 7)]
+    assert latitude_band_edges(3, 5) == [(0, 1), (1, 2), (2, 3)]  # empty bands dropped
+    for nlat in (1, 32, 94, 768):
+        for bands in (1, 2, 7, 100):
+            edges = latitude_band_edges(nlat, bands)
+            assert edges[0][0] == 0 and edges[-1][1] == nlat
+            assert all(a < b for a, b in edges)
+            assert all(edges[i][1] == edges[i + 1][0] for i in range(len(edges) - 1))
+    with pytest.raises(ValueError):
+        latitude_band_edges(0, 1)
+    with pytest.raises(ValueError):
+        latitude_band_edges(10, 0)
