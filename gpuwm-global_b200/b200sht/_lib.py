@@ -19,6 +19,10 @@ SHT_FLAG_GENERIC_FFT = 2
 SHT_WAIST_BASIS = 0
 SHT_WAIST_DBASIS = 1
 SHT_WAIST_ZONAL = 2
+SHT_TUNE_CONTRACTION = 0
+SHT_TUNE_FFT = 1
+SHT_TUNE_TILE_ORDER = 2
+SHT_TUNE_TC_CTAS = 3
 SHT_OK = 0
 SHT_ERR_ARG = 1
 SHT_ERR_CUDA = 2
@@ -62,6 +66,8 @@ SIGNATURES = {
                                            ctypes.POINTER(_P)]),
     "sht_vertical_destroy": (ctypes.c_int, [_P]),
     "sht_helmholtz_apply": (ctypes.c_int, [_P, _P, _D, _P, _P, _P, _P, _P, _P, _P]),
+    "sht_plan_set_tuning": (ctypes.c_int, [_P, ctypes.c_int, ctypes.c_int]),
+    "sht_plan_get_tuning": (ctypes.c_int, [_P, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]),
     "sht_fourier_waist": (ctypes.c_int, [_P, _P, _I64, _P, _P]),
     "sht_contract_waist": (ctypes.c_int, [_P, _P, _I64, _P, _P]),
     "sht_contract_to_waist": (ctypes.c_int, [_P, _P, _I64, ctypes.c_int, _P, _P]),

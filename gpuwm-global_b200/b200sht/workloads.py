@@ -16,6 +16,7 @@ from __future__ import annotations
 
 import torch
 
+from .autotune import tune
 from .batch import TransformBatch
 from .semi_implicit import VerticalModeOperator
 from .step import DycoreTransformStep, rossby_haurwitz_state, wave_energy
@@ -85,6 +86,8 @@ def ensemble(args, clock_sampler):
         for prec in ("split16", "float32"):
             plans = [SphericalHarmonicTransform.create(T, nlat=nl, nlon=no, precision=prec)
                      for T, nl, no, _ in specs]
+            # The project autotuner picks each plan's settings for its plane count.
+            tuned = [tune(pl, sp[3], repeats=3, warmup=1)["best"] for pl, sp in zip(plans, specs)]
             batch = TransformBatch(plans, [s[3] for s in specs])
             state = {}
 
@@ -105,7 +108,8 @@ def ensemble(args, clock_sampler):
             out[prec] = {"plane_pairs_per_s_graph": total / (ms_graph * 1e-3),
                          "ms_graph": ms_graph, "ms_batch_eager": ms_batch,
                          "ms_per_plan_eager": ms_single,
-                         "rel_spectral_l2": {"T126": errs[0], "T255": errs[1]}}
+                         "rel_spectral_l2": {"T126": errs[0], "T255": errs[1]},
+                         "autotuned": {"T126": tuned[0], "T255": tuned[1]}}
             del graph, batch, plans, state
             torch.cuda.empty_cache()
     out["clocks"] = clocks.summary()

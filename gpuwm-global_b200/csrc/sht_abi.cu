@@ -135,7 +135,9 @@ void ensure_scratch(sht_plan* p, int64_t R) {
   p->scratch_rows = R;
 }
 
-bool uses_tc(const sht_plan* p) { return p->prec == SHT_PREC_SPLIT16 && p->tc != nullptr; }
+bool uses_tc(const sht_plan* p) {
+  return p->prec == SHT_PREC_SPLIT16 && p->tc != nullptr && p->tune_contraction == 0;
+}
 
 // The row-max buffer the producer of a split-precision operand fills
 // (zeroed first), or nullptr on the FP32/FP64 paths.
@@ -287,7 +289,9 @@ template <typename T>
 void contract_batch(sht_batch* b, int kind, T* const* data, T* const* out, cudaStream_t s) {
   const int n = (int)b->plans.size();
   if constexpr (sizeof(T) == 4) {
-    if (uses_tc(b->plans[0])) {
+    bool all_tc = true;
+    for (sht_plan* p : b->plans) all_tc = all_tc && uses_tc(p);
+    if (all_tc) {
       const int dir = table_dir(kind);
       KernelScope scope(b->plans[0],
                         dir == 0 ? SHT_KIND_LEGENDRE_SYNTHESIS : SHT_KIND_LEGENDRE_ANALYSIS, s);
@@ -892,6 +896,56 @@ int sht_waist_to_grid(sht_plan* plan, const void* waist, int64_t planes, void* g
       KernelScope k(plan, SHT_KIND_FFT_INVERSE, s);
       launch_inverse_unfold<T>(plan, kUnfoldScalar, w, nullptr, planes, MP(grid), nullptr, s);
     });
+  });
+}
+
+// ------------------------------------------------------------------ tuning
+int sht_plan_set_tuning(sht_plan* plan, int key, int value) {
+  return guarded([&] {
+    check_transform_plan(plan);
+    switch (key) {
+      case SHT_TUNE_CONTRACTION:
+        SHT_REQUIRE(value == 0 || value == 1, "SHT_TUNE_CONTRACTION is 0 or 1");
+        SHT_REQUIRE(value == 0 || plan->prec == SHT_PREC_SPLIT16,
+                    "SHT_TUNE_CONTRACTION = 1 applies to split16 plans");
+        plan->tune_contraction = value;
+        break;
+      case SHT_TUNE_FFT:
+        SHT_REQUIRE(value == 0 || value == 1, "SHT_TUNE_FFT is 0 or 1");
+        if (value == 0) {
+          SHT_REQUIRE(fast_fft_supported(plan),
+                      "the register-resident FFT does not cover this grid or precision");
+          if (!plan->fast_fft) fast_fft_init_constants(nullptr);
+          plan->fast_fft = true;
+        } else {
+          plan->fast_fft = false;
+        }
+        break;
+      case SHT_TUNE_TILE_ORDER:
+        SHT_REQUIRE(value == 0 || value == 1, "SHT_TUNE_TILE_ORDER is 0 or 1");
+        plan->tune_tile_order = value;
+        break;
+      case SHT_TUNE_TC_CTAS:
+        SHT_REQUIRE(value >= 0 && value <= 4096, "SHT_TUNE_TC_CTAS is in [0, 4096]");
+        plan->tune_tc_ctas = value;
+        break;
+      default:
+        throw Error{SHT_ERR_ARG, "unknown tuning key"};
+    }
+  });
+}
+
+int sht_plan_get_tuning(sht_plan* plan, int key, int* value) {
+  return guarded([&] {
+    check_transform_plan(plan);
+    check_ptr(value, "value");
+    switch (key) {
+      case SHT_TUNE_CONTRACTION: *value = plan->tune_contraction; break;
+      case SHT_TUNE_FFT: *value = plan->fast_fft ? 0 : 1; break;
+      case SHT_TUNE_TILE_ORDER: *value = plan->tune_tile_order; break;
+      case SHT_TUNE_TC_CTAS: *value = plan->tune_tc_ctas; break;
+      default: throw Error{SHT_ERR_ARG, "unknown tuning key"};
+    }
   });
 }
 

@@ -867,7 +867,8 @@ TcTileCache* tc_plan_cache(const sht_plan* p) { return p->tc ? p->tc->tiles : nu
 void launch_gemm_tc_groups(const TcGroupSpec* g, int ngroups, TcTileCache* cache, cudaStream_t s) {
   SHT_REQUIRE(ngroups >= 1 && ngroups <= kMaxTcGroups, "tensor-core launch: 1 to 4 groups");
   SHT_REQUIRE(cache != nullptr, "tensor-core launch: no tile cache");
-  std::vector<int64_t> key;
+  const int order = g[0].plan->tune_tile_order;
+  std::vector<int64_t> key{order};
   int64_t rows = 0;
   for (int i = 0; i < ngroups; ++i) {
     SHT_REQUIRE(g[i].plan->tc != nullptr, "tensor-core tables not built");
@@ -892,11 +893,16 @@ void launch_gemm_tc_groups(const TcGroupSpec* g, int ngroups, TcTileCache* cache
         for (int i = 0; i < np; ++i) {
           const int nt = tc->nt_of[dir][i], ns = tc->nsize_of[dir][i], kst = tc->kst_of[dir][i];
           if (p->h_desc[dir][0][i].X == 0) continue;
-          for (int j = 0; j < nt; ++j)
-            for (int64_t r0 = 0; r0 < g[gi].R; r0 += BM) {
-              ShtTcTile t{gi, i, j * ns, ns, kst, (int)r0, tc->img_base[dir][i] + j};
-              v.push_back({(int64_t)ns * kst * BK + 4096, t});
-            }
+          // Order 0: a column tile's row blocks are adjacent (they share its
+          // table image); order 1: a row block's column tiles are adjacent
+          // (they share its converted data rows).
+          const int64_t nr = div_up(g[gi].R, BM);
+          for (int64_t o = 0; o < nt * nr; ++o) {
+            const int j = order == 0 ? (int)(o / nr) : (int)(o % nt);
+            const int64_t r0 = BM * (order == 0 ? o % nr : o / nt);
+            ShtTcTile t{gi, i, j * ns, ns, kst, (int)r0, tc->img_base[dir][i] + j};
+            v.push_back({(int64_t)ns * kst * BK + 4096, t});
+          }
         }
       }
       std::stable_sort(v.begin(), v.end(),
@@ -933,7 +939,8 @@ void launch_gemm_tc_groups(const TcGroupSpec* g, int ngroups, TcTileCache* cache
   a.tiles = list.d;
   a.n_tiles = list.n;
   a.err = g[0].plan->d_err;
-  const int grid = std::min(list.n, g[0].plan->tc->sm_count);
+  const int ctas = g[0].plan->tune_tc_ctas > 0 ? g[0].plan->tune_tc_ctas : g[0].plan->tc->sm_count;
+  const int grid = std::min(list.n, ctas);
   tc_gemm_kernel<<<grid, kThreads, kSmemBytes, s>>>(a);
   SHT_CUDA_OR_THROW(cudaGetLastError());
 }

@@ -62,6 +62,10 @@ struct sht_plan {
   int* d_radices = nullptr;
   bool fast_fft = false;           // register-resident kernels (sht_fft_fast.cu)
   bool force_generic_fft = false;  // SHT_FLAG_GENERIC_FFT
+  // Autotuner settings (sht_plan_set_tuning).
+  int tune_contraction = 0;  // 1: FP32 SIMT contraction on a split16 plan
+  int tune_tile_order = 0;   // tensor-core tile order (0: row blocks innermost, 1: column tiles)
+  int tune_tc_ctas = 0;      // tensor-core CTAs per launch (0: one per SM)
 
   // GEMM descriptors: [direction][flip] (direction 0 synthesis, 1 analysis).
   ShtGemmDesc* d_desc[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};

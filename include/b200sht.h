@@ -194,6 +194,25 @@ int sht_helmholtz_apply(sht_plan* plan, const sht_vertical* op, double tau_w,
                         const void* divergence, const void* theta, const void* lnps,
                         void* out_divergence, void* out_theta, void* out_lnps, void* stream);
 
+/* Autotuner settings of a plan (no counterpart call in the reference, whose
+ * tile shapes and band splits are fixed in code; b200sht/autotune.py times
+ * the combinations on the caller's plane count and keeps the fastest):
+ *   SHT_TUNE_CONTRACTION 0: the plan's own contraction; 1: FP32 SIMT on a
+ *                        split16 plan
+ *   SHT_TUNE_FFT         0: register-resident FFT (where the grid allows);
+ *                        1: shared-memory Stockham FFT
+ *   SHT_TUNE_TILE_ORDER  tensor-core work order among equal-cost tiles:
+ *                        0: row blocks of a column tile adjacent;
+ *                        1: column tiles of a row block adjacent
+ *   SHT_TUNE_TC_CTAS     tensor-core CTAs per launch; 0: one per SM
+ * Set between calls, not while a call of the plan is in flight. */
+#define SHT_TUNE_CONTRACTION 0
+#define SHT_TUNE_FFT 1
+#define SHT_TUNE_TILE_ORDER 2
+#define SHT_TUNE_TC_CTAS 3
+int sht_plan_set_tuning(sht_plan* plan, int key, int value);
+int sht_plan_get_tuning(sht_plan* plan, int key, int* value);
+
 /* The Fourier waist in the reference's layout: (planes, nlat, T+1) complex,
  * the zonal spectrum of each grid row divided by nlon and cut at m = T
  * (FourierWaist, src/arwen_global/spectral/transform.py:417-629).  The

@@ -1,0 +1,53 @@
+"""The autotuner's settings: every combination it may pick computes the same
+transform within the precision's bar, and it keeps the fastest."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def rel_l2(a, b):
+    w = np.where(np.arange(a.shape[-1]) == 0, 1.0, 2.0)[None, :]
+    return float(np.sqrt(np.sum(w * np.abs(a - b) ** 2) / np.sum(w * np.abs(b) ** 2)))
+
+
+def test_every_setting_meets_the_bar_and_tune_keeps_the_fastest(tmp_path):
+    from b200sht import SphericalHarmonicTransform
+    from b200sht.autotune import _candidates, get_tuning, set_tuning, tune
+    from b200sht.synthetic import red_spectrum
+
+    kw = dict(nlat=94, nlon=192, dealias_factor=1.49)
+    f64 = SphericalHarmonicTransform.create(62, precision="float64", **kw)
+    t = SphericalHarmonicTransform.create(62, precision="split16", **kw)
+    np_ = t.backend.to_numpy
+    coeff = red_spectrum(62, 6)
+    grid = f64.inverse(coeff)
+    want = np_(f64.forward(grid))
+    cands = _candidates(t)
+    assert len(cands) == 6  # {TC x 2 orders, SIMT} x {register FFT, Stockham FFT}
+    for cand in cands:
+        set_tuning(t, **cand)
+        assert get_tuning(t) == cand
+        assert rel_l2(np_(t.forward(grid.float())), want) < 2e-6
+        assert np.max(np.abs(np_(t.inverse(coeff)) - np_(grid))) / np.max(np.abs(np_(grid))) < 2e-6
+    report = tune(t, 6, repeats=2, warmup=1, cache=tmp_path / "tune.json")
+    assert report["best"] == get_tuning(t)
+    assert report["ms"][min(report["ms"], key=report["ms"].get)] == min(report["ms"].values())
+    again = tune(t, 6, cache=tmp_path / "tune.json")
+    assert again["cached"] and again["best"] == report["best"]
+    t.check_device()
+
+
+def test_tuning_errors():
+    from b200sht import SphericalHarmonicTransform
+    from b200sht.autotune import set_tuning
+
+    f64 = SphericalHarmonicTransform.create(21, precision="float64")
+    with pytest.raises(ValueError, match="register-resident"):
+        set_tuning(f64, fft=0)
+    with pytest.raises(ValueError, match="split16"):
+        set_tuning(f64, contraction=1)
+    with pytest.raises(ValueError, match="unknown tuning setting"):
+        set_tuning(f64, band=3)
