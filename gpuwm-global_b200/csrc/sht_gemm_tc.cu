@@ -51,6 +51,8 @@
 #include <mutex>
 #include <vector>
 
+#include <cuda.h>  // CUtensorMap (the tensor map is encoded through the runtime's driver entry point)
+
 #include "sht_plan.h"
 
 struct ShtTcTile {
@@ -86,7 +88,7 @@ namespace {
 
 constexpr int BM = 128;
 constexpr int BK = 32;
-constexpr int STAGES = 4;
+constexpr int STAGES = 3;
 constexpr int NPARTS = 2;
 constexpr int NMAIN = 3;    // main-product accumulators (contiguous K segments)
 constexpr int NMAX = 128;   // tile N; TMEM: (NMAIN + 1) x NMAX = 512 columns
@@ -103,8 +105,12 @@ constexpr int kBPart = NMAX * BK * 2;    // one FP16 part of the B stage: 16 KB
 constexpr int kALbo = (BM / 8) * 128;    // A: K-group stride (16 M-groups of 128 B)
 constexpr int kOffA = 0;                                   // [STAGES][NPARTS][kAPart]
 constexpr int kOffB = kOffA + STAGES * NPARTS * kAPart;    // [STAGES][NPARTS][kBPart]
-constexpr int kOffBar = kOffB + STAGES * NPARTS * kBPart;  // mbarriers (8 B each)
-constexpr int kNumBars = 3 * STAGES + 2 + 1;
+constexpr int kRawStage = BK * BM * 4;                     // FP32 data tile of a stage: 16 KB
+constexpr int kRawBox = BK * 32 * 4;                       // one TMA box: 32 rows x 32 k, 4 KB
+constexpr int kOffRaw = kOffB + STAGES * NPARTS * kBPart;  // [STAGES][4 boxes], 128B-swizzled
+constexpr int kOffBar = kOffRaw + STAGES * kRawStage;      // mbarriers (8 B each)
+constexpr int kNumBars = 4 * STAGES + 2 + 1;
+static_assert(kOffRaw % 1024 == 0, "128-byte swizzled TMA destinations are 1024-byte aligned");
 constexpr int kOffMisc = kOffBar + kNumBars * 8;           // tmem base, abort flag
 constexpr int kOffCs = kOffMisc + 16;                      // [epilogue warps][NMAX] floats
 constexpr int kOffStage = (kOffCs + kEpiWarps * NMAX * 4 + 127) / 128 * 128;  // staging [NMAX][BM]
@@ -142,6 +148,17 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
       "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
           smem_u32(dst)),
       "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+// TMA: one 2D box of the data operand (x = data row r, y = contraction row k)
+// into shared memory, completing on `bar`.  Boxes that reach past the
+// tensor's extent are zero-filled by the hardware.
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y,
+                                            uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3}], [%4];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
       : "memory");
 }
 __device__ __forceinline__ void fence_proxy_async() {
@@ -273,7 +290,9 @@ __device__ __forceinline__ float pow2_scale(float mx) {
 // One contraction of a launch: a table (one direction of one plan), the data
 // operand with its row maxima, and the output.  A launch runs the merged,
 // cost-sorted tiles of up to kMaxTcGroups of them.
-struct TcGroup {
+struct alignas(64) TcGroup {
+  CUtensorMap data_map;    // the data operand as a [rows][R] FP32 tensor (when use_tma)
+  int use_tma;             // 1: the loader brings the data tiles in by TMA
   const ShtGemmDesc* descs;
   const unsigned char* img;
   const int64_t* img_off;  // per (problem, n-tile) block: byte offset of k-stage 0
@@ -296,6 +315,7 @@ struct Pipe {
   uint64_t* full_a;
   uint64_t* full_b;
   uint64_t* empty;
+  uint64_t* full_raw;  // the FP32 data tile of a stage has landed (TMA)
   uint64_t* acc_full;
   uint64_t* acc_empty;
   uint64_t* done;
@@ -326,11 +346,18 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
   unsigned char* smem = smem_raw + ((1024 - (smem_u32(smem_raw) & 1023)) & 1023);
   unsigned char* sA = smem + kOffA;
   unsigned char* sB = smem + kOffB;
+  unsigned char* sRaw = smem + kOffRaw;
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem + kOffBar);
   uint32_t* tmem_base_smem = reinterpret_cast<uint32_t*>(smem + kOffMisc);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(smem + kOffMisc + 4);
-  Pipe pp{bars, bars + STAGES, bars + 2 * STAGES, bars + 3 * STAGES, bars + 3 * STAGES + 1,
-          bars + 3 * STAGES + 2, abort_flag};
+  Pipe pp{bars,
+          bars + STAGES,
+          bars + 2 * STAGES,
+          bars + 3 * STAGES,
+          bars + 4 * STAGES,
+          bars + 4 * STAGES + 1,
+          bars + 4 * STAGES + 2,
+          abort_flag};
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (threadIdx.x == 0) {
@@ -338,6 +365,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
       mbar_init(&pp.full_a[s], kConvThreads);
       mbar_init(&pp.full_b[s], 1);
       mbar_init(&pp.empty[s], 1);
+      mbar_init(&pp.full_raw[s], 1);
     }
     mbar_init(pp.acc_full, 1);
     mbar_init(pp.acc_empty, kEpiThreads);
@@ -359,14 +387,15 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
     if (lane == 0) {
       int stage = 0;
       uint32_t phase = 0;
-      int armed[STAGES];
+      int armed[STAGES], armed_raw[STAGES];
 #pragma unroll
-      for (int s = 0; s < STAGES; ++s) armed[s] = -1;
+      for (int s = 0; s < STAGES; ++s) armed[s] = armed_raw[s] = -1;
       for (int t = blockIdx.x; t < a.n_tiles && !*abort_flag; t += gridDim.x) {
         const ShtTcTile tl = a.tiles[t];
         const TcGroup& G = a.g[tl.group];
         const int part = tl.nsize * BK * 2;  // bytes of one FP16 part of one stage
         const unsigned char* src = G.img + G.img_off[tl.img];
+        const int64_t d_row = G.use_tma ? G.descs[tl.problem].d_row : 0;
         bool ok = true;
         for (int ks = 0; ks < tl.kst; ++ks) {
           if (!wait_bar(&pp.empty[stage], phase ^ 1, pp, a.err, 1)) {
@@ -380,6 +409,17 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
             bulk_g2s(dst + pt * kBPart, src + ((int64_t)ks * NPARTS + pt) * part, part,
                      &pp.full_b[stage]);
           armed[stage] = (int)phase;
+          if (G.use_tma) {
+            // The stage's FP32 data tile: rows r0 .. r0+127 as four 32-row
+            // boxes, contraction rows d_row + ks*BK .. +BK-1.
+            mbar_arrive_expect_tx(&pp.full_raw[stage], kRawStage);
+            unsigned char* raw = sRaw + stage * kRawStage;
+#pragma unroll
+            for (int q = 0; q < BM / 32; ++q)
+              tma_load_2d(raw + q * kRawBox, &G.data_map, tl.r0 + 32 * q,
+                          (int)(d_row + (int64_t)ks * BK), &pp.full_raw[stage]);
+            armed_raw[stage] = (int)phase;
+          }
           if (++stage == STAGES) { stage = 0; phase ^= 1; }
         }
         if (!ok) break;
@@ -388,10 +428,15 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
       // normal operation the MMA has already waited on them; after an abort
       // this wait is what keeps a late copy from writing freed shared memory).
       for (int s = 0; s < STAGES; ++s) {
-        if (armed[s] < 0) continue;
         long long t0 = clock64();
-        while (!mbar_try_wait(&pp.full_b[s], (uint32_t)armed[s]) && clock64() - t0 < kWaitBudget) {
-        }
+        if (armed[s] >= 0)
+          while (!mbar_try_wait(&pp.full_b[s], (uint32_t)armed[s]) && clock64() - t0 < kWaitBudget) {
+          }
+        t0 = clock64();
+        if (armed_raw[s] >= 0)
+          while (!mbar_try_wait(&pp.full_raw[s], (uint32_t)armed_raw[s]) &&
+                 clock64() - t0 < kWaitBudget) {
+          }
       }
     }
   } else if (warp == 1) {
@@ -593,8 +638,28 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
           }
         }
       };
-      auto convert_stage = [&](const float (&v)[BK / 16][8]) -> bool {
-        if (!wait_bar(&pp.empty[stage], phase ^ 1, pp, a.err, 7)) return false;
+      // The stage's data from the TMA-filled shared tile: boxes of 32 rows
+      // x 32 k with the 16-byte chunks of each 128-byte k row XOR-swizzled
+      // by (k mod 8), which makes this warp's reads (8 consecutive k of one
+      // 8-row group per quarter warp) bank-conflict free.
+      auto fetch_raw = [&](int ks, float (&v)[BK / 16][8]) {
+        const unsigned char* raw = sRaw + stage * kRawStage + (mg >> 2) * kRawBox;
+#pragma unroll
+        for (int j = 0; j < BK / 16; ++j) {
+          const int kl = (kgs + 2 * j) * 8 + kk;  // k within the stage
+          const unsigned char* row = raw + kl * 128;
+          const int c0 = (mg & 3) * 2;
+          const float4 u0 = *reinterpret_cast<const float4*>(row + ((c0 ^ (kl & 7)) << 4));
+          const float4 u1 = *reinterpret_cast<const float4*>(row + (((c0 + 1) ^ (kl & 7)) << 4));
+          const bool live = ks * BK + kl < d.K;  // rows past K belong to the next problem
+          v[j][0] = live ? u0.x : 0.f; v[j][1] = live ? u0.y : 0.f;
+          v[j][2] = live ? u0.z : 0.f; v[j][3] = live ? u0.w : 0.f;
+          v[j][4] = live ? u1.x : 0.f; v[j][5] = live ? u1.y : 0.f;
+          v[j][6] = live ? u1.z : 0.f; v[j][7] = live ? u1.w : 0.f;
+        }
+      };
+      auto convert_stage = [&](const float (&v)[BK / 16][8], bool wait_slot) -> bool {
+        if (wait_slot && !wait_bar(&pp.empty[stage], phase ^ 1, pp, a.err, 7)) return false;
         unsigned char* dst = sA + stage * NPARTS * kAPart;
 #pragma unroll
         for (int j = 0; j < BK / 16; ++j) {
@@ -619,13 +684,24 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
       };
       bool ok = true;
       float va[BK / 16][8], vb[BK / 16][8];
-      load_stage(0, va);
-      for (int ks = 0; ks < tl.kst && ok; ks += 2) {
-        if (ks + 1 < tl.kst) load_stage(ks + 1, vb);
-        ok = convert_stage(va);
-        if (!ok || ks + 1 >= tl.kst) break;
-        if (ks + 2 < tl.kst) load_stage(ks + 2, va);
-        ok = convert_stage(vb);
+      if (G.use_tma) {
+        // The loader issued this stage's data after the slot was freed, so
+        // the data's arrival is also the slot's.
+        for (int ks = 0; ks < tl.kst && ok; ++ks) {
+          ok = wait_bar(&pp.full_raw[stage], phase, pp, a.err, 8);
+          if (!ok) break;
+          fetch_raw(ks, va);
+          ok = convert_stage(va, false);
+        }
+      } else {
+        load_stage(0, va);
+        for (int ks = 0; ks < tl.kst && ok; ks += 2) {
+          if (ks + 1 < tl.kst) load_stage(ks + 1, vb);
+          ok = convert_stage(va, true);
+          if (!ok || ks + 1 >= tl.kst) break;
+          if (ks + 2 < tl.kst) load_stage(ks + 2, va);
+          ok = convert_stage(vb, true);
+        }
       }
       if (!ok) break;
     }
@@ -851,8 +927,59 @@ struct TcTileCache {
   // Key: per group (direction, R).  Lists live as long as the cache, so a
   // launch recorded in a CUDA graph keeps pointing at a live list.
   std::map<std::vector<int64_t>, List> lists;
+  // Tensor maps of data operands, by (address, R, rows).
+  std::map<std::vector<int64_t>, CUtensorMap> maps;
   std::mutex mu;
 };
+
+namespace {
+
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                                   const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                                   const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                   CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_tiled() {
+  static EncodeTiledFn fn = [] {
+    void* ptr = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &ptr, cudaEnableDefault, &q) !=
+            cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      ptr = nullptr;
+    return reinterpret_cast<EncodeTiledFn>(ptr);
+  }();
+  return fn;
+}
+
+// The data operand of a launch as a 2D FP32 tensor [rows][R] (R innermost),
+// read in 32 x 32 boxes with the 128-byte swizzle the converters undo.
+// Requires R % 4 == 0 (16-byte row pitch); false if it cannot be encoded.
+bool data_map(TcTileCache* c, const float* data, int64_t R, int64_t rows, CUtensorMap* out) {
+  if (R % 4 != 0 || R <= 0 || rows <= 0) return false;
+  std::vector<int64_t> key{(int64_t)(uintptr_t)data, R, rows};
+  auto it = c->maps.find(key);
+  if (it != c->maps.end()) {
+    *out = it->second;
+    return true;
+  }
+  EncodeTiledFn fn = encode_tiled();
+  if (fn == nullptr) return false;
+  CUtensorMap m;
+  const cuuint64_t dims[2] = {(cuuint64_t)R, (cuuint64_t)rows};
+  const cuuint64_t strides[1] = {(cuuint64_t)R * 4};
+  const cuuint32_t box[2] = {32, (cuuint32_t)BK};
+  const cuuint32_t elem[2] = {1, 1};
+  if (fn(&m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(data), dims, strides, box,
+         elem, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+         CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+    return false;
+  c->maps.emplace(key, m);
+  *out = m;
+  return true;
+}
+
+}  // namespace
 
 TcTileCache* tc_cache_create() { return new TcTileCache(); }
 
@@ -921,11 +1048,23 @@ void launch_gemm_tc_groups(const TcGroupSpec* g, int ngroups, TcTileCache* cache
   }
   if (list.n == 0) return;
   TcArgs a{};
+  // All groups of a launch take the data by TMA, or none does (the loader
+  // and the converters then agree on which barriers a stage completes).
+  bool tma = true;
+  {
+    std::lock_guard<std::mutex> lock(cache->mu);
+    for (int gi = 0; gi < ngroups && tma; ++gi) {
+      const sht_plan* p = g[gi].plan;
+      const int64_t rows = g[gi].direction == 0 ? p->cf_rows : (int64_t)(p->T + 1) * 2 * p->H;
+      tma = data_map(cache, g[gi].data, g[gi].R, rows, &a.g[gi].data_map);
+    }
+  }
   for (int gi = 0; gi < ngroups; ++gi) {
     const sht_plan* p = g[gi].plan;
     const ShtTc16* tc = p->tc;
     const int dir = g[gi].direction;
     TcGroup& G = a.g[gi];
+    G.use_tma = tma ? 1 : 0;
     G.descs = p->d_desc[dir][g[gi].flip];
     G.img = (const unsigned char*)tc->img[g[gi].table_kind];
     G.img_off = tc->d_img_off[dir];
