@@ -31,7 +31,8 @@ import torch
 from . import _lib
 
 KEYS = {"contraction": _lib.SHT_TUNE_CONTRACTION, "fft": _lib.SHT_TUNE_FFT,
-        "tile_order": _lib.SHT_TUNE_TILE_ORDER, "tc_ctas": _lib.SHT_TUNE_TC_CTAS}
+        "tile_order": _lib.SHT_TUNE_TILE_ORDER, "tc_ctas": _lib.SHT_TUNE_TC_CTAS,
+        "accumulators": _lib.SHT_TUNE_ACCUMULATORS}
 
 
 def get_tuning(transform) -> dict:
@@ -66,7 +67,8 @@ def _candidates(transform) -> list[dict]:
                                                      [0, 1] if split else [0]):
         if contraction == 1 and order == 1:
             continue  # the tile order only steers the tensor-core kernel
-        out.append({"contraction": contraction, "fft": fft, "tile_order": order, "tc_ctas": 0})
+        out.append({"contraction": contraction, "fft": fft, "tile_order": order, "tc_ctas": 0,
+                    "accumulators": current["accumulators"]})
     return out
 
 

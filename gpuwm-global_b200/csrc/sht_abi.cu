@@ -929,6 +929,10 @@ int sht_plan_set_tuning(sht_plan* plan, int key, int value) {
         SHT_REQUIRE(value >= 0 && value <= 4096, "SHT_TUNE_TC_CTAS is in [0, 4096]");
         plan->tune_tc_ctas = value;
         break;
+      case SHT_TUNE_ACCUMULATORS:
+        SHT_REQUIRE(value == 0 || value == 1, "SHT_TUNE_ACCUMULATORS is 0 or 1");
+        plan->tune_accumulators = value;
+        break;
       default:
         throw Error{SHT_ERR_ARG, "unknown tuning key"};
     }
@@ -944,6 +948,7 @@ int sht_plan_get_tuning(sht_plan* plan, int key, int* value) {
       case SHT_TUNE_FFT: *value = plan->fast_fft ? 0 : 1; break;
       case SHT_TUNE_TILE_ORDER: *value = plan->tune_tile_order; break;
       case SHT_TUNE_TC_CTAS: *value = plan->tune_tc_ctas; break;
+      case SHT_TUNE_ACCUMULATORS: *value = plan->tune_accumulators; break;
       default: throw Error{SHT_ERR_ARG, "unknown tuning key"};
     }
   });

@@ -33,8 +33,8 @@
 //   warps 2-9   epilogue: tcgen05.ld of the accumulators, unscale, stage in
 //               shared memory, release the accumulators, bulk-store the tile
 //   warps 10-17 converters for the data operand
-// Pipelines: STAGES shared-memory stages (full/empty mbarriers) and one set of
-// four TMEM accumulators of 128 columns (full/empty mbarriers).  Every
+// Pipelines: STAGES shared-memory stages (full/empty mbarriers) and one or two
+// sets of TMEM accumulators of 128 columns each (full/empty mbarriers per set).  Every
 // mbarrier wait is bounded by a clock budget; on expiry the waiting thread
 // raises the plan's error word and a CTA abort flag, and the epilogue warps
 // decide to stop together (a reduction over their named barrier) before the
@@ -90,8 +90,22 @@ constexpr int BM = 128;
 constexpr int BK = 32;
 constexpr int STAGES = 3;
 constexpr int NPARTS = 2;
-constexpr int NMAIN = 3;    // main-product accumulators (contiguous K segments)
-constexpr int NMAX = 128;   // tile N; TMEM: (NMAIN + 1) x NMAX = 512 columns
+constexpr int NMAX = 128;   // tile N
+// TMEM accumulator plans (SHT_TUNE_ACCUMULATORS).  kAccurate: the main
+// product in three K-segment accumulators + corrections, one set (512
+// columns).  kOverlapped: one main accumulator + corrections, two sets, so the
+// epilogue drains one tile while the MMA fills the next (faster; the longer
+// truncated main sums raise the split error from about 3.6e-7 to 1.2e-6).
+template <int NMAIN_, int NBUF_>
+struct AccPlan {
+  static constexpr int NMAIN = NMAIN_;  // main-product accumulators (contiguous K segments)
+  static constexpr int NBUF = NBUF_;    // accumulator sets
+  static constexpr int kAccCols = (NMAIN + 1) * NMAX;  // one set: NMAIN mains + corrections
+  static_assert(NBUF * kAccCols <= 512, "TMEM holds 512 columns");
+};
+using kAccurate = AccPlan<3, 1>;
+using kOverlapped = AccPlan<1, 2>;
+constexpr int kMaxNBuf = 2;
 constexpr int kEpiWarps = 8;                     // two per TMEM lane quarter
 constexpr int kEpiThreads = kEpiWarps * 32;
 constexpr int kConvThreads = 256;
@@ -109,7 +123,7 @@ constexpr int kRawStage = BK * BM * 4;                     // FP32 data tile of 
 constexpr int kRawBox = BK * 32 * 4;                       // one TMA box: 32 rows x 32 k, 4 KB
 constexpr int kOffRaw = kOffB + STAGES * NPARTS * kBPart;  // [STAGES][4 boxes], 128B-swizzled
 constexpr int kOffBar = kOffRaw + STAGES * kRawStage;      // mbarriers (8 B each)
-constexpr int kNumBars = 4 * STAGES + 2 + 1;
+constexpr int kNumBars = 4 * STAGES + 2 * kMaxNBuf + 1;
 static_assert(kOffRaw % 1024 == 0, "128-byte swizzled TMA destinations are 1024-byte aligned");
 constexpr int kOffMisc = kOffBar + kNumBars * 8;           // tmem base, abort flag
 constexpr int kOffCs = kOffMisc + 16;                      // [epilogue warps][NMAX] floats
@@ -340,7 +354,9 @@ __device__ bool wait_bar(uint64_t* bar, uint32_t parity, const Pipe& pp, unsigne
 
 // 576 threads = 18 warps, 5 on the busiest of the four SM sub-partitions,
 // whose 16 384 registers cap a thread at 96.
+template <typename Acc>
 __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_constant__ TcArgs a) {
+  constexpr int NMAIN = Acc::NMAIN, NBUF = Acc::NBUF, kAccCols = Acc::kAccCols;
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   // 1024-byte align the working area.
   unsigned char* smem = smem_raw + ((1024 - (smem_u32(smem_raw) & 1023)) & 1023);
@@ -355,8 +371,8 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
           bars + 2 * STAGES,
           bars + 3 * STAGES,
           bars + 4 * STAGES,
-          bars + 4 * STAGES + 1,
-          bars + 4 * STAGES + 2,
+          bars + 4 * STAGES + kMaxNBuf,
+          bars + 4 * STAGES + 2 * kMaxNBuf,
           abort_flag};
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -367,8 +383,10 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
       mbar_init(&pp.empty[s], 1);
       mbar_init(&pp.full_raw[s], 1);
     }
-    mbar_init(pp.acc_full, 1);
-    mbar_init(pp.acc_empty, kEpiThreads);
+    for (int b = 0; b < kMaxNBuf; ++b) {
+      mbar_init(&pp.acc_full[b], 1);
+      mbar_init(&pp.acc_empty[b], kEpiThreads);
+    }
     mbar_init(pp.done, 1);
     *abort_flag = 0;
     fence_barrier_init();
@@ -444,13 +462,15 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
     if (lane == 0) {
       int stage = 0;
       uint32_t phase = 0;
-      uint32_t acc_phase = 0;
+      uint32_t acc_it = 0;  // accumulator set = acc_it % NBUF, parity = (acc_it / NBUF) & 1
       bool issued = false;
-      const uint32_t d_corr = tmem_base + NMAIN * NMAX;  // the last 128 columns
       for (int t = blockIdx.x; t < a.n_tiles && !*abort_flag; t += gridDim.x) {
         const ShtTcTile tl = a.tiles[t];
         if (tl.kst == 0) continue;
-        if (!wait_bar(pp.acc_empty, acc_phase ^ 1, pp, a.err, 2)) break;
+        const uint32_t buf = acc_it % NBUF, acc_phase = (acc_it / NBUF) & 1;
+        if (!wait_bar(&pp.acc_empty[buf], acc_phase ^ 1, pp, a.err, 2)) break;
+        const uint32_t d_set = tmem_base + buf * kAccCols;
+        const uint32_t d_corr = d_set + NMAIN * NMAX;
         tc_fence_after();
         const uint32_t idesc = instr_desc(tl.nsize);
         const uint32_t lbo_b = (uint32_t)tl.nsize * 16;
@@ -478,7 +498,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
             const uint32_t accum_main = seg == seg_prev ? 1u : 0u;
             seg_prev = seg;
             const uint32_t accum_corr = step > 0 ? 1u : 0u;
-            mma_f16(tmem_base + (uint32_t)(seg * NMAX), da1, db1, idesc, accum_main);  // a1 b1
+            mma_f16(d_set + (uint32_t)(seg * NMAX), da1, db1, idesc, accum_main);  // a1 b1
             mma_f16(d_corr, da1, db2, idesc, accum_corr);                              // a1 b2
             mma_f16(d_corr, da2, db1, idesc, 1u);                                      // a2 b1
           }
@@ -487,8 +507,8 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
           if (++stage == STAGES) { stage = 0; phase ^= 1; }
         }
         if (!ok) break;
-        mma_commit(pp.acc_full);
-        acc_phase ^= 1;
+        mma_commit(&pp.acc_full[buf]);
+        ++acc_it;
       }
       if (issued) {
         // All issued MMAs complete before TMEM is released.
@@ -515,7 +535,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
     const int et = threadIdx.x - 64;  // 0 .. kEpiThreads - 1
     float* cs_s = reinterpret_cast<float*>(smem + kOffCs) + (warp - 2) * NMAX;  // this warp's copy
     float* stage_s = reinterpret_cast<float*>(smem + kOffStage);
-    uint32_t acc_phase = 0;
+    uint32_t acc_it = 0;
     for (int t = blockIdx.x; t < a.n_tiles; t += gridDim.x) {
       const ShtTcTile tl = a.tiles[t];
       const TcGroup& G = a.g[tl.group];
@@ -544,11 +564,12 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
         }
         __syncwarp();
       }
-      const bool failed = !wait_bar(pp.acc_full, acc_phase, pp, a.err, 5);
+      const uint32_t buf = acc_it % NBUF, acc_phase = (acc_it / NBUF) & 1;
+      const bool failed = !wait_bar(&pp.acc_full[buf], acc_phase, pp, a.err, 5);
       bulk_wait_read();  // this thread's stores of the previous tile have read the staging
       if (epi_bar_or(failed)) break;
       tc_fence_after();
-      const uint32_t lane_off = (uint32_t)(eg * 32) << 16;
+      const uint32_t lane_off = ((uint32_t)(eg * 32) << 16) + buf * kAccCols;
       // A tile with fewer K steps than NMAIN leaves the last main
       // accumulators unwritten: only the segments that exist are read.
       const int nsteps = tl.kst * (BK / 16);
@@ -573,8 +594,8 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
         }
       }
       tc_fence_before();
-      mbar_arrive(pp.acc_empty);
-      acc_phase ^= 1;
+      mbar_arrive(&pp.acc_empty[buf]);
+      ++acc_it;
       fence_proxy_async();  // the staging writes, visible to the bulk-copy proxy
       epi_bar();
       const int ncols = min(tl.nsize, d.X - tl.n0);
@@ -893,7 +914,9 @@ void build_tc_tables(sht_plan* p, const double* basis64, const double* dbasis64,
       cudaFree(db[dir]);
       cudaFree(colmul[dir]);
     }
-    SHT_CUDA_OR_THROW(cudaFuncSetAttribute(tc_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    SHT_CUDA_OR_THROW(cudaFuncSetAttribute(tc_gemm_kernel<kOverlapped>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes));
+    SHT_CUDA_OR_THROW(cudaFuncSetAttribute(tc_gemm_kernel<kAccurate>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            kSmemBytes));
   } catch (...) {
     p->tc = tc;
@@ -1080,7 +1103,10 @@ void launch_gemm_tc_groups(const TcGroupSpec* g, int ngroups, TcTileCache* cache
   a.err = g[0].plan->d_err;
   const int ctas = g[0].plan->tune_tc_ctas > 0 ? g[0].plan->tune_tc_ctas : g[0].plan->tc->sm_count;
   const int grid = std::min(list.n, ctas);
-  tc_gemm_kernel<<<grid, kThreads, kSmemBytes, s>>>(a);
+  if (g[0].plan->tune_accumulators == 1)
+    tc_gemm_kernel<kOverlapped><<<grid, kThreads, kSmemBytes, s>>>(a);
+  else
+    tc_gemm_kernel<kAccurate><<<grid, kThreads, kSmemBytes, s>>>(a);
   SHT_CUDA_OR_THROW(cudaGetLastError());
 }
 

@@ -205,11 +205,17 @@ int sht_helmholtz_apply(sht_plan* plan, const sht_vertical* op, double tau_w,
  *                        0: row blocks of a column tile adjacent;
  *                        1: column tiles of a row block adjacent
  *   SHT_TUNE_TC_CTAS     tensor-core CTAs per launch; 0: one per SM
+ *   SHT_TUNE_ACCUMULATORS tensor-core accumulators: 0: the main product in
+ *                        three K-segment accumulators (split error ~3.6e-7 at
+ *                        T511); 1: one, double-buffered so the epilogue
+ *                        overlaps the next tile (~4 % faster pair, error
+ *                        ~1.2e-6, still within 2e-6)
  * Set between calls, not while a call of the plan is in flight. */
 #define SHT_TUNE_CONTRACTION 0
 #define SHT_TUNE_FFT 1
 #define SHT_TUNE_TILE_ORDER 2
 #define SHT_TUNE_TC_CTAS 3
+#define SHT_TUNE_ACCUMULATORS 4
 int sht_plan_set_tuning(sht_plan* plan, int key, int value);
 int sht_plan_get_tuning(sht_plan* plan, int key, int* value);
 

@@ -51,3 +51,25 @@ def test_tuning_errors():
         set_tuning(f64, contraction=1)
     with pytest.raises(ValueError, match="unknown tuning setting"):
         set_tuning(f64, band=3)
+
+
+@pytest.mark.parametrize("acc", [0, 1])
+def test_accumulator_plans_meet_the_bar_at_t255(acc):
+    from b200sht import SphericalHarmonicTransform, VorticityDivergenceOperator
+    from b200sht.autotune import set_tuning
+    from b200sht.synthetic import red_spectrum
+
+    kw = dict(nlat=384, nlon=768)
+    f64 = SphericalHarmonicTransform.create(255, precision="float64", **kw)
+    t = SphericalHarmonicTransform.create(255, precision="split16", **kw)
+    set_tuning(t, accumulators=acc)
+    np_ = t.backend.to_numpy
+    coeff = red_spectrum(255, 4)
+    grid = f64.inverse(coeff)
+    assert rel_l2(np_(t.forward(grid.float())), np_(f64.forward(grid))) < 2e-6
+    g = np_(t.inverse(coeff))
+    assert np.max(np.abs(g - np_(grid))) / np.max(np.abs(np_(grid))) < 2e-6
+    u64, v64 = VorticityDivergenceOperator(f64).wind_from_vordiv(coeff, coeff[::-1].copy())
+    u, v = VorticityDivergenceOperator(t).wind_from_vordiv(coeff, coeff[::-1].copy())
+    assert np.max(np.abs(np_(u) - np_(u64))) / np.max(np.abs(np_(u64))) < 2e-6
+    t.check_device()
