@@ -423,6 +423,155 @@ __global__ void __launch_bounds__(kWarps * 32) fast_inverse_unfold(FastUnfoldArg
   }
 }
 
+// The scalar inverse (one waist column per plane: scalar, zonal, meridional)
+// two latitude pairs per CTA, h and h + ceil(H/2): the waist slices of the
+// second pair stream into a shared staging buffer with cp.async (no
+// registers held) while the warps FFT the first, so the load latency that a
+// one-pair CTA exposes at its barrier overlaps the butterflies.
+__device__ __forceinline__ void cp_async16(void* dst, const void* src, uint32_t src_bytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(
+                   (uint32_t)__cvta_generic_to_shared(dst)),
+               "l"(src), "r"(src_bytes)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// Entangle, FFT and store this warp's row (plane p0 + gp, side) of pair h.
+template <int FF>
+__device__ __forceinline__ void inverse_row_out(const FastUnfoldArgs& a, float2* reg,
+                                                const float2* tws, const float2* __restrict__ tn,
+                                                float* __restrict__ out, int64_t plane, int j,
+                                                int lane) {
+  constexpr int L = 32 * FF;
+  float2 z[FF];
+#pragma unroll
+  for (int i = 0; i < FF; ++i) {
+    int k = lane + 32 * i;
+    float2 xk = k <= a.T ? reg[k] : make_float2(0.f, 0.f);
+    int kc = L - k;
+    float2 xc = (k > 0 && kc <= a.T) ? cconjf(reg[kc]) : make_float2(0.f, 0.f);
+    if (k == 0) xk.y = 0.f;
+    float2 sm = caddf(xk, xc), df = csubf(xk, xc);
+    float2 wd = cmulf(cconjf(tn[k]), df);
+    z[i] = make_float2(sm.x - wd.y, sm.y + wd.x);
+  }
+  __syncwarp();
+  warp_fft<FF, true>(z, reg, tws, lane);
+  float2* dst = reinterpret_cast<float2*>(out + (plane * a.nlat + j) * (int64_t)a.nlon);
+#pragma unroll 4
+  for (int i = 0; i < FF; ++i) __stcs(dst + lane + 32 * i, reg[lane + 32 * i]);
+}
+
+template <int FF>
+__global__ void __launch_bounds__(kWarps * 32) fast_inverse_pair(FastUnfoldArgs a,
+                                                                 const float2* __restrict__ wP,
+                                                                 const float2* __restrict__ twL,
+                                                                 const float2* __restrict__ twN,
+                                                                 float* __restrict__ out, int Hh) {
+  constexpr int G = 4;  // planes per CTA
+  extern __shared__ float2 smem_dyn[];
+  auto rows = [&](int w) { return smem_dyn + w * WarpSmem<FF>::kFloats2; };
+  float2* tws = smem_dyn + kWarps * WarpSmem<FF>::kFloats2;
+  float2* stage = tws + FF * 32;  // [(m, s)][G] waist slices of the second pair
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int h0 = blockIdx.y, h1 = blockIdx.y + Hh;
+  const bool has1 = h1 < a.H;
+  const int64_t p0 = (int64_t)blockIdx.x * G;
+  const int64_t Rc = a.planes;
+  const int nms = 2 * (a.T + 1);
+  load_lane_twiddles<FF>(tws, twL);
+  if (has1) {
+    for (int e = threadIdx.x; e < 2 * nms; e += blockDim.x) {
+      const int ms = e >> 1, c = e & 1;
+      const int64_t pc = p0 + 2 * c;
+      const int64_t valid = a.planes - pc;
+      const uint32_t bytes = valid >= 2 ? 16u : (valid == 1 ? 8u : 0u);
+      const float2* src = bytes ? wP + ((int64_t)ms * a.H + h1) * Rc + pc : wP;
+      cp_async16(stage + ms * G + 2 * c, src, bytes);
+    }
+    cp_async_commit();
+  }
+  const float2* tn = opaque(twN);
+  const int gp = warp >> 1, side = warp & 1;
+  const int64_t plane = p0 + gp;
+  // Pair h0: the waist slices through registers, 4 items in flight per thread.
+  {
+    const bool eq = a.nlat_odd && h0 == a.H - 1;
+    constexpr int kBatch = 4;
+    const int total = (a.T + 1) * G;
+    for (int base = threadIdx.x; base < total; base += kBatch * blockDim.x) {
+      float2 S[kBatch], D[kBatch];
+#pragma unroll
+      for (int u = 0; u < kBatch; ++u) {
+        const int t = base + u * blockDim.x;
+        const int m = t / G, g = t - m * G;
+        if (t < total && p0 + g < a.planes) {
+          S[u] = __ldcs(wP + ((int64_t)(m * 2 + 0) * a.H + h0) * Rc + p0 + g);
+          D[u] = __ldcs(wP + ((int64_t)(m * 2 + 1) * a.H + h0) * Rc + p0 + g);
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < kBatch; ++u) {
+        const int t = base + u * blockDim.x;
+        const int m = t / G, g = t - m * G;
+        if (t >= total || p0 + g >= a.planes) continue;
+#pragma unroll
+        for (int sd = 0; sd < 2; ++sd) {
+          if (sd == 1 && eq) continue;
+          const float sgn = sd ? -1.f : 1.f;
+          const float2 x = make_float2(S[u].x + sgn * D[u].x, S[u].y + sgn * D[u].y);
+          rows(g * 2 + sd)[m] =
+              a.mode == kUnfoldZonal ? make_float2(-(float)m * x.y, (float)m * x.x) : x;
+        }
+      }
+    }
+    __syncthreads();
+    if (plane < a.planes && !(eq && side == 1))
+      inverse_row_out<FF>(a, rows(warp), tws, tn, out, plane, side ? a.nlat - 1 - h0 : h0, lane);
+  }
+  if (!has1) return;
+  // Pair h1: from the staging buffer.
+  cp_async_wait_all();
+  __syncthreads();  // every thread's copies landed; the rows of h0 are free
+  {
+    const bool eq = a.nlat_odd && h1 == a.H - 1;
+    for (int t = threadIdx.x; t < (a.T + 1) * G; t += blockDim.x) {
+      const int m = t / G, g = t - m * G;
+      if (p0 + g >= a.planes) continue;
+      const float2 S = stage[(m * 2 + 0) * G + g], D = stage[(m * 2 + 1) * G + g];
+#pragma unroll
+      for (int sd = 0; sd < 2; ++sd) {
+        if (sd == 1 && eq) continue;
+        const float sgn = sd ? -1.f : 1.f;
+        const float2 x = make_float2(S.x + sgn * D.x, S.y + sgn * D.y);
+        rows(g * 2 + sd)[m] =
+            a.mode == kUnfoldZonal ? make_float2(-(float)m * x.y, (float)m * x.x) : x;
+      }
+    }
+    __syncthreads();
+    if (plane < a.planes && !(eq && side == 1))
+      inverse_row_out<FF>(a, rows(warp), tws, tn, out, plane, side ? a.nlat - 1 - h1 : h1, lane);
+  }
+}
+
+// The waist rows must be 16-byte aligned for cp.async: an even plane count.
+template <int FF>
+void launch_inv_pair(const sht_plan* p, int mode, const float* wP, int64_t planes, float* out,
+                     cudaStream_t s) {
+  FastUnfoldArgs a{p->nlat, p->nlon, p->T, p->H, p->nlat_odd ? 1 : 0, mode, 4, planes,
+                   (float)p->radius};
+  const int Hh = (int)div_up(p->H, 2);
+  dim3 grid((unsigned)div_up(planes, 4), (unsigned)Hh);
+  const size_t sm =
+      sizeof(float2) * (kWarps * WarpSmem<FF>::kFloats2 + FF * 32 + 2 * (p->T + 1) * 4);
+  SHT_CUDA_OR_THROW(cudaFuncSetAttribute(fast_inverse_pair<FF>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  fast_inverse_pair<FF><<<grid, kWarps * 32, sm, s>>>(a, (const float2*)wP, (const float2*)p->tw_l,
+                                                      (const float2*)p->tw_n, out, Hh);
+  SHT_CUDA_OR_THROW(cudaGetLastError());
+}
+
 template <int FF>
 void launch_fwd(const sht_plan* p, const float* g0, const float* g1, int64_t planes, float* wfold,
                 cudaStream_t s, float* rowmax) {
@@ -461,6 +610,8 @@ void launch_inv(const sht_plan* p, int mode, const float* wP, const float* wD, i
     launch_inv_nf<FF, 4>(p, mode, wP, wD, planes, out0, out1, s);
   else if (mode == kUnfoldGradient)
     launch_inv_nf<FF, 2>(p, mode, wP, wD, planes, out0, out1, s);
+  else if (planes % 2 == 0)
+    launch_inv_pair<FF>(p, mode, wP, planes, out0, s);
   else
     launch_inv_nf<FF, 1>(p, mode, wP, wD, planes, out0, out1, s);
 }
