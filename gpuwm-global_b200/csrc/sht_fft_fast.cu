@@ -242,8 +242,11 @@ __global__ void __launch_bounds__(kWarps * 32) fast_forward_fold(FastFoldArgs a,
   const int64_t p0 = (int64_t)blockIdx.x * a.G;
   const bool eq = a.nlat_odd && h == a.H - 1;
   const int pf = warp >> 1, side = warp & 1;
-  const int nper = a.G * a.F;
-  const int f = pf % a.F, gp = pf / a.F;
+  // Columns per CTA: 4 planes of one field or 2 planes of two, always
+  // kWarps / 2 (a compile-time divisor in the loops below).
+  constexpr int nper = kWarps / 2;
+  const int fsh = a.F == 2 ? 1 : 0;  // log2 of the field count
+  const int f = pf & (a.F - 1), gp = pf >> fsh;
   const int64_t plane = p0 + gp;
   const bool active = pf < nper && plane < a.planes && !(eq && side == 1);
   float2* reg = smem(warp);
@@ -266,7 +269,7 @@ __global__ void __launch_bounds__(kWarps * 32) fast_forward_fold(FastFoldArgs a,
   float mre = 0.f, mim = 0.f;         // this thread's column maxima (q = tid % nper)
   for (int t = threadIdx.x; t < (a.T + 1) * nper; t += blockDim.x) {
     int m = t / nper, q = t - m * nper;
-    int gq = q / a.F;
+    int gq = q >> fsh;
     if (p0 + gq >= a.planes) continue;
     float2 w = twN[m];
     float2 X[2];
@@ -293,7 +296,7 @@ __global__ void __launch_bounds__(kWarps * 32) fast_forward_fold(FastFoldArgs a,
   }
   if (rowmax != nullptr) {
     const int q = threadIdx.x % nper;  // fixed per thread: blockDim % nper == 0
-    rowmax_merge(rowmax, p0 * a.F + q, p0 + q / a.F < a.planes, mre, mim, nper);
+    rowmax_merge(rowmax, p0 * a.F + q, p0 + (q >> fsh) < a.planes, mre, mim, nper);
   }
 }
 
@@ -337,13 +340,14 @@ __global__ void __launch_bounds__(kWarps * 32) fast_inverse_unfold(FastUnfoldArg
   // antisymmetric pairs each), then combines them: the loads of a batch are
   // in flight together instead of one dependent round trip per item.
   constexpr int kBatch = NF == 4 ? 2 : 4;
-  const int total = (a.T + 1) * a.G;
+  constexpr int G = kWarps / 2 / NO;  // planes per CTA
+  const int total = (a.T + 1) * G;
   for (int base = threadIdx.x; base < total; base += kBatch * blockDim.x) {
     float2 S[kBatch][NF], D[kBatch][NF];
 #pragma unroll
     for (int u = 0; u < kBatch; ++u) {
       const int t = base + u * blockDim.x;
-      const int m = t / a.G, gp = t - m * a.G;
+      const int m = t / G, gp = t - m * G;
       if (t < total && p0 + gp < a.planes) {
         const int64_t r = (p0 + gp) * (NF == 4 ? 2 : 1);
         const int64_t c0 = ((int64_t)(m * 2 + 0) * a.H + h) * Rc + r;
@@ -360,7 +364,7 @@ __global__ void __launch_bounds__(kWarps * 32) fast_inverse_unfold(FastUnfoldArg
 #pragma unroll
     for (int u = 0; u < kBatch; ++u) {
       const int t = base + u * blockDim.x;
-      const int m = t / a.G, gp = t - m * a.G;
+      const int m = t / G, gp = t - m * G;
       if (t >= total || p0 + gp >= a.planes) continue;
 #pragma unroll
       for (int sd = 0; sd < 2; ++sd) {
@@ -391,7 +395,7 @@ __global__ void __launch_bounds__(kWarps * 32) fast_inverse_unfold(FastUnfoldArg
   const int po = warp >> 1, side = warp & 1;
   const int o = po % NO, gp = po / NO;
   const int64_t plane = p0 + gp;
-  if (po >= a.G * NO || plane >= a.planes || (eq && side == 1)) return;
+  if (po >= G * NO || plane >= a.planes || (eq && side == 1)) return;
   float2* reg = smem(warp);
   const float2* tn = opaque(twN);
   // Stage 2: entangle z[k] for k = lane + 32 j straight into registers.
