@@ -16,7 +16,8 @@
 namespace sht {
 namespace {
 
-// exp(-2 pi i k / 24), exp(-2 pi i k / 32) and exp(-2 pi i k / 16).
+// exp(-2 pi i k / 24), exp(-2 pi i k / 32) and exp(-2 pi i k / 16), uploaded
+// once per process: read as constant-bank operands of the butterfly FMAs.
 __constant__ float2 c_w24[24];
 __constant__ float2 c_w32[32];
 __constant__ float2 c_w16[16];
@@ -180,7 +181,7 @@ __device__ __forceinline__ void load_lane_twiddles(float2* tws, const float2* __
 
 // The L-point complex FFT of one warp's row: in registers z[j] = x[l + 32 j]
 // (lane l); out: the natural-order spectrum written to `reg` (length L).
-template <int F, bool INV>
+template <int F, bool INV, bool UNIFORM = false>
 __device__ __forceinline__ void warp_fft(float2 (&z)[F], float2* reg, const float2* tws, int lane) {
   dftF<F, INV>(z);
   // exp(-+2 pi i lane k1 / L)
@@ -190,14 +191,25 @@ __device__ __forceinline__ void warp_fft(float2 (&z)[F], float2* reg, const floa
   for (int k1 = 0; k1 < F; ++k1) reg[k1 * WarpSmem<F>::kStride + lane] = z[k1];
   __syncwarp();
   float2 y[32];
-  if (lane < F) {
+  if constexpr (UNIFORM) {
+    // Lanes >= F repeat another lane's row (a broadcast read) and drop their
+    // result: a branch around the whole 32-point DFT costs ~70 registers
+    // once the row pass sits inside a loop.
+    const int row = lane % F;
 #pragma unroll
-    for (int l = 0; l < 32; ++l) y[l] = reg[lane * WarpSmem<F>::kStride + l];
-  }
-  __syncwarp();
-  if (lane < F) {
+    for (int l = 0; l < 32; ++l) y[l] = reg[row * WarpSmem<F>::kStride + l];
+    __syncwarp();
     dft32<INV>(y);
-    // output index k = lane + F k2 (natural order)
+  } else {
+    if (lane < F) {
+#pragma unroll
+      for (int l = 0; l < 32; ++l) y[l] = reg[lane * WarpSmem<F>::kStride + l];
+    }
+    __syncwarp();
+    if (lane < F) dft32<INV>(y);
+  }
+  // output index k = lane + F k2 (natural order)
+  if (lane < F) {
 #pragma unroll
     for (int k2 = 0; k2 < 32; ++k2) reg[lane + F * k2] = y[k2];
   }
@@ -251,7 +263,9 @@ __global__ void __launch_bounds__(kWarps * 32) fast_forward_fold(FastFoldArgs a,
   const bool active = pf < nper && plane < a.planes && !(eq && side == 1);
   float2* reg = smem(warp);
   float2* tws = smem_dyn + kWarps * WarpSmem<FF>::kFloats2;
+  float2* twn = tws + FF * 32;  // the untangling twiddles exp(-2 pi i m / nlon), m <= T
   load_lane_twiddles<FF>(tws, twL);
+  for (int m = threadIdx.x; m <= a.T; m += blockDim.x) twn[m] = twN[m];
   __syncthreads();
   if (active) {
     const int j = side ? (a.nlat - 1 - h) : h;
@@ -264,14 +278,16 @@ __global__ void __launch_bounds__(kWarps * 32) fast_forward_fold(FastFoldArgs a,
   }
   __syncthreads();
   // Untangle, scale, fold, write: thread -> (m, pf) with pf fastest.
-  const float inv_n = 1.0f / (float)a.nlon;
+  // 0.5 / nlon: (x / 2) / nlon and x * (0.5 / nlon) round alike (both
+  // scalings by 2 are exact).
+  const float half_inv_n = 0.5f / (float)a.nlon;
   const int64_t Rc = a.planes * a.F;  // complex columns per waist row
   float mre = 0.f, mim = 0.f;         // this thread's column maxima (q = tid % nper)
   for (int t = threadIdx.x; t < (a.T + 1) * nper; t += blockDim.x) {
     int m = t / nper, q = t - m * nper;
     int gq = q >> fsh;
     if (p0 + gq >= a.planes) continue;
-    float2 w = twN[m];
+    float2 w = twn[m];
     float2 X[2];
 #pragma unroll
     for (int sd = 0; sd < 2; ++sd) {
@@ -284,7 +300,7 @@ __global__ void __launch_bounds__(kWarps * 32) fast_forward_fold(FastFoldArgs a,
       float2 zc = cconjf(zr[m == 0 ? 0 : L - m]);
       float2 ev = caddf(zk, zc), od = csubf(zk, zc);
       float2 t1 = cmulf(w, od);
-      X[sd] = make_float2(0.5f * (ev.x + t1.y) * inv_n, 0.5f * (ev.y - t1.x) * inv_n);
+      X[sd] = make_float2((ev.x + t1.y) * half_inv_n, (ev.y - t1.x) * half_inv_n);
     }
     float2 S = eq ? X[0] : caddf(X[0], X[1]);
     float2 D = eq ? make_float2(0.f, 0.f) : csubf(X[0], X[1]);
@@ -428,10 +444,10 @@ __global__ void __launch_bounds__(kWarps * 32) fast_inverse_unfold(FastUnfoldArg
 }
 
 // The scalar inverse (one waist column per plane: scalar, zonal, meridional)
-// two latitude pairs per CTA, h and h + ceil(H/2): the waist slices of the
-// second pair stream into a shared staging buffer with cp.async (no
-// registers held) while the warps FFT the first, so the load latency that a
-// one-pair CTA exposes at its barrier overlaps the butterflies.
+// as a persistent kernel: each CTA walks a strided list of items (4 planes x
+// one latitude pair), and the waist slices of its next item stream into a
+// shared staging buffer with cp.async (no registers held) while the warps
+// FFT the current one.  Only a CTA's first item exposes the gather latency.
 __device__ __forceinline__ void cp_async16(void* dst, const void* src, uint32_t src_bytes) {
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(
                    (uint32_t)__cvta_generic_to_shared(dst)),
@@ -444,7 +460,7 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 // Entangle, FFT and store this warp's row (plane p0 + gp, side) of pair h.
 template <int FF>
 __device__ __forceinline__ void inverse_row_out(const FastUnfoldArgs& a, float2* reg,
-                                                const float2* tws, const float2* __restrict__ tn,
+                                                const float2* tws, const float2* tn,
                                                 float* __restrict__ out, int64_t plane, int j,
                                                 int lane) {
   constexpr int L = 32 * FF;
@@ -461,85 +477,55 @@ __device__ __forceinline__ void inverse_row_out(const FastUnfoldArgs& a, float2*
     z[i] = make_float2(sm.x - wd.y, sm.y + wd.x);
   }
   __syncwarp();
-  warp_fft<FF, true>(z, reg, tws, lane);
+  warp_fft<FF, true, true>(z, reg, tws, lane);
   float2* dst = reinterpret_cast<float2*>(out + (plane * a.nlat + j) * (int64_t)a.nlon);
 #pragma unroll 4
   for (int i = 0; i < FF; ++i) __stcs(dst + lane + 32 * i, reg[lane + 32 * i]);
 }
 
 template <int FF>
-__global__ void __launch_bounds__(kWarps * 32) fast_inverse_pair(FastUnfoldArgs a,
-                                                                 const float2* __restrict__ wP,
-                                                                 const float2* __restrict__ twL,
-                                                                 const float2* __restrict__ twN,
-                                                                 float* __restrict__ out, int Hh) {
-  constexpr int G = 4;  // planes per CTA
+__global__ void __launch_bounds__(kWarps * 32, 2) fast_inverse_pair(FastUnfoldArgs a,
+                                                                    const float2* __restrict__ wP,
+                                                                    const float2* __restrict__ twL,
+                                                                    const float2* __restrict__ twN,
+                                                                    float* __restrict__ out,
+                                                                    int n_pb) {
+  constexpr int G = 4;  // planes per item
   extern __shared__ float2 smem_dyn[];
   auto rows = [&](int w) { return smem_dyn + w * WarpSmem<FF>::kFloats2; };
   float2* tws = smem_dyn + kWarps * WarpSmem<FF>::kFloats2;
-  float2* stage = tws + FF * 32;  // [(m, s)][G] waist slices of the second pair
+  float2* twn = tws + FF * 32;    // the entangling twiddles exp(-2 pi i k / nlon), k < L
+  float2* stage = twn + 32 * FF;  // [(m, s)][G] waist slices of the item in flight
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int h0 = blockIdx.y, h1 = blockIdx.y + Hh;
-  const bool has1 = h1 < a.H;
-  const int64_t p0 = (int64_t)blockIdx.x * G;
   const int64_t Rc = a.planes;
   const int nms = 2 * (a.T + 1);
-  load_lane_twiddles<FF>(tws, twL);
-  if (has1) {
+  const int64_t n_items = (int64_t)n_pb * a.H;
+  // Item i: plane block i % n_pb (fastest: CTAs that run together touch
+  // adjacent slices of every waist row), latitude pair i / n_pb.
+  auto prefetch = [&](int64_t item) {
+    const int h = (int)(item / n_pb);
+    const int64_t p0 = (item - (int64_t)h * n_pb) * G;
     for (int e = threadIdx.x; e < 2 * nms; e += blockDim.x) {
       const int ms = e >> 1, c = e & 1;
       const int64_t pc = p0 + 2 * c;
       const int64_t valid = a.planes - pc;
       const uint32_t bytes = valid >= 2 ? 16u : (valid == 1 ? 8u : 0u);
-      const float2* src = bytes ? wP + ((int64_t)ms * a.H + h1) * Rc + pc : wP;
+      const float2* src = bytes ? wP + ((int64_t)ms * a.H + h) * Rc + pc : wP;
       cp_async16(stage + ms * G + 2 * c, src, bytes);
     }
     cp_async_commit();
-  }
-  const float2* tn = opaque(twN);
+  };
+  int64_t item = blockIdx.x;
+  if (item < n_items) prefetch(item);
+  load_lane_twiddles<FF>(tws, twL);
+  for (int k = threadIdx.x; k < 32 * FF; k += blockDim.x) twn[k] = twN[k];
   const int gp = warp >> 1, side = warp & 1;
-  const int64_t plane = p0 + gp;
-  // Pair h0: the waist slices through registers, 4 items in flight per thread.
-  {
-    const bool eq = a.nlat_odd && h0 == a.H - 1;
-    constexpr int kBatch = 4;
-    const int total = (a.T + 1) * G;
-    for (int base = threadIdx.x; base < total; base += kBatch * blockDim.x) {
-      float2 S[kBatch], D[kBatch];
-#pragma unroll
-      for (int u = 0; u < kBatch; ++u) {
-        const int t = base + u * blockDim.x;
-        const int m = t / G, g = t - m * G;
-        if (t < total && p0 + g < a.planes) {
-          S[u] = __ldcs(wP + ((int64_t)(m * 2 + 0) * a.H + h0) * Rc + p0 + g);
-          D[u] = __ldcs(wP + ((int64_t)(m * 2 + 1) * a.H + h0) * Rc + p0 + g);
-        }
-      }
-#pragma unroll
-      for (int u = 0; u < kBatch; ++u) {
-        const int t = base + u * blockDim.x;
-        const int m = t / G, g = t - m * G;
-        if (t >= total || p0 + g >= a.planes) continue;
-#pragma unroll
-        for (int sd = 0; sd < 2; ++sd) {
-          if (sd == 1 && eq) continue;
-          const float sgn = sd ? -1.f : 1.f;
-          const float2 x = make_float2(S[u].x + sgn * D[u].x, S[u].y + sgn * D[u].y);
-          rows(g * 2 + sd)[m] =
-              a.mode == kUnfoldZonal ? make_float2(-(float)m * x.y, (float)m * x.x) : x;
-        }
-      }
-    }
-    __syncthreads();
-    if (plane < a.planes && !(eq && side == 1))
-      inverse_row_out<FF>(a, rows(warp), tws, tn, out, plane, side ? a.nlat - 1 - h0 : h0, lane);
-  }
-  if (!has1) return;
-  // Pair h1: from the staging buffer.
-  cp_async_wait_all();
-  __syncthreads();  // every thread's copies landed; the rows of h0 are free
-  {
-    const bool eq = a.nlat_odd && h1 == a.H - 1;
+  for (; item < n_items; item += gridDim.x) {
+    const int h = (int)(item / n_pb);
+    const int64_t p0 = (item - (int64_t)h * n_pb) * G;
+    const bool eq = a.nlat_odd && h == a.H - 1;
+    cp_async_wait_all();
+    __syncthreads();  // the item's slices landed; every warp stored its previous row
     for (int t = threadIdx.x; t < (a.T + 1) * G; t += blockDim.x) {
       const int m = t / G, g = t - m * G;
       if (p0 + g >= a.planes) continue;
@@ -553,26 +539,52 @@ __global__ void __launch_bounds__(kWarps * 32) fast_inverse_pair(FastUnfoldArgs 
             a.mode == kUnfoldZonal ? make_float2(-(float)m * x.y, (float)m * x.x) : x;
       }
     }
-    __syncthreads();
+    __syncthreads();  // the staging buffer is free again
+    if (item + gridDim.x < n_items) prefetch(item + gridDim.x);
+    const int64_t plane = p0 + gp;
+    // The lane index, made opaque per item: the per-lane masks and offsets of
+    // the row pass are rebuilt every item instead of held across the loop.
+    int ln = lane;
+    asm volatile("" : "+r"(ln));
     if (plane < a.planes && !(eq && side == 1))
-      inverse_row_out<FF>(a, rows(warp), tws, tn, out, plane, side ? a.nlat - 1 - h1 : h1, lane);
+      inverse_row_out<FF>(a, rows(warp), tws, twn, out, plane, side ? a.nlat - 1 - h : h, ln);
   }
 }
 
+// SMs of the current device, and resident CTAs per SM of a kernel with the
+// given block and dynamic shared memory (the latter also raised to `sm`).
+int sm_count() {
+  int dev = 0, sms = 0;
+  SHT_CUDA_OR_THROW(cudaGetDevice(&dev));
+  SHT_CUDA_OR_THROW(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  return sms;
+}
+template <typename K>
+int resident_ctas(K kernel, int threads, size_t sm) {
+  SHT_CUDA_OR_THROW(
+      cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  int per_sm = 0;
+  SHT_CUDA_OR_THROW(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, sm));
+  SHT_REQUIRE(per_sm > 0, "FFT kernel does not fit on an SM");
+  return per_sm;
+}
+
 // The waist rows must be 16-byte aligned for cp.async: an even plane count.
+// One persistent CTA per resident slot.
 template <int FF>
 void launch_inv_pair(const sht_plan* p, int mode, const float* wP, int64_t planes, float* out,
                      cudaStream_t s) {
   FastUnfoldArgs a{p->nlat, p->nlon, p->T, p->H, p->nlat_odd ? 1 : 0, mode, 4, planes,
                    (float)p->radius};
-  const int Hh = (int)div_up(p->H, 2);
-  dim3 grid((unsigned)div_up(planes, 4), (unsigned)Hh);
+  const int n_pb = (int)div_up(planes, 4);
   const size_t sm =
-      sizeof(float2) * (kWarps * WarpSmem<FF>::kFloats2 + FF * 32 + 2 * (p->T + 1) * 4);
-  SHT_CUDA_OR_THROW(cudaFuncSetAttribute(fast_inverse_pair<FF>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-  fast_inverse_pair<FF><<<grid, kWarps * 32, sm, s>>>(a, (const float2*)wP, (const float2*)p->tw_l,
-                                                      (const float2*)p->tw_n, out, Hh);
+      sizeof(float2) * (kWarps * WarpSmem<FF>::kFloats2 + 2 * FF * 32 + 2 * (p->T + 1) * 4);
+  const int64_t n_items = (int64_t)n_pb * p->H;
+  if (n_items == 0) return;
+  const int64_t ctas = std::min<int64_t>(
+      n_items, (int64_t)resident_ctas(fast_inverse_pair<FF>, kWarps * 32, sm) * sm_count());
+  fast_inverse_pair<FF><<<(unsigned)ctas, kWarps * 32, sm, s>>>(
+      a, (const float2*)wP, (const float2*)p->tw_l, (const float2*)p->tw_n, out, n_pb);
   SHT_CUDA_OR_THROW(cudaGetLastError());
 }
 
@@ -582,7 +594,7 @@ void launch_fwd(const sht_plan* p, const float* g0, const float* g1, int64_t pla
   FastFoldArgs a{p->nlat, p->nlon, p->T, p->H, p->nlat_odd ? 1 : 0, g1 ? 2 : 1, 0, planes};
   a.G = kWarps / 2 / a.F;
   dim3 grid((unsigned)div_up(planes, a.G), (unsigned)p->H);
-  const size_t sm = sizeof(float2) * (kWarps * WarpSmem<FF>::kFloats2 + FF * 32);
+  const size_t sm = sizeof(float2) * (kWarps * WarpSmem<FF>::kFloats2 + FF * 32 + p->T + 1);
   SHT_CUDA_OR_THROW(cudaFuncSetAttribute(fast_forward_fold<FF>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
   fast_forward_fold<FF><<<grid, kWarps * 32, sm, s>>>(a, g0, g1 ? g1 : g0, (const float2*)p->tw_l,
