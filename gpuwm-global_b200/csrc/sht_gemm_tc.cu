@@ -88,7 +88,7 @@ namespace {
 
 constexpr int BM = 128;
 constexpr int BK = 32;
-constexpr int STAGES = 3;
+constexpr int STAGES = 4;
 constexpr int NPARTS = 2;
 constexpr int NMAX = 128;   // tile N
 // TMEM accumulator plans (SHT_TUNE_ACCUMULATORS).  kAccurate: the main
@@ -126,9 +126,8 @@ constexpr int kOffBar = kOffRaw + STAGES * kRawStage;      // mbarriers (8 B eac
 constexpr int kNumBars = 4 * STAGES + 2 * kMaxNBuf + 1;
 static_assert(kOffRaw % 1024 == 0, "128-byte swizzled TMA destinations are 1024-byte aligned");
 constexpr int kOffMisc = kOffBar + kNumBars * 8;           // tmem base, abort flag
-constexpr int kOffCs = kOffMisc + 16;                      // [epilogue warps][NMAX] floats
-constexpr int kOffStage = (kOffCs + kEpiWarps * NMAX * 4 + 127) / 128 * 128;  // staging [NMAX][BM]
-constexpr int kSmemBytes = kOffStage + NMAX * BM * 4 + 1024;  // + alignment slack
+constexpr int kOffCs = (kOffMisc + 16 + 127) / 128 * 128;  // [epilogue warps][NMAX] floats
+constexpr int kSmemBytes = kOffCs + kEpiWarps * NMAX * 4 + 1024;  // + alignment slack
 static_assert(kSmemBytes <= 227 * 1024, "shared memory plan exceeds 227 KB");
 
 // ---------------------------------------------------------------- PTX
@@ -178,20 +177,6 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, i
 __device__ __forceinline__ void fence_proxy_async() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
-// Bulk shared -> global store of one staged output row, tracked by the
-// issuing thread's bulk group.
-__device__ __forceinline__ void bulk_s2g(void* dst, const void* src, uint32_t bytes) {
-  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst),
-               "r"(smem_u32(src)), "r"(bytes)
-               : "memory");
-}
-__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
-// The committed bulk stores have finished reading shared memory.
-__device__ __forceinline__ void bulk_wait_read() {
-  asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
-}
-// The committed bulk stores have completed.
-__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
 // Named barrier 1 over the eight epilogue warps; returns the OR of `pred`
 // over their 256 threads.
 __device__ __forceinline__ bool epi_bar_or(bool pred) {
@@ -204,7 +189,6 @@ __device__ __forceinline__ bool epi_bar_or(bool pred) {
       : "memory");
   return out != 0;
 }
-__device__ __forceinline__ void epi_bar() { asm volatile("bar.sync 1, 256;" ::: "memory"); }
 __device__ __forceinline__ void fence_barrier_init() {
   asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 }
@@ -520,21 +504,20 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
     }
   } else if (warp < kConvWarp0) {
     // ----------------------------------------------------------- epilogue
-    // Per tile: TMEM -> registers -> scaled values in the staging buffer
-    // [column][row].  The accumulator goes back to the MMA warp as soon as the
-    // staging is written; the staged columns (one output row x each, the data
-    // rows r contiguous) then leave as bulk shared->global stores, one per
-    // thread, which run while the next tile's MMAs do.  Two warps share each
-    // TMEM lane quarter, one per half of the tile's columns.  Every decision
-    // that steers the epilogue's named barrier is reduced over its eight
-    // warps (epi_bar_or), so all 256 threads take the same path, and the
-    // warp-collective tcgen05.ld is entered warp-uniformly.
+    // Per tile: TMEM -> registers -> scaled values stored straight to global
+    // memory.  Thread `row` of a warp pair owns one data row r of the tile and
+    // half of its columns; for each column the warp's 32 lanes write 32
+    // consecutive r (one 128-byte line per store), so no staging through
+    // shared memory is needed (the tensor core's operand reads have its whole
+    // bandwidth).  The accumulator goes back to the MMA warp once its last
+    // chunk is in registers.  Every decision that steers the epilogue's named
+    // barrier is reduced over its eight warps (epi_bar_or), so all 256 threads
+    // take the same path, and the warp-collective tcgen05.ld is entered
+    // warp-uniformly.
     const int eg = warp & 3;  // TMEM lane group accessible to this warp
     const int half = (warp - 2) / 4;
     const int row = eg * 32 + lane;
-    const int et = threadIdx.x - 64;  // 0 .. kEpiThreads - 1
     float* cs_s = reinterpret_cast<float*>(smem + kOffCs) + (warp - 2) * NMAX;  // this warp's copy
-    float* stage_s = reinterpret_cast<float*>(smem + kOffStage);
     uint32_t acc_it = 0;
     for (int t = blockIdx.x; t < a.n_tiles; t += gridDim.x) {
       const ShtTcTile tl = a.tiles[t];
@@ -566,7 +549,6 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
       }
       const uint32_t buf = acc_it % NBUF, acc_phase = (acc_it / NBUF) & 1;
       const bool failed = !wait_bar(&pp.acc_full[buf], acc_phase, pp, a.err, 5);
-      bulk_wait_read();  // this thread's stores of the previous tile have read the staging
       if (epi_bar_or(failed)) break;
       tc_fence_after();
       const uint32_t lane_off = ((uint32_t)(eg * 32) << 16) + buf * kAccCols;
@@ -574,47 +556,64 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
       // accumulators unwritten: only the segments that exist are read.
       const int nsteps = tl.kst * (BK / 16);
       const int nseg = nsteps < NMAIN ? nsteps : NMAIN;
-      for (int c0 = cbeg; c0 < cend; c0 += 16) {
-        // All four accumulators of the chunk are loaded before one wait.
-        uint32_t rc[16], rm[NMAIN][16];
-        tmem_ld16_async(tmem_base + lane_off + (uint32_t)(NMAIN * NMAX + c0), rc);  // corrections
-#pragma unroll
-        for (int g = 0; g < NMAIN; ++g)
-          if (g < nseg) tmem_ld16_async(tmem_base + lane_off + (uint32_t)(g * NMAX + c0), rm[g]);
-        tmem_wait16<true>(rc);
-#pragma unroll
-        for (int g = 0; g < NMAIN; ++g) tmem_wait16<false>(rm[g]);
-#pragma unroll
-        for (int i = 0; i < 16; ++i) {
-          float acc = __uint_as_float(rc[i]);
-#pragma unroll
-          for (int g = 0; g < NMAIN; ++g)
-            if (g < nseg) acc += __uint_as_float(rm[g][i]);
-          stage_s[(c0 + i) * BM + row] = acc * rs * cs_s[c0 + i];
-        }
-      }
-      tc_fence_before();
-      mbar_arrive(&pp.acc_empty[buf]);
-      ++acc_it;
-      fence_proxy_async();  // the staging writes, visible to the bulk-copy proxy
-      epi_bar();
+      // Columns past the problem's extent are not stored.
       const int ncols = min(tl.nsize, d.X - tl.n0);
-      if ((R & 3) == 0) {
-        // 16-byte aligned rows: epilogue thread `et` sends staged column `et`.
-        if (et < ncols) {
-          const int64_t nrows = R - tl.r0 < BM ? R - tl.r0 : (int64_t)BM;
-          bulk_s2g(outb + (int64_t)(tl.n0 + et) * R + tl.r0, stage_s + et * BM,
-                   (uint32_t)(nrows * 4));
+      float* dst = outb + (int64_t)tl.n0 * R + r;
+      bool released = false;
+      for (int c0 = cbeg; c0 < cend; c0 += 16) {
+        // The corrections and the first main segment, then the other
+        // segments one at a time: the sum is formed in the order corrections
+        // + segment 0 + segment 1 + ..., with at most 32 registers of
+        // accumulator data live.
+        float acc[16];
+        {
+          uint32_t rc[16], rm[16];
+          tmem_ld16_async(tmem_base + lane_off + (uint32_t)(NMAIN * NMAX + c0), rc);
+          tmem_ld16_async(tmem_base + lane_off + (uint32_t)c0, rm);
+          tmem_wait16<true>(rc);
+          tmem_wait16<false>(rm);
+#pragma unroll
+          for (int i = 0; i < 16; ++i) acc[i] = __uint_as_float(rc[i]) + __uint_as_float(rm[i]);
         }
-        bulk_commit();
-      } else if (r < R) {
-        // Row lengths that are not a multiple of 4 floats: plain stores of
-        // this thread's own row, over its half of the columns.
-        for (int c = cbeg; c < min(ncols, cend); ++c)
-          outb[(int64_t)(tl.n0 + c) * R + r] = stage_s[c * BM + row];
+#pragma unroll
+        for (int g = 1; g < NMAIN; ++g) {
+          if (g < nseg) {
+            uint32_t rm[16];
+            tmem_ld16_async(tmem_base + lane_off + (uint32_t)(g * NMAX + c0), rm);
+            tmem_wait16<true>(rm);
+#pragma unroll
+            for (int i = 0; i < 16; ++i) acc[i] += __uint_as_float(rm[i]);
+          }
+        }
+        if (c0 + 16 >= cend) {
+          // The last chunk is in registers: the accumulator set is free.
+          tc_fence_before();
+          mbar_arrive(&pp.acc_empty[buf]);
+          released = true;
+        }
+        if (r < R) {
+          // 32-bit column offsets (R < 2^26 is checked at launch): a 64-bit
+          // address per store would hold 32 more registers.
+          float* col = dst + (int64_t)c0 * R;
+          const int r32 = (int)R;
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            const float4 c4 = *reinterpret_cast<const float4*>(cs_s + c0 + 4 * q);
+            const float cq[4] = {c4.x, c4.y, c4.z, c4.w};
+#pragma unroll
+            for (int i4 = 0; i4 < 4; ++i4) {
+              const int i = 4 * q + i4;
+              if (c0 + i < ncols) col[i * r32] = acc[i] * rs * cq[i4];
+            }
+          }
+        }
       }
+      if (!released) {  // no columns in this warp's half
+        tc_fence_before();
+        mbar_arrive(&pp.acc_empty[buf]);
+      }
+      ++acc_it;
     }
-    bulk_wait_all();
   } else {
     // --------------------------------------------------------- converters
     // Thread -> (kk = ct % 8, 8-row group mg = (ct/8) % 16), K groups
@@ -1022,6 +1021,7 @@ void launch_gemm_tc_groups(const TcGroupSpec* g, int ngroups, TcTileCache* cache
   int64_t rows = 0;
   for (int i = 0; i < ngroups; ++i) {
     SHT_REQUIRE(g[i].plan->tc != nullptr, "tensor-core tables not built");
+    SHT_REQUIRE(g[i].R < ((int64_t)1 << 26), "tensor-core launch: too many data rows");
     key.push_back(g[i].direction);
     key.push_back(g[i].R);
     rows += g[i].R;
