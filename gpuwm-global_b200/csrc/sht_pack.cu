@@ -18,20 +18,21 @@ namespace {
 
 template <typename T> using V2 = typename Vec2<T>::type;
 
-// Row of (m, q, i) in the folded operand: orders below m fill
-// sum_{m' < m} (T + 1 - m') rows; parity 1 follows the parity-0 block.
-__device__ __forceinline__ int64_t cf_row(int T, int m, int q, int i) {
-  int64_t base = (int64_t)m * (T + 1) - (int64_t)m * (m - 1) / 2;
-  return base + (q ? parity_count(T, m, 0) : 0) + i;
+// Row base of order m in the folded operand Cfold (orders below m fill
+// sum_{m' < m} (T + 1 - m') rows); with size0 the size of its parity-0
+// block, row(m, q, i) = base + (q ? size0 : 0) + i.
+__device__ __forceinline__ int64_t cf_base(int T, int m) {
+  return (int64_t)m * (T + 1) - (int64_t)m * (m - 1) / 2;
 }
 
 // One CTA: 32 orders x NB degrees x 32 planes.  All NB x 4 loads of a thread
 // are issued before the CTA's one barrier, and the row maxima are merged over
-// the whole block before one atomic per column.
+// the whole block before one atomic per column.  INVLAP: divide by the
+// Laplacian eigenvalue -n(n+1)/a^2 (zero at degree 0, Imag = 0 at m = 0).
 template <typename T> struct PackCfg { static constexpr int NB = sizeof(T) == 4 ? 4 : 2; };
 
-template <typename T>
-__global__ void __launch_bounds__(256) pack_kernel(int Tn, double radius, int mode,
+template <typename T, bool INVLAP>
+__global__ void __launch_bounds__(256) pack_kernel(int Tn, double radius,
                                                    const V2<T>* __restrict__ c0,
                                                    const V2<T>* __restrict__ c1, int64_t planes,
                                                    int F, V2<T>* __restrict__ cf,
@@ -47,41 +48,49 @@ __global__ void __launch_bounds__(256) pack_kernel(int Tn, double radius, int mo
   const V2<T>* src = f ? c1 : c0;
   const int tx = threadIdx.x, ty = threadIdx.y;
   const int64_t t1 = Tn + 1;
+  {
+    const int m = m0 + tx;
+    V2<T> v[NB][4];
 #pragma unroll
-  for (int nb = 0; nb < NB; ++nb) {
-    const int n = n0 + nb;
+    for (int nb = 0; nb < NB; ++nb) {
+      const int n = n0 + nb;
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      const int pp = ty + 8 * k;
-      const int64_t p = p0 + pp;
-      const int m = m0 + tx;
-      V2<T> v = mk2<T>(T(0), T(0));
-      if (p < planes && n <= Tn && m <= n) v = __ldcs(src + (p * t1 + n) * t1 + m);
-      tile[nb][pp][tx] = v;
+      for (int k = 0; k < 4; ++k) {
+        const int64_t p = p0 + ty + 8 * k;
+        v[nb][k] = mk2<T>(T(0), T(0));
+        if (p < planes && n <= Tn && m <= n) v[nb][k] = __ldcs(src + (p * t1 + n) * t1 + m);
+      }
     }
+#pragma unroll
+    for (int nb = 0; nb < NB; ++nb)
+#pragma unroll
+      for (int k = 0; k < 4; ++k) tile[nb][ty + 8 * k][tx] = v[nb][k];
   }
   __syncthreads();
   const int64_t Rc = planes * F;
   const int64_t p = p0 + tx;
   float mre = 0.f, mim = 0.f;
   if (p < planes) {
+    V2<T>* col = cf + p * F + f;
 #pragma unroll
-    for (int nb = 0; nb < NB; ++nb) {
-      const int n = n0 + nb;
-      if (n > Tn) break;
-      const T eig = T(-((double)n * ((double)n + 1.0)) / (radius * radius));
+    for (int k = 0; k < 4; ++k) {
+      const int m = m0 + ty + 8 * k;
+      if (m > Tn) break;
+      const int64_t base = cf_base(Tn, m);
+      const int size0 = parity_count(Tn, m, 0);
 #pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        const int m = m0 + ty + 8 * k;
-        if (m > n) break;
+      for (int nb = 0; nb < NB; ++nb) {
+        const int n = n0 + nb;
+        if (n > Tn || m > n) continue;
         const int q = (n - m) & 1, i = (n - m) >> 1;
         V2<T> v = tile[nb][tx][ty + 8 * k];
-        if (mode == kPackInvLap) {
+        if constexpr (INVLAP) {
+          const T eig = T(-((double)n * ((double)n + 1.0)) / (radius * radius));
           // c / eig (complex by real), zero at degree 0
           v = n == 0 ? mk2<T>(T(0), T(0)) : mk2<T>(v.x / eig, v.y / eig);
           if (m == 0) v.y = T(0);  // project() inside inverse_laplacian
         }
-        cf[cf_row(Tn, m, q, i) * Rc + p * F + f] = v;
+        col[(base + (q ? size0 : 0) + i) * Rc] = v;
         mre = fmaxf(mre, (float)fabs(v.x));
         mim = fmaxf(mim, (float)fabs(v.y));
       }
@@ -106,53 +115,83 @@ __global__ void __launch_bounds__(256) pack_kernel(int Tn, double radius, int mo
 }
 
 // One CTA: 32 orders x NB degrees x 32 planes, every load issued before the
-// CTA's one barrier.
-template <typename T> struct UnpackCfg { static constexpr int NB = sizeof(T) == 4 ? 2 : 1; };
+// CTA's one barrier; a CTA wholly above the triangle writes zeros only.
+template <typename T, int MODE> struct UnpackCfg {
+  static constexpr int NO = MODE == kUnpackScalar ? 1 : 2;  // output fields
+  static constexpr int NB = sizeof(T) == 4 ? 2 : 1;
+};
 
-template <typename T>
-__global__ void __launch_bounds__(256) unpack_kernel(int Tn, int mode, const V2<T>* __restrict__ cf0,
+template <typename T, int MODE>
+__global__ void __launch_bounds__(256) unpack_kernel(int Tn, const V2<T>* __restrict__ cf0,
                                                      const V2<T>* __restrict__ cf1, int64_t planes,
                                                      V2<T>* __restrict__ o0, V2<T>* __restrict__ o1) {
-  constexpr int NB = UnpackCfg<T>::NB;
-  __shared__ V2<T> tile[2][NB][32][33];
+  constexpr int NB = UnpackCfg<T, MODE>::NB, NO = UnpackCfg<T, MODE>::NO;
+  __shared__ V2<T> tile[NO][NB][32][33];
   const int m0 = blockIdx.x * 32;
   const int n0 = blockIdx.y * NB;
   const int64_t p0 = (int64_t)blockIdx.z * 32;
   const int tx = threadIdx.x, ty = threadIdx.y;
   const int64_t t1 = Tn + 1;
-  const int F = mode == kUnpackVorDiv ? 2 : 1;
-  const int64_t Rc = planes * F;
-  const int64_t p = p0 + tx;
+  const V2<T> zero = mk2<T>(T(0), T(0));
+  if (m0 > n0 + NB - 1) {
 #pragma unroll
-  for (int nb = 0; nb < NB; ++nb) {
-    const int n = n0 + nb;
+    for (int nb = 0; nb < NB; ++nb) {
+      const int n = n0 + nb;
+      if (n > Tn) break;
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const int64_t pl = p0 + ty + 8 * k;
+        const int m = m0 + tx;
+        if (pl >= planes || m > Tn) continue;
+        const int64_t off = (pl * t1 + n) * t1 + m;
+        o0[off] = zero;
+        if (NO == 2) o1[off] = zero;
+      }
+    }
+    return;
+  }
+  const int64_t Rc = planes * NO;
+  const int64_t p = p0 + tx;
+  {
+    V2<T> va[NB][4], vb[NB][4];
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
-      const int mm = ty + 8 * k;
-      const int m = m0 + mm;
-      V2<T> va = mk2<T>(T(0), T(0)), vb = va;
-      if (n <= Tn && m <= n && p < planes) {
-        const int q = (n - m) & 1, i = (n - m) >> 1;
-        const int64_t row = cf_row(Tn, m, q, i);
-        if (mode == kUnpackScalar) {
-          va = __ldcs(cf0 + row * Rc + p);
-        } else {
-          // rot/shear rows hold (u, v) per plane: columns 2p (u), 2p+1 (v).
-          const V2<T> ru = __ldcs(cf0 + row * Rc + 2 * p), rv = __ldcs(cf0 + row * Rc + 2 * p + 1);
-          const V2<T> su = __ldcs(cf1 + row * Rc + 2 * p), sv = __ldcs(cf1 + row * Rc + 2 * p + 1);
-          const T mf = T(m);
-          // zeta = i m rot[v] + shear[u];  D = i m rot[u] - shear[v]
-          va = mk2<T>(-mf * rv.y + su.x, mf * rv.x + su.y);
-          vb = mk2<T>(-mf * ru.y - sv.x, mf * ru.x - sv.y);
-        }
-        if (m == 0) {
-          va.y = T(0);
-          vb.y = T(0);
+      const int m = m0 + ty + 8 * k;
+      const int64_t base = m <= Tn ? cf_base(Tn, m) : 0;
+      const int size0 = m <= Tn ? parity_count(Tn, m, 0) : 0;
+#pragma unroll
+      for (int nb = 0; nb < NB; ++nb) {
+        const int n = n0 + nb;
+        va[nb][k] = zero;
+        vb[nb][k] = zero;
+        if (n <= Tn && m <= n && p < planes) {
+          const int q = (n - m) & 1, i = (n - m) >> 1;
+          const int64_t row = base + (q ? size0 : 0) + i;
+          if constexpr (MODE == kUnpackScalar) {
+            va[nb][k] = __ldcs(cf0 + row * Rc + p);
+          } else {
+            // rot/shear rows hold (u, v) per plane: columns 2p (u), 2p+1 (v).
+            const V2<T> ru = __ldcs(cf0 + row * Rc + 2 * p), rv = __ldcs(cf0 + row * Rc + 2 * p + 1);
+            const V2<T> su = __ldcs(cf1 + row * Rc + 2 * p), sv = __ldcs(cf1 + row * Rc + 2 * p + 1);
+            const T mf = T(m);
+            // zeta = i m rot[v] + shear[u];  D = i m rot[u] - shear[v]
+            va[nb][k] = mk2<T>(-mf * rv.y + su.x, mf * rv.x + su.y);
+            vb[nb][k] = mk2<T>(-mf * ru.y - sv.x, mf * ru.x - sv.y);
+          }
+          if (m == 0) {
+            va[nb][k].y = T(0);
+            vb[nb][k].y = T(0);
+          }
         }
       }
-      tile[0][nb][tx][mm] = va;
-      tile[1][nb][tx][mm] = vb;
     }
+#pragma unroll
+    for (int nb = 0; nb < NB; ++nb)
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        tile[0][nb][tx][ty + 8 * k] = va[nb][k];
+        if (NO == 2) tile[NO - 1][nb][tx][ty + 8 * k] = vb[nb][k];
+      }
   }
   __syncthreads();
 #pragma unroll
@@ -168,7 +207,7 @@ __global__ void __launch_bounds__(256) unpack_kernel(int Tn, int mode, const V2<
       const int64_t off = (pl * t1 + n) * t1 + m;
       // Above the triangle the tile holds zeros.
       o0[off] = tile[0][nb][pp][tx];
-      if (mode == kUnpackVorDiv) o1[off] = tile[1][nb][pp][tx];
+      if (NO == 2) o1[off] = tile[NO - 1][nb][pp][tx];
     }
   }
 }
@@ -204,9 +243,25 @@ void launch_pack(const sht_plan* p, const T* coeff0, const T* coeff1, int64_t pl
   dim3 grid((unsigned)div_up(p->T + 1, 32), (unsigned)div_up(p->T + 1, PackCfg<T>::NB),
             (unsigned)(div_up(planes, 32) * F));
   SHT_REQUIRE(grid.z <= 65535, "too many planes for one pack launch");
-  pack_kernel<T><<<grid, dim3(32, 8), 0, s>>>(p->T, p->radius, mode, (const V2<T>*)coeff0,
-                                              (const V2<T>*)coeff1, planes, F, (V2<T>*)cfold,
-                                              rowmax);
+  if (mode == kPackInvLap)
+    pack_kernel<T, true><<<grid, dim3(32, 8), 0, s>>>(p->T, p->radius, (const V2<T>*)coeff0,
+                                                      (const V2<T>*)coeff1, planes, F,
+                                                      (V2<T>*)cfold, rowmax);
+  else
+    pack_kernel<T, false><<<grid, dim3(32, 8), 0, s>>>(p->T, p->radius, (const V2<T>*)coeff0,
+                                                       (const V2<T>*)coeff1, planes, F,
+                                                       (V2<T>*)cfold, rowmax);
+  SHT_CUDA_OR_THROW(cudaGetLastError());
+}
+
+template <typename T, int MODE>
+void launch_unpack_mode(const sht_plan* p, const T* cf0, const T* cf1, int64_t planes, T* out0,
+                        T* out1, cudaStream_t s) {
+  dim3 grid((unsigned)div_up(p->T + 1, 32), (unsigned)div_up(p->T + 1, UnpackCfg<T, MODE>::NB),
+            (unsigned)div_up(planes, 32));
+  SHT_REQUIRE(grid.z <= 65535, "too many planes for one unpack launch");
+  unpack_kernel<T, MODE><<<grid, dim3(32, 8), 0, s>>>(p->T, (const V2<T>*)cf0, (const V2<T>*)cf1,
+                                                      planes, (V2<T>*)out0, (V2<T>*)out1);
   SHT_CUDA_OR_THROW(cudaGetLastError());
 }
 
@@ -214,12 +269,10 @@ template <typename T>
 void launch_unpack(const sht_plan* p, int mode, const T* cf0, const T* cf1, int64_t planes,
                    T* out0, T* out1, cudaStream_t s) {
   if (planes == 0) return;
-  dim3 grid((unsigned)div_up(p->T + 1, 32), (unsigned)div_up(p->T + 1, UnpackCfg<T>::NB),
-            (unsigned)div_up(planes, 32));
-  SHT_REQUIRE(grid.z <= 65535, "too many planes for one unpack launch");
-  unpack_kernel<T><<<grid, dim3(32, 8), 0, s>>>(p->T, mode, (const V2<T>*)cf0, (const V2<T>*)cf1,
-                                                planes, (V2<T>*)out0, (V2<T>*)out1);
-  SHT_CUDA_OR_THROW(cudaGetLastError());
+  if (mode == kUnpackVorDiv)
+    launch_unpack_mode<T, kUnpackVorDiv>(p, cf0, cf1, planes, out0, out1, s);
+  else
+    launch_unpack_mode<T, kUnpackScalar>(p, cf0, cf1, planes, out0, out1, s);
 }
 
 template <typename T>
