@@ -930,7 +930,7 @@ int sht_plan_set_tuning(sht_plan* plan, int key, int value) {
         plan->tune_tc_ctas = value;
         break;
       case SHT_TUNE_ACCUMULATORS:
-        SHT_REQUIRE(value == 0 || value == 1, "SHT_TUNE_ACCUMULATORS is 0 or 1");
+        SHT_REQUIRE(value >= 0 && value <= 2, "SHT_TUNE_ACCUMULATORS is 0, 1 or 2");
         plan->tune_accumulators = value;
         break;
       default:

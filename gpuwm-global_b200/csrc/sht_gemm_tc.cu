@@ -30,10 +30,13 @@
 // gradient or wind synthesis, or the plans of a batch):
 //   warp 0      bulk-copy loader for the table stages; owns TMEM alloc/free
 //   warp 1      MMA issuer (one thread)
-//   warps 2-9   epilogue: tcgen05.ld of the accumulators, unscale, stage in
-//               shared memory, release the accumulators, bulk-store the tile
-//   warps 10-17 converters for the data operand
-// Pipelines: STAGES shared-memory stages (full/empty mbarriers) and one or two
+//   warps 2-9   epilogue: tcgen05.ld of the accumulators, unscale, release
+//               the accumulators, store the tile to global memory
+//   warps 10-17 converters for the data operand (into shared memory, or into
+//               TMEM for the kTmemA plan)
+// Pipelines: S shared-memory stages (full/empty mbarriers), NA data-operand
+// slots (the shared stages themselves, or TMEM slots with their own
+// full/empty mbarriers) and one or two
 // sets of TMEM accumulators of 128 columns each (full/empty mbarriers per set).  Every
 // mbarrier wait is bounded by a clock budget; on expiry the waiting thread
 // raises the plan's error word and a CTA abort flag, and the epilogue warps
@@ -88,23 +91,8 @@ namespace {
 
 constexpr int BM = 128;
 constexpr int BK = 32;
-constexpr int STAGES = 4;
 constexpr int NPARTS = 2;
 constexpr int NMAX = 128;   // tile N
-// TMEM accumulator plans (SHT_TUNE_ACCUMULATORS).  kAccurate: the main
-// product in three K-segment accumulators + corrections, one set (512
-// columns).  kOverlapped: one main accumulator + corrections, two sets, so the
-// epilogue drains one tile while the MMA fills the next (faster; the longer
-// truncated main sums raise the split error from about 3.6e-7 to 1.2e-6).
-template <int NMAIN_, int NBUF_>
-struct AccPlan {
-  static constexpr int NMAIN = NMAIN_;  // main-product accumulators (contiguous K segments)
-  static constexpr int NBUF = NBUF_;    // accumulator sets
-  static constexpr int kAccCols = (NMAIN + 1) * NMAX;  // one set: NMAIN mains + corrections
-  static_assert(NBUF * kAccCols <= 512, "TMEM holds 512 columns");
-};
-using kAccurate = AccPlan<3, 1>;
-using kOverlapped = AccPlan<1, 2>;
 constexpr int kMaxNBuf = 2;
 constexpr int kEpiWarps = 8;                     // two per TMEM lane quarter
 constexpr int kEpiThreads = kEpiWarps * 32;
@@ -113,22 +101,51 @@ constexpr int kConvWarp0 = 2 + kEpiWarps;
 constexpr int kThreads = kConvWarp0 * 32 + kConvThreads;  // 576
 constexpr long long kWaitBudget = 4000000000LL;  // clock cycles (~2 s)
 
-// Shared-memory plan (bytes).
+// Shared-memory pieces (bytes).
 constexpr int kAPart = BM * BK * 2;      // one FP16 part of the A stage: 8 KB
-constexpr int kBPart = NMAX * BK * 2;    // one FP16 part of the B stage: 16 KB
+constexpr int kBPart = NMAX * BK * 2;    // one FP16 part of the B stage: 8 KB
 constexpr int kALbo = (BM / 8) * 128;    // A: K-group stride (16 M-groups of 128 B)
-constexpr int kOffA = 0;                                   // [STAGES][NPARTS][kAPart]
-constexpr int kOffB = kOffA + STAGES * NPARTS * kAPart;    // [STAGES][NPARTS][kBPart]
-constexpr int kRawStage = BK * BM * 4;                     // FP32 data tile of a stage: 16 KB
-constexpr int kRawBox = BK * 32 * 4;                       // one TMA box: 32 rows x 32 k, 4 KB
-constexpr int kOffRaw = kOffB + STAGES * NPARTS * kBPart;  // [STAGES][4 boxes], 128B-swizzled
-constexpr int kOffBar = kOffRaw + STAGES * kRawStage;      // mbarriers (8 B each)
-constexpr int kNumBars = 4 * STAGES + 2 * kMaxNBuf + 1;
-static_assert(kOffRaw % 1024 == 0, "128-byte swizzled TMA destinations are 1024-byte aligned");
-constexpr int kOffMisc = kOffBar + kNumBars * 8;           // tmem base, abort flag
-constexpr int kOffCs = (kOffMisc + 16 + 127) / 128 * 128;  // [epilogue warps][NMAX] floats
-constexpr int kSmemBytes = kOffCs + kEpiWarps * NMAX * 4 + 1024;  // + alignment slack
-static_assert(kSmemBytes <= 227 * 1024, "shared memory plan exceeds 227 KB");
+constexpr int kRawStage = BK * BM * 4;   // FP32 data tile of a stage: 16 KB
+constexpr int kRawBox = BK * 32 * 4;     // one TMA box: 32 rows x 32 k, 4 KB
+
+// TMEM accumulator plans (SHT_TUNE_ACCUMULATORS).  kAccurate: the main
+// product in three K-segment accumulators + corrections, one set (512
+// columns).  kOverlapped: one main accumulator + corrections, two sets, so the
+// epilogue drains one tile while the MMA fills the next (faster; the longer
+// truncated main sums raise the split error from about 3.6e-7 to 1.2e-6).
+// kTmemA: two K-segment accumulators + corrections (384 columns) and the
+// converted data operand in the other 128 TMEM columns, so the MMA reads only
+// the table operand from shared memory (split error ~6e-7 at T511).
+template <int NMAIN_, int NBUF_, bool A_TMEM_ = false>
+struct AccPlan {
+  static constexpr int NMAIN = NMAIN_;  // main-product accumulators (contiguous K segments)
+  static constexpr int NBUF = NBUF_;    // accumulator sets
+  static constexpr int kAccCols = (NMAIN + 1) * NMAX;  // one set: NMAIN mains + corrections
+  // A_TMEM: the data operand's hi and lo FP16 parts (16 columns each per
+  // slot) live in TMEM after the accumulators.
+  static constexpr bool A_TMEM = A_TMEM_;
+  // Six shared stages with four TMEM slots measured slower than four and
+  // four (the extra slot commit per stage; the table loads are bandwidth-,
+  // not depth-limited), so both plans run four.
+  static constexpr int S = 4;   // shared stages: table (+ raw data) (+ A)
+  static constexpr int NA = 4;  // data-operand slots (TMEM or shared)
+  static constexpr int kATmem = NBUF * kAccCols;  // first A column in TMEM
+  static_assert(kATmem + (A_TMEM ? NA * 32 : 0) <= 512, "TMEM holds 512 columns");
+  // Shared-memory plan.
+  static constexpr int kOffA = 0;                                             // [NA][NPARTS][kAPart]
+  static constexpr int kOffB = kOffA + (A_TMEM ? 0 : NA * NPARTS * kAPart);   // [S][NPARTS][kBPart]
+  static constexpr int kOffRaw = kOffB + S * NPARTS * kBPart;                 // [S][4 boxes], swizzled
+  static constexpr int kOffBar = kOffRaw + S * kRawStage;                     // mbarriers (8 B each)
+  static constexpr int kNumBars = 3 * S + 2 * NA + 2 * kMaxNBuf + 1;
+  static_assert(kOffRaw % 1024 == 0, "128-byte swizzled TMA destinations are 1024-byte aligned");
+  static constexpr int kOffMisc = kOffBar + kNumBars * 8;           // tmem base, abort flag
+  static constexpr int kOffCs = (kOffMisc + 16 + 127) / 128 * 128;  // [epilogue warps][NMAX] floats
+  static constexpr int kSmemBytes = kOffCs + kEpiWarps * NMAX * 4 + 1024;  // + alignment slack
+  static_assert(kSmemBytes <= 227 * 1024, "shared memory plan exceeds 227 KB");
+};
+using kAccurate = AccPlan<3, 1>;
+using kOverlapped = AccPlan<1, 2>;
+using kTmemA = AccPlan<2, 1, true>;
 
 // ---------------------------------------------------------------- PTX
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -218,6 +235,27 @@ __device__ __forceinline__ void mma_f16(uint32_t d_tmem, uint64_t adesc, uint64_
       "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
       "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
       : "memory");
+}
+// The same with A from tensor memory (K-major: row m in lane m, two FP16 K
+// values per 32-bit column, the even one in the low half).
+__device__ __forceinline__ void mma_f16_ts(uint32_t d_tmem, uint32_t a_tmem, uint64_t bdesc,
+                                           uint32_t idesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, p;\n\t}" ::"r"(d_tmem),
+      "r"(a_tmem), "l"(bdesc), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+// tcgen05.st of 8 consecutive columns of this warp's 32 lanes, and the wait
+// for this thread's stores.
+__device__ __forceinline__ void tmem_st8(uint32_t taddr, const uint32_t (&r)[8]) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"r"(taddr),
+      "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7])
+      : "memory");
+}
+__device__ __forceinline__ void tmem_wait_st() {
+  asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
 }
 __device__ __forceinline__ void mma_commit(uint64_t* bar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
@@ -310,10 +348,11 @@ struct TcArgs {
 };
 
 struct Pipe {
-  uint64_t* full_a;
-  uint64_t* full_b;
-  uint64_t* empty;
-  uint64_t* full_raw;  // the FP32 data tile of a stage has landed (TMA)
+  uint64_t* full_a;    // [NA] the data operand of a slot is converted
+  uint64_t* full_b;    // [S]
+  uint64_t* empty;     // [S] the MMAs of a shared stage are done
+  uint64_t* full_raw;  // [S] the FP32 data tile of a stage has landed (TMA)
+  uint64_t* a_empty;   // [NA] the MMAs of a TMEM data slot are done (A_TMEM)
   uint64_t* acc_full;
   uint64_t* acc_empty;
   uint64_t* done;
@@ -341,28 +380,33 @@ __device__ bool wait_bar(uint64_t* bar, uint32_t parity, const Pipe& pp, unsigne
 template <typename Acc>
 __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_constant__ TcArgs a) {
   constexpr int NMAIN = Acc::NMAIN, NBUF = Acc::NBUF, kAccCols = Acc::kAccCols;
+  constexpr int S = Acc::S, NA = Acc::NA;
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   // 1024-byte align the working area.
   unsigned char* smem = smem_raw + ((1024 - (smem_u32(smem_raw) & 1023)) & 1023);
-  unsigned char* sA = smem + kOffA;
-  unsigned char* sB = smem + kOffB;
-  unsigned char* sRaw = smem + kOffRaw;
-  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + kOffBar);
-  uint32_t* tmem_base_smem = reinterpret_cast<uint32_t*>(smem + kOffMisc);
-  volatile int* abort_flag = reinterpret_cast<volatile int*>(smem + kOffMisc + 4);
+  unsigned char* sA = smem + Acc::kOffA;
+  unsigned char* sB = smem + Acc::kOffB;
+  unsigned char* sRaw = smem + Acc::kOffRaw;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + Acc::kOffBar);
+  uint32_t* tmem_base_smem = reinterpret_cast<uint32_t*>(smem + Acc::kOffMisc);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(smem + Acc::kOffMisc + 4);
   Pipe pp{bars,
-          bars + STAGES,
-          bars + 2 * STAGES,
-          bars + 3 * STAGES,
-          bars + 4 * STAGES,
-          bars + 4 * STAGES + kMaxNBuf,
-          bars + 4 * STAGES + 2 * kMaxNBuf,
+          bars + NA,
+          bars + NA + S,
+          bars + NA + 2 * S,
+          bars + NA + 3 * S,
+          bars + 2 * NA + 3 * S,
+          bars + 2 * NA + 3 * S + kMaxNBuf,
+          bars + 2 * NA + 3 * S + 2 * kMaxNBuf,
           abort_flag};
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (threadIdx.x == 0) {
-    for (int s = 0; s < STAGES; ++s) {
+    for (int s = 0; s < NA; ++s) {
       mbar_init(&pp.full_a[s], kConvThreads);
+      mbar_init(&pp.a_empty[s], 1);
+    }
+    for (int s = 0; s < S; ++s) {
       mbar_init(&pp.full_b[s], 1);
       mbar_init(&pp.empty[s], 1);
       mbar_init(&pp.full_raw[s], 1);
@@ -389,9 +433,9 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
     if (lane == 0) {
       int stage = 0;
       uint32_t phase = 0;
-      int armed[STAGES], armed_raw[STAGES];
+      int armed[S], armed_raw[S];
 #pragma unroll
-      for (int s = 0; s < STAGES; ++s) armed[s] = armed_raw[s] = -1;
+      for (int s = 0; s < S; ++s) armed[s] = armed_raw[s] = -1;
       for (int t = blockIdx.x; t < a.n_tiles && !*abort_flag; t += gridDim.x) {
         const ShtTcTile tl = a.tiles[t];
         const TcGroup& G = a.g[tl.group];
@@ -422,14 +466,14 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
                           (int)(d_row + (int64_t)ks * BK), &pp.full_raw[stage]);
             armed_raw[stage] = (int)phase;
           }
-          if (++stage == STAGES) { stage = 0; phase ^= 1; }
+          if (++stage == S) { stage = 0; phase ^= 1; }
         }
         if (!ok) break;
       }
       // Drain: the copies of every armed stage land before the CTA exits (in
       // normal operation the MMA has already waited on them; after an abort
       // this wait is what keeps a late copy from writing freed shared memory).
-      for (int s = 0; s < STAGES; ++s) {
+      for (int s = 0; s < S; ++s) {
         long long t0 = clock64();
         if (armed[s] >= 0)
           while (!mbar_try_wait(&pp.full_b[s], (uint32_t)armed[s]) && clock64() - t0 < kWaitBudget) {
@@ -444,8 +488,10 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
   } else if (warp == 1) {
     // --------------------------------------------------------------- MMA
     if (lane == 0) {
-      int stage = 0;
+      int stage = 0;  // shared stage (table; data when !A_TMEM)
       uint32_t phase = 0;
+      int aslot = 0;  // TMEM data slot (A_TMEM)
+      uint32_t aphase = 0;
       uint32_t acc_it = 0;  // accumulator set = acc_it % NBUF, parity = (acc_it / NBUF) & 1
       bool issued = false;
       for (int t = blockIdx.x; t < a.n_tiles && !*abort_flag; t += gridDim.x) {
@@ -456,13 +502,15 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
         const uint32_t d_set = tmem_base + buf * kAccCols;
         const uint32_t d_corr = d_set + NMAIN * NMAX;
         tc_fence_after();
-        const uint32_t idesc = instr_desc(tl.nsize);
+        // A from TMEM is K-major (no transpose bit).
+        const uint32_t idesc = Acc::A_TMEM ? instr_desc(tl.nsize) & ~(1u << 15) : instr_desc(tl.nsize);
         const uint32_t lbo_b = (uint32_t)tl.nsize * 16;
         const int nsteps = tl.kst * (BK / 16);  // K steps of 16 in the tile
         int seg_prev = -1;
         bool ok = true;
         for (int ks = 0; ks < tl.kst; ++ks) {
-          if (!wait_bar(&pp.full_a[stage], phase, pp, a.err, 3) ||
+          if (!wait_bar(Acc::A_TMEM ? &pp.full_a[aslot] : &pp.full_a[stage],
+                        Acc::A_TMEM ? aphase : phase, pp, a.err, 3) ||
               !wait_bar(&pp.full_b[stage], phase, pp, a.err, 4)) {
             ok = false;
             break;
@@ -482,13 +530,25 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
             const uint32_t accum_main = seg == seg_prev ? 1u : 0u;
             seg_prev = seg;
             const uint32_t accum_corr = step > 0 ? 1u : 0u;
-            mma_f16(d_set + (uint32_t)(seg * NMAX), da1, db1, idesc, accum_main);  // a1 b1
-            mma_f16(d_corr, da1, db2, idesc, accum_corr);                              // a1 b2
-            mma_f16(d_corr, da2, db1, idesc, 1u);                                      // a2 b1
+            if constexpr (Acc::A_TMEM) {
+              const uint32_t ta1 = tmem_base + (uint32_t)(Acc::kATmem + aslot * 32 + j * 8);
+              const uint32_t ta2 = ta1 + 16;
+              mma_f16_ts(d_set + (uint32_t)(seg * NMAX), ta1, db1, idesc, accum_main);  // a1 b1
+              mma_f16_ts(d_corr, ta1, db2, idesc, accum_corr);                              // a1 b2
+              mma_f16_ts(d_corr, ta2, db1, idesc, 1u);                                      // a2 b1
+            } else {
+              mma_f16(d_set + (uint32_t)(seg * NMAX), da1, db1, idesc, accum_main);  // a1 b1
+              mma_f16(d_corr, da1, db2, idesc, accum_corr);                              // a1 b2
+              mma_f16(d_corr, da2, db1, idesc, 1u);                                      // a2 b1
+            }
           }
           issued = true;
           mma_commit(&pp.empty[stage]);  // frees the stage when these MMAs finish
-          if (++stage == STAGES) { stage = 0; phase ^= 1; }
+          if (++stage == S) { stage = 0; phase ^= 1; }
+          if constexpr (Acc::A_TMEM) {
+            mma_commit(&pp.a_empty[aslot]);  // and the TMEM data slot
+            if (++aslot == NA) { aslot = 0; aphase ^= 1; }
+          }
         }
         if (!ok) break;
         mma_commit(&pp.acc_full[buf]);
@@ -517,7 +577,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
     const int eg = warp & 3;  // TMEM lane group accessible to this warp
     const int half = (warp - 2) / 4;
     const int row = eg * 32 + lane;
-    float* cs_s = reinterpret_cast<float*>(smem + kOffCs) + (warp - 2) * NMAX;  // this warp's copy
+    float* cs_s = reinterpret_cast<float*>(smem + Acc::kOffCs) + (warp - 2) * NMAX;  // this warp's copy
     uint32_t acc_it = 0;
     for (int t = blockIdx.x; t < a.n_tiles; t += gridDim.x) {
       const ShtTcTile tl = a.tiles[t];
@@ -614,6 +674,75 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
       }
       ++acc_it;
     }
+  } else if constexpr (Acc::A_TMEM) {
+    // ------------------------------------------- converters (A into TMEM)
+    // Warp -> TMEM lane quarter q4 = warp % 4 (the lanes it may access) and
+    // K half kh; lane -> data row q4*32 + lane of the tile.  Each thread
+    // splits its row's 16 K values of the stage into FP16 hi/lo pairs and
+    // stores them as 8 + 8 columns of the stage's A slot.
+    const int q4 = warp & 3, kh = (warp - kConvWarp0) >> 2;
+    const int rowi = q4 * 32 + lane;
+    const uint32_t lane_base = tmem_base + ((uint32_t)(q4 * 32) << 16);
+    int stage = 0;  // shared stage of the raw data (TMA)
+    uint32_t phase = 0;
+    int aslot = 0;  // TMEM data slot
+    uint32_t aphase = 0;
+    for (int t = blockIdx.x; t < a.n_tiles; t += gridDim.x) {
+      const ShtTcTile tl = a.tiles[t];
+      if (tl.kst == 0) continue;
+      const TcGroup& G = a.g[tl.group];
+      const ShtGemmDesc d = G.descs[tl.problem];
+      const int64_t R = G.R;
+      const int64_t r = tl.r0 + rowi;
+      const float sc = r < R ? pow2_scale(G.rowmax[r]) : 1.f;
+      const float* Db = G.data + d.d_row * R;
+      bool ok = true;
+      for (int ks = 0; ks < tl.kst; ++ks) {
+        float v[16];
+        // The TMEM slot's previous MMAs are done.
+        ok = wait_bar(&pp.a_empty[aslot], aphase ^ 1, pp, a.err, 7);
+        if (!ok) break;
+        if (G.use_tma) {
+          // Box q4 of the stage holds rows q4*32 .. +31 as 128-byte k rows,
+          // 16-byte chunks swizzled by k % 8.
+          ok = wait_bar(&pp.full_raw[stage], phase, pp, a.err, 8);
+          if (!ok) break;
+          const unsigned char* box = sRaw + stage * kRawStage + q4 * kRawBox;
+#pragma unroll
+          for (int i = 0; i < 16; ++i) {
+            const int kl = kh * 16 + i;
+            const float x = *reinterpret_cast<const float*>(
+                box + kl * 128 + ((((lane >> 2) ^ (kl & 7))) << 4) + (lane & 3) * 4);
+            v[i] = ks * BK + kl < d.K ? x : 0.f;  // rows past K belong to the next problem
+          }
+        } else {
+#pragma unroll
+          for (int i = 0; i < 16; ++i) {
+            const int k = ks * BK + kh * 16 + i;
+            v[i] = (k < d.K && r < R) ? __ldg(Db + (int64_t)k * R + r) : 0.f;
+          }
+        }
+        uint32_t hi[8], lo[8];
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+          const float x0 = v[2 * c] * sc, x1 = v[2 * c + 1] * sc;
+          const float a0 = round_to_11_bits(x0), a1 = round_to_11_bits(x1);
+          const __half2 h1 = __floats2half2_rn(a0, a1);           // exact: 11 significant bits
+          const __half2 h2 = __floats2half2_rn(x0 - a0, x1 - a1);  // the remainder, exact in FP32
+          hi[c] = *reinterpret_cast<const uint32_t*>(&h1);
+          lo[c] = *reinterpret_cast<const uint32_t*>(&h2);
+        }
+        const uint32_t ta = lane_base + (uint32_t)(Acc::kATmem + aslot * 32 + kh * 8);
+        tmem_st8(ta, hi);
+        tmem_st8(ta + 16, lo);
+        tmem_wait_st();
+        tc_fence_before();
+        mbar_arrive(&pp.full_a[aslot]);
+        if (++aslot == NA) { aslot = 0; aphase ^= 1; }
+        if (++stage == S) { stage = 0; phase ^= 1; }
+      }
+      if (!ok) break;
+    }
   } else {
     // --------------------------------------------------------- converters
     // Thread -> (kk = ct % 8, 8-row group mg = (ct/8) % 16), K groups
@@ -699,7 +828,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
         }
         fence_proxy_async();
         mbar_arrive(&pp.full_a[stage]);
-        if (++stage == STAGES) { stage = 0; phase ^= 1; }
+        if (++stage == S) { stage = 0; phase ^= 1; }
         return true;
       };
       bool ok = true;
@@ -914,9 +1043,12 @@ void build_tc_tables(sht_plan* p, const double* basis64, const double* dbasis64,
       cudaFree(colmul[dir]);
     }
     SHT_CUDA_OR_THROW(cudaFuncSetAttribute(tc_gemm_kernel<kOverlapped>,
-                                           cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes));
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           kOverlapped::kSmemBytes));
     SHT_CUDA_OR_THROW(cudaFuncSetAttribute(tc_gemm_kernel<kAccurate>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           kSmemBytes));
+                                           kAccurate::kSmemBytes));
+    SHT_CUDA_OR_THROW(cudaFuncSetAttribute(tc_gemm_kernel<kTmemA>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           kTmemA::kSmemBytes));
   } catch (...) {
     p->tc = tc;
     destroy_tc_tables(p);
@@ -1104,9 +1236,11 @@ void launch_gemm_tc_groups(const TcGroupSpec* g, int ngroups, TcTileCache* cache
   const int ctas = g[0].plan->tune_tc_ctas > 0 ? g[0].plan->tune_tc_ctas : g[0].plan->tc->sm_count;
   const int grid = std::min(list.n, ctas);
   if (g[0].plan->tune_accumulators == 1)
-    tc_gemm_kernel<kOverlapped><<<grid, kThreads, kSmemBytes, s>>>(a);
+    tc_gemm_kernel<kOverlapped><<<grid, kThreads, kOverlapped::kSmemBytes, s>>>(a);
+  else if (g[0].plan->tune_accumulators == 2)
+    tc_gemm_kernel<kTmemA><<<grid, kThreads, kTmemA::kSmemBytes, s>>>(a);
   else
-    tc_gemm_kernel<kAccurate><<<grid, kThreads, kSmemBytes, s>>>(a);
+    tc_gemm_kernel<kAccurate><<<grid, kThreads, kAccurate::kSmemBytes, s>>>(a);
   SHT_CUDA_OR_THROW(cudaGetLastError());
 }
 

@@ -66,7 +66,8 @@ struct sht_plan {
   int tune_contraction = 0;  // 1: FP32 SIMT contraction on a split16 plan
   int tune_tile_order = 0;   // tensor-core tile order (0: row blocks innermost, 1: column tiles)
   int tune_tc_ctas = 0;      // tensor-core CTAs per launch (0: one per SM)
-  int tune_accumulators = 0; // tensor-core accumulators (0: three K segments; 1: one, double-buffered)
+  int tune_accumulators = 0; // tensor-core accumulators (0: three K segments; 1: one, double-buffered;
+                             // 2: two K segments, data operand in TMEM)
 
   // GEMM descriptors: [direction][flip] (direction 0 synthesis, 1 analysis).
   ShtGemmDesc* d_desc[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};

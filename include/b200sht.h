@@ -208,8 +208,10 @@ int sht_helmholtz_apply(sht_plan* plan, const sht_vertical* op, double tau_w,
  *   SHT_TUNE_ACCUMULATORS tensor-core accumulators: 0: the main product in
  *                        three K-segment accumulators (split error ~3.6e-7 at
  *                        T511); 1: one, double-buffered so the epilogue
- *                        overlaps the next tile (~4 % faster pair, error
- *                        ~1.2e-6, still within 2e-6)
+ *                        overlaps the next tile (~3 % faster pair, error
+ *                        ~1.2e-6, still within 2e-6); 2: two K segments with
+ *                        the data operand held in tensor memory (~1 % faster,
+ *                        error ~6e-7)
  * Set between calls, not while a call of the plan is in flight. */
 #define SHT_TUNE_CONTRACTION 0
 #define SHT_TUNE_FFT 1

@@ -51,9 +51,11 @@ def test_tuning_errors():
         set_tuning(f64, contraction=1)
     with pytest.raises(ValueError, match="unknown tuning setting"):
         set_tuning(f64, band=3)
+    with pytest.raises(ValueError, match="SHT_TUNE_ACCUMULATORS"):
+        set_tuning(f64, accumulators=3)
 
 
-@pytest.mark.parametrize("acc", [0, 1])
+@pytest.mark.parametrize("acc", [0, 1, 2])
 def test_accumulator_plans_meet_the_bar_at_t255(acc):
     from b200sht import SphericalHarmonicTransform, VorticityDivergenceOperator
     from b200sht.autotune import set_tuning
