@@ -52,6 +52,9 @@ SIGNATURES = {
                                             ctypes.c_int, ctypes.c_int]),
     "sht_forward": (ctypes.c_int, [_P, _P, _I64, _P, _P]),
     "sht_forward_static_scratch": (ctypes.c_int, [_P, _P, _I64, _P, _P]),
+    "sht_forward_host": (ctypes.c_int, [_P, _P, _I64, _P, _I64]),
+    "sht_inverse_host": (ctypes.c_int, [_P, _P, _I64, _P, _I64]),
+    "sht_round_trip_host": (ctypes.c_int, [_P, _P, _I64, _P, _I64]),
     "sht_inverse": (ctypes.c_int, [_P, _P, _I64, _P, _P]),
     "sht_inverse_meridional_derivative": (ctypes.c_int, [_P, _P, _I64, _P, _P]),
     "sht_inverse_zonal_derivative": (ctypes.c_int, [_P, _P, _I64, _P, _P]),

@@ -251,6 +251,49 @@ class SphericalHarmonicTransform:
         """spectral -> grid (transform.py:1742)."""
         return self._synth("sht_inverse", coeff)
 
+    # ------------------------------------------------- host-resident batches
+    def _host_call(self, name, src, in_dtype, in_tail, out_tail, out_dtype, out, chunk):
+        """One host-streamed C-ABI call: host input, host output."""
+        x = torch.as_tensor(src)
+        if x.device.type != "cpu":
+            raise ValueError("host-streamed calls take host (CPU) arrays")
+        if x.dtype != in_dtype:
+            x = x.to(in_dtype)
+        x = x.contiguous()
+        if tuple(x.shape[-2:]) != in_tail:
+            raise ValueError(f"input has trailing shape {tuple(x.shape[-2:])}, expected {in_tail}")
+        lead = tuple(x.shape[:-2])
+        if out is None:
+            out = torch.empty((*lead, *out_tail), dtype=out_dtype, pin_memory=True)
+        elif (out.device.type != "cpu" or out.dtype != out_dtype or not out.is_contiguous()
+              or tuple(out.shape) != (*lead, *out_tail)):
+            raise ValueError("out must be a contiguous host tensor of shape "
+                             f"{(*lead, *out_tail)} and dtype {out_dtype}")
+        self.contraction_count += 1
+        _lib.call(name, self.plan.handle, x.data_ptr(), self._planes(x), out.data_ptr(), int(chunk))
+        return out
+
+    def forward_host(self, field, *, out=None, chunk: int = 0):
+        """grid -> spectral for host-resident fields, copies pipelined with the
+        transforms in chunks of planes (sht_forward_host); returns a host
+        tensor (page-locked when allocated here)."""
+        return self._host_call("sht_forward_host", field, self.backend.float_dtype,
+                               self.grid.shape, self.spectral_shape, self.backend.complex_dtype,
+                               out, chunk)
+
+    def inverse_host(self, coeff, *, out=None, chunk: int = 0):
+        """spectral -> grid for host-resident coefficients (sht_inverse_host)."""
+        return self._host_call("sht_inverse_host", coeff, self.backend.complex_dtype,
+                               self.spectral_shape, self.grid.shape, self.backend.float_dtype,
+                               out, chunk)
+
+    def round_trip_host(self, field, *, out=None, chunk: int = 0):
+        """inverse(forward(field)) for host-resident fields (sht_round_trip_host):
+        grid in, grid out, the coefficients stay on the device."""
+        return self._host_call("sht_round_trip_host", field, self.backend.float_dtype,
+                               self.grid.shape, self.grid.shape, self.backend.float_dtype,
+                               out, chunk)
+
     def inverse_meridional_derivative(self, coeff):
         """d field / d latitude in grid space (transform.py:1748)."""
         return self._synth("sht_inverse_meridional_derivative", coeff)

@@ -86,6 +86,17 @@ struct sht_plan {
   unsigned* d_err = nullptr;
   cudaStream_t last_stream = nullptr;
 
+  // Host-resident streaming (sht_*_host): copy-in, compute and copy-out
+  // streams and kHostSlots device slots of (input, intermediate, output)
+  // chunk buffers, created on first use.
+  static constexpr int kHostSlots = 3;
+  struct HostStream {
+    cudaStream_t s_in = nullptr, s_comp = nullptr, s_out = nullptr;
+    cudaEvent_t h2d[kHostSlots] = {}, comp[kHostSlots] = {}, d2h[kHostSlots] = {};
+    void* buf[kHostSlots][3] = {};  // [slot][input, intermediate, output]
+    size_t cap[3] = {0, 0, 0};      // bytes per slot of each buffer
+  } hs;
+
   // Per-kernel timing (sht_plan_set_timing / sht_plan_read_timing).
   struct TimingRec {
     int kind;

@@ -128,6 +128,24 @@ int sht_forward_static_scratch(sht_plan* plan, const void* grid, int64_t planes,
 /* spectral -> grid.  SphericalHarmonicTransform.inverse (transform.py:1742). */
 int sht_inverse(sht_plan* plan, const void* coeff, int64_t planes, void* grid, void* stream);
 
+/* Host-resident fields.  The reference accepts host (numpy) arrays and
+ * moves them to its backend's device inside forward/inverse
+ * (transform.py:1486, 1742); these are that path for whole batches: planes
+ * move host -> device -> host in chunks of `chunk` planes (0: about a
+ * sixteenth of the planes, even) on three internal streams, so the copies of
+ * neighbouring chunks overlap each other and the transforms.  Host buffers
+ * should be page-locked (cudaHostAlloc / cudaHostRegister) for the copies to
+ * run asynchronously; pageable memory works, without the overlap.  The
+ * calls return when the output is on the host.  sht_round_trip_host is the
+ * forward transform followed by the inverse (grid in, grid out, the
+ * spectral coefficients never leave the device). */
+int sht_forward_host(sht_plan* plan, const void* host_grid, int64_t planes, void* host_coeff,
+                     int64_t chunk);
+int sht_inverse_host(sht_plan* plan, const void* host_coeff, int64_t planes, void* host_grid,
+                     int64_t chunk);
+int sht_round_trip_host(sht_plan* plan, const void* host_grid, int64_t planes, void* host_out,
+                        int64_t chunk);
+
 /* d/dphi synthesis.  inverse_meridional_derivative (transform.py:1748). */
 int sht_inverse_meridional_derivative(sht_plan* plan, const void* coeff, int64_t planes,
                                       void* grid, void* stream);
