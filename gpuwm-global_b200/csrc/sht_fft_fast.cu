@@ -483,17 +483,19 @@ __device__ __forceinline__ void inverse_row_out(const FastUnfoldArgs& a, float2*
   for (int i = 0; i < FF; ++i) __stcs(dst + lane + 32 * i, reg[lane + 32 * i]);
 }
 
-template <int FF>
-__global__ void __launch_bounds__(kWarps * 32, 2) fast_inverse_pair(FastUnfoldArgs a,
-                                                                    const float2* __restrict__ wP,
-                                                                    const float2* __restrict__ twL,
-                                                                    const float2* __restrict__ twN,
-                                                                    float* __restrict__ out,
-                                                                    int n_pb) {
-  constexpr int G = 4;  // planes per item
+// G planes per item (even), 2G warps per CTA: one row (plane, side) each.
+template <int FF, int G>
+__global__ void __launch_bounds__(2 * G * 32, 8 / G) fast_inverse_pair(FastUnfoldArgs a,
+                                                                       const float2* __restrict__ wP,
+                                                                       const float2* __restrict__ twL,
+                                                                       const float2* __restrict__ twN,
+                                                                       float* __restrict__ out,
+                                                                       int n_pb) {
+  static_assert(G % 2 == 0, "cp.async moves planes in pairs");
+  constexpr int kW = 2 * G;  // warps
   extern __shared__ float2 smem_dyn[];
   auto rows = [&](int w) { return smem_dyn + w * WarpSmem<FF>::kFloats2; };
-  float2* tws = smem_dyn + kWarps * WarpSmem<FF>::kFloats2;
+  float2* tws = smem_dyn + kW * WarpSmem<FF>::kFloats2;
   float2* twn = tws + FF * 32;    // the entangling twiddles exp(-2 pi i k / nlon), k < L
   float2* stage = twn + 32 * FF;  // [(m, s)][G] waist slices of the item in flight
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -505,8 +507,9 @@ __global__ void __launch_bounds__(kWarps * 32, 2) fast_inverse_pair(FastUnfoldAr
   auto prefetch = [&](int64_t item) {
     const int h = (int)(item / n_pb);
     const int64_t p0 = (item - (int64_t)h * n_pb) * G;
-    for (int e = threadIdx.x; e < 2 * nms; e += blockDim.x) {
-      const int ms = e >> 1, c = e & 1;
+    constexpr int kPairs = G / 2;  // 16-byte chunks (plane pairs) per waist slice
+    for (int e = threadIdx.x; e < kPairs * nms; e += blockDim.x) {
+      const int ms = e / kPairs, c = e - ms * kPairs;
       const int64_t pc = p0 + 2 * c;
       const int64_t valid = a.planes - pc;
       const uint32_t bytes = valid >= 2 ? 16u : (valid == 1 ? 8u : 0u);
@@ -571,19 +574,21 @@ int resident_ctas(K kernel, int threads, size_t sm) {
 
 // The waist rows must be 16-byte aligned for cp.async: an even plane count.
 // One persistent CTA per resident slot.
+constexpr int kInvPairPlanes = 2;  // planes per item of the persistent inverse
 template <int FF>
 void launch_inv_pair(const sht_plan* p, int mode, const float* wP, int64_t planes, float* out,
                      cudaStream_t s) {
-  FastUnfoldArgs a{p->nlat, p->nlon, p->T, p->H, p->nlat_odd ? 1 : 0, mode, 4, planes,
+  constexpr int G = kInvPairPlanes, kW = 2 * G;
+  FastUnfoldArgs a{p->nlat, p->nlon, p->T, p->H, p->nlat_odd ? 1 : 0, mode, G, planes,
                    (float)p->radius};
-  const int n_pb = (int)div_up(planes, 4);
+  const int n_pb = (int)div_up(planes, G);
   const size_t sm =
-      sizeof(float2) * (kWarps * WarpSmem<FF>::kFloats2 + 2 * FF * 32 + 2 * (p->T + 1) * 4);
+      sizeof(float2) * (kW * WarpSmem<FF>::kFloats2 + 2 * FF * 32 + 2 * (p->T + 1) * G);
   const int64_t n_items = (int64_t)n_pb * p->H;
   if (n_items == 0) return;
   const int64_t ctas = std::min<int64_t>(
-      n_items, (int64_t)resident_ctas(fast_inverse_pair<FF>, kWarps * 32, sm) * sm_count());
-  fast_inverse_pair<FF><<<(unsigned)ctas, kWarps * 32, sm, s>>>(
+      n_items, (int64_t)resident_ctas(fast_inverse_pair<FF, G>, kW * 32, sm) * sm_count());
+  fast_inverse_pair<FF, G><<<(unsigned)ctas, kW * 32, sm, s>>>(
       a, (const float2*)wP, (const float2*)p->tw_l, (const float2*)p->tw_n, out, n_pb);
   SHT_CUDA_OR_THROW(cudaGetLastError());
 }
