@@ -458,19 +458,20 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
 // Entangle, FFT and store this warp's row (plane p0 + gp, side) of pair h.
-template <int FF>
+template <int FF, int TC>
 __device__ __forceinline__ void inverse_row_out(const FastUnfoldArgs& a, float2* reg,
                                                 const float2* tws, const float2* tn,
                                                 float* __restrict__ out, int64_t plane, int j,
                                                 int lane) {
   constexpr int L = 32 * FF;
+  const int T = TC >= 0 ? TC : a.T;  // compile-time on the linear grid
   float2 z[FF];
 #pragma unroll
   for (int i = 0; i < FF; ++i) {
     int k = lane + 32 * i;
-    float2 xk = k <= a.T ? reg[k] : make_float2(0.f, 0.f);
+    float2 xk = k <= T ? reg[k] : make_float2(0.f, 0.f);
     int kc = L - k;
-    float2 xc = (k > 0 && kc <= a.T) ? cconjf(reg[kc]) : make_float2(0.f, 0.f);
+    float2 xc = (k > 0 && kc <= T) ? cconjf(reg[kc]) : make_float2(0.f, 0.f);
     if (k == 0) xk.y = 0.f;
     float2 sm = caddf(xk, xc), df = csubf(xk, xc);
     float2 wd = cmulf(cconjf(tn[k]), df);
@@ -484,7 +485,9 @@ __device__ __forceinline__ void inverse_row_out(const FastUnfoldArgs& a, float2*
 }
 
 // G planes per item (even), 2G warps per CTA: one row (plane, side) each.
-template <int FF, int G>
+// TC >= 0: the truncation as a compile-time constant (the linear grid,
+// T + 1 = 2 nlon / 3), which fixes every order bound of the row pass.
+template <int FF, int G, int TC>
 __global__ void __launch_bounds__(2 * G * 32, 8 / G) fast_inverse_pair(FastUnfoldArgs a,
                                                                        const float2* __restrict__ wP,
                                                                        const float2* __restrict__ twL,
@@ -529,7 +532,8 @@ __global__ void __launch_bounds__(2 * G * 32, 8 / G) fast_inverse_pair(FastUnfol
     const bool eq = a.nlat_odd && h == a.H - 1;
     cp_async_wait_all();
     __syncthreads();  // the item's slices landed; every warp stored its previous row
-    for (int t = threadIdx.x; t < (a.T + 1) * G; t += blockDim.x) {
+    const int T = TC >= 0 ? TC : a.T;
+    for (int t = threadIdx.x; t < (T + 1) * G; t += blockDim.x) {
       const int m = t / G, g = t - m * G;
       if (p0 + g >= a.planes) continue;
       const float2 S = stage[(m * 2 + 0) * G + g], D = stage[(m * 2 + 1) * G + g];
@@ -550,7 +554,7 @@ __global__ void __launch_bounds__(2 * G * 32, 8 / G) fast_inverse_pair(FastUnfol
     int ln = lane;
     asm volatile("" : "+r"(ln));
     if (plane < a.planes && !(eq && side == 1))
-      inverse_row_out<FF>(a, rows(warp), tws, twn, out, plane, side ? a.nlat - 1 - h : h, ln);
+      inverse_row_out<FF, TC>(a, rows(warp), tws, twn, out, plane, side ? a.nlat - 1 - h : h, ln);
   }
 }
 
@@ -575,9 +579,9 @@ int resident_ctas(K kernel, int threads, size_t sm) {
 // The waist rows must be 16-byte aligned for cp.async: an even plane count.
 // One persistent CTA per resident slot.
 constexpr int kInvPairPlanes = 2;  // planes per item of the persistent inverse
-template <int FF>
-void launch_inv_pair(const sht_plan* p, int mode, const float* wP, int64_t planes, float* out,
-                     cudaStream_t s) {
+template <int FF, int TC>
+void launch_inv_pair_t(const sht_plan* p, int mode, const float* wP, int64_t planes, float* out,
+                       cudaStream_t s) {
   constexpr int G = kInvPairPlanes, kW = 2 * G;
   FastUnfoldArgs a{p->nlat, p->nlon, p->T, p->H, p->nlat_odd ? 1 : 0, mode, G, planes,
                    (float)p->radius};
@@ -587,10 +591,20 @@ void launch_inv_pair(const sht_plan* p, int mode, const float* wP, int64_t plane
   const int64_t n_items = (int64_t)n_pb * p->H;
   if (n_items == 0) return;
   const int64_t ctas = std::min<int64_t>(
-      n_items, (int64_t)resident_ctas(fast_inverse_pair<FF, G>, kW * 32, sm) * sm_count());
-  fast_inverse_pair<FF, G><<<(unsigned)ctas, kW * 32, sm, s>>>(
+      n_items, (int64_t)resident_ctas(fast_inverse_pair<FF, G, TC>, kW * 32, sm) * sm_count());
+  fast_inverse_pair<FF, G, TC><<<(unsigned)ctas, kW * 32, sm, s>>>(
       a, (const float2*)wP, (const float2*)p->tw_l, (const float2*)p->tw_n, out, n_pb);
   SHT_CUDA_OR_THROW(cudaGetLastError());
+}
+template <int FF>
+void launch_inv_pair(const sht_plan* p, int mode, const float* wP, int64_t planes, float* out,
+                     cudaStream_t s) {
+  // The linear grid's truncation, T + 1 = 2 nlon / 3 = 64 F / 3, when it is whole.
+  constexpr int TLIN = (64 * FF) % 3 == 0 ? 64 * FF / 3 - 1 : -1;
+  if (TLIN >= 0 && p->T == TLIN)
+    launch_inv_pair_t<FF, TLIN>(p, mode, wP, planes, out, s);
+  else
+    launch_inv_pair_t<FF, -1>(p, mode, wP, planes, out, s);
 }
 
 // Warps per CTA of the forward FFT.  Eight: each CTA then writes 32-byte
