@@ -236,7 +236,7 @@ struct FastFoldArgs {
 
 // grid -> waist [m][s][h][r], r = (p*F + f)*2 + c.  A CTA of W warps: warp
 // w handles (pf = w >> 1, side = w & 1) with pf = gp*F + f.
-template <int FF, int W>
+template <int FF, int W, int TC>
 __global__ void __launch_bounds__(W * 32, 24 / W) fast_forward_fold(FastFoldArgs a,
                                                                  const float* __restrict__ g0,
                                                                  const float* __restrict__ g1,
@@ -283,7 +283,8 @@ __global__ void __launch_bounds__(W * 32, 24 / W) fast_forward_fold(FastFoldArgs
   const float half_inv_n = 0.5f / (float)a.nlon;
   const int64_t Rc = a.planes * a.F;  // complex columns per waist row
   float mre = 0.f, mim = 0.f;         // this thread's column maxima (q = tid % nper)
-  for (int t = threadIdx.x; t < (a.T + 1) * nper; t += blockDim.x) {
+  const int T = TC >= 0 ? TC : a.T;   // compile-time on the linear grid
+  for (int t = threadIdx.x; t < (T + 1) * nper; t += blockDim.x) {
     int m = t / nper, q = t - m * nper;
     int gq = q >> fsh;
     if (p0 + gq >= a.planes) continue;
@@ -611,20 +612,30 @@ void launch_inv_pair(const sht_plan* p, int mode, const float* wP, int64_t plane
 // (full-sector) pieces of every waist row; four (16-byte pieces, six CTAs
 // per SM) measured 0.72 ms against 0.43 ms at T511 x 200 planes.
 constexpr int kFwdWarps = 8;
-template <int FF>
-void launch_fwd(const sht_plan* p, const float* g0, const float* g1, int64_t planes, float* wfold,
-                cudaStream_t s, float* rowmax) {
+template <int FF, int TC>
+void launch_fwd_t(const sht_plan* p, const float* g0, const float* g1, int64_t planes,
+                  float* wfold, cudaStream_t s, float* rowmax) {
   constexpr int W = kFwdWarps;
   FastFoldArgs a{p->nlat, p->nlon, p->T, p->H, p->nlat_odd ? 1 : 0, g1 ? 2 : 1, 0, planes};
   a.G = W / 2 / a.F;
   dim3 grid((unsigned)div_up(planes, a.G), (unsigned)p->H);
   const size_t sm = sizeof(float2) * (W * WarpSmem<FF>::kFloats2 + FF * 32 + p->T + 1);
-  SHT_CUDA_OR_THROW(cudaFuncSetAttribute(fast_forward_fold<FF, W>,
+  SHT_CUDA_OR_THROW(cudaFuncSetAttribute(fast_forward_fold<FF, W, TC>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-  fast_forward_fold<FF, W><<<grid, W * 32, sm, s>>>(a, g0, g1 ? g1 : g0, (const float2*)p->tw_l,
-                                                    (const float2*)p->tw_n, (float2*)wfold,
-                                                    rowmax);
+  fast_forward_fold<FF, W, TC><<<grid, W * 32, sm, s>>>(a, g0, g1 ? g1 : g0,
+                                                        (const float2*)p->tw_l,
+                                                        (const float2*)p->tw_n, (float2*)wfold,
+                                                        rowmax);
   SHT_CUDA_OR_THROW(cudaGetLastError());
+}
+template <int FF>
+void launch_fwd(const sht_plan* p, const float* g0, const float* g1, int64_t planes, float* wfold,
+                cudaStream_t s, float* rowmax) {
+  constexpr int TLIN = (64 * FF) % 3 == 0 ? 64 * FF / 3 - 1 : -1;  // T + 1 = 2 nlon / 3
+  if (TLIN >= 0 && p->T == TLIN)
+    launch_fwd_t<FF, TLIN>(p, g0, g1, planes, wfold, s, rowmax);
+  else
+    launch_fwd_t<FF, -1>(p, g0, g1, planes, wfold, s, rowmax);
 }
 
 template <int FF, int NF>
