@@ -232,7 +232,14 @@ __device__ __forceinline__ const float2* opaque(const float2* p) {
 struct FastFoldArgs {
   int nlat, nlon, T, H, nlat_odd, F, G;  // F: fields per plane; G: planes per CTA
   int64_t planes;
+  int pf_dist;  // latitude pairs ahead whose rows a CTA prefetches into L2 (0: none)
 };
+
+// Bulk prefetch of a contiguous global range into L2 (16-byte aligned, a
+// multiple of 16 bytes).
+__device__ __forceinline__ void prefetch_l2(const void* p, uint32_t bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
 
 // grid -> waist [m][s][h][r], r = (p*F + f)*2 + c.  A CTA of W warps: warp
 // w handles (pf = w >> 1, side = w & 1) with pf = gp*F + f.
@@ -264,6 +271,19 @@ __global__ void __launch_bounds__(W * 32, 24 / W) fast_forward_fold(FastFoldArgs
   float2* reg = smem(warp);
   float2* tws = smem_dyn + W * WarpSmem<FF>::kFloats2;
   float2* twn = tws + FF * 32;  // the untangling twiddles exp(-2 pi i m / nlon), m <= T
+  // The rows of the CTA about one resident wave later (same plane block,
+  // pf_dist latitude pairs on) are pulled into L2 now, so that CTA's loads
+  // hit L2 instead of waiting on DRAM at its start.
+  if (a.pf_dist > 0 && threadIdx.x < W) {
+    const int hp = h + a.pf_dist;
+    const int pf2 = threadIdx.x >> 1, sd2 = threadIdx.x & 1;
+    const int64_t pl2 = p0 + (pf2 >> fsh);
+    if (hp < a.H && pl2 < a.planes && !(a.nlat_odd && hp == a.H - 1 && sd2 == 1)) {
+      const int j2 = sd2 ? (a.nlat - 1 - hp) : hp;
+      prefetch_l2(((pf2 & (a.F - 1)) ? g1 : g0) + (pl2 * a.nlat + j2) * (int64_t)a.nlon,
+                  (uint32_t)(a.nlon * sizeof(float)));
+    }
+  }
   load_lane_twiddles<FF>(tws, twL);
   for (int m = threadIdx.x; m <= a.T; m += blockDim.x) twn[m] = twN[m];
   __syncthreads();
@@ -608,6 +628,8 @@ void launch_inv_pair(const sht_plan* p, int mode, const float* wP, int64_t plane
     launch_inv_pair_t<FF, -1>(p, mode, wP, planes, out, s);
 }
 
+// L2 prefetch of the rows one resident wave ahead in the forward FFT.
+constexpr bool kFwdPrefetch = true;
 // Warps per CTA of the forward FFT.  Eight: each CTA then writes 32-byte
 // (full-sector) pieces of every waist row; four (16-byte pieces, six CTAs
 // per SM) measured 0.72 ms against 0.43 ms at T511 x 200 planes.
@@ -616,12 +638,14 @@ template <int FF, int TC>
 void launch_fwd_t(const sht_plan* p, const float* g0, const float* g1, int64_t planes,
                   float* wfold, cudaStream_t s, float* rowmax) {
   constexpr int W = kFwdWarps;
-  FastFoldArgs a{p->nlat, p->nlon, p->T, p->H, p->nlat_odd ? 1 : 0, g1 ? 2 : 1, 0, planes};
+  FastFoldArgs a{p->nlat, p->nlon, p->T, p->H, p->nlat_odd ? 1 : 0, g1 ? 2 : 1, 0, planes, 0};
   a.G = W / 2 / a.F;
   dim3 grid((unsigned)div_up(planes, a.G), (unsigned)p->H);
   const size_t sm = sizeof(float2) * (W * WarpSmem<FF>::kFloats2 + FF * 32 + p->T + 1);
-  SHT_CUDA_OR_THROW(cudaFuncSetAttribute(fast_forward_fold<FF, W, TC>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  // One resident wave of CTAs, in latitude pairs (grid.x CTAs per pair);
+  // resident_ctas also raises the kernel's shared-memory limit to `sm`.
+  const int64_t wave = (int64_t)resident_ctas(fast_forward_fold<FF, W, TC>, W * 32, sm) * sm_count();
+  a.pf_dist = kFwdPrefetch ? (int)div_up(wave, (int64_t)grid.x) : 0;
   fast_forward_fold<FF, W, TC><<<grid, W * 32, sm, s>>>(a, g0, g1 ? g1 : g0,
                                                         (const float2*)p->tw_l,
                                                         (const float2*)p->tw_n, (float2*)wfold,
