@@ -192,10 +192,11 @@ __device__ __forceinline__ void warp_fft(float2 (&z)[F], float2* reg, const floa
   __syncwarp();
   float2 y[32];
   if constexpr (UNIFORM) {
-    // Lanes >= F repeat another lane's row (a broadcast read) and drop their
-    // result: a branch around the whole 32-point DFT costs ~70 registers
-    // once the row pass sits inside a loop.
-    const int row = lane % F;
+    // Lanes >= F repeat another lane's row and drop their result: a branch
+    // around the whole 32-point DFT costs ~70 registers once the row pass
+    // sits inside a loop.  For F > 16 they take rows F-16 .. 15, whose banks
+    // differ from those of rows 16 .. F-1 read by the same half-warp.
+    const int row = lane < F ? lane : (F > 16 ? lane - 16 : lane % F);
 #pragma unroll
     for (int l = 0; l < 32; ++l) y[l] = reg[row * WarpSmem<F>::kStride + l];
     __syncwarp();
@@ -521,7 +522,7 @@ __global__ void __launch_bounds__(2 * G * 32, 8 / G) fast_inverse_pair(FastUnfol
   auto rows = [&](int w) { return smem_dyn + w * WarpSmem<FF>::kFloats2; };
   float2* tws = smem_dyn + kW * WarpSmem<FF>::kFloats2;
   float2* twn = tws + FF * 32;    // the entangling twiddles exp(-2 pi i k / nlon), k < L
-  float2* stage = twn + 32 * FF;  // [(m, s)][G] waist slices of the item in flight
+  float2* stage = twn + 32 * FF;  // [s][m][G] waist slices of the item in flight
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int64_t Rc = a.planes;
   const int nms = 2 * (a.T + 1);
@@ -538,7 +539,9 @@ __global__ void __launch_bounds__(2 * G * 32, 8 / G) fast_inverse_pair(FastUnfol
       const int64_t valid = a.planes - pc;
       const uint32_t bytes = valid >= 2 ? 16u : (valid == 1 ? 8u : 0u);
       const float2* src = bytes ? wP + ((int64_t)ms * a.H + h) * Rc + pc : wP;
-      cp_async16(stage + ms * G + 2 * c, src, bytes);
+      // S (s = 0) and D (s = 1) in separate halves, orders contiguous: the
+      // unfold's reads of one half are then consecutive 8-byte words.
+      cp_async16(stage + ((ms & 1) * (a.T + 1) + (ms >> 1)) * G + 2 * c, src, bytes);
     }
     cp_async_commit();
   };
@@ -557,7 +560,7 @@ __global__ void __launch_bounds__(2 * G * 32, 8 / G) fast_inverse_pair(FastUnfol
     for (int t = threadIdx.x; t < (T + 1) * G; t += blockDim.x) {
       const int m = t / G, g = t - m * G;
       if (p0 + g >= a.planes) continue;
-      const float2 S = stage[(m * 2 + 0) * G + g], D = stage[(m * 2 + 1) * G + g];
+      const float2 S = stage[m * G + g], D = stage[((T + 1) + m) * G + g];
 #pragma unroll
       for (int sd = 0; sd < 2; ++sd) {
         if (sd == 1 && eq) continue;
