@@ -181,8 +181,12 @@ __device__ __forceinline__ void load_lane_twiddles(float2* tws, const float2* __
 
 // The L-point complex FFT of one warp's row: in registers z[j] = x[l + 32 j]
 // (lane l); out: the natural-order spectrum written to `reg` (length L).
+// With `out` given, the natural-order spectrum goes straight from the
+// 32-point DFT's registers to `out` (streaming stores, 32 x F consecutive
+// 8-byte words per store instruction) instead of to `reg`.
 template <int F, bool INV, bool UNIFORM = false>
-__device__ __forceinline__ void warp_fft(float2 (&z)[F], float2* reg, const float2* tws, int lane) {
+__device__ __forceinline__ void warp_fft(float2 (&z)[F], float2* reg, const float2* tws, int lane,
+                                         float2* __restrict__ out = nullptr) {
   dftF<F, INV>(z);
   // exp(-+2 pi i lane k1 / L)
 #pragma unroll
@@ -210,6 +214,13 @@ __device__ __forceinline__ void warp_fft(float2 (&z)[F], float2* reg, const floa
     if (lane < F) dft32<INV>(y);
   }
   // output index k = lane + F k2 (natural order)
+  if (out != nullptr) {
+    if (lane < F) {
+#pragma unroll
+      for (int k2 = 0; k2 < 32; ++k2) __stcs(out + lane + F * k2, y[k2]);
+    }
+    return;
+  }
   if (lane < F) {
 #pragma unroll
     for (int k2 = 0; k2 < 32; ++k2) reg[lane + F * k2] = y[k2];
@@ -500,10 +511,9 @@ __device__ __forceinline__ void inverse_row_out(const FastUnfoldArgs& a, float2*
     z[i] = make_float2(sm.x - wd.y, sm.y + wd.x);
   }
   __syncwarp();
-  warp_fft<FF, true, true>(z, reg, tws, lane);
   float2* dst = reinterpret_cast<float2*>(out + (plane * a.nlat + j) * (int64_t)a.nlon);
-#pragma unroll 4
-  for (int i = 0; i < FF; ++i) __stcs(dst + lane + 32 * i, reg[lane + 32 * i]);
+  warp_fft<FF, true, true>(z, reg, tws, lane, dst);
+  __syncwarp();  // every lane's reads of reg are done before the next item's unfold
 }
 
 // G planes per item (even), 2G warps per CTA: one row (plane, side) each.
