@@ -516,25 +516,36 @@ __device__ __forceinline__ void inverse_row_out(const FastUnfoldArgs& a, float2*
   __syncwarp();  // every lane's reads of reg are done before the next item's unfold
 }
 
-// G planes per item (even), 2G warps per CTA: one row (plane, side) each.
-// TC >= 0: the truncation as a compile-time constant (the linear grid,
-// T + 1 = 2 nlon / 3), which fixes every order bound of the row pass.
-template <int FF, int G, int TC>
-__global__ void __launch_bounds__(2 * G * 32, 8 / G) fast_inverse_pair(FastUnfoldArgs a,
-                                                                       const float2* __restrict__ wP,
-                                                                       const float2* __restrict__ twL,
-                                                                       const float2* __restrict__ twN,
-                                                                       float* __restrict__ out,
-                                                                       int n_pb) {
-  static_assert(G % 2 == 0, "cp.async moves planes in pairs");
-  constexpr int kW = 2 * G;  // warps
+// Persistent inverse over items of one latitude pair: NF waist columns per
+// plane (1: scalar/zonal/meridional; 2: gradient, the P and dP syntheses of
+// one field; 4: wind, P and dP of psi and chi) and NO = 1 or 2 output fields.
+// An item holds G planes (2 for NF = 1, 2; 1 for NF = 4), so every waist
+// slice it needs is one 16-byte chunk per (buffer, S/D, order): two planes,
+// or psi and chi of one plane.  2 x G x NO warps, one output row (plane,
+// field, side) each.  TC >= 0: the truncation as a compile-time constant
+// (the linear grid, T + 1 = 2 nlon / 3), which fixes every order bound.
+template <int NF> struct InvCfg {
+  static constexpr int NO = NF == 1 ? 1 : 2;  // output fields
+  static constexpr int NB = NF == 1 ? 1 : 2;  // waist buffers (P, dP)
+  static constexpr int G = NF == 4 ? 1 : 2;   // planes per item
+  static constexpr int W = 2 * G * NO;        // warps
+};
+
+template <int FF, int NF, int TC>
+__global__ void __launch_bounds__(InvCfg<NF>::W * 32, 16 / InvCfg<NF>::W)
+    fast_inverse_pair(FastUnfoldArgs a, const float2* __restrict__ wP,
+                      const float2* __restrict__ wD, const double* __restrict__ coslat,
+                      const float2* __restrict__ twL, const float2* __restrict__ twN,
+                      float* __restrict__ out0, float* __restrict__ out1, int n_pb) {
+  constexpr int G = InvCfg<NF>::G, NO = InvCfg<NF>::NO, NB = InvCfg<NF>::NB;
+  constexpr int kW = InvCfg<NF>::W;
   extern __shared__ float2 smem_dyn[];
   auto rows = [&](int w) { return smem_dyn + w * WarpSmem<FF>::kFloats2; };
   float2* tws = smem_dyn + kW * WarpSmem<FF>::kFloats2;
   float2* twn = tws + FF * 32;    // the entangling twiddles exp(-2 pi i k / nlon), k < L
-  float2* stage = twn + 32 * FF;  // [s][m][G] waist slices of the item in flight
+  float2* stage = twn + 32 * FF;  // [buffer][s][m][2] waist slices of the item in flight
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int64_t Rc = a.planes;
+  const int64_t Rc = NF == 4 ? 2 * a.planes : a.planes;  // waist columns per row
   const int nms = 2 * (a.T + 1);
   const int64_t n_items = (int64_t)n_pb * a.H;
   // Item i: plane block i % n_pb (fastest: CTAs that run together touch
@@ -542,16 +553,15 @@ __global__ void __launch_bounds__(2 * G * 32, 8 / G) fast_inverse_pair(FastUnfol
   auto prefetch = [&](int64_t item) {
     const int h = (int)(item / n_pb);
     const int64_t p0 = (item - (int64_t)h * n_pb) * G;
-    constexpr int kPairs = G / 2;  // 16-byte chunks (plane pairs) per waist slice
-    for (int e = threadIdx.x; e < kPairs * nms; e += blockDim.x) {
-      const int ms = e / kPairs, c = e - ms * kPairs;
-      const int64_t pc = p0 + 2 * c;
-      const int64_t valid = a.planes - pc;
-      const uint32_t bytes = valid >= 2 ? 16u : (valid == 1 ? 8u : 0u);
-      const float2* src = bytes ? wP + ((int64_t)ms * a.H + h) * Rc + pc : wP;
+    const int64_t c0 = NF == 4 ? 2 * p0 : p0;          // first waist column
+    const int64_t valid = NF == 4 ? 2 : a.planes - p0;  // columns that exist (>= 1)
+    const uint32_t bytes = valid >= 2 ? 16u : 8u;
+    for (int e = threadIdx.x; e < NB * nms; e += blockDim.x) {
+      const int b = e / nms, ms = e - b * nms;
+      const float2* src = (b ? wD : wP) + ((int64_t)ms * a.H + h) * Rc + c0;
       // S (s = 0) and D (s = 1) in separate halves, orders contiguous: the
       // unfold's reads of one half are then consecutive 8-byte words.
-      cp_async16(stage + ((ms & 1) * (a.T + 1) + (ms >> 1)) * G + 2 * c, src, bytes);
+      cp_async16(stage + ((b * 2 + (ms & 1)) * (a.T + 1) + (ms >> 1)) * 2, src, bytes);
     }
     cp_async_commit();
   };
@@ -559,25 +569,54 @@ __global__ void __launch_bounds__(2 * G * 32, 8 / G) fast_inverse_pair(FastUnfol
   if (item < n_items) prefetch(item);
   load_lane_twiddles<FF>(tws, twL);
   for (int k = threadIdx.x; k < 32 * FF; k += blockDim.x) twn[k] = twN[k];
-  const int gp = warp >> 1, side = warp & 1;
+  const int po = warp >> 1, side = warp & 1;
+  const int o = po % NO, gp = po / NO;
+  const float inv_a = 1.0f / a.radius;
   for (; item < n_items; item += gridDim.x) {
     const int h = (int)(item / n_pb);
     const int64_t p0 = (item - (int64_t)h * n_pb) * G;
     const bool eq = a.nlat_odd && h == a.H - 1;
+    const int jrow[2] = {h, a.nlat - 1 - h};
     cp_async_wait_all();
     __syncthreads();  // the item's slices landed; every warp stored its previous row
     const int T = TC >= 0 ? TC : a.T;
-    for (int t = threadIdx.x; t < (T + 1) * G; t += blockDim.x) {
+    const int T1 = T + 1;
+    for (int t = threadIdx.x; t < T1 * G; t += blockDim.x) {
       const int m = t / G, g = t - m * G;
       if (p0 + g >= a.planes) continue;
-      const float2 S = stage[m * G + g], D = stage[((T + 1) + m) * G + g];
+      // the NF symmetric / antisymmetric pairs of (m, plane g)
+      float2 S[NF], D[NF];
+#pragma unroll
+      for (int k = 0; k < NF; ++k) {
+        const int b = NF == 1 ? 0 : (NF == 2 ? k : k >> 1);
+        const int c = NF == 4 ? (k & 1) : g;
+        S[k] = stage[((b * 2 + 0) * T1 + m) * 2 + c];
+        D[k] = stage[((b * 2 + 1) * T1 + m) * 2 + c];
+      }
 #pragma unroll
       for (int sd = 0; sd < 2; ++sd) {
         if (sd == 1 && eq) continue;
         const float sgn = sd ? -1.f : 1.f;
-        const float2 x = make_float2(S.x + sgn * D.x, S.y + sgn * D.y);
-        rows(g * 2 + sd)[m] =
-            a.mode == kUnfoldZonal ? make_float2(-(float)m * x.y, (float)m * x.x) : x;
+        float2 x[NF];
+#pragma unroll
+        for (int k = 0; k < NF; ++k) x[k] = make_float2(S[k].x + sgn * D[k].x, S[k].y + sgn * D[k].y);
+        if constexpr (NF == 1) {
+          rows(g * 2 + sd)[m] =
+              a.mode == kUnfoldZonal ? make_float2(-(float)m * x[0].y, (float)m * x[0].x) : x[0];
+        } else if constexpr (NF == 2) {
+          // gradient: (i m P) / (a cos phi) east, (dP) / a north; the
+          // divisions applied here, ahead of the (linear) FFT
+          const float ie = 1.0f / (a.radius * (float)coslat[jrow[sd]]);
+          rows((g * NO + 0) * 2 + sd)[m] = make_float2(-(float)m * x[0].y * ie, (float)m * x[0].x * ie);
+          rows((g * NO + 1) * 2 + sd)[m] = make_float2(x[1].x * inv_a, x[1].y * inv_a);
+        } else {
+          // x = {P psi, P chi, dP psi, dP chi}
+          const float im_over = (float)m / (a.radius * (float)coslat[jrow[sd]]);
+          rows((g * NO + 0) * 2 + sd)[m] = make_float2(-x[2].x * inv_a - im_over * x[1].y,
+                                                       -x[2].y * inv_a + im_over * x[1].x);
+          rows((g * NO + 1) * 2 + sd)[m] = make_float2(-im_over * x[0].y + x[3].x * inv_a,
+                                                       im_over * x[0].x + x[3].y * inv_a);
+        }
       }
     }
     __syncthreads();  // the staging buffer is free again
@@ -588,7 +627,7 @@ __global__ void __launch_bounds__(2 * G * 32, 8 / G) fast_inverse_pair(FastUnfol
     int ln = lane;
     asm volatile("" : "+r"(ln));
     if (plane < a.planes && !(eq && side == 1))
-      inverse_row_out<FF, TC>(a, rows(warp), tws, twn, out, plane, side ? a.nlat - 1 - h : h, ln);
+      inverse_row_out<FF, TC>(a, rows(warp), tws, twn, o ? out1 : out0, plane, jrow[side], ln);
   }
 }
 
@@ -612,33 +651,35 @@ int resident_ctas(K kernel, int threads, size_t sm) {
 
 // The waist rows must be 16-byte aligned for cp.async: an even plane count.
 // One persistent CTA per resident slot.
-constexpr int kInvPairPlanes = 2;  // planes per item of the persistent inverse
-template <int FF, int TC>
-void launch_inv_pair_t(const sht_plan* p, int mode, const float* wP, int64_t planes, float* out,
-                       cudaStream_t s) {
-  constexpr int G = kInvPairPlanes, kW = 2 * G;
+template <int FF, int NF, int TC>
+void launch_inv_pair_t(const sht_plan* p, int mode, const float* wP, const float* wD,
+                       int64_t planes, float* out0, float* out1, cudaStream_t s) {
+  constexpr int G = InvCfg<NF>::G, kW = InvCfg<NF>::W, NB = InvCfg<NF>::NB;
   FastUnfoldArgs a{p->nlat, p->nlon, p->T, p->H, p->nlat_odd ? 1 : 0, mode, G, planes,
                    (float)p->radius};
   const int n_pb = (int)div_up(planes, G);
-  const size_t sm =
-      sizeof(float2) * (kW * WarpSmem<FF>::kFloats2 + 2 * FF * 32 + 2 * (p->T + 1) * G);
+  const size_t sm = sizeof(float2) * (kW * WarpSmem<FF>::kFloats2 + 2 * FF * 32 +
+                                      (size_t)NB * 2 * (p->T + 1) * 2);
   const int64_t n_items = (int64_t)n_pb * p->H;
   if (n_items == 0) return;
   const int64_t ctas = std::min<int64_t>(
-      n_items, (int64_t)resident_ctas(fast_inverse_pair<FF, G, TC>, kW * 32, sm) * sm_count());
-  fast_inverse_pair<FF, G, TC><<<(unsigned)ctas, kW * 32, sm, s>>>(
-      a, (const float2*)wP, (const float2*)p->tw_l, (const float2*)p->tw_n, out, n_pb);
+      n_items, (int64_t)resident_ctas(fast_inverse_pair<FF, NF, TC>, kW * 32, sm) * sm_count());
+  fast_inverse_pair<FF, NF, TC><<<(unsigned)ctas, kW * 32, sm, s>>>(
+      a, (const float2*)wP, (const float2*)(wD ? wD : wP), p->d_coslat, (const float2*)p->tw_l,
+      (const float2*)p->tw_n, out0, out1 ? out1 : out0, n_pb);
   SHT_CUDA_OR_THROW(cudaGetLastError());
 }
-template <int FF>
-void launch_inv_pair(const sht_plan* p, int mode, const float* wP, int64_t planes, float* out,
-                     cudaStream_t s) {
+// The waist rows must be 16-byte aligned for cp.async: for NF = 1, 2 (one
+// waist column per plane) an even plane count; NF = 4 (two per plane) any.
+template <int FF, int NF>
+void launch_inv_pair(const sht_plan* p, int mode, const float* wP, const float* wD,
+                     int64_t planes, float* out0, float* out1, cudaStream_t s) {
   // The linear grid's truncation, T + 1 = 2 nlon / 3 = 64 F / 3, when it is whole.
   constexpr int TLIN = (64 * FF) % 3 == 0 ? 64 * FF / 3 - 1 : -1;
   if (TLIN >= 0 && p->T == TLIN)
-    launch_inv_pair_t<FF, TLIN>(p, mode, wP, planes, out, s);
+    launch_inv_pair_t<FF, NF, TLIN>(p, mode, wP, wD, planes, out0, out1, s);
   else
-    launch_inv_pair_t<FF, -1>(p, mode, wP, planes, out, s);
+    launch_inv_pair_t<FF, NF, -1>(p, mode, wP, wD, planes, out0, out1, s);
 }
 
 // L2 prefetch of the rows one resident wave ahead in the forward FFT.
@@ -695,11 +736,13 @@ template <int FF>
 void launch_inv(const sht_plan* p, int mode, const float* wP, const float* wD, int64_t planes,
                 float* out0, float* out1, cudaStream_t s) {
   if (mode == kUnfoldWind)
-    launch_inv_nf<FF, 4>(p, mode, wP, wD, planes, out0, out1, s);
+    launch_inv_pair<FF, 4>(p, mode, wP, wD, planes, out0, out1, s);
+  else if (mode == kUnfoldGradient && planes % 2 == 0)
+    launch_inv_pair<FF, 2>(p, mode, wP, wD, planes, out0, out1, s);
   else if (mode == kUnfoldGradient)
     launch_inv_nf<FF, 2>(p, mode, wP, wD, planes, out0, out1, s);
   else if (planes % 2 == 0)
-    launch_inv_pair<FF>(p, mode, wP, planes, out0, s);
+    launch_inv_pair<FF, 1>(p, mode, wP, wD, planes, out0, out1, s);
   else
     launch_inv_nf<FF, 1>(p, mode, wP, wD, planes, out0, out1, s);
 }
