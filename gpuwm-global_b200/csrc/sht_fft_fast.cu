@@ -228,6 +228,77 @@ __device__ __forceinline__ void warp_fft(float2 (&z)[F], float2* reg, const floa
   __syncwarp();
 }
 
+// R rows per warp: for small F one row leaves most lanes idle in the
+// 32-point stage (F of 32), so a warp takes R rows, the largest power of two
+// with R x F <= 24 (16 to 24 busy lanes; a power of two so that a CTA's
+// column count stays a divisor of 32).  Row r's
+// registers z[r][j] = x_r[l + 32 j]; its shared slot is reg + r * slot (the
+// slot's first F x 33 entries hold the transpose, then the natural-order
+// spectrum).  With `out`, row r's spectrum goes straight from the 32-point
+// DFT's registers to out + r * out_stride instead of to its slot.
+template <int F> struct RowsPerWarp {
+  static constexpr int R = 24 / F >= 8 ? 8 : (24 / F >= 4 ? 4 : (24 / F >= 2 ? 2 : 1));
+};
+
+template <int F, int R, bool INV, bool UNIFORM>
+__device__ __forceinline__ void warp_fft_rows(float2 (&z)[R][F], float2* reg, int slot,
+                                              const float2* tws, int lane,
+                                              float2* __restrict__ out = nullptr,
+                                              int64_t out_stride = 0) {
+  constexpr int NL = R * F;  // lanes busy in the 32-point stage
+#pragma unroll
+  for (int r = 0; r < R; ++r) dftF<F, INV>(z[r]);
+  // exp(-+2 pi i lane k1 / L), one table read for all R rows
+#pragma unroll
+  for (int k1 = 1; k1 < F; ++k1) {
+    const float2 w = tw<INV>(tws[k1 * 32 + lane]);
+#pragma unroll
+    for (int r = 0; r < R; ++r) z[r][k1] = cmulf(z[r][k1], w);
+  }
+#pragma unroll
+  for (int r = 0; r < R; ++r)
+#pragma unroll
+    for (int k1 = 0; k1 < F; ++k1) reg[r * slot + k1 * WarpSmem<F>::kStride + lane] = z[r][k1];
+  __syncwarp();
+  // lane -> (row r2, column kk) of the transpose.  Lanes >= NL repeat a busy
+  // lane's column (UNIFORM) and drop the result: a branch around the whole
+  // 32-point DFT costs ~70 registers once the row pass sits inside a loop.
+  // For NL > 16 they take lanes NL-16 .. 15, whose banks differ from those
+  // of lanes 16 .. NL-1 read by the same half-warp.
+  const int lr = lane < NL ? lane : (NL > 16 ? lane - 16 : lane % NL);
+  const int r2 = lr / F, kk = lr - r2 * F;
+  const float2* col = reg + r2 * slot + kk * WarpSmem<F>::kStride;
+  float2 y[32];
+  if constexpr (UNIFORM) {
+#pragma unroll
+    for (int l = 0; l < 32; ++l) y[l] = col[l];
+    __syncwarp();
+    dft32<INV>(y);
+  } else {
+    if (lane < NL) {
+#pragma unroll
+      for (int l = 0; l < 32; ++l) y[l] = col[l];
+    }
+    __syncwarp();
+    if (lane < NL) dft32<INV>(y);
+  }
+  // output index k = kk + F k2 (natural order) of row r2
+  if (out != nullptr) {
+    if (lane < NL) {
+      float2* o = out + r2 * out_stride + kk;
+#pragma unroll
+      for (int k2 = 0; k2 < 32; ++k2) __stcs(o + F * k2, y[k2]);
+    }
+    return;
+  }
+  if (lane < NL) {
+    float2* o = reg + r2 * slot + kk;
+#pragma unroll
+    for (int k2 = 0; k2 < 32; ++k2) o[F * k2] = y[k2];
+  }
+  __syncwarp();
+}
+
 // A CTA runs kWarps warps, one grid row each: G planes x NF fields x the two
 // hemisphere rows (8 rows).
 constexpr int kWarps = 8;
@@ -253,63 +324,73 @@ __device__ __forceinline__ void prefetch_l2(const void* p, uint32_t bytes) {
   asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
 }
 
-// grid -> waist [m][s][h][r], r = (p*F + f)*2 + c.  A CTA of W warps: warp
-// w handles (pf = w >> 1, side = w & 1) with pf = gp*F + f.
+// grid -> waist [m][s][h][r], r = (p*F + f)*2 + c.  A CTA of W warps holds
+// W x R row slots, slot s = q * 2 + side for column q = gp*F + f (plane gp of
+// the CTA's block, field f); warp w transforms slots w, w + W, ... (R rows,
+// all on one side).
 template <int FF, int W, int TC>
 __global__ void __launch_bounds__(W * 32, 24 / W) fast_forward_fold(FastFoldArgs a,
-                                                                 const float* __restrict__ g0,
-                                                                 const float* __restrict__ g1,
-                                                                 const float2* __restrict__ twL,
-                                                                 const float2* __restrict__ twN,
-                                                                 float2* __restrict__ wfold,
-                                                                 float* __restrict__ rowmax) {
+                                                                    const float* __restrict__ g0,
+                                                                    const float* __restrict__ g1,
+                                                                    const float2* __restrict__ twL,
+                                                                    const float2* __restrict__ twN,
+                                                                    float2* __restrict__ wfold,
+                                                                    float* __restrict__ rowmax) {
   constexpr int L = 32 * FF;
+  constexpr int R = RowsPerWarp<FF>::R;
+  constexpr int SL = WarpSmem<FF>::kFloats2;  // floats2 per row slot
   extern __shared__ float2 smem_dyn[];
-  auto smem = [&](int w) { return smem_dyn + w * WarpSmem<FF>::kFloats2; };
+  auto smem = [&](int slot) { return smem_dyn + slot * SL; };
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   // Plane blocks vary fastest over the grid: CTAs that run together touch
   // adjacent slices of every waist row.
   const int h = blockIdx.y;
   const int64_t p0 = (int64_t)blockIdx.x * a.G;
   const bool eq = a.nlat_odd && h == a.H - 1;
-  const int pf = warp >> 1, side = warp & 1;
-  // Columns per CTA: W / 2 planes of one field or W / 4 planes of two,
-  // always W / 2 (a compile-time divisor in the loops below).
-  constexpr int nper = W / 2;
+  // Columns per CTA: W / 2 x R (a compile-time divisor in the loops below).
+  constexpr int nper = W / 2 * R;
   const int fsh = a.F == 2 ? 1 : 0;  // log2 of the field count
-  const int f = pf & (a.F - 1), gp = pf >> fsh;
-  const int64_t plane = p0 + gp;
-  const bool active = pf < nper && plane < a.planes && !(eq && side == 1);
-  float2* reg = smem(warp);
-  float2* tws = smem_dyn + W * WarpSmem<FF>::kFloats2;
+  float2* tws = smem_dyn + W * R * SL;
   float2* twn = tws + FF * 32;  // the untangling twiddles exp(-2 pi i m / nlon), m <= T
   // The rows of the CTA about one resident wave later (same plane block,
   // pf_dist latitude pairs on) are pulled into L2 now, so that CTA's loads
   // hit L2 instead of waiting on DRAM at its start.
-  if (a.pf_dist > 0 && threadIdx.x < W) {
+  if (a.pf_dist > 0 && threadIdx.x < W * R) {
     const int hp = h + a.pf_dist;
-    const int pf2 = threadIdx.x >> 1, sd2 = threadIdx.x & 1;
-    const int64_t pl2 = p0 + (pf2 >> fsh);
+    const int q2 = threadIdx.x >> 1, sd2 = threadIdx.x & 1;
+    const int64_t pl2 = p0 + (q2 >> fsh);
     if (hp < a.H && pl2 < a.planes && !(a.nlat_odd && hp == a.H - 1 && sd2 == 1)) {
       const int j2 = sd2 ? (a.nlat - 1 - hp) : hp;
-      prefetch_l2(((pf2 & (a.F - 1)) ? g1 : g0) + (pl2 * a.nlat + j2) * (int64_t)a.nlon,
+      prefetch_l2(((q2 & (a.F - 1)) ? g1 : g0) + (pl2 * a.nlat + j2) * (int64_t)a.nlon,
                   (uint32_t)(a.nlon * sizeof(float)));
     }
   }
   load_lane_twiddles<FF>(tws, twL);
   for (int m = threadIdx.x; m <= a.T; m += blockDim.x) twn[m] = twN[m];
   __syncthreads();
-  if (active) {
+  {
+    float2 z[R][FF];
+    const int side = warp & 1;  // W is even: every slot w + W r has this side
     const int j = side ? (a.nlat - 1 - h) : h;
-    const float2* src =
-        reinterpret_cast<const float2*>((f ? g1 : g0) + (plane * a.nlat + j) * (int64_t)a.nlon);
-    float2 z[FF];
 #pragma unroll
-    for (int i = 0; i < FF; ++i) z[i] = __ldcs(src + lane + 32 * i);
-    warp_fft<FF, false>(z, reg, tws, lane);
+    for (int r = 0; r < R; ++r) {
+      const int q = (warp + W * r) >> 1;
+      const int f = q & (a.F - 1);
+      const int64_t plane = p0 + (q >> fsh);
+      if (plane < a.planes && !(eq && side == 1)) {
+        const float2* src =
+            reinterpret_cast<const float2*>((f ? g1 : g0) + (plane * a.nlat + j) * (int64_t)a.nlon);
+#pragma unroll
+        for (int i = 0; i < FF; ++i) z[r][i] = __ldcs(src + lane + 32 * i);
+      } else {
+#pragma unroll
+        for (int i = 0; i < FF; ++i) z[r][i] = make_float2(0.f, 0.f);
+      }
+    }
+    warp_fft_rows<FF, R, false, false>(z, smem(warp), W * SL, tws, lane);
   }
   __syncthreads();
-  // Untangle, scale, fold, write: thread -> (m, pf) with pf fastest.
+  // Untangle, scale, fold, write: thread -> (m, q) with q fastest.
   // 0.5 / nlon: (x / 2) / nlon and x * (0.5 / nlon) round alike (both
   // scalings by 2 are exact).
   const float half_inv_n = 0.5f / (float)a.nlon;
@@ -692,10 +773,11 @@ template <int FF, int TC>
 void launch_fwd_t(const sht_plan* p, const float* g0, const float* g1, int64_t planes,
                   float* wfold, cudaStream_t s, float* rowmax) {
   constexpr int W = kFwdWarps;
+  constexpr int R = RowsPerWarp<FF>::R;
   FastFoldArgs a{p->nlat, p->nlon, p->T, p->H, p->nlat_odd ? 1 : 0, g1 ? 2 : 1, 0, planes, 0};
-  a.G = W / 2 / a.F;
+  a.G = W / 2 * R / a.F;  // planes per CTA
   dim3 grid((unsigned)div_up(planes, a.G), (unsigned)p->H);
-  const size_t sm = sizeof(float2) * (W * WarpSmem<FF>::kFloats2 + FF * 32 + p->T + 1);
+  const size_t sm = sizeof(float2) * (W * R * WarpSmem<FF>::kFloats2 + FF * 32 + p->T + 1);
   // One resident wave of CTAs, in latitude pairs (grid.x CTAs per pair);
   // resident_ctas also raises the kernel's shared-memory limit to `sm`.
   const int64_t wave = (int64_t)resident_ctas(fast_forward_fold<FF, W, TC>, W * 32, sm) * sm_count();
