@@ -380,13 +380,11 @@ sht_vertical* vertical_upload(const sht_plan* plan, int nlev, const double* b, c
   try {
     if (plan->prec == SHT_PREC_F64) {
       SHT_CUDA_OR_THROW(cudaMalloc(&op->mats, sizeof(double) * nm));
-      SHT_CUDA_OR_THROW(cudaMemcpy(op->mats, host.data(), sizeof(double) * nm,
-                                   cudaMemcpyHostToDevice));
+      upload_now(op->mats, host.data(), sizeof(double) * nm);
     } else {
       std::vector<float> conv(host.begin(), host.end());
       SHT_CUDA_OR_THROW(cudaMalloc(&op->mats, sizeof(float) * nm));
-      SHT_CUDA_OR_THROW(cudaMemcpy(op->mats, conv.data(), sizeof(float) * nm,
-                                   cudaMemcpyHostToDevice));
+      upload_now(op->mats, conv.data(), sizeof(float) * nm);
     }
   } catch (...) {
     if (op->mats) cudaFree(op->mats);
@@ -652,9 +650,10 @@ int sht_plan_check(sht_plan* plan) {
     if (h[0] != 0) {
       char buf[256];
       snprintf(buf, sizeof(buf),
-               "device error word 0x%x: a kernel gave up on a bounded wait "
-               "(tile %u, stage %u)",
-               h[0], h[1], h[2]);
+               "device error word 0x%x: %s (tile %u, stage %u)", h[0],
+               (h[0] & kErrBadTile) ? "a tensor-core launch met an invalid tile and stopped"
+                                    : "a kernel gave up on a bounded wait",
+               h[1], h[2]);
       throw Error{SHT_ERR_DEVICE, buf};
     }
   });

@@ -42,6 +42,19 @@ constexpr unsigned kErrMbarTimeout = 1u;
 constexpr unsigned kErrBadTile = 2u;
 
 inline int64_t div_up(int64_t a, int64_t b) { return (a + b - 1) / b; }
+
+// Host -> device copy of bookkeeping (tile lists, descriptors, operator
+// matrices) that has landed on the device when it returns.  cudaMemcpy from
+// pageable memory may return while its DMA is still queued on the legacy
+// stream, and kernels launched on non-blocking streams (the host-streamed
+// calls, CUDA graphs, other libraries' streams) are not ordered after it, so
+// a first launch could read the buffer before it is written.  Not for use
+// during stream capture.
+inline void upload_now(void* dst, const void* src, size_t bytes) {
+  if (bytes == 0) return;
+  SHT_CUDA_OR_THROW(cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice));
+  SHT_CUDA_OR_THROW(cudaDeviceSynchronize());
+}
 inline int64_t round_up(int64_t a, int64_t b) { return div_up(a, b) * b; }
 
 // Number of degrees n in [m, T] with (n - m) % 2 == q.

@@ -244,7 +244,7 @@ template <int F, int R, bool INV, bool UNIFORM>
 __device__ __forceinline__ void warp_fft_rows(float2 (&z)[R][F], float2* reg, int slot,
                                               const float2* tws, int lane,
                                               float2* __restrict__ out = nullptr,
-                                              int64_t out_stride = 0) {
+                                              int64_t out_stride = 0, int nvalid = R) {
   constexpr int NL = R * F;  // lanes busy in the 32-point stage
 #pragma unroll
   for (int r = 0; r < R; ++r) dftF<F, INV>(z[r]);
@@ -284,7 +284,7 @@ __device__ __forceinline__ void warp_fft_rows(float2 (&z)[R][F], float2* reg, in
   }
   // output index k = kk + F k2 (natural order) of row r2
   if (out != nullptr) {
-    if (lane < NL) {
+    if (lane < NL && r2 < nvalid) {
       float2* o = out + r2 * out_stride + kk;
 #pragma unroll
       for (int k2 = 0; k2 < 32; ++k2) __stcs(o + F * k2, y[k2]);
@@ -571,29 +571,33 @@ __device__ __forceinline__ void cp_async16(void* dst, const void* src, uint32_t 
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
-// Entangle, FFT and store this warp's row (plane p0 + gp, side) of pair h.
-template <int FF, int TC>
-__device__ __forceinline__ void inverse_row_out(const FastUnfoldArgs& a, float2* reg,
-                                                const float2* tws, const float2* tn,
-                                                float* __restrict__ out, int64_t plane, int j,
-                                                int lane) {
+// Entangle, FFT and store this warp's R rows (slots reg + r * slot, output
+// rows out_row0 + r * out_stride floats2, the first `nvalid` of them stored).
+template <int FF, int R, int TC>
+__device__ __forceinline__ void inverse_rows_out(const FastUnfoldArgs& a, float2* reg, int slot,
+                                                 const float2* tws, const float2* tn,
+                                                 float2* __restrict__ out_row0, int64_t out_stride,
+                                                 int lane, int nvalid) {
   constexpr int L = 32 * FF;
   const int T = TC >= 0 ? TC : a.T;  // compile-time on the linear grid
-  float2 z[FF];
+  float2 z[R][FF];
 #pragma unroll
-  for (int i = 0; i < FF; ++i) {
-    int k = lane + 32 * i;
-    float2 xk = k <= T ? reg[k] : make_float2(0.f, 0.f);
-    int kc = L - k;
-    float2 xc = (k > 0 && kc <= T) ? cconjf(reg[kc]) : make_float2(0.f, 0.f);
-    if (k == 0) xk.y = 0.f;
-    float2 sm = caddf(xk, xc), df = csubf(xk, xc);
-    float2 wd = cmulf(cconjf(tn[k]), df);
-    z[i] = make_float2(sm.x - wd.y, sm.y + wd.x);
+  for (int r = 0; r < R; ++r) {
+    const float2* x = reg + r * slot;
+#pragma unroll
+    for (int i = 0; i < FF; ++i) {
+      int k = lane + 32 * i;
+      float2 xk = k <= T ? x[k] : make_float2(0.f, 0.f);
+      int kc = L - k;
+      float2 xc = (k > 0 && kc <= T) ? cconjf(x[kc]) : make_float2(0.f, 0.f);
+      if (k == 0) xk.y = 0.f;
+      float2 sm = caddf(xk, xc), df = csubf(xk, xc);
+      float2 wd = cmulf(cconjf(tn[k]), df);
+      z[r][i] = make_float2(sm.x - wd.y, sm.y + wd.x);
+    }
   }
   __syncwarp();
-  float2* dst = reinterpret_cast<float2*>(out + (plane * a.nlat + j) * (int64_t)a.nlon);
-  warp_fft<FF, true, true>(z, reg, tws, lane, dst);
+  warp_fft_rows<FF, R, true, true>(z, reg, slot, tws, lane, out_row0, out_stride, nvalid);
   __syncwarp();  // every lane's reads of reg are done before the next item's unfold
 }
 
@@ -608,7 +612,7 @@ __device__ __forceinline__ void inverse_row_out(const FastUnfoldArgs& a, float2*
 template <int NF> struct InvCfg {
   static constexpr int NO = NF == 1 ? 1 : 2;  // output fields
   static constexpr int NB = NF == 1 ? 1 : 2;  // waist buffers (P, dP)
-  static constexpr int G = NF == 4 ? 1 : 2;   // planes per item
+  static constexpr int G = NF == 4 ? 1 : 2;   // planes per warp row group
   static constexpr int W = 2 * G * NO;        // warps
 };
 
@@ -618,13 +622,16 @@ __global__ void __launch_bounds__(InvCfg<NF>::W * 32, 16 / InvCfg<NF>::W)
                       const float2* __restrict__ wD, const double* __restrict__ coslat,
                       const float2* __restrict__ twL, const float2* __restrict__ twN,
                       float* __restrict__ out0, float* __restrict__ out1, int n_pb) {
-  constexpr int G = InvCfg<NF>::G, NO = InvCfg<NF>::NO, NB = InvCfg<NF>::NB;
-  constexpr int kW = InvCfg<NF>::W;
+  constexpr int NO = InvCfg<NF>::NO, NB = InvCfg<NF>::NB, kW = InvCfg<NF>::W;
+  constexpr int R = RowsPerWarp<FF>::R;     // rows per warp
+  constexpr int GI = InvCfg<NF>::G * R;      // planes per item
+  constexpr int CW = NF == 4 ? 2 * GI : GI;  // waist columns per item (even)
+  constexpr int SL = WarpSmem<FF>::kFloats2;
   extern __shared__ float2 smem_dyn[];
-  auto rows = [&](int w) { return smem_dyn + w * WarpSmem<FF>::kFloats2; };
-  float2* tws = smem_dyn + kW * WarpSmem<FF>::kFloats2;
+  auto rows = [&](int slot) { return smem_dyn + slot * SL; };
+  float2* tws = smem_dyn + kW * R * SL;
   float2* twn = tws + FF * 32;    // the entangling twiddles exp(-2 pi i k / nlon), k < L
-  float2* stage = twn + 32 * FF;  // [buffer][s][m][2] waist slices of the item in flight
+  float2* stage = twn + 32 * FF;  // [buffer][s][m][CW] waist slices of the item in flight
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int64_t Rc = NF == 4 ? 2 * a.planes : a.planes;  // waist columns per row
   const int nms = 2 * (a.T + 1);
@@ -633,16 +640,16 @@ __global__ void __launch_bounds__(InvCfg<NF>::W * 32, 16 / InvCfg<NF>::W)
   // adjacent slices of every waist row), latitude pair i / n_pb.
   auto prefetch = [&](int64_t item) {
     const int h = (int)(item / n_pb);
-    const int64_t p0 = (item - (int64_t)h * n_pb) * G;
-    const int64_t c0 = NF == 4 ? 2 * p0 : p0;          // first waist column
-    const int64_t valid = NF == 4 ? 2 : a.planes - p0;  // columns that exist (>= 1)
-    const uint32_t bytes = valid >= 2 ? 16u : 8u;
-    for (int e = threadIdx.x; e < NB * nms; e += blockDim.x) {
-      const int b = e / nms, ms = e - b * nms;
-      const float2* src = (b ? wD : wP) + ((int64_t)ms * a.H + h) * Rc + c0;
-      // S (s = 0) and D (s = 1) in separate halves, orders contiguous: the
-      // unfold's reads of one half are then consecutive 8-byte words.
-      cp_async16(stage + ((b * 2 + (ms & 1)) * (a.T + 1) + (ms >> 1)) * 2, src, bytes);
+    const int64_t p0 = (item - (int64_t)h * n_pb) * GI;
+    const int64_t c0 = NF == 4 ? 2 * p0 : p0;  // first waist column
+    for (int e = threadIdx.x; e < NB * nms * (CW / 2); e += blockDim.x) {
+      const int c = e % (CW / 2), bms = e / (CW / 2);
+      const int b = bms / nms, ms = bms - b * nms;
+      const int64_t valid = Rc - (c0 + 2 * c);  // columns that exist from this chunk on
+      const uint32_t bytes = valid >= 2 ? 16u : (valid == 1 ? 8u : 0u);
+      const float2* src = bytes ? (b ? wD : wP) + ((int64_t)ms * a.H + h) * Rc + c0 + 2 * c : wP;
+      // S (s = 0) and D (s = 1) in separate halves, orders contiguous.
+      cp_async16(stage + ((b * 2 + (ms & 1)) * (a.T + 1) + (ms >> 1)) * CW + 2 * c, src, bytes);
     }
     cp_async_commit();
   };
@@ -650,29 +657,29 @@ __global__ void __launch_bounds__(InvCfg<NF>::W * 32, 16 / InvCfg<NF>::W)
   if (item < n_items) prefetch(item);
   load_lane_twiddles<FF>(tws, twL);
   for (int k = threadIdx.x; k < 32 * FF; k += blockDim.x) twn[k] = twN[k];
-  const int po = warp >> 1, side = warp & 1;
-  const int o = po % NO, gp = po / NO;
+  // warp w: slots w, w + kW, ...; slot s = (gg * NO + o) * 2 + side
+  const int side = warp & 1, o = (warp >> 1) % NO, gp = (warp >> 1) / NO;
   const float inv_a = 1.0f / a.radius;
   for (; item < n_items; item += gridDim.x) {
     const int h = (int)(item / n_pb);
-    const int64_t p0 = (item - (int64_t)h * n_pb) * G;
+    const int64_t p0 = (item - (int64_t)h * n_pb) * GI;
     const bool eq = a.nlat_odd && h == a.H - 1;
     const int jrow[2] = {h, a.nlat - 1 - h};
     cp_async_wait_all();
-    __syncthreads();  // the item's slices landed; every warp stored its previous row
+    __syncthreads();  // the item's slices landed; every warp stored its previous rows
     const int T = TC >= 0 ? TC : a.T;
     const int T1 = T + 1;
-    for (int t = threadIdx.x; t < T1 * G; t += blockDim.x) {
-      const int m = t / G, g = t - m * G;
+    for (int t = threadIdx.x; t < T1 * GI; t += blockDim.x) {
+      const int m = t / GI, g = t - m * GI;
       if (p0 + g >= a.planes) continue;
       // the NF symmetric / antisymmetric pairs of (m, plane g)
       float2 S[NF], D[NF];
 #pragma unroll
       for (int k = 0; k < NF; ++k) {
         const int b = NF == 1 ? 0 : (NF == 2 ? k : k >> 1);
-        const int c = NF == 4 ? (k & 1) : g;
-        S[k] = stage[((b * 2 + 0) * T1 + m) * 2 + c];
-        D[k] = stage[((b * 2 + 1) * T1 + m) * 2 + c];
+        const int c = NF == 4 ? 2 * g + (k & 1) : g;
+        S[k] = stage[((b * 2 + 0) * T1 + m) * CW + c];
+        D[k] = stage[((b * 2 + 1) * T1 + m) * CW + c];
       }
 #pragma unroll
       for (int sd = 0; sd < 2; ++sd) {
@@ -702,13 +709,21 @@ __global__ void __launch_bounds__(InvCfg<NF>::W * 32, 16 / InvCfg<NF>::W)
     }
     __syncthreads();  // the staging buffer is free again
     if (item + gridDim.x < n_items) prefetch(item + gridDim.x);
-    const int64_t plane = p0 + gp;
+    const int64_t plane = p0 + gp;  // the warp's first row; the others are GI / R apart
     // The lane index, made opaque per item: the per-lane masks and offsets of
     // the row pass are rebuilt every item instead of held across the loop.
     int ln = lane;
     asm volatile("" : "+r"(ln));
-    if (plane < a.planes && !(eq && side == 1))
-      inverse_row_out<FF, TC>(a, rows(warp), tws, twn, o ? out1 : out0, plane, jrow[side], ln);
+    if (plane < a.planes && !(eq && side == 1)) {
+      constexpr int G = InvCfg<NF>::G;
+      float* out = o ? out1 : out0;
+      float2* row0 = reinterpret_cast<float2*>(out + (plane * a.nlat + jrow[side]) * (int64_t)a.nlon);
+      const int64_t stride = (int64_t)G * a.nlat * a.nlon / 2;  // floats2 between the warp's rows
+      // rows past the plane count are transformed but not stored
+      const int64_t left = (a.planes - plane + G - 1) / G;
+      const int nvalid = left < R ? (int)left : R;
+      inverse_rows_out<FF, R, TC>(a, rows(warp), kW * SL, tws, twn, row0, stride, ln, nvalid);
+    }
   }
 }
 
@@ -735,12 +750,13 @@ int resident_ctas(K kernel, int threads, size_t sm) {
 template <int FF, int NF, int TC>
 void launch_inv_pair_t(const sht_plan* p, int mode, const float* wP, const float* wD,
                        int64_t planes, float* out0, float* out1, cudaStream_t s) {
-  constexpr int G = InvCfg<NF>::G, kW = InvCfg<NF>::W, NB = InvCfg<NF>::NB;
-  FastUnfoldArgs a{p->nlat, p->nlon, p->T, p->H, p->nlat_odd ? 1 : 0, mode, G, planes,
+  constexpr int kW = InvCfg<NF>::W, NB = InvCfg<NF>::NB, R = RowsPerWarp<FF>::R;
+  constexpr int GI = InvCfg<NF>::G * R, CW = NF == 4 ? 2 * GI : GI;
+  FastUnfoldArgs a{p->nlat, p->nlon, p->T, p->H, p->nlat_odd ? 1 : 0, mode, GI, planes,
                    (float)p->radius};
-  const int n_pb = (int)div_up(planes, G);
-  const size_t sm = sizeof(float2) * (kW * WarpSmem<FF>::kFloats2 + 2 * FF * 32 +
-                                      (size_t)NB * 2 * (p->T + 1) * 2);
+  const int n_pb = (int)div_up(planes, GI);
+  const size_t sm = sizeof(float2) * (kW * R * WarpSmem<FF>::kFloats2 + 2 * FF * 32 +
+                                      (size_t)NB * 2 * (p->T + 1) * CW);
   const int64_t n_items = (int64_t)n_pb * p->H;
   if (n_items == 0) return;
   const int64_t ctas = std::min<int64_t>(

@@ -203,13 +203,11 @@ void build_gemm_items(sht_plan* p) {
     for (auto& it : items) flat.push_back(it.second);
     p->n_items[dir] = (int)flat.size();
     SHT_CUDA_OR_THROW(cudaMalloc(&p->d_items[dir], sizeof(ShtGemmItem) * std::max<size_t>(flat.size(), 1)));
-    SHT_CUDA_OR_THROW(cudaMemcpy(p->d_items[dir], flat.data(), sizeof(ShtGemmItem) * flat.size(),
-                                 cudaMemcpyHostToDevice));
+    upload_now(p->d_items[dir], flat.data(), sizeof(ShtGemmItem) * flat.size());
     for (int f = 0; f < 2; ++f) {
       auto& v = p->h_desc[dir][f];
       SHT_CUDA_OR_THROW(cudaMalloc(&p->d_desc[dir][f], sizeof(ShtGemmDesc) * std::max<size_t>(v.size(), 1)));
-      SHT_CUDA_OR_THROW(cudaMemcpy(p->d_desc[dir][f], v.data(), sizeof(ShtGemmDesc) * v.size(),
-                                   cudaMemcpyHostToDevice));
+      upload_now(p->d_desc[dir][f], v.data(), sizeof(ShtGemmDesc) * v.size());
     }
   }
 }

@@ -359,6 +359,22 @@ struct Pipe {
   volatile int* abort;
 };
 
+// A tile whose fields could make a TMA load, an MMA or an address invalid
+// (row offset not a multiple of 32, group or width out of range) is never
+// issued: the role that reads it raises kErrBadTile and the abort flag.
+__device__ __forceinline__ bool tile_ok(const ShtTcTile& tl) {
+  return tl.group >= 0 && tl.group < kMaxTcGroups && tl.r0 >= 0 && (tl.r0 & 31) == 0 &&
+         tl.kst >= 0 && tl.nsize >= 0 && tl.nsize <= NMAX && (tl.nsize & 15) == 0 &&
+         (tl.kst == 0 || tl.nsize >= 16);
+}
+__device__ __forceinline__ bool reject_tile(const ShtTcTile& tl, volatile int* abort_flag,
+                                            unsigned* err) {
+  if (tile_ok(tl)) return false;
+  *abort_flag = 1;
+  atomicOr(err, kErrBadTile);
+  return true;
+}
+
 // Bounded wait: returns false (and raises the abort flag) when the clock
 // budget runs out or another role has aborted.
 __device__ bool wait_bar(uint64_t* bar, uint32_t parity, const Pipe& pp, unsigned* err, int where) {
@@ -438,6 +454,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
       for (int s = 0; s < S; ++s) armed[s] = armed_raw[s] = -1;
       for (int t = blockIdx.x; t < a.n_tiles && !*abort_flag; t += gridDim.x) {
         const ShtTcTile tl = a.tiles[t];
+        if (reject_tile(tl, abort_flag, a.err)) break;
         const TcGroup& G = a.g[tl.group];
         const int part = tl.nsize * BK * 2;  // bytes of one FP16 part of one stage
         const unsigned char* src = G.img + G.img_off[tl.img];
@@ -496,6 +513,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
       bool issued = false;
       for (int t = blockIdx.x; t < a.n_tiles && !*abort_flag; t += gridDim.x) {
         const ShtTcTile tl = a.tiles[t];
+        if (reject_tile(tl, abort_flag, a.err)) break;
         if (tl.kst == 0) continue;
         const uint32_t buf = acc_it % NBUF, acc_phase = (acc_it / NBUF) & 1;
         if (!wait_bar(&pp.acc_empty[buf], acc_phase ^ 1, pp, a.err, 2)) break;
@@ -581,6 +599,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
     uint32_t acc_it = 0;
     for (int t = blockIdx.x; t < a.n_tiles; t += gridDim.x) {
       const ShtTcTile tl = a.tiles[t];
+      if (reject_tile(tl, abort_flag, a.err)) break;  // the same tile for all 256 threads
       const TcGroup& G = a.g[tl.group];
       const ShtGemmDesc d = G.descs[tl.problem];
       const int64_t R = G.R;
@@ -689,6 +708,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
     uint32_t aphase = 0;
     for (int t = blockIdx.x; t < a.n_tiles; t += gridDim.x) {
       const ShtTcTile tl = a.tiles[t];
+      if (reject_tile(tl, abort_flag, a.err)) break;
       if (tl.kst == 0) continue;
       const TcGroup& G = a.g[tl.group];
       const ShtGemmDesc d = G.descs[tl.problem];
@@ -754,6 +774,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
     uint32_t phase = 0;
     for (int t = blockIdx.x; t < a.n_tiles; t += gridDim.x) {
       const ShtTcTile tl = a.tiles[t];
+      if (reject_tile(tl, abort_flag, a.err)) break;
       if (tl.kst == 0) continue;
       const TcGroup& G = a.g[tl.group];
       const ShtGemmDesc d = G.descs[tl.problem];
@@ -1004,22 +1025,18 @@ void build_tc_tables(sht_plan* p, const double* basis64, const double* dbasis64,
       tc->img_bytes[dir] = off;
       tc->cs_elems[dir] = cso;
       SHT_CUDA_OR_THROW(cudaMalloc(&tc->d_img_off[dir], 8 * std::max<size_t>(tc->img_off[dir].size(), 1)));
-      SHT_CUDA_OR_THROW(cudaMemcpy(tc->d_img_off[dir], tc->img_off[dir].data(),
-                                   8 * tc->img_off[dir].size(), cudaMemcpyHostToDevice));
+      upload_now(tc->d_img_off[dir], tc->img_off[dir].data(), 8 * tc->img_off[dir].size());
       SHT_CUDA_OR_THROW(cudaMalloc(&tc->d_cs_off[dir], 8 * np));
-      SHT_CUDA_OR_THROW(cudaMemcpy(tc->d_cs_off[dir], tc->cs_off[dir].data(), 8 * np,
-                                   cudaMemcpyHostToDevice));
+      upload_now(tc->d_cs_off[dir], tc->cs_off[dir].data(), 8 * np);
     }
     ShtGemmDesc* dd[2];
     BlockInfo* db[2];
     float* colmul[2];
     for (int dir = 0; dir < 2; ++dir) {
       SHT_CUDA_OR_THROW(cudaMalloc(&dd[dir], sizeof(ShtGemmDesc) * d64[dir].size()));
-      SHT_CUDA_OR_THROW(cudaMemcpy(dd[dir], d64[dir].data(), sizeof(ShtGemmDesc) * d64[dir].size(),
-                                   cudaMemcpyHostToDevice));
+      upload_now(dd[dir], d64[dir].data(), sizeof(ShtGemmDesc) * d64[dir].size());
       SHT_CUDA_OR_THROW(cudaMalloc(&db[dir], sizeof(BlockInfo) * std::max<size_t>(blocks[dir].size(), 1)));
-      SHT_CUDA_OR_THROW(cudaMemcpy(db[dir], blocks[dir].data(), sizeof(BlockInfo) * blocks[dir].size(),
-                                   cudaMemcpyHostToDevice));
+      upload_now(db[dir], blocks[dir].data(), sizeof(BlockInfo) * blocks[dir].size());
       SHT_CUDA_OR_THROW(cudaMalloc(&colmul[dir], 4 * std::max<int64_t>(tc->cs_elems[dir], 1)));
     }
     for (int kind = 0; kind < 5; ++kind) {
@@ -1194,8 +1211,14 @@ void launch_gemm_tc_groups(const TcGroupSpec* g, int ngroups, TcTileCache* cache
       for (auto& e : v) flat.push_back(e.second);
       TcTileCache::List fresh;
       SHT_CUDA_OR_THROW(cudaMalloc(&fresh.d, sizeof(ShtTcTile) * std::max<size_t>(flat.size(), 1)));
-      SHT_CUDA_OR_THROW(cudaMemcpy(fresh.d, flat.data(), sizeof(ShtTcTile) * flat.size(),
-                                   cudaMemcpyHostToDevice));
+      // The launch below may be on a non-blocking stream: the list must be on
+      // the device before it is read (upload_now).
+      cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+      SHT_CUDA_OR_THROW(cudaStreamIsCapturing(s, &cap));
+      SHT_REQUIRE(cap == cudaStreamCaptureStatusNone,
+                  "tensor-core tile list built during stream capture: run the call once before "
+                  "capturing it");
+      upload_now(fresh.d, flat.data(), sizeof(ShtTcTile) * flat.size());
       fresh.n = (int)flat.size();
       found = cache->lists.emplace(key, fresh).first;
     }
