@@ -179,55 +179,6 @@ __device__ __forceinline__ void load_lane_twiddles(float2* tws, const float2* __
   }
 }
 
-// The L-point complex FFT of one warp's row: in registers z[j] = x[l + 32 j]
-// (lane l); out: the natural-order spectrum written to `reg` (length L).
-// With `out` given, the natural-order spectrum goes straight from the
-// 32-point DFT's registers to `out` (streaming stores, 32 x F consecutive
-// 8-byte words per store instruction) instead of to `reg`.
-template <int F, bool INV, bool UNIFORM = false>
-__device__ __forceinline__ void warp_fft(float2 (&z)[F], float2* reg, const float2* tws, int lane,
-                                         float2* __restrict__ out = nullptr) {
-  dftF<F, INV>(z);
-  // exp(-+2 pi i lane k1 / L)
-#pragma unroll
-  for (int k1 = 1; k1 < F; ++k1) z[k1] = cmulf(z[k1], tw<INV>(tws[k1 * 32 + lane]));
-#pragma unroll
-  for (int k1 = 0; k1 < F; ++k1) reg[k1 * WarpSmem<F>::kStride + lane] = z[k1];
-  __syncwarp();
-  float2 y[32];
-  if constexpr (UNIFORM) {
-    // Lanes >= F repeat another lane's row and drop their result: a branch
-    // around the whole 32-point DFT costs ~70 registers once the row pass
-    // sits inside a loop.  For F > 16 they take rows F-16 .. 15, whose banks
-    // differ from those of rows 16 .. F-1 read by the same half-warp.
-    const int row = lane < F ? lane : (F > 16 ? lane - 16 : lane % F);
-#pragma unroll
-    for (int l = 0; l < 32; ++l) y[l] = reg[row * WarpSmem<F>::kStride + l];
-    __syncwarp();
-    dft32<INV>(y);
-  } else {
-    if (lane < F) {
-#pragma unroll
-      for (int l = 0; l < 32; ++l) y[l] = reg[lane * WarpSmem<F>::kStride + l];
-    }
-    __syncwarp();
-    if (lane < F) dft32<INV>(y);
-  }
-  // output index k = lane + F k2 (natural order)
-  if (out != nullptr) {
-    if (lane < F) {
-#pragma unroll
-      for (int k2 = 0; k2 < 32; ++k2) __stcs(out + lane + F * k2, y[k2]);
-    }
-    return;
-  }
-  if (lane < F) {
-#pragma unroll
-    for (int k2 = 0; k2 < 32; ++k2) reg[lane + F * k2] = y[k2];
-  }
-  __syncwarp();
-}
-
 // R rows per warp: for small F one row leaves most lanes idle in the
 // 32-point stage (F of 32), so a warp takes R rows, the largest power of two
 // with R x F <= 24 (16 to 24 busy lanes; a power of two so that a CTA's
@@ -297,6 +248,14 @@ __device__ __forceinline__ void warp_fft_rows(float2 (&z)[R][F], float2* reg, in
     for (int k2 = 0; k2 < 32; ++k2) o[F * k2] = y[k2];
   }
   __syncwarp();
+}
+
+// The L-point complex FFT of one warp's row: in registers z[j] = x[l + 32 j]
+// (lane l); out: the natural-order spectrum written to `reg` (length L).
+template <int F, bool INV>
+__device__ __forceinline__ void warp_fft(float2 (&z)[F], float2* reg, const float2* tws, int lane) {
+  float2(&z1)[1][F] = *reinterpret_cast<float2(*)[1][F]>(&z);
+  warp_fft_rows<F, 1, INV, false>(z1, reg, 0, tws, lane);
 }
 
 // A CTA runs kWarps warps, one grid row each: G planes x NF fields x the two
