@@ -420,7 +420,7 @@ __global__ void __launch_bounds__(kWarps * 32) fast_inverse_unfold(FastUnfoldArg
   const bool eq = a.nlat_odd && h == a.H - 1;
   const int64_t Rc = a.planes * (NF == 4 ? 2 : 1);
   const float inv_a = 1.0f / a.radius;
-  const int jrow[2] = {h, a.nlat - 1 - h};
+  const int jmir = a.nlat - 1 - h;  // the mirror row (side 1)
 
   float2* tws = smem_dyn + kWarps * WarpSmem<FF>::kFloats2;
   load_lane_twiddles<FF>(tws, twL);
@@ -471,7 +471,7 @@ __global__ void __launch_bounds__(kWarps * 32) fast_inverse_unfold(FastUnfoldArg
           o1 = x[1];
         } else {
           // x = {P psi, P chi, dP psi, dP chi}
-          const float im_over = (float)m / (a.radius * (float)coslat[jrow[sd]]);
+          const float im_over = (float)m / (a.radius * (float)coslat[sd ? jmir : h]);
           o0 = make_float2(-x[2].x * inv_a - im_over * x[1].y, -x[2].y * inv_a + im_over * x[1].x);
           o1 = make_float2(-im_over * x[0].y + x[3].x * inv_a, im_over * x[0].x + x[3].y * inv_a);
         }
@@ -503,7 +503,7 @@ __global__ void __launch_bounds__(kWarps * 32) fast_inverse_unfold(FastUnfoldArg
   __syncwarp();
   warp_fft<FF, true>(z, reg, tws, lane);
   // Stage 3: natural-order z[n] -> x[2n], x[2n+1] with the row scaling.
-  const int j = jrow[side];
+  const int j = side ? jmir : h;
   // The gradient divides the grid by (a cos phi) and by a, as the reference does.
   const bool divide = NF == 2;
   const float den = o == 0 ? a.radius * (float)coslat[j] : a.radius;
@@ -601,14 +601,17 @@ __global__ void __launch_bounds__(InvCfg<NF>::W * 32, 16 / InvCfg<NF>::W)
     const int h = (int)(item / n_pb);
     const int64_t p0 = (item - (int64_t)h * n_pb) * GI;
     const int64_t c0 = NF == 4 ? 2 * p0 : p0;  // first waist column
-    for (int e = threadIdx.x; e < NB * nms * (CW / 2); e += blockDim.x) {
-      const int c = e % (CW / 2), bms = e / (CW / 2);
-      const int b = bms / nms, ms = bms - b * nms;
-      const int64_t valid = Rc - (c0 + 2 * c);  // columns that exist from this chunk on
-      const uint32_t bytes = valid >= 2 ? 16u : (valid == 1 ? 8u : 0u);
-      const float2* src = bytes ? (b ? wD : wP) + ((int64_t)ms * a.H + h) * Rc + c0 + 2 * c : wP;
-      // S (s = 0) and D (s = 1) in separate halves, orders contiguous.
-      cp_async16(stage + ((b * 2 + (ms & 1)) * (a.T + 1) + (ms >> 1)) * CW + 2 * c, src, bytes);
+#pragma unroll
+    for (int b = 0; b < NB; ++b) {
+      const float2* w = b ? wD : wP;
+      for (int e = threadIdx.x; e < nms * (CW / 2); e += blockDim.x) {
+        const int c = e % (CW / 2), ms = e / (CW / 2);  // compile-time divisor
+        const int64_t valid = Rc - (c0 + 2 * c);  // columns that exist from this chunk on
+        const uint32_t bytes = valid >= 2 ? 16u : (valid == 1 ? 8u : 0u);
+        const float2* src = bytes ? w + ((int64_t)ms * a.H + h) * Rc + c0 + 2 * c : wP;
+        // S (s = 0) and D (s = 1) in separate halves, orders contiguous.
+        cp_async16(stage + ((b * 2 + (ms & 1)) * (a.T + 1) + (ms >> 1)) * CW + 2 * c, src, bytes);
+      }
     }
     cp_async_commit();
   };
@@ -623,7 +626,7 @@ __global__ void __launch_bounds__(InvCfg<NF>::W * 32, 16 / InvCfg<NF>::W)
     const int h = (int)(item / n_pb);
     const int64_t p0 = (item - (int64_t)h * n_pb) * GI;
     const bool eq = a.nlat_odd && h == a.H - 1;
-    const int jrow[2] = {h, a.nlat - 1 - h};
+    const int jmir = a.nlat - 1 - h;  // the mirror row (side 1)
     cp_async_wait_all();
     __syncthreads();  // the item's slices landed; every warp stored its previous rows
     const int T = TC >= 0 ? TC : a.T;
@@ -653,12 +656,12 @@ __global__ void __launch_bounds__(InvCfg<NF>::W * 32, 16 / InvCfg<NF>::W)
         } else if constexpr (NF == 2) {
           // gradient: (i m P) / (a cos phi) east, (dP) / a north; the
           // divisions applied here, ahead of the (linear) FFT
-          const float ie = 1.0f / (a.radius * (float)coslat[jrow[sd]]);
+          const float ie = 1.0f / (a.radius * (float)coslat[sd ? jmir : h]);
           rows((g * NO + 0) * 2 + sd)[m] = make_float2(-(float)m * x[0].y * ie, (float)m * x[0].x * ie);
           rows((g * NO + 1) * 2 + sd)[m] = make_float2(x[1].x * inv_a, x[1].y * inv_a);
         } else {
           // x = {P psi, P chi, dP psi, dP chi}
-          const float im_over = (float)m / (a.radius * (float)coslat[jrow[sd]]);
+          const float im_over = (float)m / (a.radius * (float)coslat[sd ? jmir : h]);
           rows((g * NO + 0) * 2 + sd)[m] = make_float2(-x[2].x * inv_a - im_over * x[1].y,
                                                        -x[2].y * inv_a + im_over * x[1].x);
           rows((g * NO + 1) * 2 + sd)[m] = make_float2(-im_over * x[0].y + x[3].x * inv_a,
@@ -676,7 +679,7 @@ __global__ void __launch_bounds__(InvCfg<NF>::W * 32, 16 / InvCfg<NF>::W)
     if (plane < a.planes && !(eq && side == 1)) {
       constexpr int G = InvCfg<NF>::G;
       float* out = o ? out1 : out0;
-      float2* row0 = reinterpret_cast<float2*>(out + (plane * a.nlat + jrow[side]) * (int64_t)a.nlon);
+      float2* row0 = reinterpret_cast<float2*>(out + (plane * a.nlat + (side ? jmir : h)) * (int64_t)a.nlon);
       const int64_t stride = (int64_t)G * a.nlat * a.nlon / 2;  // floats2 between the warp's rows
       // rows past the plane count are transformed but not stored
       const int64_t left = (a.planes - plane + G - 1) / G;
