@@ -524,7 +524,10 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
         const uint32_t idesc = Acc::A_TMEM ? instr_desc(tl.nsize) & ~(1u << 15) : instr_desc(tl.nsize);
         const uint32_t lbo_b = (uint32_t)tl.nsize * 16;
         const int nsteps = tl.kst * (BK / 16);  // K steps of 16 in the tile
-        int seg_prev = -1;
+        // Segment of step k: floor(k * NMAIN / nsteps), advanced at the
+        // boundaries ceil(s * nsteps / NMAIN) instead of divided per step.
+        int seg = 0, seg_prev = -1;
+        int next_b = NMAIN > 1 ? (nsteps + NMAIN - 1) / NMAIN : nsteps;
         bool ok = true;
         for (int ks = 0; ks < tl.kst; ++ks) {
           if (!wait_bar(Acc::A_TMEM ? &pp.full_a[aslot] : &pp.full_a[stage],
@@ -544,7 +547,10 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
             const uint64_t db1 = smem_desc(b0 + j * 2 * lbo_b, lbo_b, 128);
             const uint64_t db2 = smem_desc(b0 + kBPart + j * 2 * lbo_b, lbo_b, 128);
             const int step = ks * (BK / 16) + j;
-            const int seg = step * NMAIN / nsteps;  // contiguous thirds of the K steps
+            if (step >= next_b && seg < NMAIN - 1) {  // contiguous thirds of the K steps
+              ++seg;
+              next_b = ((seg + 1) * nsteps + NMAIN - 1) / NMAIN;
+            }
             const uint32_t accum_main = seg == seg_prev ? 1u : 0u;
             seg_prev = seg;
             const uint32_t accum_corr = step > 0 ? 1u : 0u;
