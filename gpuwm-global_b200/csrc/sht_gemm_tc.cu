@@ -375,6 +375,13 @@ __device__ __forceinline__ bool reject_tile(const ShtTcTile& tl, volatile int* a
   return true;
 }
 
+__device__ bool wait_bar(uint64_t* bar, uint32_t parity, const Pipe& pp, unsigned* err, int where);
+// The common case inline: the phase has already completed.
+__device__ __forceinline__ bool wait_fast(uint64_t* bar, uint32_t parity, const Pipe& pp,
+                                          unsigned* err, int where) {
+  return mbar_try_wait(bar, parity) || wait_bar(bar, parity, pp, err, where);
+}
+
 // Bounded wait: returns false (and raises the abort flag) when the clock
 // budget runs out or another role has aborted.
 __device__ bool wait_bar(uint64_t* bar, uint32_t parity, const Pipe& pp, unsigned* err, int where) {
@@ -530,22 +537,23 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
         int next_b = NMAIN > 1 ? (nsteps + NMAIN - 1) / NMAIN : nsteps;
         bool ok = true;
         for (int ks = 0; ks < tl.kst; ++ks) {
-          if (!wait_bar(Acc::A_TMEM ? &pp.full_a[aslot] : &pp.full_a[stage],
-                        Acc::A_TMEM ? aphase : phase, pp, a.err, 3) ||
-              !wait_bar(&pp.full_b[stage], phase, pp, a.err, 4)) {
+          if (!wait_fast(Acc::A_TMEM ? &pp.full_a[aslot] : &pp.full_a[stage],
+                         Acc::A_TMEM ? aphase : phase, pp, a.err, 3) ||
+              !wait_fast(&pp.full_b[stage], phase, pp, a.err, 4)) {
             ok = false;
             break;
           }
           tc_fence_after();
-          const uint32_t a0 = smem_u32(sA + stage * NPARTS * kAPart);
-          const uint32_t b0 = smem_u32(sB + stage * NPARTS * kBPart);
+          // Descriptors of the stage's operands; a K step of 16 (two K groups
+          // of 8) advances the start-address field by 2 LBO / 16.
+          const uint64_t da0 = smem_desc(smem_u32(sA + stage * NPARTS * kAPart), kALbo, 128);
+          const uint64_t db0 = smem_desc(smem_u32(sB + stage * NPARTS * kBPart), lbo_b, 128);
 #pragma unroll
           for (int j = 0; j < BK / 16; ++j) {
-            // one K step of 16 = two K groups of 8
-            const uint64_t da1 = smem_desc(a0 + j * 2 * kALbo, kALbo, 128);
-            const uint64_t da2 = smem_desc(a0 + kAPart + j * 2 * kALbo, kALbo, 128);
-            const uint64_t db1 = smem_desc(b0 + j * 2 * lbo_b, lbo_b, 128);
-            const uint64_t db2 = smem_desc(b0 + kBPart + j * 2 * lbo_b, lbo_b, 128);
+            const uint64_t da1 = da0 + (uint64_t)(j * 2 * kALbo / 16);
+            const uint64_t da2 = da1 + (uint64_t)(kAPart / 16);
+            const uint64_t db1 = db0 + (uint64_t)(j * 2 * lbo_b / 16);
+            const uint64_t db2 = db1 + (uint64_t)(kBPart / 16);
             const int step = ks * (BK / 16) + j;
             if (step >= next_b && seg < NMAIN - 1) {  // contiguous thirds of the K steps
               ++seg;
