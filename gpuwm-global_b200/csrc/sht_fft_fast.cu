@@ -349,42 +349,48 @@ __global__ void __launch_bounds__(W * 32, 24 / W) fast_forward_fold(FastFoldArgs
     warp_fft_rows<FF, R, false, false>(z, smem(warp), W * SL, tws, lane);
   }
   __syncthreads();
-  // Untangle, scale, fold, write: thread -> (m, q) with q fastest.
+  // Untangle, scale, fold, write.
   // 0.5 / nlon: (x / 2) / nlon and x * (0.5 / nlon) round alike (both
   // scalings by 2 are exact).
   const float half_inv_n = 0.5f / (float)a.nlon;
   const int64_t Rc = a.planes * a.F;  // complex columns per waist row
-  float mre = 0.f, mim = 0.f;         // this thread's column maxima (q = tid % nper)
+  float mre = 0.f, mim = 0.f;         // this thread's column maxima
   const int T = TC >= 0 ? TC : a.T;   // compile-time on the linear grid
-  for (int t = threadIdx.x; t < (T + 1) * nper; t += blockDim.x) {
-    int m = t / nper, q = t - m * nper;
-    int gq = q >> fsh;
-    if (p0 + gq >= a.planes) continue;
-    float2 w = twn[m];
-    float2 X[2];
+  // Thread -> column q (fixed: blockDim is a multiple of nper) and orders
+  // m0, m0 + mstep, ...; the waist pointers advance by a constant stride.
+  const int q = threadIdx.x % nper;
+  const int mstep = (W * 32) / nper;
+  if (p0 + (q >> fsh) < a.planes) {
+    const float2* zr0 = smem(q * 2);
+    const float2* zr1 = smem(q * 2 + 1);
+    const int64_t dsd = (int64_t)a.H * Rc;  // S row -> D row of the same order
+    const int64_t dm = (int64_t)(2 * mstep) * dsd;
+    float2* dst = wfold + ((int64_t)(2 * (threadIdx.x / nper)) * a.H + h) * Rc + p0 * a.F + q;
+    for (int m = threadIdx.x / nper; m <= T; m += mstep, dst += dm) {
+      const float2 w = twn[m];
+      const int mc = m == 0 ? 0 : L - m;
+      float2 X[2];
 #pragma unroll
-    for (int sd = 0; sd < 2; ++sd) {
-      if (sd == 1 && eq) {
-        X[1] = make_float2(0.f, 0.f);
-        continue;
+      for (int sd = 0; sd < 2; ++sd) {
+        if (sd == 1 && eq) {
+          X[1] = make_float2(0.f, 0.f);
+          continue;
+        }
+        const float2* zr = sd ? zr1 : zr0;
+        const float2 zk = zr[m], zc = cconjf(zr[mc]);
+        const float2 ev = caddf(zk, zc), od = csubf(zk, zc);
+        const float2 t1 = cmulf(w, od);
+        X[sd] = make_float2((ev.x + t1.y) * half_inv_n, (ev.y - t1.x) * half_inv_n);
       }
-      const float2* zr = smem(q * 2 + sd);
-      float2 zk = zr[m];
-      float2 zc = cconjf(zr[m == 0 ? 0 : L - m]);
-      float2 ev = caddf(zk, zc), od = csubf(zk, zc);
-      float2 t1 = cmulf(w, od);
-      X[sd] = make_float2((ev.x + t1.y) * half_inv_n, (ev.y - t1.x) * half_inv_n);
+      const float2 S = eq ? X[0] : caddf(X[0], X[1]);
+      const float2 D = eq ? make_float2(0.f, 0.f) : csubf(X[0], X[1]);
+      __stcs(dst, S);
+      __stcs(dst + dsd, D);
+      mre = fmaxf(mre, fmaxf(fabsf(S.x), fabsf(D.x)));
+      mim = fmaxf(mim, fmaxf(fabsf(S.y), fabsf(D.y)));
     }
-    float2 S = eq ? X[0] : caddf(X[0], X[1]);
-    float2 D = eq ? make_float2(0.f, 0.f) : csubf(X[0], X[1]);
-    int64_t col = p0 * a.F + q;
-    __stcs(&wfold[((int64_t)(m * 2 + 0) * a.H + h) * Rc + col], S);
-    __stcs(&wfold[((int64_t)(m * 2 + 1) * a.H + h) * Rc + col], D);
-    mre = fmaxf(mre, fmaxf(fabsf(S.x), fabsf(D.x)));
-    mim = fmaxf(mim, fmaxf(fabsf(S.y), fabsf(D.y)));
   }
   if (rowmax != nullptr) {
-    const int q = threadIdx.x % nper;  // fixed per thread: blockDim % nper == 0
     rowmax_merge(rowmax, p0 * a.F + q, p0 + (q >> fsh) < a.planes, mre, mim, nper);
   }
 }
