@@ -536,31 +536,18 @@ __device__ __forceinline__ void cp_async16(void* dst, const void* src, uint32_t 
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
-// Entangle, FFT and store this warp's R rows (slots reg + r * slot, output
-// rows out_row0 + r * out_stride floats2, the first `nvalid` of them stored).
-template <int FF, int R, int TC>
-__device__ __forceinline__ void inverse_rows_out(const FastUnfoldArgs& a, float2* reg, int slot,
-                                                 const float2* tws, const float2* tn,
+// FFT and store this warp's R rows: slot reg + r * slot holds row r's
+// entangled sequence Z[0..L) in natural order (written by the unfold pass);
+// output rows out_row0 + r * out_stride floats2, the first `nvalid` stored.
+template <int FF, int R>
+__device__ __forceinline__ void inverse_rows_out(float2* reg, int slot, const float2* tws,
                                                  float2* __restrict__ out_row0, int64_t out_stride,
                                                  int lane, int nvalid) {
-  constexpr int L = 32 * FF;
-  const int T = TC >= 0 ? TC : a.T;  // compile-time on the linear grid
   float2 z[R][FF];
 #pragma unroll
-  for (int r = 0; r < R; ++r) {
-    const float2* x = reg + r * slot;
+  for (int r = 0; r < R; ++r)
 #pragma unroll
-    for (int i = 0; i < FF; ++i) {
-      int k = lane + 32 * i;
-      float2 xk = k <= T ? x[k] : make_float2(0.f, 0.f);
-      int kc = L - k;
-      float2 xc = (k > 0 && kc <= T) ? cconjf(x[kc]) : make_float2(0.f, 0.f);
-      if (k == 0) xk.y = 0.f;
-      float2 sm = caddf(xk, xc), df = csubf(xk, xc);
-      float2 wd = cmulf(cconjf(tn[k]), df);
-      z[r][i] = make_float2(sm.x - wd.y, sm.y + wd.x);
-    }
-  }
+    for (int i = 0; i < FF; ++i) z[r][i] = reg[r * slot + lane + 32 * i];
   __syncwarp();
   warp_fft_rows<FF, R, true, true>(z, reg, slot, tws, lane, out_row0, out_stride, nvalid);
   __syncwarp();  // every lane's reads of reg are done before the next item's unfold
@@ -592,6 +579,7 @@ __global__ void __launch_bounds__(InvCfg<NF>::W * 32, 16 / InvCfg<NF>::W)
   constexpr int GI = InvCfg<NF>::G * R;      // planes per item
   constexpr int CW = NF == 4 ? 2 * GI : GI;  // waist columns per item (even)
   constexpr int SL = WarpSmem<FF>::kFloats2;
+  constexpr int L = 32 * FF;  // complex row length (nlon / 2)
   extern __shared__ float2 smem_dyn[];
   auto rows = [&](int slot) { return smem_dyn + slot * SL; };
   float2* tws = smem_dyn + kW * R * SL;
@@ -637,42 +625,99 @@ __global__ void __launch_bounds__(InvCfg<NF>::W * 32, 16 / InvCfg<NF>::W)
     __syncthreads();  // the item's slices landed; every warp stored its previous rows
     const int T = TC >= 0 ? TC : a.T;
     const int T1 = T + 1;
-    for (int t = threadIdx.x; t < T1 * GI; t += blockDim.x) {
-      const int m = t / GI, g = t - m * GI;
-      if (p0 + g >= a.planes) continue;
-      // the NF symmetric / antisymmetric pairs of (m, plane g)
+    // Row scale factors of the two sides: 1 / (a cos phi) (gradient, wind).
+    float ie[2] = {0.f, 0.f};
+    if constexpr (NF != 1) {
+      ie[0] = 1.0f / (a.radius * (float)coslat[h]);
+      ie[1] = 1.0f / (a.radius * (float)coslat[jmir]);
+    }
+    // x[o][sd]: the spectrum of order j (j <= T) of output field o on side
+    // sd, from the symmetric and antisymmetric parts of plane g.
+    auto order_values = [&](int j, int g, float2 (&x)[NO][2]) {
       float2 S[NF], D[NF];
 #pragma unroll
       for (int k = 0; k < NF; ++k) {
         const int b = NF == 1 ? 0 : (NF == 2 ? k : k >> 1);
         const int c = NF == 4 ? 2 * g + (k & 1) : g;
-        S[k] = stage[((b * 2 + 0) * T1 + m) * CW + c];
-        D[k] = stage[((b * 2 + 1) * T1 + m) * CW + c];
+        S[k] = stage[((b * 2 + 0) * T1 + j) * CW + c];
+        D[k] = stage[((b * 2 + 1) * T1 + j) * CW + c];
       }
+      const float mf = (float)j;
 #pragma unroll
       for (int sd = 0; sd < 2; ++sd) {
-        if (sd == 1 && eq) continue;
         const float sgn = sd ? -1.f : 1.f;
-        float2 x[NF];
+        float2 v[NF];
 #pragma unroll
-        for (int k = 0; k < NF; ++k) x[k] = make_float2(S[k].x + sgn * D[k].x, S[k].y + sgn * D[k].y);
+        for (int k = 0; k < NF; ++k) v[k] = make_float2(S[k].x + sgn * D[k].x, S[k].y + sgn * D[k].y);
         if constexpr (NF == 1) {
-          rows(g * 2 + sd)[m] =
-              a.mode == kUnfoldZonal ? make_float2(-(float)m * x[0].y, (float)m * x[0].x) : x[0];
+          x[0][sd] = a.mode == kUnfoldZonal ? make_float2(-mf * v[0].y, mf * v[0].x) : v[0];
         } else if constexpr (NF == 2) {
           // gradient: (i m P) / (a cos phi) east, (dP) / a north; the
           // divisions applied here, ahead of the (linear) FFT
-          const float ie = 1.0f / (a.radius * (float)coslat[sd ? jmir : h]);
-          rows((g * NO + 0) * 2 + sd)[m] = make_float2(-(float)m * x[0].y * ie, (float)m * x[0].x * ie);
-          rows((g * NO + 1) * 2 + sd)[m] = make_float2(x[1].x * inv_a, x[1].y * inv_a);
+          x[0][sd] = make_float2(-mf * v[0].y * ie[sd], mf * v[0].x * ie[sd]);
+          x[1][sd] = make_float2(v[1].x * inv_a, v[1].y * inv_a);
         } else {
-          // x = {P psi, P chi, dP psi, dP chi}
-          const float im_over = (float)m / (a.radius * (float)coslat[sd ? jmir : h]);
-          rows((g * NO + 0) * 2 + sd)[m] = make_float2(-x[2].x * inv_a - im_over * x[1].y,
-                                                       -x[2].y * inv_a + im_over * x[1].x);
-          rows((g * NO + 1) * 2 + sd)[m] = make_float2(-im_over * x[0].y + x[3].x * inv_a,
-                                                       im_over * x[0].x + x[3].y * inv_a);
+          // v = {P psi, P chi, dP psi, dP chi}
+          const float im_over = mf * ie[sd];
+          x[0][sd] = make_float2(-v[2].x * inv_a - im_over * v[1].y, -v[2].y * inv_a + im_over * v[1].x);
+          x[1][sd] = make_float2(-im_over * v[0].y + v[3].x * inv_a, im_over * v[0].x + v[3].y * inv_a);
         }
+      }
+    };
+    // Entangle into the rows: Z[k] = A + conj(C) + i conj(w_k) (A - conj(C))
+    // with A = X[k], C = X[L - k], w_k = exp(-2 pi i k / nlon), for the
+    // half-length complex FFT of the real row.  Z[L - k] takes the same A, C
+    // and w_k (w_{L-k} = -conj(w_k)): with sm = A + conj(C) and
+    // t = conj(w_k)(A - conj(C)), Z[k] = sm + i t and Z[L - k] = conj(sm) + i conj(t).
+    auto entangle = [&](int g, int k, const float2 (&A)[NO][2], const float2 (&C)[NO][2], float2 w,
+                        bool pair) {
+#pragma unroll
+      for (int o = 0; o < NO; ++o)
+#pragma unroll
+        for (int sd = 0; sd < 2; ++sd) {
+          if (sd == 1 && eq) continue;
+          float2* row = rows((g * NO + o) * 2 + sd);
+          const float2 p = A[o][sd], q = C[o][sd];
+          const float2 sm = make_float2(p.x + q.x, p.y - q.y), df = make_float2(p.x - q.x, p.y + q.y);
+          const float2 t = cmulf(cconjf(w), df);
+          row[k] = make_float2(sm.x - t.y, sm.y + t.x);
+          if (pair) row[L - k] = make_float2(sm.x + t.y, t.x - sm.y);
+        }
+    };
+    // Thread -> (k, plane g), k < L / 2: Z[k] and Z[L - k]; k = 0 also
+    // writes the self-paired middle entry Z[L / 2].
+    for (int t = threadIdx.x; t < (L / 2) * GI; t += blockDim.x) {
+      const int k = t / GI, g = t - k * GI;  // GI: a compile-time power of two
+      if (p0 + g >= a.planes) continue;
+      const int kc = L - k;
+      float2 A[NO][2], C[NO][2];
+      if (k <= T) {
+        order_values(k, g, A);
+      } else {
+#pragma unroll
+        for (int o = 0; o < NO; ++o) A[o][0] = A[o][1] = make_float2(0.f, 0.f);
+      }
+      if (k > 0 && kc <= T) {
+        order_values(kc, g, C);
+      } else {
+#pragma unroll
+        for (int o = 0; o < NO; ++o) C[o][0] = C[o][1] = make_float2(0.f, 0.f);
+      }
+      if (k == 0) {
+        // order 0 is real; its partner L lies outside the row
+#pragma unroll
+        for (int o = 0; o < NO; ++o) A[o][0].y = A[o][1].y = 0.f;
+      }
+      entangle(g, k, A, C, twn[k], k > 0);
+      if (k == 0) {
+        float2 M[NO][2];
+        if (L / 2 <= T) {
+          order_values(L / 2, g, M);
+        } else {
+#pragma unroll
+          for (int o = 0; o < NO; ++o) M[o][0] = M[o][1] = make_float2(0.f, 0.f);
+        }
+        entangle(g, L / 2, M, M, twn[L / 2], false);
       }
     }
     __syncthreads();  // the staging buffer is free again
@@ -690,7 +735,7 @@ __global__ void __launch_bounds__(InvCfg<NF>::W * 32, 16 / InvCfg<NF>::W)
       // rows past the plane count are transformed but not stored
       const int64_t left = (a.planes - plane + G - 1) / G;
       const int nvalid = left < R ? (int)left : R;
-      inverse_rows_out<FF, R, TC>(a, rows(warp), kW * SL, tws, twn, row0, stride, ln, nvalid);
+      inverse_rows_out<FF, R>(rows(warp), kW * SL, tws, row0, stride, ln, nvalid);
     }
   }
 }
