@@ -51,12 +51,14 @@ def parse():
     ap.add_argument("--profile-only", action="store_true",
                     help="one plan, warmup + steps of the pair, no checks (small ncu case)")
     ap.add_argument("--precision", default="split16", choices=["split16", "float32", "float64"])
-    ap.add_argument("--workload", default="pair", choices=["pair", "ensemble", "step"],
+    ap.add_argument("--workload", default="pair", choices=["pair", "ensemble", "step", "sl_gather"],
                     help="pair: the T511 L40 transform pair (default); ensemble: 32 members "
                          "at T126 + the T255 control as one batch; step: the full T511 "
                          "dycore-step transform set as one CUDA graph, with the "
                          "Rossby-Haurwitz wave's energy drift over --drift-steps steps")
     ap.add_argument("--drift-steps", type=int, default=100)
+    ap.add_argument("--sl-fields", type=int, default=16, help="sl_gather: fields per call")
+    ap.add_argument("--sl-levels", type=int, default=40, help="sl_gather: levels")
     return ap.parse_args()
 
 
@@ -177,6 +179,25 @@ def cpu_oracle_rate(T, planes, reps=2):
     return planes / best, best
 
 
+def cpu_sl_gather_rate():
+    """Point-fields/s of the CPU oracle's cubic quasi-monotone gather on a
+    bounded sample: one field of 4 levels on the 768 x 1536 grid."""
+    import numpy as np
+
+    from oracle import sl_gather as O
+
+    nlev = 4
+    lat = np.sort(np.arcsin(np.polynomial.legendre.leggauss(768)[0]))
+    xi, phi, level = O.departure_sample(nlev, lat, 1536, 11, cells=1.0, dtype=np.float32)
+    f = np.random.default_rng(5).standard_normal((nlev, 768, 1536)).astype(np.float32)
+    t0 = time.perf_counter()
+    O.gather([f], xi, phi, level, lat, 1536, dtype=np.float32)
+    dt = time.perf_counter() - t0
+    return {"value": nlev * 768 * 1536 / dt, "unit": "point-fields/s", "cores": 1,
+            "kind": "port",
+            "sample": f"1 field x 4 levels x 768 x 1536, cubic quasi-monotone, numpy ({dt:.1f} s)"}
+
+
 def run_reference(args):
     ws, rank, _ = dist_setup()
     if rank != 0:
@@ -219,7 +240,10 @@ def main():
     if args.workload != "pair":
         from b200sht.workloads import run_workload
 
-        print(json.dumps(run_workload(args, ClockSampler)), flush=True)
+        line = run_workload(args, ClockSampler)
+        if args.workload == "sl_gather" and not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_sl_gather_rate()
+        print(json.dumps(line), flush=True)
         return
     import torch
     import torch.distributed as dist

@@ -29,6 +29,8 @@ SHT_ERR_ARG = 1
 SHT_ERR_CUDA = 2
 SHT_ERR_DEVICE = 3
 SHT_ERR_STATE = 4
+SHT_SL_NONE = 0
+SHT_SL_QUASI_MONOTONE = 1
 #: Kernel kinds of sht_plan_read_timing, in order.
 KERNEL_KINDS = ("fft_forward", "fft_inverse", "legendre_analysis", "legendre_synthesis", "pack",
                 "unpack", "elementwise", "helmholtz")
@@ -38,6 +40,7 @@ _P = ctypes.c_void_p
 _I64 = ctypes.c_int64
 _D = ctypes.c_double
 _DP = ctypes.POINTER(ctypes.c_double)
+_I32P = ctypes.POINTER(ctypes.c_int32)
 SIGNATURES = {
     "sht_abi_version": (ctypes.c_int, []),
     "sht_last_error": (ctypes.c_char_p, []),
@@ -81,6 +84,15 @@ SIGNATURES = {
     "sht_batch_destroy": (ctypes.c_int, [_P]),
     "sht_batch_forward": (ctypes.c_int, [_P, ctypes.POINTER(_P), ctypes.POINTER(_P), _P]),
     "sht_batch_inverse": (ctypes.c_int, [_P, ctypes.POINTER(_P), ctypes.POINTER(_P), _P]),
+    "sht_sl_tables_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, _DP, _DP, ctypes.c_int,
+                                            ctypes.POINTER(_P)]),
+    "sht_sl_tables_destroy": (ctypes.c_int, [_P]),
+    "sht_sl_tables_read": (ctypes.c_int, [_P, ctypes.c_int, _DP, _DP, _I32P, _I32P, _I32P,
+                                          ctypes.POINTER(ctypes.c_int),
+                                          ctypes.POINTER(ctypes.c_int), _DP]),
+    "sht_sl_gather": (ctypes.c_int, [_P, ctypes.c_int, ctypes.c_int, ctypes.c_int, _P, _I64,
+                                     ctypes.c_int, _P, _P, _P, _P, _P, _P]),
+    "sht_sl_gather_linear": (ctypes.c_int, [_P, _P, _I64, ctypes.c_int, _P, _P, _P, _P, _P]),
 }
 
 _lib = None

@@ -11,6 +11,10 @@ GPU and cast to f32.
 as one CUDA graph per 300 s step, split16 and float32, with the
 Rossby-Haurwitz wave-4 state plus 1 % red noise iterated for ``drift_steps``
 steps and the wave's spectral energy drift reported against the FP64 path.
+
+``sl_gather``: the semi-Lagrangian gather of 16 fields at T511 L40 (cubic
+quasi-monotone headline, cubic and quintic unlimited, trilinear) at the
+departure points of a solid-body rotation across both poles.
 """
 from __future__ import annotations
 
@@ -174,6 +178,97 @@ def step(args, clock_sampler):
     return out
 
 
+def rotation_departures(lat, nlon, nlev, *, speed=80.0, dt=300.0, radius=6371220.0,
+                        dtype=torch.float32, device=None):
+    """Departure coordinates of a solid-body rotation about the axis
+    through (0 N, 0 E), whose flow crosses both poles: every arrival point
+    rotated back by speed * dt / radius radians (0.94 equatorial cells at
+    T511), the angle varied by +-20 % over the levels, and the departure
+    level k - 0.6 sin(2 lambda) cos(phi), which reaches both half layers."""
+    dev = device or torch.device("cuda", torch.cuda.current_device())
+    lat = torch.as_tensor(lat, dtype=torch.float64, device=dev)
+    lon = torch.arange(nlon, dtype=torch.float64, device=dev) * (2 * torch.pi / nlon)
+    k = torch.arange(nlev, dtype=torch.float64, device=dev)
+    th = -(speed * dt / radius) * (1.0 + 0.2 * torch.cos(torch.pi * k / max(nlev - 1, 1)))
+    cl, sl = torch.cos(lat)[None, :, None], torch.sin(lat)[None, :, None]
+    x = cl * torch.cos(lon)[None, None, :]
+    y = cl * torch.sin(lon)[None, None, :]
+    c, s = torch.cos(th)[:, None, None], torch.sin(th)[:, None, None]
+    y2, z2 = y * c - sl * s, y * s + sl * c
+    x2 = x.expand_as(y2)
+    phi = torch.atan2(z2, torch.sqrt(x2 * x2 + y2 * y2))
+    lam = torch.remainder(torch.atan2(y2, x2), 2 * torch.pi)
+    xi = lam * (nlon / (2 * torch.pi))
+    level = k[:, None, None] - 0.6 * torch.sin(2 * lon)[None, None, :] * cl
+    level = level.expand_as(xi)
+    return (xi.to(dtype).contiguous(), phi.to(dtype).contiguous(),
+            level.to(dtype).contiguous())
+
+
+def sl_gather(args, clock_sampler):
+    """The semi-Lagrangian gather of 16 fields (the reference's batch) at
+    T511 L40 on the 768 x 1536 grid, float32: cubic quasi-monotone (the
+    limited species, headline), cubic unlimited, quintic unlimited (the
+    dynamical bundle) and the trilinear value."""
+    from .grid import GaussianGrid
+    from .semilag import SphericalGridTables, Stencil, gather_batch, gather_linear_batch
+
+    nlev, nfield = getattr(args, "sl_levels", 40), getattr(args, "sl_fields", 16)
+    grid = GaussianGrid.create(511, nlat=768, nlon=1536)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    tables = SphericalGridTables.create(grid, dtype=torch.float32)
+    xi, phi, level = rotation_departures(grid.lat_rad, grid.nlon, nlev)
+    st = Stencil(xi=xi, phi=phi, level=level, tables=tables)
+    gen = torch.Generator(device=dev).manual_seed(20261203)
+    src = torch.randn((nfield, nlev, grid.nlat, grid.nlon), generator=gen, device=dev,
+                      dtype=torch.float32)
+    fields = list(src)
+    npts = nlev * grid.nlat * grid.nlon
+    cases = {"cubic_quasi_monotone": dict(monotone=True, order=4),
+             "cubic_none": dict(monotone=False, order=4),
+             "quintic_none": dict(monotone=False, order=6)}
+    out = {"metric": f"Semi-Lagrangian gather point-fields/s (T511 L{nlev}, {nfield} fields, "
+                     "cubic quasi-monotone)",
+           "unit": "point-fields/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+           "higher_is_better": True, "dtype": "f32",
+           "data": "synthetic: seeded normal fields; departure points of a solid-body rotation "
+                   "across both poles (0.94 equatorial cells) and +-0.6 levels",
+           "config": {"workload": f"{nfield} fields x {nlev} levels x 768 x 1536, one gather "
+                                  "call of 16 fields per step",
+                      "points": npts, "fields": nfield,
+                      "l2": f"inputs larger than L2 ({npts * nfield * 4 / 1e9:.1f} GB of "
+                            "source fields)"}}
+    peak = None
+    try:
+        import json
+        from pathlib import Path
+
+        mp = Path(__file__).resolve().parents[2] / "MEASURED_PEAKS.json"
+        peak = float(json.loads(mp.read_text())["hbm_gbs"]) if mp.exists() else 6650.0
+    except Exception:
+        peak = 6650.0
+    with clock_sampler(torch.cuda.current_device()) as clocks:
+        for name, kw in cases.items():
+            ms = _time(lambda: gather_batch(fields, st, batch=nfield, **kw), args.steps,
+                       args.warmup)
+            byts = npts * (3 * 4 + nfield * 8)
+            out[name] = {"ms": ms, "point_fields_per_s": npts * nfield / (ms * 1e-3),
+                         "algorithmic_gb_per_s": byts / (ms * 1e-3) / 1e9}
+        ms = _time(lambda: gather_linear_batch(fields, st, batch=nfield), args.steps, args.warmup)
+        out["trilinear"] = {"ms": ms, "point_fields_per_s": npts * nfield / (ms * 1e-3)}
+    head = out["cubic_quasi_monotone"]
+    out["clocks"] = clocks.summary()
+    out["value"] = head["point_fields_per_s"]
+    out["ms_per_step"] = head["ms"]
+    out["gpu_launches"] = (len(cases) + 1) * args.steps
+    out["roofline"] = {"bound": "hbm", "achieved": head["algorithmic_gb_per_s"], "peak": peak,
+                       "unit": "GB/s", "frac": head["algorithmic_gb_per_s"] / peak,
+                       "traffic": None, "kernel": "sl_gather_kernel<float, 4, qm>",
+                       "algorithmic_bytes_per_point": 3 * 4 + nfield * 8}
+    return out
+
+
 def run_workload(args, clock_sampler):
     torch.cuda.set_device(0)
-    return {"ensemble": ensemble, "step": step}[args.workload](args, clock_sampler)
+    return {"ensemble": ensemble, "step": step,
+            "sl_gather": sl_gather}[args.workload](args, clock_sampler)

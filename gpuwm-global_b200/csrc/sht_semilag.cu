@@ -1,0 +1,634 @@
+// Semi-Lagrangian interpolation at departure points on the Gaussian grid:
+// the tricubic (4 x 4 x 4) and quintic-horizontal (6 x 6 x 4) gathers with
+// the quasi-monotone limiter and its clip deficit, and the trilinear gather
+// inside the limiter's cell (the reference's semilag/kernels.cu entry
+// families sl_gather_*, sl_gather5_*, sl_linear_*; their numpy
+// specification is semilag/interpolate.py:505-725, the tables
+// semilag/tables.py:51-236).
+//
+// Geometry of the stencil (the reference's conventions, which a drop-in
+// must keep):
+//   * zonal: uniform nodes lon[i] = 2 pi i / nlon, periodic; the departure
+//     point is a continuous zonal index; equispaced Lagrange weights;
+//   * meridional: the Gauss nodes extended by NH/2 reflected rows beyond
+//     each pole (a row past a pole is the ring on the other
+//     side read half a turn round), Lagrange weights on the true node
+//     latitudes from reciprocal denominators tabulated per stencil start;
+//   * vertical: four-point cubic in the continuous level index, the index
+//     clamped to the boundary interfaces [-1/2, nlev - 1/2], the stencil
+//     start to [0, nlev - 4];
+//   * every weight set normalised by its sum (exact identity at a node);
+//   * taps summed as differences from the stencil node nearest the point,
+//     the centre added back once;
+//   * unlimited fields: the half layer outside the outermost full level is
+//     held between that level's value and the linear reconstruction at the
+//     interface; limited fields: clipped to the [min, max] of the 2 x 2 x 2
+//     cell around the point, the deficit being raw - kept.
+//
+// B200 layout: one thread per arrival point, consecutive threads along a
+// latitude row (the departure points of a warp are neighbours, so its tap
+// loads share cache lines), rows taken with all their levels together (the
+// four arrival levels whose stencils read one source level plane run at the
+// same time, so the plane comes from DRAM about once); the geometry tables
+// (a few tens of KB) are read through the read-only path; in-plane offsets
+// are 32-bit; the F fields of one call share the index and weight
+// computation, two fields per pass on the four-point stencil.  The gather is bound by
+// its tap loads (64 or 144 per point per field, nearly all L1/L2 hits) and
+// by HBM for the coordinates, sources and outputs.
+#include <algorithm>
+#include <cmath>
+#include <type_traits>
+
+#include "sht_common.cuh"
+
+struct SlWidth {
+  int ghost = 0;                // reflected rows beyond each pole
+  int rows = 0;                 // extended rows: nlat + 2 ghost
+  int bins = 0;                 // bracket lookup bins
+  double lut_scale = 0.0;       // bins per radian
+  std::vector<double> lat_ext;  // [rows]
+  std::vector<double> mrden;    // [(nlat + 1) x NH]
+  std::vector<int32_t> mlut, rowoff, rowshift;
+  void* d_lat_ext = nullptr;    // element type of the tables
+  void* d_mrden = nullptr;
+  int32_t* d_mlut = nullptr;
+  int32_t* d_rowoff = nullptr;
+  int32_t* d_rowshift = nullptr;
+};
+
+struct sht_sl_tables {
+  int nlat = 0, nlon = 0, prec = 0, device = 0;
+  SlWidth w4, w6;  // w6 empty when nlat < 6
+};
+
+namespace sht {
+namespace {
+
+template <class F>
+int guarded(F&& f) {
+  try {
+    clear_error();
+    f();
+    return SHT_OK;
+  } catch (const Error& e) {
+    set_error(e.msg);
+    return e.code;
+  } catch (const std::exception& e) {
+    set_error(e.what());
+    return SHT_ERR_STATE;
+  }
+}
+
+constexpr double kHalfPi = 1.57079632679489661923;
+
+// ------------------------------------------------------------- weights
+
+// Lagrange weights on the equispaced nodes 0 .. NH-1 at t, normalised.
+template <typename T, int NH>
+__device__ __forceinline__ void equispaced_weights(T t, T (&w)[NH]) {
+  if constexpr (NH == 4) {
+    const T d0 = t, d1 = t - T(1), d2 = t - T(2), d3 = t - T(3);
+    w[0] = -d1 * d2 * d3 * T(1.0 / 6.0);
+    w[1] = d0 * d2 * d3 * T(0.5);
+    w[2] = -d0 * d1 * d3 * T(0.5);
+    w[3] = d0 * d1 * d2 * T(1.0 / 6.0);
+  } else {
+    T d[6];
+#pragma unroll
+    for (int q = 0; q < 6; ++q) d[q] = t - T(q);
+    // 1 / prod_{q != m} (m - q): -1/120, 1/24, -1/12, 1/12, -1/24, 1/120
+    const T c[6] = {T(-1.0 / 120.0), T(1.0 / 24.0), T(-1.0 / 12.0),
+                    T(1.0 / 12.0),   T(-1.0 / 24.0), T(1.0 / 120.0)};
+#pragma unroll
+    for (int m = 0; m < 6; ++m) {
+      T prod = T(1);
+#pragma unroll
+      for (int q = 0; q < 6; ++q)
+        if (q != m) prod *= d[q];
+      w[m] = prod * c[m];
+    }
+  }
+  T sum = w[0];
+#pragma unroll
+  for (int q = 1; q < NH; ++q) sum += w[q];
+  const T inv = T(1) / sum;
+#pragma unroll
+  for (int q = 0; q < NH; ++q) w[q] *= inv;
+}
+
+// The extended row m0 with lat_ext[m0] <= p < lat_ext[m0 + 1], held in
+// [G, nj + G] (G = 1 for the four-row stencil m0-1 .. m0+2, 2 for the
+// six-row stencil m0-2 .. m0+3) so that the stencil stays in the table: a
+// lookup bin, then exact steps (zero or one for Gauss nodes).
+template <typename T>
+__device__ __forceinline__ int bracket(T p, const T* __restrict__ lat_ext,
+                                       const int32_t* __restrict__ mlut, int nb, int nj, int G,
+                                       T lut_scale) {
+  int b = (int)((p + T(kHalfPi)) * lut_scale);
+  b = min(max(b, 0), nb - 1);
+  int m0 = __ldg(mlut + b);
+  while (m0 > G && p < __ldg(lat_ext + m0)) --m0;
+  while (m0 < nj + G && p >= __ldg(lat_ext + m0 + 1)) ++m0;
+  return m0;
+}
+
+// Memory index (k, j, i) of the t-th point in (j, k, i) order.
+__device__ __forceinline__ int64_t point_index(int64_t t, int nk, int nj, int ni) {
+  const int i = (int)(t % ni);
+  const int64_t r = t / ni;
+  const int k = (int)(r % nk), j = (int)(r / nk);
+  return ((int64_t)k * nj + j) * ni + i;
+}
+
+template <typename T>
+struct SlArgs {
+  const T* src;    // [F][nk][nj][ni]
+  const T* xi;     // [nk][nj][ni] continuous zonal index
+  const T* phi;    // latitude, radians
+  const T* lev;    // continuous full-level index
+  const T* lat_ext;
+  const T* mrden;
+  const int32_t* mlut;
+  const int32_t* rowoff;
+  const int32_t* rowshift;
+  T* out;          // [F][nk][nj][ni]
+  T* cut;          // clip deficit (or null)
+  int F, nk, nj, ni, nb;
+  T lut_scale;
+};
+
+// --------------------------------------------------------------- gather
+template <typename T, int NH, bool QM, bool DEF>
+__global__ void __launch_bounds__(256, (sizeof(T) == 4 && NH == 4) ? 3 : 2) sl_gather_kernel(const SlArgs<T> a) {
+  constexpr int G = NH / 2 - 1;  // zonal lead and meridional start offset
+  constexpr int MID = NH / 2 - 1;
+  const int plane = a.nj * a.ni;
+  const int64_t n = (int64_t)a.nk * plane;
+  // Threads walk the points row by row with the levels of a row together:
+  // a source level plane is read by the stencils of four arrival levels,
+  // which then run at the same time and find it in L2 (level-major order
+  // brought every plane in from DRAM about four times).
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const int64_t gid = point_index(t, a.nk, a.nj, a.ni);
+
+  const T p = min(max(a.phi[gid], T(-kHalfPi)), T(kHalfPi));
+  const T xk = min(max(a.lev[gid], T(-0.5)), T(a.nk) - T(0.5));
+  const bool below = xk < T(0);
+  const bool outside = below || xk > T(a.nk - 1);
+  const int c_edge = below ? 0 : 3, c_next = below ? 1 : 2;
+  const T xi = a.xi[gid];
+
+  // zonal: periodic, never clamped
+  const T fi = floor(xi);
+  const int i0 = (int)fi - G;
+  T wx[NH];
+  equispaced_weights<T, NH>(xi - T(i0), wx);
+  int col[NH], colh[NH];
+  col[0] = i0 % a.ni;
+  if (col[0] < 0) col[0] += a.ni;
+#pragma unroll
+  for (int q = 1; q < NH; ++q) col[q] = col[q - 1] + 1 == a.ni ? 0 : col[q - 1] + 1;
+  const int half = a.ni >> 1;
+#pragma unroll
+  for (int q = 0; q < NH; ++q) colh[q] = col[q] >= a.ni - half ? col[q] + half - a.ni : col[q] + half;
+
+  // meridional: true nodes, the poles by reflection
+  const int sst = bracket<T>(p, a.lat_ext, a.mlut, a.nb, a.nj, G, a.lut_scale) - G;
+  T d[NH], wy[NH];
+#pragma unroll
+  for (int m = 0; m < NH; ++m) d[m] = p - __ldg(a.lat_ext + sst + m);
+  {
+    T sum = T(0);
+#pragma unroll
+    for (int m = 0; m < NH; ++m) {
+      T prod = T(1);
+      bool first = true;
+#pragma unroll
+      for (int q = 0; q < NH; ++q) {
+        if (q == m) continue;
+        prod = first ? d[q] : prod * d[q];
+        first = false;
+      }
+      wy[m] = prod * __ldg(a.mrden + NH * sst + m);
+      sum = m == 0 ? wy[0] : sum + wy[m];
+    }
+    const T inv = T(1) / sum;
+#pragma unroll
+    for (int m = 0; m < NH; ++m) wy[m] *= inv;
+  }
+
+  // vertical: uniform in the level index, start clamped to the data
+  const int kb = min(max((int)floor(xk), 0), a.nk - 2);
+  const int k0 = min(max(kb - 1, 0), a.nk - 4);
+  const int kbox = kb - k0;
+  T wz[4];
+  equispaced_weights<T, 4>(xk - T(k0), wz);
+
+  int adr[NH][NH];  // in-plane offsets of the stencil's taps
+#pragma unroll
+  for (int m = 0; m < NH; ++m) {
+    const int ro = __ldg(a.rowoff + sst + m);
+    const bool sh = __ldg(a.rowshift + sst + m) != 0;
+#pragma unroll
+    for (int q = 0; q < NH; ++q) adr[m][q] = ro + (sh ? colh[q] : col[q]);
+  }
+  // the node nearest the point in each direction
+  const int cx = (xi - fi >= T(0.5)) ? MID + 1 : MID;
+  const int cy = (d[MID] >= __ldg(a.lat_ext + sst + MID + 1) - p) ? MID + 1 : MID;
+  const int kn = min(max((int)floor(xk + T(0.5)), 0), a.nk - 1);
+  int centre = adr[MID][MID];
+#pragma unroll
+  for (int m = MID; m <= MID + 1; ++m)
+#pragma unroll
+    for (int q = MID; q <= MID + 1; ++q)
+      if (m == cy && q == cx) centre = adr[m][q];
+
+  const int64_t fstride = n;
+  const int64_t cofs = (int64_t)kn * plane + centre;
+  // NB fields per pass share every address; their taps are in flight
+  // together (one level at a time: a fully unrolled level loop holds every
+  // level's loads and weights at once, 180+ registers).
+  auto fields = [&](auto nb_tag, int f0) {
+    constexpr int NB = decltype(nb_tag)::value;
+    const T* s[NB];
+    T base[NB], acc[NB], lo[NB], hi[NB], f_edge[NB], f_next[NB];
+#pragma unroll
+    for (int b = 0; b < NB; ++b) {
+      s[b] = a.src + (f0 + b) * fstride;
+      base[b] = __ldg(s[b] + cofs);
+      acc[b] = lo[b] = hi[b] = f_edge[b] = f_next[b] = T(0);
+    }
+    bool boxed = false;
+#pragma unroll 1
+    for (int c = 0; c < 4; ++c) {
+      const int64_t lofs = (int64_t)(k0 + c) * plane;
+      const T wzc = c == 0 ? wz[0] : (c == 1 ? wz[1] : (c == 2 ? wz[2] : wz[3]));
+      const bool inbox = QM && (c == kbox || c == kbox + 1);
+      T rowsum[NB];
+#pragma unroll
+      for (int b = 0; b < NB; ++b) rowsum[b] = T(0);
+#pragma unroll
+      for (int m = 0; m < NH; ++m) {
+        T v[NB][NH];
+#pragma unroll
+        for (int b = 0; b < NB; ++b)
+#pragma unroll
+          for (int q = 0; q < NH; ++q) v[b][q] = __ldg(s[b] + lofs + adr[m][q]);
+#pragma unroll
+        for (int b = 0; b < NB; ++b) {
+          if (inbox && (m == MID || m == MID + 1)) {
+            const T vmin = min(v[b][MID], v[b][MID + 1]), vmax = max(v[b][MID], v[b][MID + 1]);
+            lo[b] = boxed ? min(lo[b], vmin) : vmin;
+            hi[b] = boxed ? max(hi[b], vmax) : vmax;
+          }
+          T colsum = wx[0] * (v[b][0] - base[b]);
+#pragma unroll
+          for (int q = 1; q < NH; ++q) colsum += wx[q] * (v[b][q] - base[b]);
+          rowsum[b] += wy[m] * colsum;
+        }
+        if (inbox && (m == MID || m == MID + 1)) boxed = true;
+      }
+#pragma unroll
+      for (int b = 0; b < NB; ++b) {
+        acc[b] += wzc * rowsum[b];
+        if (c == c_edge) f_edge[b] = rowsum[b];
+        if (c == c_next) f_next[b] = rowsum[b];
+      }
+    }
+#pragma unroll
+    for (int b = 0; b < NB; ++b) {
+      T r = acc[b];
+      if (!QM && outside) {
+        const T f_face = f_edge[b] + T(0.5) * (f_edge[b] - f_next[b]);
+        r = min(max(r, min(f_edge[b], f_face)), max(f_edge[b], f_face));
+      }
+      r += base[b];
+      const T kept = QM ? min(max(r, lo[b]), hi[b]) : r;
+      a.out[(f0 + b) * fstride + gid] = kept;
+      if (DEF) a.cut[(f0 + b) * fstride + gid] = r - kept;
+    }
+  };
+  // Two fields per pass on the four-point stencil; the six-point one
+  // takes one (two would hold 190+ registers).
+  constexpr int NB = NH == 4 ? 2 : 1;
+  int f = 0;
+  for (; f + NB <= a.F; f += NB) fields(std::integral_constant<int, NB>{}, f);
+  if (f < a.F) fields(std::integral_constant<int, 1>{}, f);
+}
+
+// ------------------------------------------------------------ trilinear
+// Inside the limiter's cell: columns floor(xi), +1; extended rows m0, m0+1
+// of the cubic bracket; levels kb, kb+1 with the index held in [0, nk-1].
+template <typename T>
+__global__ void __launch_bounds__(256) sl_linear_kernel(const SlArgs<T> a) {
+  const int plane = a.nj * a.ni;
+  const int64_t n = (int64_t)a.nk * plane;
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const int64_t gid = point_index(t, a.nk, a.nj, a.ni);  // rows with their levels together
+  const T p = min(max(a.phi[gid], T(-kHalfPi)), T(kHalfPi));
+  const T xk = min(max(a.lev[gid], T(0)), T(a.nk - 1));
+  const T xi = a.xi[gid];
+  const T fi = floor(xi);
+  const T ax = xi - fi;
+  int c0 = ((int)fi) % a.ni;
+  if (c0 < 0) c0 += a.ni;
+  const int c1 = c0 + 1 == a.ni ? 0 : c0 + 1;
+  const int half = a.ni >> 1;
+  const int h0 = c0 >= a.ni - half ? c0 + half - a.ni : c0 + half;
+  const int h1 = c1 >= a.ni - half ? c1 + half - a.ni : c1 + half;
+  const int m0 = bracket<T>(p, a.lat_ext, a.mlut, a.nb, a.nj, 1, a.lut_scale);
+  const T la = __ldg(a.lat_ext + m0), lb = __ldg(a.lat_ext + m0 + 1);
+  const T ay = min(max((p - la) / (lb - la), T(0)), T(1));
+  const int r0 = __ldg(a.rowoff + m0), r1 = __ldg(a.rowoff + m0 + 1);
+  const bool s0 = __ldg(a.rowshift + m0) != 0, s1 = __ldg(a.rowshift + m0 + 1) != 0;
+  const int i00 = r0 + (s0 ? h0 : c0), i01 = r0 + (s0 ? h1 : c1);
+  const int i10 = r1 + (s1 ? h0 : c0), i11 = r1 + (s1 ? h1 : c1);
+  const int kb = min(max((int)floor(xk), 0), a.nk - 2);
+  const T az = xk - T(kb);
+  const T bx = T(1) - ax, by = T(1) - ay, bz = T(1) - az;
+  for (int f = 0; f < a.F; ++f) {
+    const T* s0p = a.src + f * n + (int64_t)kb * plane;
+    const T* s1p = s0p + plane;
+    const T t0 = by * (bx * __ldg(s0p + i00) + ax * __ldg(s0p + i01)) +
+                 ay * (bx * __ldg(s0p + i10) + ax * __ldg(s0p + i11));
+    const T t1 = by * (bx * __ldg(s1p + i00) + ax * __ldg(s1p + i01)) +
+                 ay * (bx * __ldg(s1p + i10) + ax * __ldg(s1p + i11));
+    a.out[f * n + gid] = bz * t0 + az * t1;
+  }
+}
+
+// ----------------------------------------------------------- tables
+// The pole-extended table of one stencil width (semilag/tables.py:51-95,
+// 164-217): G reflected rows each side, the data row and zonal shift each
+// extended row reads, the reciprocal Lagrange denominators of every stencil
+// start, and the bracket lookup (4 bins per extended row).
+void build_width(SlWidth& w, const std::vector<double>& lat, int nlon, int NH) {
+  const int nlat = (int)lat.size();
+  const int G = NH / 2;  // 2 (cubic) or 3 (quintic)
+  w.ghost = G;
+  w.rows = nlat + 2 * G;
+  w.lat_ext.assign(w.rows, 0.0);
+  for (int g = 0; g < G; ++g) {
+    w.lat_ext[G - 1 - g] = -kPi - lat[g];
+    w.lat_ext[nlat + G + g] = kPi - lat[nlat - 1 - g];
+  }
+  for (int j = 0; j < nlat; ++j) w.lat_ext[G + j] = lat[j];
+  for (int r = 1; r < w.rows; ++r)
+    SHT_REQUIRE(w.lat_ext[r] > w.lat_ext[r - 1],
+                "the pole-extended latitude table is not strictly ascending; the grid's "
+                "outermost rings sit closer to a pole than the reflection of the rings inside "
+                "them, which no Gaussian grid does and which the bracket search cannot represent");
+  w.rowoff.resize(w.rows);
+  w.rowshift.resize(w.rows);
+  for (int r = 0; r < w.rows; ++r) {
+    const int row = r - G;
+    const int data = row < 0 ? -1 - row : (row >= nlat ? 2 * nlat - 1 - row : row);
+    w.rowoff[r] = data * nlon;
+    w.rowshift[r] = (row < 0 || row >= nlat) ? nlon / 2 : 0;
+  }
+  w.mrden.assign((size_t)(nlat + 1) * NH, 0.0);
+  for (int s = 0; s <= nlat; ++s)
+    for (int m = 0; m < NH; ++m) {
+      double den = 1.0;
+      for (int q = 0; q < NH; ++q)
+        if (q != m) den *= w.lat_ext[s + m] - w.lat_ext[s + q];
+      w.mrden[(size_t)s * NH + m] = 1.0 / den;
+    }
+  w.bins = 4 * w.rows;
+  w.lut_scale = w.bins / kPi;
+  w.mlut.resize(w.bins);
+  const int lo = G - 1, hi = nlat + G - 1;  // bracket range of the width
+  for (int b = 0; b < w.bins; ++b) {
+    const double centre = -0.5 * kPi + (b + 0.5) / w.lut_scale;
+    // searchsorted(lat_ext, centre, side="right") - 1
+    const int m0 = (int)(std::upper_bound(w.lat_ext.begin(), w.lat_ext.end(), centre) -
+                         w.lat_ext.begin()) - 1;
+    w.mlut[b] = std::min(std::max(m0, lo), hi);
+  }
+}
+
+template <typename T>
+void upload_width(SlWidth& w) {
+  std::vector<T> le(w.lat_ext.begin(), w.lat_ext.end()), md(w.mrden.begin(), w.mrden.end());
+  SHT_CUDA_OR_THROW(cudaMalloc(&w.d_lat_ext, le.size() * sizeof(T)));
+  SHT_CUDA_OR_THROW(cudaMalloc(&w.d_mrden, md.size() * sizeof(T)));
+  SHT_CUDA_OR_THROW(cudaMalloc(&w.d_mlut, w.mlut.size() * sizeof(int32_t)));
+  SHT_CUDA_OR_THROW(cudaMalloc(&w.d_rowoff, w.rowoff.size() * sizeof(int32_t)));
+  SHT_CUDA_OR_THROW(cudaMalloc(&w.d_rowshift, w.rowshift.size() * sizeof(int32_t)));
+  upload_now(w.d_lat_ext, le.data(), le.size() * sizeof(T));
+  upload_now(w.d_mrden, md.data(), md.size() * sizeof(T));
+  upload_now(w.d_mlut, w.mlut.data(), w.mlut.size() * sizeof(int32_t));
+  upload_now(w.d_rowoff, w.rowoff.data(), w.rowoff.size() * sizeof(int32_t));
+  upload_now(w.d_rowshift, w.rowshift.data(), w.rowshift.size() * sizeof(int32_t));
+}
+
+void free_width(SlWidth& w) {
+  cudaFree(w.d_lat_ext);
+  cudaFree(w.d_mrden);
+  cudaFree(w.d_mlut);
+  cudaFree(w.d_rowoff);
+  cudaFree(w.d_rowshift);
+  w.d_lat_ext = w.d_mrden = nullptr;
+  w.d_mlut = w.d_rowoff = w.d_rowshift = nullptr;
+}
+
+const SlWidth& width_of(const sht_sl_tables* t, int order) {
+  SHT_REQUIRE(order == 4 || order == 6,
+              "the semi-Lagrangian gather's horizontal order must be one of 4, 6, got " +
+                  std::to_string(order));
+  if (order == 6)
+    SHT_REQUIRE(t->w6.rows > 0, "the quintic gather needs six meridional rows and this grid has " +
+                                    std::to_string(t->nlat) +
+                                    "; the six-point tables were not built");
+  return order == 6 ? t->w6 : t->w4;
+}
+
+template <typename T>
+SlArgs<T> make_args(const sht_sl_tables* t, const SlWidth& w, const void* src, int64_t F,
+                    int nlev, const void* xi, const void* phi, const void* lev, void* out,
+                    void* cut) {
+  SlArgs<T> a;
+  a.src = (const T*)src;
+  a.xi = (const T*)xi;
+  a.phi = (const T*)phi;
+  a.lev = (const T*)lev;
+  a.lat_ext = (const T*)w.d_lat_ext;
+  a.mrden = (const T*)w.d_mrden;
+  a.mlut = w.d_mlut;
+  a.rowoff = w.d_rowoff;
+  a.rowshift = w.d_rowshift;
+  a.out = (T*)out;
+  a.cut = (T*)cut;
+  a.F = (int)F;
+  a.nk = nlev;
+  a.nj = t->nlat;
+  a.ni = t->nlon;
+  a.nb = w.bins;
+  a.lut_scale = (T)w.lut_scale;
+  return a;
+}
+
+template <typename T, int NH>
+void launch_gather(const SlArgs<T>& a, bool qm, bool def, cudaStream_t s) {
+  const int64_t n = (int64_t)a.nk * a.nj * a.ni;
+  const unsigned blocks = (unsigned)div_up(n, 256);
+  if (qm && def)
+    sl_gather_kernel<T, NH, true, true><<<blocks, 256, 0, s>>>(a);
+  else if (qm)
+    sl_gather_kernel<T, NH, true, false><<<blocks, 256, 0, s>>>(a);
+  else
+    sl_gather_kernel<T, NH, false, false><<<blocks, 256, 0, s>>>(a);
+  SHT_CUDA_OR_THROW(cudaGetLastError());
+}
+
+void check_call(const sht_sl_tables* t, const void* src, int64_t fields, int nlev, const void* xi,
+                const void* phi, const void* lev, const void* out) {
+  SHT_REQUIRE(t != nullptr, "null semi-Lagrangian tables");
+  SHT_REQUIRE(src && xi && phi && lev && out, "null array pointer");
+  SHT_REQUIRE(fields >= 1 && fields <= (1 << 20), "fields must be in [1, 2^20]");
+  SHT_REQUIRE(nlev >= 4, "a four-point vertical stencil needs nlev >= 4, got " +
+                             std::to_string(nlev));
+  const int64_t npts = (int64_t)nlev * t->nlat * t->nlon;
+  SHT_REQUIRE(npts < ((int64_t)1 << 31) && fields * npts < ((int64_t)1 << 46),
+              "the gather's volume is too large for one call");
+  int dev = 0;
+  SHT_CUDA_OR_THROW(cudaGetDevice(&dev));
+  SHT_REQUIRE(dev == t->device, "the tables live on another device");
+}
+
+}  // namespace
+}  // namespace sht
+
+using namespace sht;
+
+extern "C" {
+
+int sht_sl_tables_create(int nlat, int nlon, const double* lat_rad, const double* lon_rad,
+                         int precision, sht_sl_tables** out) {
+  return guarded([&] {
+    SHT_REQUIRE(out != nullptr, "null output handle");
+    *out = nullptr;
+    SHT_REQUIRE(lat_rad != nullptr, "null latitude table");
+    SHT_REQUIRE(precision == SHT_PREC_F64 || precision == SHT_PREC_F32,
+                "the semi-Lagrangian gather is compiled for float32 and float64 only");
+    SHT_REQUIRE(nlat >= 4, "a four-point meridional stencil needs nlat >= 4, got " +
+                               std::to_string(nlat));
+    SHT_REQUIRE(nlon >= 4 && nlon % 2 == 0,
+                "nlon must be even so the polar reflection is an exact shift of nlon/2 columns, "
+                "got " + std::to_string(nlon));
+    std::vector<double> lat(lat_rad, lat_rad + nlat);
+    for (int j = 1; j < nlat; ++j)
+      SHT_REQUIRE(lat[j] > lat[j - 1],
+                  "lat_rad must be strictly ascending; the bracket search and the pole "
+                  "reflection both read it as a monotone table");
+    if (lon_rad != nullptr) {
+      const double dlam = 2.0 * kPi / nlon;
+      double drift = 0.0;
+      for (int i = 0; i < nlon; ++i) drift = std::max(drift, std::fabs(lon_rad[i] - i * dlam));
+      SHT_REQUIRE(drift <= 1e-12,
+                  "the zonal weights are the equispaced cubic Lagrange weights, which needs "
+                  "lon[i] = i*2*pi/nlon");
+    }
+    auto* t = new sht_sl_tables;
+    try {
+      t->nlat = nlat;
+      t->nlon = nlon;
+      t->prec = precision;
+      SHT_CUDA_OR_THROW(cudaGetDevice(&t->device));
+      build_width(t->w4, lat, nlon, 4);
+      if (nlat >= 6) build_width(t->w6, lat, nlon, 6);
+      if (precision == SHT_PREC_F64) {
+        upload_width<double>(t->w4);
+        if (nlat >= 6) upload_width<double>(t->w6);
+      } else {
+        upload_width<float>(t->w4);
+        if (nlat >= 6) upload_width<float>(t->w6);
+      }
+    } catch (...) {
+      free_width(t->w4);
+      free_width(t->w6);
+      delete t;
+      throw;
+    }
+    *out = t;
+  });
+}
+
+int sht_sl_tables_destroy(sht_sl_tables* tables) {
+  return guarded([&] {
+    if (!tables) return;
+    free_width(tables->w4);
+    free_width(tables->w6);
+    delete tables;
+  });
+}
+
+int sht_sl_tables_read(const sht_sl_tables* tables, int order, double* lat_ext, double* mrden,
+                       int32_t* mlut, int32_t* rowoff, int32_t* rowshift, int* rows, int* bins,
+                       double* lut_scale) {
+  return guarded([&] {
+    SHT_REQUIRE(tables != nullptr, "null semi-Lagrangian tables");
+    const SlWidth& w = width_of(tables, order);
+    if (rows) *rows = w.rows;
+    if (bins) *bins = w.bins;
+    if (lut_scale) *lut_scale = w.lut_scale;
+    if (lat_ext) std::copy(w.lat_ext.begin(), w.lat_ext.end(), lat_ext);
+    if (mrden) std::copy(w.mrden.begin(), w.mrden.end(), mrden);
+    if (mlut) std::copy(w.mlut.begin(), w.mlut.end(), mlut);
+    if (rowoff) std::copy(w.rowoff.begin(), w.rowoff.end(), rowoff);
+    if (rowshift) std::copy(w.rowshift.begin(), w.rowshift.end(), rowshift);
+  });
+}
+
+int sht_sl_gather(const sht_sl_tables* tables, int order, int limiter, int deficit,
+                  const void* src, int64_t fields, int nlev, const void* xi, const void* phi,
+                  const void* level, void* out, void* cut, void* stream) {
+  return guarded([&] {
+    check_call(tables, src, fields, nlev, xi, phi, level, out);
+    SHT_REQUIRE(limiter == SHT_SL_NONE || limiter == SHT_SL_QUASI_MONOTONE,
+                "the semi-Lagrangian gather's limiter must be one of 'quasi_monotone', 'none'");
+    const SlWidth& w = width_of(tables, order);
+    if (deficit) {
+      SHT_REQUIRE(limiter != SHT_SL_NONE,
+                  "the clip deficit is the mass the limiter moved, so an unlimited gather has "
+                  "none to report; ask for a limiter or do not ask for the deficit");
+      SHT_REQUIRE(order == 4, "the clip deficit is reported by the cubic gather only");
+      SHT_REQUIRE(cut != nullptr, "null deficit array");
+    }
+    const bool qm = limiter == SHT_SL_QUASI_MONOTONE, def = deficit != 0;
+    cudaStream_t s = (cudaStream_t)stream;
+    if (tables->prec == SHT_PREC_F64) {
+      auto a = make_args<double>(tables, w, src, fields, nlev, xi, phi, level, out, cut);
+      if (order == 6) launch_gather<double, 6>(a, qm, false, s);
+      else launch_gather<double, 4>(a, qm, def, s);
+    } else {
+      auto a = make_args<float>(tables, w, src, fields, nlev, xi, phi, level, out, cut);
+      if (order == 6) launch_gather<float, 6>(a, qm, false, s);
+      else launch_gather<float, 4>(a, qm, def, s);
+    }
+  });
+}
+
+int sht_sl_gather_linear(const sht_sl_tables* tables, const void* src, int64_t fields, int nlev,
+                         const void* xi, const void* phi, const void* level, void* out,
+                         void* stream) {
+  return guarded([&] {
+    check_call(tables, src, fields, nlev, xi, phi, level, out);
+    const SlWidth& w = tables->w4;
+    const int64_t n = (int64_t)nlev * tables->nlat * tables->nlon;
+    const unsigned blocks = (unsigned)div_up(n, 256);
+    cudaStream_t s = (cudaStream_t)stream;
+    if (tables->prec == SHT_PREC_F64) {
+      auto a = make_args<double>(tables, w, src, fields, nlev, xi, phi, level, out, nullptr);
+      sl_linear_kernel<double><<<blocks, 256, 0, s>>>(a);
+    } else {
+      auto a = make_args<float>(tables, w, src, fields, nlev, xi, phi, level, out, nullptr);
+      sl_linear_kernel<float><<<blocks, 256, 0, s>>>(a);
+    }
+    SHT_CUDA_OR_THROW(cudaGetLastError());
+  });
+}
+
+}  // extern "C"

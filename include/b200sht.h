@@ -287,6 +287,46 @@ int sht_batch_forward(sht_batch* batch, const void* const* grids, void* const* c
 int sht_batch_inverse(sht_batch* batch, const void* const* coeffs, void* const* grids,
                       void* stream);
 
+/* Semi-Lagrangian interpolation at departure points (the reference's
+ * semilag/interpolate.py gather_batch / gather_linear_batch and the kernels
+ * they launch, semilag/kernels.cu sl_gather_*, sl_gather5_*, sl_linear_*).
+ *
+ * sht_sl_tables_create builds the grid's geometry once (the reference's
+ * SphericalGridTables.create, semilag/tables.py:136-258): the pole-extended
+ * latitude tables of the four-point (and, for nlat >= 6, six-point)
+ * meridional stencils, the row offsets and zonal shifts each extended row
+ * reads, the reciprocal Lagrange denominators and the bracket lookup, in
+ * float64 on the host and uploaded in the precision's element type
+ * (SHT_PREC_F64: double, SHT_PREC_F32: float).  lat_rad: nlat ascending
+ * Gauss latitudes; lon_rad (optional): checked to be i*2*pi/nlon.
+ *
+ * sht_sl_gather reads `fields` source volumes src[f][nlev][nlat][nlon] at the
+ * departure coordinates xi (continuous zonal index), phi (latitude) and level
+ * (continuous full-level index), each [nlev][nlat][nlon], into
+ * out[f][nlev][nlat][nlon]: order 4 = tricubic, 6 = quintic horizontal with
+ * the cubic vertical; limiter SHT_SL_QUASI_MONOTONE clips to the 2x2x2 cell
+ * around the point; with deficit != 0 (cubic, limited) cut[f] receives raw
+ * minus kept.  sht_sl_gather_linear is the trilinear value inside that cell.
+ * Stream-ordered; every pointer is device memory the caller owns. */
+typedef struct sht_sl_tables sht_sl_tables;
+#define SHT_SL_NONE 0
+#define SHT_SL_QUASI_MONOTONE 1
+int sht_sl_tables_create(int nlat, int nlon, const double* lat_rad, const double* lon_rad,
+                         int precision, sht_sl_tables** out);
+int sht_sl_tables_destroy(sht_sl_tables* tables);
+/* Host copies of one width's tables (order 4 or 6): lat_ext[rows],
+ * mrden[(nlat + 1) * order], mlut[bins], rowoff[rows], rowshift[rows];
+ * any pointer may be null. */
+int sht_sl_tables_read(const sht_sl_tables* tables, int order, double* lat_ext, double* mrden,
+                       int32_t* mlut, int32_t* rowoff, int32_t* rowshift, int* rows, int* bins,
+                       double* lut_scale);
+int sht_sl_gather(const sht_sl_tables* tables, int order, int limiter, int deficit,
+                  const void* src, int64_t fields, int nlev, const void* xi, const void* phi,
+                  const void* level, void* out, void* cut, void* stream);
+int sht_sl_gather_linear(const sht_sl_tables* tables, const void* src, int64_t fields, int nlev,
+                         const void* xi, const void* phi, const void* level, void* out,
+                         void* stream);
+
 #ifdef __cplusplus
 }
 #endif

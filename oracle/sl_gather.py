@@ -1,0 +1,220 @@
+"""CPU oracle of the semi-Lagrangian gathers -- TEST INFRASTRUCTURE ONLY.
+
+Imported by ``tests/``, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU
+legs as the checker; the product path (``b200sht.semilag``) never imports
+it.  A numpy restatement, in float64 or the tables' float32, of:
+
+* the pole-extended geometry tables of the four- and six-point meridional
+  stencils (the reference's ``semilag/tables.py:51-95`` and ``:136-217``);
+* the tricubic / quintic-horizontal gather with the quasi-monotone limiter,
+  its clip deficit and the half-layer hold at the vertical boundaries
+  (``semilag/interpolate.py:536-669``, the numpy specification the
+  reference grades its kernel against);
+* the trilinear gather inside the limiter's cell
+  (``semilag/interpolate.py:672-725``).
+
+Pinned against ``tests/golden/sl_gather_*.npz``, outputs of the reference's
+own ``gather_batch`` / ``gather_linear_batch`` (numpy backend) recorded by
+``tests/golden/make_golden_sl.py``.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+BINS_PER_ROW = 4
+
+
+def build_tables(lat: np.ndarray, nlon: int, order: int = 4) -> dict:
+    """Extended latitudes, row offsets/shifts, reciprocal Lagrange
+    denominators and the bracket lookup of one stencil width
+    (tables.py:164-196 for order 4, :51-95 for order 6)."""
+    lat = np.asarray(lat, dtype=np.float64)
+    nlat = lat.shape[0]
+    ghost = order // 2
+    rows = nlat + 2 * ghost
+    lat_ext = np.empty(rows)
+    for g in range(ghost):
+        lat_ext[ghost - 1 - g] = -math.pi - lat[g]
+        lat_ext[nlat + ghost + g] = math.pi - lat[nlat - 1 - g]
+    lat_ext[ghost:nlat + ghost] = lat
+    row = np.arange(rows) - ghost
+    data = np.where(row < 0, -1 - row, np.where(row >= nlat, 2 * nlat - 1 - row, row))
+    rowoff = (data * nlon).astype(np.int32)
+    rowshift = np.where((row < 0) | (row >= nlat), nlon // 2, 0).astype(np.int32)
+    nodes = lat_ext[np.arange(nlat + 1)[:, None] + np.arange(order)[None, :]]
+    mrden = np.empty((nlat + 1, order))
+    for m in range(order):
+        den = np.ones(nlat + 1)
+        for q in range(order):
+            if q != m:
+                den = den * (nodes[:, m] - nodes[:, q])
+        mrden[:, m] = 1.0 / den
+    bins = BINS_PER_ROW * rows
+    scale = bins / math.pi
+    centres = -0.5 * math.pi + (np.arange(bins) + 0.5) / scale
+    mlut = np.clip(np.searchsorted(lat_ext, centres, side="right") - 1,
+                   ghost - 1, nlat + ghost - 1).astype(np.int32)
+    return dict(lat_ext=lat_ext, rowoff=rowoff, rowshift=rowshift, mrden=mrden, mlut=mlut,
+                bins=bins, lut_scale=scale, ghost=ghost)
+
+
+def _equispaced(t: np.ndarray, n: int) -> np.ndarray:
+    """Normalised Lagrange weights on the nodes 0 .. n-1 at t."""
+    cols = []
+    for m in range(n):
+        num = np.ones_like(t)
+        den = 1.0
+        for q in range(n):
+            if q != m:
+                num = num * (t - q)
+                den *= (m - q)
+        cols.append(num / den)
+    w = np.stack(cols, axis=-1)
+    return w / w.sum(axis=-1, keepdims=True)
+
+
+def gather(fields, xi, phi, level, lat, nlon, *, order=4, limiter="quasi_monotone",
+           deficit=False, dtype=np.float64):
+    """Every field (nlev, nlat, nlon) read at the departure coordinates
+    (interpolate.py:536-669).  Returns values, or (values, deficits)."""
+    dtype = np.dtype(dtype)
+    sc = dtype.type
+    tab = build_tables(lat, nlon, order)
+    lat_ext = tab["lat_ext"].astype(dtype)
+    mrden = tab["mrden"].astype(dtype)
+    nh, ghost = order, order // 2 - 1
+    mid = nh // 2 - 1
+    nlev, nlat, _ = np.shape(xi)
+    plane = nlat * nlon
+    flat = [np.ascontiguousarray(f, dtype=dtype).reshape(-1) for f in fields]
+    outs = [np.empty((nlev, plane), dtype) for _ in fields]
+    cuts = [np.zeros((nlev, plane), dtype) for _ in fields]
+    half_pi = sc(np.pi / 2.0)
+    for k in range(nlev):
+        p = np.clip(np.asarray(phi[k], dtype).reshape(-1), -half_pi, half_pi)
+        xk = np.clip(np.asarray(level[k], dtype).reshape(-1), sc(-0.5), sc(nlev - 0.5))
+        below = xk < 0
+        outside = below | (xk > sc(nlev - 1))
+        c_edge = np.where(below, 0, 3)
+        c_next = np.where(below, 1, 2)
+        x = np.asarray(xi[k], dtype).reshape(-1)
+        fx = np.floor(x)
+        i0 = fx.astype(np.int64) - ghost
+        wx = _equispaced(x - i0.astype(dtype), nh).astype(dtype)
+        cols = (i0[:, None] + np.arange(nh)) % nlon
+        colh = (cols + nlon // 2) % nlon
+        m0 = np.clip(np.searchsorted(lat_ext.astype(np.float64), p.astype(np.float64),
+                                     side="right") - 1, ghost, nlat + ghost)
+        sst = m0 - ghost
+        nodes = lat_ext[sst[:, None] + np.arange(nh)]
+        d = p[:, None] - nodes
+        wy = np.stack([np.prod(np.delete(d, m, axis=1), axis=1) for m in range(nh)], axis=-1)
+        wy = wy * mrden[sst]
+        wy = wy / wy.sum(axis=-1, keepdims=True)
+        kb = np.clip(np.floor(xk).astype(np.int64), 0, nlev - 2)
+        k0 = np.clip(kb - 1, 0, nlev - 4)
+        kbox = kb - k0
+        wz = _equispaced(xk - k0.astype(dtype), 4).astype(dtype)
+        ridx = sst[:, None] + np.arange(nh)
+        shifted = tab["rowshift"][ridx] > 0
+        adr = (tab["rowoff"][ridx][:, :, None]
+               + np.where(shifted[:, :, None], colh[:, None, :], cols[:, None, :]))
+        cx = np.where(x - fx >= sc(0.5), mid + 1, mid)
+        cy = np.where(p - nodes[:, mid] >= nodes[:, mid + 1] - p, mid + 1, mid)
+        kn = np.clip(np.floor(xk + sc(0.5)).astype(np.int64), 0, nlev - 1)
+        pts = np.arange(p.shape[0])
+        centre = kn * plane + adr[pts, cy, cx]
+        for fi, f in enumerate(flat):
+            base = f[centre]
+            acc = np.zeros(p.shape, dtype)
+            lo = np.full(p.shape, np.inf, dtype)
+            hi = np.full(p.shape, -np.inf, dtype)
+            f_edge = np.zeros(p.shape, dtype)
+            f_next = np.zeros(p.shape, dtype)
+            for c in range(4):
+                v = f[(k0 + c)[:, None, None] * plane + adr]
+                inner = np.einsum("pa,pra,pr->p", wx, v - base[:, None, None], wy)
+                acc = acc + wz[:, c] * inner
+                f_edge = np.where(c_edge == c, inner, f_edge)
+                f_next = np.where(c_next == c, inner, f_next)
+                if limiter != "none":
+                    inbox = (c == kbox) | (c == kbox + 1)
+                    box = v[:, mid:mid + 2, mid:mid + 2].reshape(-1, 4)
+                    lo = np.where(inbox, np.minimum(lo, box.min(axis=1)), lo)
+                    hi = np.where(inbox, np.maximum(hi, box.max(axis=1)), hi)
+            if limiter == "none":
+                face = f_edge + sc(0.5) * (f_edge - f_next)
+                held = np.minimum(np.maximum(acc, np.minimum(f_edge, face)),
+                                  np.maximum(f_edge, face))
+                acc = np.where(outside, held, acc)
+            acc = acc + base
+            kept = np.minimum(np.maximum(acc, lo), hi) if limiter != "none" else acc
+            outs[fi][k] = kept
+            if deficit:
+                cuts[fi][k] = acc - kept
+    shape = np.shape(xi)
+    values = [o.reshape(shape) for o in outs]
+    if not deficit:
+        return values
+    return list(zip(values, [c.reshape(shape) for c in cuts]))
+
+
+def gather_linear(fields, xi, phi, level, lat, nlon, *, dtype=np.float64):
+    """Trilinear value inside the limiter's cell (interpolate.py:672-725)."""
+    dtype = np.dtype(dtype)
+    sc = dtype.type
+    tab = build_tables(lat, nlon, 4)
+    lat_ext = tab["lat_ext"].astype(dtype)
+    nlev, nlat, _ = np.shape(xi)
+    plane = nlat * nlon
+    flat = [np.ascontiguousarray(f, dtype=dtype).reshape(-1) for f in fields]
+    outs = [np.empty((nlev, plane), dtype) for _ in fields]
+    half_pi = sc(np.pi / 2.0)
+    for k in range(nlev):
+        p = np.clip(np.asarray(phi[k], dtype).reshape(-1), -half_pi, half_pi)
+        xk = np.clip(np.asarray(level[k], dtype).reshape(-1), sc(0.0), sc(nlev - 1))
+        x = np.asarray(xi[k], dtype).reshape(-1)
+        fx = np.floor(x)
+        ax = x - fx
+        c0 = fx.astype(np.int64) % nlon
+        c1 = (c0 + 1) % nlon
+        h0 = (c0 + nlon // 2) % nlon
+        h1 = (c1 + nlon // 2) % nlon
+        m0 = np.clip(np.searchsorted(lat_ext.astype(np.float64), p.astype(np.float64),
+                                     side="right") - 1, 1, nlat + 1)
+        la, lb = lat_ext[m0], lat_ext[m0 + 1]
+        ay = np.clip((p - la) / (lb - la), sc(0.0), sc(1.0))
+        r0, r1 = tab["rowoff"][m0], tab["rowoff"][m0 + 1]
+        s0, s1 = tab["rowshift"][m0] > 0, tab["rowshift"][m0 + 1] > 0
+        i00 = r0 + np.where(s0, h0, c0)
+        i01 = r0 + np.where(s0, h1, c1)
+        i10 = r1 + np.where(s1, h0, c0)
+        i11 = r1 + np.where(s1, h1, c1)
+        kb = np.clip(np.floor(xk).astype(np.int64), 0, nlev - 2)
+        az = xk - kb.astype(dtype)
+        o0 = kb * plane
+        o1 = o0 + plane
+        bx, by, bz = 1 - ax, 1 - ay, 1 - az
+        for fi, f in enumerate(flat):
+            t0 = by * (bx * f[o0 + i00] + ax * f[o0 + i01]) + ay * (bx * f[o0 + i10] + ax * f[o0 + i11])
+            t1 = by * (bx * f[o1 + i00] + ax * f[o1 + i01]) + ay * (bx * f[o1 + i10] + ax * f[o1 + i11])
+            outs[fi][k] = bz * t0 + az * t1
+    return [o.reshape(np.shape(xi)) for o in outs]
+
+
+def departure_sample(nlev, lat, nlon, seed, *, cells=1.5, dtype=np.float64):
+    """Seeded departure coordinates: every arrival point displaced by up to
+    `cells` grid cells zonally and meridionally (the meridional offset in
+    radians of one equatorial cell, so rows next to a pole reach past it)
+    and up to one level vertically, reaching the half layers."""
+    rng = np.random.default_rng(seed)
+    lat = np.asarray(lat, dtype=np.float64)
+    nlat = lat.shape[0]
+    shape = (nlev, nlat, nlon)
+    dlat = math.pi / nlat
+    xi = np.arange(nlon)[None, None, :] + rng.uniform(-cells, cells, shape)
+    phi = lat[None, :, None] + rng.uniform(-cells, cells, shape) * dlat
+    level = np.arange(nlev)[:, None, None] + rng.uniform(-1.0, 1.0, shape)
+    return xi.astype(dtype), phi.astype(dtype), level.astype(dtype)

@@ -1,0 +1,162 @@
+"""The semi-Lagrangian gathers on the GPU (sht_sl_gather, sht_sl_gather_linear)
+against the reference's recorded outputs and against the oracle.
+
+Tolerances: float64 1e-12 of the field's range; float32 4e-6 of it (the
+kernel contracts a*b+c into FMAs where numpy rounds twice, and the
+meridional weights' normalisation is a reciprocal multiply against numpy's
+division)."""
+from __future__ import annotations
+
+import types
+
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+CASES = [("cubic_qm", 4, "quasi_monotone", False), ("cubic_qm_deficit", 4, "quasi_monotone", True),
+         ("cubic_none", 4, "none", False), ("quintic_qm", 6, "quasi_monotone", False),
+         ("quintic_none", 6, "none", False)]
+TOL = {"f64": 1e-12, "f32": 4e-6}
+DT = {"f64": torch.float64, "f32": torch.float32}
+
+
+def _grid(lat, nlon):
+    lat = np.asarray(lat, np.float64)
+    return types.SimpleNamespace(nlat=lat.shape[0], nlon=int(nlon), lat_rad=lat,
+                                 lon_rad=np.arange(nlon) * 2 * np.pi / nlon, radius_m=6371220.0)
+
+
+def _setup(g, tag):
+    from b200sht.semilag import SphericalGridTables, Stencil
+
+    tables = SphericalGridTables.create(_grid(g["lat"], g["nlon"]), dtype=DT[tag])
+    dev = lambda a: torch.as_tensor(a, device="cuda")
+    st = Stencil(xi=dev(g["xi"]), phi=dev(g["phi"]), level=dev(g["level"]), tables=tables)
+    fields = [dev(f) for f in g["fields"]]
+    return tables, st, fields
+
+
+def _close(got, want, tag, scale=None):
+    """max |got - want| within TOL of the range of `scale` (default: want)."""
+    got = got.cpu().numpy() if isinstance(got, torch.Tensor) else got
+    ref = want if scale is None else scale
+    rng = max(float(np.max(ref) - np.min(ref)), 1e-300)
+    err = float(np.max(np.abs(got - want))) / rng
+    assert err <= TOL[tag], err
+
+
+@pytest.mark.parametrize("tag", ["f64", "f32"])
+@pytest.mark.parametrize("order", [4, 6])
+def test_tables_match_reference(golden, tag, order):
+    g = golden(f"sl_gather_{tag}.npz")
+    tables, _, _ = _setup(g, tag)
+    t = tables.host_tables(order)
+    for key in ("lat_ext", "mrden", "rowoff", "rowshift", "mlut"):
+        np.testing.assert_array_equal(t[key], g[f"{key}{order}"].reshape(t[key].shape))
+
+
+@pytest.mark.parametrize("tag", ["f64", "f32"])
+@pytest.mark.parametrize("name,order,limiter,deficit", CASES)
+def test_gather_matches_reference(golden, tag, name, order, limiter, deficit):
+    from b200sht.semilag import gather_batch
+
+    g = golden(f"sl_gather_{tag}.npz")
+    _, st, fields = _setup(g, tag)
+    out = gather_batch(fields, st, monotone=limiter, deficit=deficit, order=order)
+    torch.cuda.synchronize()
+    for i, item in enumerate(out):
+        if deficit:
+            _close(item[0], g[name][i], tag)
+            # the deficit to the same absolute accuracy as the values
+            _close(item[1], g[name + "_cut"][i], tag, scale=g[name][i])
+        else:
+            _close(item, g[name][i], tag)
+
+
+@pytest.mark.parametrize("tag", ["f64", "f32"])
+def test_linear_matches_reference(golden, tag):
+    from b200sht.semilag import gather_linear_batch
+
+    g = golden(f"sl_gather_{tag}.npz")
+    _, st, fields = _setup(g, tag)
+    for i, v in enumerate(gather_linear_batch(fields, st)):
+        _close(v, g["linear"][i], tag)
+
+
+@pytest.mark.parametrize("tag", ["f64", "f32"])
+@pytest.mark.parametrize("order", [4, 6])
+@pytest.mark.parametrize("limiter", ["quasi_monotone", "none"])
+def test_larger_grid_against_oracle(tag, order, limiter):
+    """A 48 x 96 grid, 8 levels, 3 fields, departure points up to 3 cells
+    away (past both poles and into both half layers), against the oracle."""
+    from b200sht.semilag import SphericalGridTables, Stencil, gather_batch
+    from oracle import sl_gather as O
+
+    nlat, nlon, nlev = 48, 96, 8
+    lat = np.sort(np.arcsin(np.polynomial.legendre.leggauss(nlat)[0]))
+    dtype = np.float64 if tag == "f64" else np.float32
+    xi, phi, level = O.departure_sample(nlev, lat, nlon, 7, cells=3.0, dtype=dtype)
+    rng = np.random.default_rng(3)
+    fields = [rng.standard_normal((nlev, nlat, nlon)).astype(dtype) for _ in range(3)]
+    tables = SphericalGridTables.create(_grid(lat, nlon), dtype=DT[tag])
+    dev = lambda a: torch.as_tensor(a, device="cuda")
+    st = Stencil(xi=dev(xi), phi=dev(phi), level=dev(level), tables=tables)
+    got = gather_batch([dev(f) for f in fields], st, monotone=limiter, order=order, batch=2)
+    want = O.gather(fields, xi, phi, level, lat, nlon, order=order, limiter=limiter, dtype=dtype)
+    for a, b in zip(got, want):
+        _close(a, b, tag)
+
+
+@pytest.mark.parametrize("tag", ["f64", "f32"])
+@pytest.mark.parametrize("order", [4, 6])
+@pytest.mark.parametrize("limiter", ["quasi_monotone", "none"])
+def test_zero_displacement_is_the_identity(tag, order, limiter):
+    """Every weight set is normalised, so a point that departs from itself
+    reads its own value exactly, polar rows and boundary levels included."""
+    from b200sht.semilag import SphericalGridTables, gather, gather_linear_batch, zero_stencil
+
+    nlat, nlon, nlev = 16, 32, 6
+    lat = np.sort(np.arcsin(np.polynomial.legendre.leggauss(nlat)[0]))
+    tables = SphericalGridTables.create(_grid(lat, nlon), dtype=DT[tag])
+    st = zero_stencil(tables, nlev)
+    f = torch.randn((nlev, nlat, nlon), dtype=DT[tag], device="cuda")
+    assert torch.equal(gather(f, st, monotone=limiter, order=order), f)
+    assert torch.equal(gather_linear_batch([f], st)[0], f)
+
+
+def test_batches_and_single_fields_agree(golden):
+    from b200sht.semilag import gather, gather_batch
+
+    g = golden("sl_gather_f64.npz")
+    _, st, fields = _setup(g, "f64")
+    many = gather_batch(fields * 3, st, batch=4)
+    one = [gather(f, st) for f in fields * 3]
+    for a, b in zip(many, one):
+        assert torch.equal(a, b)
+
+
+def test_errors_name_the_reason(golden):
+    from b200sht.semilag import SphericalGridTables, Stencil, gather_batch
+
+    g = golden("sl_gather_f64.npz")
+    tables, st, fields = _setup(g, "f64")
+    with pytest.raises(ValueError, match="limiter must be one of"):
+        gather_batch(fields, st, monotone="positive_definite")
+    with pytest.raises(ValueError, match="horizontal order must be one of"):
+        gather_batch(fields, st, order=5)
+    with pytest.raises(ValueError, match="unlimited gather has none"):
+        gather_batch(fields, st, monotone=False, deficit=True)
+    with pytest.raises(ValueError, match="cubic gather only"):
+        gather_batch(fields, st, deficit=True, order=6)
+    with pytest.raises(ValueError, match="where the stencil reads"):
+        gather_batch([fields[0][:, :, :-2]], st)
+    with pytest.raises(ValueError, match="mixed-precision"):
+        gather_batch([fields[0].float()], st)
+    with pytest.raises(ValueError, match="nlev >= 4"):
+        Stencil(xi=st.xi[:3], phi=st.phi[:3], level=st.level[:3], tables=tables)
+    with pytest.raises(ValueError, match="nlon must be even"):
+        SphericalGridTables.create(_grid(g["lat"], 25))
+    with pytest.raises(ValueError, match="strictly ascending"):
+        SphericalGridTables.create(_grid(g["lat"][::-1], 24))
