@@ -133,10 +133,13 @@ __device__ __forceinline__ int bracket(T p, const T* __restrict__ lat_ext,
 }
 
 // Memory index (k, j, i) of the t-th point in (j, k, i) order.
+// (Below 2^31 points, which the host checks: 32-bit divisions.)
 __device__ __forceinline__ int64_t point_index(int64_t t, int nk, int nj, int ni) {
-  const int i = (int)(t % ni);
-  const int64_t r = t / ni;
-  const int k = (int)(r % nk), j = (int)(r / nk);
+  const unsigned u = (unsigned)t;
+  const unsigned r = u / (unsigned)ni;
+  const unsigned i = u - r * (unsigned)ni;
+  const unsigned j = r / (unsigned)nk;
+  const unsigned k = r - j * (unsigned)nk;
   return ((int64_t)k * nj + j) * ni + i;
 }
 
