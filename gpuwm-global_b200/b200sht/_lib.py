@@ -93,6 +93,8 @@ SIGNATURES = {
     "sht_sl_gather": (ctypes.c_int, [_P, ctypes.c_int, ctypes.c_int, ctypes.c_int, _P, _I64,
                                      ctypes.c_int, _P, _P, _P, _P, _P, _P]),
     "sht_sl_gather_linear": (ctypes.c_int, [_P, _P, _I64, ctypes.c_int, _P, _P, _P, _P, _P]),
+    "sht_sl_departure": (ctypes.c_int, [_P, ctypes.c_int, _P, _P, _P, _P, _P, _P, _P, _P,
+                                        ctypes.c_int, _D, _D, _P, _P, _P, _P, _P, _P]),
 }
 
 _lib = None

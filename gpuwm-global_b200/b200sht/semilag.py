@@ -1,11 +1,14 @@
 """Semi-Lagrangian interpolation at departure points, on the GPU.
 
-Mirrors the reference's ``arwen_global.semilag.tables.SphericalGridTables``
-and ``arwen_global.semilag.interpolate`` (``Stencil``, ``zero_stencil``,
+Mirrors the reference's ``arwen_global.semilag.tables.SphericalGridTables``,
+``arwen_global.semilag.interpolate`` (``Stencil``, ``zero_stencil``,
 ``gather_batch``, ``gather``, ``gather_linear_batch``; semilag/tables.py:98-258,
-semilag/interpolate.py:87-500) with the same argument meaning and the same
-``ValueError`` wording; the interpolation runs in ``libb200sht.so``
-(``sht_sl_gather``, ``sht_sl_gather_linear``).  Arrays are CUDA tensors:
+semilag/interpolate.py:87-500) and the fixed-point departure search of
+``arwen_global.semilag.trajectory`` (``CartesianWind``, ``cartesian_wind``,
+``local_wind``, ``departure_points``, ``TrajectoryDiagnostics``) with the same
+argument meaning and the same ``ValueError`` wording; the interpolation and
+the search run in ``libb200sht.so`` (``sht_sl_gather``,
+``sht_sl_gather_linear``, ``sht_sl_departure``).  Arrays are CUDA tensors:
 fields and departure coordinates ``(nlev, nlat, nlon)`` in the tables'
 dtype (float32 or float64).  The whole-grid form only: a latitude-band
 window (the reference's ``BandWindow``) is not part of this engine, whose
@@ -286,3 +289,162 @@ def gather_linear_batch(fields: Sequence[torch.Tensor], stencil: Stencil, *,
                   _stream())
         out.extend(dst[i] for i in range(count))
     return out
+
+
+# --------------------------------------------------------------- trajectory
+# The reference's semilag/trajectory.py: CartesianWind, cartesian_wind,
+# local_wind, TrajectoryDiagnostics, meridional_grid_length_m and
+# departure_points (trajectory.py:50-120, 158-358, 440-490).
+
+#: Solvers of the departure-point equation.  Only the fixed-point pass (the
+#: reference's default and its numpy specification) is built here.
+TRAJECTORY_SOLVERS = ("fixed_point", "newton", "newton_ls")
+
+
+@dataclass(frozen=True)
+class CartesianWind:
+    """Geocentric Cartesian components of the horizontal wind (m/s) and the
+    vertical velocity in level indices per second, at full levels."""
+
+    vx: Any
+    vy: Any
+    vz: Any
+    level_rate: Any
+
+    @property
+    def shape(self) -> tuple[int, int, int]:
+        return tuple(int(s) for s in self.vx.shape)  # type: ignore[return-value]
+
+    def arrays(self) -> tuple:
+        return (self.vx, self.vy, self.vz, self.level_rate)
+
+
+def _trig(tables: SphericalGridTables):
+    nlat, nlon = tables.shape
+    host = tables.host_tables(4)
+    dev, dt = tables.device, tables.dtype
+    lat = torch.as_tensor(host["lat_ext"][2:nlat + 2], dtype=dt, device=dev)
+    lon = torch.as_tensor(np.arange(nlon) * tables.dlam, dtype=dt, device=dev)
+    return (torch.sin(lat)[None, :, None], torch.cos(lat)[None, :, None],
+            torch.sin(lon)[None, None, :], torch.cos(lon)[None, None, :])
+
+
+def cartesian_wind(u, v, tables: SphericalGridTables):
+    """Local east-north wind as geocentric Cartesian components."""
+    sph, cph, sla, cla = _trig(tables)
+    vx = -u * sla - v * sph * cla
+    vy = u * cla - v * sph * sla
+    vz = v * cph + torch.zeros_like(u)
+    return vx, vy, vz
+
+
+def local_wind(vx, vy, vz, tables: SphericalGridTables):
+    """Geocentric Cartesian components back to the local east-north wind."""
+    sph, cph, sla, cla = _trig(tables)
+    u = -vx * sla + vy * cla
+    v = -vx * sph * cla - vy * sph * sla + vz * cph
+    return u, v
+
+
+@dataclass(frozen=True)
+class TrajectoryDiagnostics:
+    iterations: int
+    dt_s: float
+    #: largest last-iteration move, metres, and in meridional grid lengths
+    move_max_m: float
+    move_max_cells: float
+    #: largest last-iteration move of the level coordinate
+    move_max_levels: float
+    #: largest displacement of the finished trajectory
+    displacement_max_m: float
+    displacement_max_cells: float
+    displacement_max_levels: float
+
+    def as_dict(self) -> dict:
+        return {
+            "semilag_trajectory_iterations": self.iterations,
+            "semilag_trajectory_dt_s": self.dt_s,
+            "semilag_trajectory_move_max_m": self.move_max_m,
+            "semilag_trajectory_move_max_cells": self.move_max_cells,
+            "semilag_trajectory_move_max_levels": self.move_max_levels,
+            "semilag_displacement_max_m": self.displacement_max_m,
+            "semilag_displacement_max_cells": self.displacement_max_cells,
+            "semilag_displacement_max_levels": self.displacement_max_levels,
+        }
+
+
+def meridional_grid_length_m(tables: SphericalGridTables) -> np.ndarray:
+    """``a * dphi`` per latitude row (half the spread of the neighbouring
+    rows, the pole rows through their reflections)."""
+    lat_ext = tables.host_tables(4)["lat_ext"]
+    nlat = tables.nlat
+    return tables.radius_m * 0.5 * (lat_ext[3:nlat + 3] - lat_ext[1:nlat + 1])
+
+
+def _diagnostics(stencil: Stencil, move_m, move_k, tables, dt_s, iterations):
+    nlev, nlat, nlon = stencil.shape
+    dt = tables.dtype
+    dev = tables.device
+    cell = torch.as_tensor(meridional_grid_length_m(tables), dtype=dt, device=dev)[None, :, None]
+    lat = torch.as_tensor(tables.host_tables(4)["lat_ext"][2:nlat + 2], dtype=dt,
+                          device=dev)[None, :, None]
+    index = torch.arange(nlon, dtype=dt, device=dev)[None, None, :]
+    lev0 = torch.arange(nlev, dtype=dt, device=dev)[:, None, None]
+    # great-circle distance through the haversine (no floor from arccos)
+    dphi = 0.5 * (stencil.phi - lat)
+    dlon = 0.5 * (stencil.xi - index) * tables.dlam
+    hav = torch.sin(dphi) ** 2 + torch.cos(lat) * torch.cos(stencil.phi) * torch.sin(dlon) ** 2
+    dist = (2.0 * tables.radius_m) * torch.arcsin(torch.sqrt(torch.clamp(hav, 0.0, 1.0)))
+    maxima = torch.stack([move_m.max(), (move_m / cell).max(), move_k.max(), dist.max(),
+                          (dist / cell).max(), (stencil.level - lev0).abs().max()]).tolist()
+    return TrajectoryDiagnostics(int(iterations), float(dt_s), *[float(x) for x in maxima])
+
+
+def search_into(tables: SphericalGridTables, fields: Sequence[torch.Tensor], iterations: int,
+                dt_s: float, outs: Sequence[torch.Tensor]) -> None:
+    """The search kernel alone: ``fields`` = (vx, vy, vz, level_rate) of the
+    advecting wind then of the extrapolated one, contiguous; ``outs`` = xi,
+    phi, level, move_m, move_k.  No checks beyond the library's."""
+    nlev = int(fields[0].shape[0])
+    _lib.call("sht_sl_departure", tables._handle, nlev, *[_ptr(t) for t in fields],
+              int(iterations), float(dt_s), float(tables.radius_m), *[_ptr(t) for t in outs],
+              _stream())
+
+
+def departure_points(wind: CartesianWind, tables: SphericalGridTables, dt_s: float, *,
+                     iterations: int = 3, extrapolated: CartesianWind | None = None,
+                     solver: str = "fixed_point") -> tuple[Stencil, TrajectoryDiagnostics]:
+    """The departure point of every arrival point of the grid (the
+    fixed-point search, all iterations in one launch)."""
+    shape = wind.shape
+    nlev, nrows, nlon = shape
+    if (nrows, nlon) != tables.shape:
+        raise ValueError(f"the wind is {(nrows, nlon)} where {tables.shape} rows were expected "
+                         f"on a {tables.shape} grid")
+    if nlev < 4:
+        raise ValueError(f"nlev >= 4 is required, got {nlev}")
+    if int(iterations) < 1:
+        raise ValueError(
+            "the departure-point search needs at least one iteration; zero would ship the "
+            "explicit first guess, which is first order in dt and is not a trajectory")
+    if solver not in TRAJECTORY_SOLVERS:
+        raise ValueError(f"trajectory solver must be one of {TRAJECTORY_SOLVERS}, got {solver!r}")
+    if solver != "fixed_point":
+        raise ValueError(f"trajectory solver {solver!r} is not built in this engine; the "
+                         "fixed-point pass is")
+    ex = wind if extrapolated is None else extrapolated
+    for name, arr in (("wind", wind), ("extrapolated", ex)):
+        for field in arr.arrays():
+            if tuple(int(s) for s in field.shape) != shape:
+                raise ValueError(f"{name} fields must all be {shape}")
+            if field.dtype != tables.dtype:
+                raise ValueError(f"{name} is {field.dtype} where the grid tables were built for "
+                                 f"{tables.dtype}")
+            if not field.is_cuda:
+                raise ValueError(f"{name} fields must be CUDA tensors")
+    ins = [f.contiguous() for f in wind.arrays()] + [f.contiguous() for f in ex.arrays()]
+    outs = [torch.empty(shape, dtype=tables.dtype, device=ins[0].device) for _ in range(5)]
+    search_into(tables, ins, int(iterations), float(dt_s), outs)
+    xi, phi, lev, move_m, move_k = outs
+    stencil = Stencil(xi=xi, phi=phi, level=lev, tables=tables)
+    return stencil, _diagnostics(stencil, move_m, move_k, tables, dt_s, iterations)

@@ -211,7 +211,8 @@ def sl_gather(args, clock_sampler):
     limited species, headline), cubic unlimited, quintic unlimited (the
     dynamical bundle) and the trilinear value."""
     from .grid import GaussianGrid
-    from .semilag import SphericalGridTables, Stencil, gather_batch, gather_linear_batch
+    from .semilag import (SphericalGridTables, Stencil, gather_batch, gather_linear_batch,
+                          search_into)
 
     nlev, nfield = getattr(args, "sl_levels", 40), getattr(args, "sl_fields", 16)
     grid = GaussianGrid.create(511, nlat=768, nlon=1536)
@@ -256,11 +257,26 @@ def sl_gather(args, clock_sampler):
                          "algorithmic_gb_per_s": byts / (ms * 1e-3) / 1e9}
         ms = _time(lambda: gather_linear_batch(fields, st, batch=nfield), args.steps, args.warmup)
         out["trilinear"] = {"ms": ms, "point_fields_per_s": npts * nfield / (ms * 1e-3)}
+        # the fixed-point departure search, 3 iterations, on the rotation's
+        # wind as Cartesian components (80 m/s) and a +-1.5e-3 levels/s rate
+        lat = torch.as_tensor(grid.lat_rad, dtype=torch.float64, device=dev)[None, :, None]
+        lon = torch.as_tensor(grid.lon_rad, dtype=torch.float64, device=dev)[None, None, :]
+        shape = (nlev, grid.nlat, grid.nlon)
+        vz_ = (80.0 * torch.cos(lat) * torch.sin(lon)).expand(shape)
+        vy_ = (-80.0 * torch.sin(lat)).expand(shape)
+        wind = [torch.zeros(shape, dtype=torch.float32, device=dev), vy_.float().contiguous(),
+                vz_.float().contiguous(),
+                (1.5e-3 * torch.sin(2 * lon) * torch.cos(lat)).expand(shape).float().contiguous()]
+        dep = [torch.empty(shape, dtype=torch.float32, device=dev) for _ in range(5)]
+        ms = _time(lambda: search_into(tables, wind + wind, 3, 300.0, dep), args.steps,
+                   args.warmup)
+        out["departure_search_3_iterations"] = {"ms": ms, "points_per_s": npts / (ms * 1e-3)}
+        del wind, dep
     head = out["cubic_quasi_monotone"]
     out["clocks"] = clocks.summary()
     out["value"] = head["point_fields_per_s"]
     out["ms_per_step"] = head["ms"]
-    out["gpu_launches"] = (len(cases) + 1) * args.steps
+    out["gpu_launches"] = (len(cases) + 2) * args.steps
     out["roofline"] = {"bound": "hbm", "achieved": head["algorithmic_gb_per_s"], "peak": peak,
                        "unit": "GB/s", "frac": head["algorithmic_gb_per_s"] / peak,
                        "traffic": None, "kernel": "sl_gather_kernel<float, 4, qm>",

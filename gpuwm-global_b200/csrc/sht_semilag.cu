@@ -362,6 +362,127 @@ __global__ void __launch_bounds__(256) sl_linear_kernel(const SlArgs<T> a) {
   }
 }
 
+// ------------------------------------------------------ departure search
+// The fixed-point departure-point search of the reference
+// (semilag/trajectory.py:553-618, kernels.cu sl_departure_*), all
+// iterations in one launch: with a the arrival point's unit vector, V the
+// Cartesian wind (m/s) and s the level rate (levels/s) at full levels,
+//   first guess  q = normalize(a - dt V(a) / r),  k_q = k - dt s(a);
+//   iteration    q' = normalize(a - dt/2 (V_ex(a) + V(q)) / r),
+//                k_q' = k - dt/2 (s_ex(a) + s(q, k_q)),
+// V(q), s(q) read trilinearly in the cubic gather's cell, levels clamped to
+// the boundary interfaces [-1/2, nlev - 1/2].  Outputs the departure
+// coordinates (continuous zonal index, latitude, level) and the last
+// iteration's move (metres along the great circle, levels).
+template <typename T>
+struct SlDepArgs {
+  const T *vx, *vy, *vz, *sv;      // advecting wind [nk][nj][ni]
+  const T *vxe, *vye, *vze, *sve;  // extrapolated wind at the arrival points
+  const T* lat_ext;
+  const int32_t *mlut, *rowoff, *rowshift;
+  T *xi, *phi, *lev, *move_m, *move_k;
+  int iters, nk, nj, ni, nb;
+  double dlam;  // 2 pi / nlon (the arrival longitudes are formed in double)
+  T dt, radius, inv_dlam, lut_scale;
+};
+
+template <typename T>
+__device__ __forceinline__ void trilinear4(const SlDepArgs<T>& a, T lam, T phid, T xkd,
+                                           T (&w)[4]) {
+  const T p = min(max(phid, T(-kHalfPi)), T(kHalfPi));
+  const T xk = min(max(xkd, T(0)), T(a.nk - 1));
+  const T x = lam * a.inv_dlam;
+  const T fi = floor(x);
+  const T ax = x - fi;
+  int c0 = ((int)fi) % a.ni;
+  if (c0 < 0) c0 += a.ni;
+  const int c1 = c0 + 1 == a.ni ? 0 : c0 + 1;
+  const int half = a.ni >> 1;
+  const int h0 = c0 >= a.ni - half ? c0 + half - a.ni : c0 + half;
+  const int h1 = c1 >= a.ni - half ? c1 + half - a.ni : c1 + half;
+  const int m0 = bracket<T>(p, a.lat_ext, a.mlut, a.nb, a.nj, 1, a.lut_scale);
+  const T la = __ldg(a.lat_ext + m0), lb = __ldg(a.lat_ext + m0 + 1);
+  const T ay = (p - la) / (lb - la);
+  const int r0 = __ldg(a.rowoff + m0), r1 = __ldg(a.rowoff + m0 + 1);
+  const bool s0 = __ldg(a.rowshift + m0) != 0, s1 = __ldg(a.rowshift + m0 + 1) != 0;
+  const int i00 = r0 + (s0 ? h0 : c0), i01 = r0 + (s0 ? h1 : c1);
+  const int i10 = r1 + (s1 ? h0 : c0), i11 = r1 + (s1 ? h1 : c1);
+  const int k0 = min(max((int)floor(xk), 0), a.nk - 2);
+  const T az = xk - T(k0);
+  const int64_t plane = (int64_t)a.nj * a.ni;
+  const int64_t o0 = (int64_t)k0 * plane, o1 = o0 + plane;
+  const T bx = T(1) - ax, by = T(1) - ay, bz = T(1) - az;
+  const T* f[4] = {a.vx, a.vy, a.vz, a.sv};
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const T* s0p = f[q] + o0;
+    const T* s1p = f[q] + o1;
+    const T t0 = by * (bx * __ldg(s0p + i00) + ax * __ldg(s0p + i01)) +
+                 ay * (bx * __ldg(s0p + i10) + ax * __ldg(s0p + i11));
+    const T t1 = by * (bx * __ldg(s1p + i00) + ax * __ldg(s1p + i01)) +
+                 ay * (bx * __ldg(s1p + i10) + ax * __ldg(s1p + i11));
+    w[q] = bz * t0 + az * t1;
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) sl_departure_kernel(const SlDepArgs<T> a) {
+  const int64_t n = (int64_t)a.nk * a.nj * a.ni;
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const int64_t gid = point_index(t, a.nk, a.nj, a.ni);  // rows with their levels together
+  const int plane = a.nj * a.ni;
+  const int k = (int)(gid / plane);
+  const int rem = (int)(gid - (int64_t)k * plane);
+  const int j = rem / a.ni, i = rem - j * a.ni;
+  // the arrival point: table latitude and i * dlam (formed in double, as
+  // the host computes the grid's longitudes), both in T
+  const T lat = __ldg(a.lat_ext + j + 2);
+  const T lon = T((double)i * a.dlam);
+  const T sph = sin(lat), cph = cos(lat), sla = sin(lon), cla = cos(lon);
+  const T ax = cph * cla, ay = cph * sla, az = sph;
+  const T inv_r = T(1) / a.radius;
+  const T dt = a.dt, hdt = T(0.5) * a.dt;
+  T qx = ax - dt * a.vx[gid] * inv_r;
+  T qy = ay - dt * a.vy[gid] * inv_r;
+  T qz = az - dt * a.vz[gid] * inv_r;
+  T nrm = sqrt(qx * qx + qy * qy + qz * qz);
+  qx /= nrm;
+  qy /= nrm;
+  qz /= nrm;
+  const T klo = T(-0.5), khi = T(a.nk) - T(0.5);
+  T qk = min(max(T(k) - dt * a.sv[gid], klo), khi);
+  const T ex = a.vxe[gid], ey = a.vye[gid], ez = a.vze[gid], es = a.sve[gid];
+  T last_m = T(0), last_k = T(0);
+  for (int it = 0; it < a.iters; ++it) {
+    const T lam = atan2(qy, qx);
+    const T phid = atan2(qz, sqrt(qx * qx + qy * qy));
+    T w[4];
+    trilinear4<T>(a, lam, phid, qk, w);
+    T px = ax - hdt * (ex + w[0]) * inv_r;
+    T py = ay - hdt * (ey + w[1]) * inv_r;
+    T pz = az - hdt * (ez + w[2]) * inv_r;
+    nrm = sqrt(px * px + py * py + pz * pz);
+    px /= nrm;
+    py /= nrm;
+    pz /= nrm;
+    const T pk = min(max(T(k) - hdt * (es + w[3]), klo), khi);
+    const T cx = px - qx, cy = py - qy, cz = pz - qz;
+    const T chord = sqrt(cx * cx + cy * cy + cz * cz);
+    last_m = a.radius * T(2) * asin(min(max(T(0.5) * chord, T(0)), T(1)));
+    last_k = fabs(pk - qk);
+    qx = px;
+    qy = py;
+    qz = pz;
+    qk = pk;
+  }
+  a.xi[gid] = atan2(qy, qx) * a.inv_dlam;
+  a.phi[gid] = atan2(qz, sqrt(qx * qx + qy * qy));
+  a.lev[gid] = qk;
+  a.move_m[gid] = last_m;
+  a.move_k[gid] = last_k;
+}
+
 // ----------------------------------------------------------- tables
 // The pole-extended table of one stencil width (semilag/tables.py:51-95,
 // 164-217): G reflected rows each side, the data row and zonal shift each
@@ -629,6 +750,53 @@ int sht_sl_gather_linear(const sht_sl_tables* tables, const void* src, int64_t f
     } else {
       auto a = make_args<float>(tables, w, src, fields, nlev, xi, phi, level, out, nullptr);
       sl_linear_kernel<float><<<blocks, 256, 0, s>>>(a);
+    }
+    SHT_CUDA_OR_THROW(cudaGetLastError());
+  });
+}
+
+int sht_sl_departure(const sht_sl_tables* tables, int nlev, const void* vx, const void* vy,
+                     const void* vz, const void* level_rate, const void* vx_ex,
+                     const void* vy_ex, const void* vz_ex, const void* level_rate_ex,
+                     int iterations, double dt, double radius, void* xi, void* phi,
+                     void* level, void* move_m, void* move_k, void* stream) {
+  return guarded([&] {
+    check_call(tables, vx, 1, nlev, vy, vz, level_rate, xi);
+    SHT_REQUIRE(vx_ex && vy_ex && vz_ex && level_rate_ex && phi && level && move_m && move_k,
+                "null array pointer");
+    SHT_REQUIRE(iterations >= 1,
+                "the departure-point search needs at least one iteration; zero would ship the "
+                "explicit first guess, which is first order in dt and is not a trajectory");
+    SHT_REQUIRE(std::isfinite(dt) && std::isfinite(radius) && radius > 0.0,
+                "dt and radius must be finite, radius positive");
+    const SlWidth& w = tables->w4;
+    const int64_t n = (int64_t)nlev * tables->nlat * tables->nlon;
+    const unsigned blocks = (unsigned)div_up(n, 256);
+    cudaStream_t s = (cudaStream_t)stream;
+    auto fill = [&](auto* a) {
+      using T = std::remove_cv_t<std::remove_pointer_t<decltype(a->vx)>>;
+      a->vx = (const T*)vx; a->vy = (const T*)vy; a->vz = (const T*)vz;
+      a->sv = (const T*)level_rate;
+      a->vxe = (const T*)vx_ex; a->vye = (const T*)vy_ex; a->vze = (const T*)vz_ex;
+      a->sve = (const T*)level_rate_ex;
+      a->lat_ext = (const T*)w.d_lat_ext;
+      a->mlut = w.d_mlut; a->rowoff = w.d_rowoff; a->rowshift = w.d_rowshift;
+      a->xi = (T*)xi; a->phi = (T*)phi; a->lev = (T*)level;
+      a->move_m = (T*)move_m; a->move_k = (T*)move_k;
+      a->iters = iterations; a->nk = nlev; a->nj = tables->nlat; a->ni = tables->nlon;
+      a->nb = w.bins;
+      const double dlam = 2.0 * kPi / tables->nlon;
+      a->dt = (T)dt; a->radius = (T)radius; a->dlam = dlam; a->inv_dlam = (T)(1.0 / dlam);
+      a->lut_scale = (T)w.lut_scale;
+    };
+    if (tables->prec == SHT_PREC_F64) {
+      SlDepArgs<double> a;
+      fill(&a);
+      sl_departure_kernel<double><<<blocks, 256, 0, s>>>(a);
+    } else {
+      SlDepArgs<float> a;
+      fill(&a);
+      sl_departure_kernel<float><<<blocks, 256, 0, s>>>(a);
     }
     SHT_CUDA_OR_THROW(cudaGetLastError());
   });

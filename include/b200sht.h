@@ -326,6 +326,20 @@ int sht_sl_gather(const sht_sl_tables* tables, int order, int limiter, int defic
 int sht_sl_gather_linear(const sht_sl_tables* tables, const void* src, int64_t fields, int nlev,
                          const void* xi, const void* phi, const void* level, void* out,
                          void* stream);
+/* The fixed-point departure-point search (the reference's
+ * semilag/trajectory.py departure_points with solver "fixed_point", kernels.cu
+ * sl_departure_*): vx, vy, vz (geocentric Cartesian wind, m/s) and
+ * level_rate (levels/s) at full levels, [nlev][nlat][nlon]; the *_ex fields
+ * (the extrapolated flow) are read at the arrival points only.  All
+ * `iterations` (>= 1) in one launch; writes the departure coordinates xi
+ * (continuous zonal index), phi (radians), level (continuous level index,
+ * clamped to [-1/2, nlev - 1/2]) and the last iteration's move in metres
+ * and in levels.  radius: the sphere's radius in metres. */
+int sht_sl_departure(const sht_sl_tables* tables, int nlev, const void* vx, const void* vy,
+                     const void* vz, const void* level_rate, const void* vx_ex,
+                     const void* vy_ex, const void* vz_ex, const void* level_rate_ex,
+                     int iterations, double dt, double radius, void* xi, void* phi,
+                     void* level, void* move_m, void* move_k, void* stream);
 
 #ifdef __cplusplus
 }

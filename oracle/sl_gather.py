@@ -11,10 +11,13 @@ it.  A numpy restatement, in float64 or the tables' float32, of:
   (``semilag/interpolate.py:536-669``, the numpy specification the
   reference grades its kernel against);
 * the trilinear gather inside the limiter's cell
-  (``semilag/interpolate.py:672-725``).
+  (``semilag/interpolate.py:672-725``);
+* the fixed-point departure-point search and its trilinear wind read
+  (``semilag/trajectory.py:493-618``).
 
 Pinned against ``tests/golden/sl_gather_*.npz``, outputs of the reference's
-own ``gather_batch`` / ``gather_linear_batch`` (numpy backend) recorded by
+own ``gather_batch`` / ``gather_linear_batch`` / ``departure_points`` (numpy
+backend) recorded by
 ``tests/golden/make_golden_sl.py``.
 """
 from __future__ import annotations
@@ -218,3 +221,115 @@ def departure_sample(nlev, lat, nlon, seed, *, cells=1.5, dtype=np.float64):
     phi = lat[None, :, None] + rng.uniform(-cells, cells, shape) * dlat
     level = np.arange(nlev)[:, None, None] + rng.uniform(-1.0, 1.0, shape)
     return xi.astype(dtype), phi.astype(dtype), level.astype(dtype)
+
+
+def _trilinear_at(fields, lam, phi, lev, tab, nlat, nlon, dtype):
+    """The search's trilinear read at (longitude, latitude, level)
+    (trajectory.py:493-550): the cubic gather's cell, no clamp on the
+    meridional fraction, the level held in [0, nlev - 1]."""
+    sc = dtype.type
+    nlev = fields[0].shape[0]
+    lat_ext = tab["lat_ext"].astype(dtype)
+    half_pi = sc(np.pi / 2.0)
+    p = np.clip(phi, -half_pi, half_pi)
+    xk = np.clip(lev, sc(0.0), sc(nlev - 1))
+    x = lam * sc(1.0 / (2.0 * math.pi / nlon))
+    fx = np.floor(x)
+    ax = (x - fx).astype(dtype)
+    c0 = fx.astype(np.int64) % nlon
+    c1 = (c0 + 1) % nlon
+    h0, h1 = (c0 + nlon // 2) % nlon, (c1 + nlon // 2) % nlon
+    m0 = np.clip(np.searchsorted(lat_ext.astype(np.float64), p.astype(np.float64),
+                                 side="right") - 1, 1, nlat + 1)
+    la, lb = lat_ext[m0], lat_ext[m0 + 1]
+    ay = ((p - la) / (lb - la)).astype(dtype)
+    r0, r1 = tab["rowoff"][m0], tab["rowoff"][m0 + 1]
+    s0, s1 = tab["rowshift"][m0] > 0, tab["rowshift"][m0 + 1] > 0
+    i00, i01 = r0 + np.where(s0, h0, c0), r0 + np.where(s0, h1, c1)
+    i10, i11 = r1 + np.where(s1, h0, c0), r1 + np.where(s1, h1, c1)
+    k0 = np.clip(np.floor(xk).astype(np.int64), 0, nlev - 2)
+    az = (xk - k0).astype(dtype)
+    plane = nlat * nlon
+    bx, by, bz = 1.0 - ax, 1.0 - ay, 1.0 - az
+    out = []
+    for f in fields:
+        flat = np.ascontiguousarray(f).reshape(-1)
+        b0 = k0 * plane
+        b1 = b0 + plane
+        t0 = by * (bx * flat[b0 + i00] + ax * flat[b0 + i01]) + ay * (bx * flat[b0 + i10] + ax * flat[b0 + i11])
+        t1 = by * (bx * flat[b1 + i00] + ax * flat[b1 + i01]) + ay * (bx * flat[b1 + i10] + ax * flat[b1 + i11])
+        out.append((bz * t0 + az * t1).astype(dtype))
+    return out
+
+
+def departure(wind, lat, nlon, dt, *, iterations=3, extrapolated=None, radius=6371220.0,
+              dtype=np.float64):
+    """The fixed-point departure-point search (trajectory.py:553-618):
+    wind = (vx, vy, vz, level_rate), each (nlev, nlat, nlon).  Returns
+    xi, phi, level, move_m, move_k."""
+    dtype = np.dtype(dtype)
+    sc = dtype.type
+    tab = build_tables(lat, nlon, 4)
+    vx, vy, vz, sv = [np.asarray(w, dtype) for w in wind]
+    ex = [np.asarray(w, dtype) for w in (extrapolated or wind)]
+    nlev, nlat, _ = vx.shape
+    shape = vx.shape
+    latd = tab["lat_ext"][2:nlat + 2].astype(dtype)
+    lon = (np.arange(nlon) * (2.0 * math.pi / nlon)).astype(dtype)
+    sph, cph = np.sin(latd)[None, :, None], np.cos(latd)[None, :, None]
+    sla, cla = np.sin(lon)[None, None, :], np.cos(lon)[None, None, :]
+    ax = np.broadcast_to(cph * cla, shape).astype(dtype)
+    ay = np.broadcast_to(cph * sla, shape).astype(dtype)
+    az = np.broadcast_to(sph + 0.0 * cla, shape).astype(dtype)
+    ak = np.broadcast_to(np.arange(nlev, dtype=dtype)[:, None, None], shape).astype(dtype)
+    r = sc(radius)
+    inv_r = sc(1.0) / r
+    dts = sc(dt)
+    hdt = sc(0.5) * dts
+    qx, qy, qz = ax - dts * vx * inv_r, ay - dts * vy * inv_r, az - dts * vz * inv_r
+    nrm = np.sqrt(qx * qx + qy * qy + qz * qz)
+    qx, qy, qz = qx / nrm, qy / nrm, qz / nrm
+    klo, khi = sc(-0.5), sc(nlev - 0.5)
+    qk = np.clip(ak - dts * sv, klo, khi)
+    move_m = np.zeros(shape, dtype)
+    move_k = np.zeros(shape, dtype)
+    for _ in range(iterations):
+        lam = np.arctan2(qy, qx)
+        phi = np.arctan2(qz, np.sqrt(qx * qx + qy * qy))
+        w = _trilinear_at([vx, vy, vz, sv], lam, phi, qk, tab, nlat, nlon, dtype)
+        px = ax - hdt * (ex[0] + w[0]) * inv_r
+        py = ay - hdt * (ex[1] + w[1]) * inv_r
+        pz = az - hdt * (ex[2] + w[2]) * inv_r
+        nrm = np.sqrt(px * px + py * py + pz * pz)
+        px, py, pz = px / nrm, py / nrm, pz / nrm
+        pk = np.clip(ak - hdt * (ex[3] + w[3]), klo, khi)
+        chord = np.sqrt((px - qx) ** 2 + (py - qy) ** 2 + (pz - qz) ** 2)
+        move_m = r * 2.0 * np.arcsin(np.clip(0.5 * chord, sc(0.0), sc(1.0)))
+        move_k = np.abs(pk - qk)
+        qx, qy, qz, qk = px, py, pz, pk
+    xi = (np.arctan2(qy, qx) * sc(1.0 / (2.0 * math.pi / nlon))).astype(dtype)
+    phi = np.arctan2(qz, np.sqrt(qx * qx + qy * qy)).astype(dtype)
+    return xi, phi, qk.astype(dtype), move_m.astype(dtype), move_k.astype(dtype)
+
+
+def rotation_wind(lat, nlon, nlev, *, speed=40.0, seed=0, dtype=np.float64):
+    """Seeded advecting flow: a solid-body rotation about the axis through
+    (0 N, 0 E) (its flow crosses both poles) as Cartesian components, plus
+    a little noise, and a level rate reaching the half layers in one 300 s
+    step."""
+    rng = np.random.default_rng(seed)
+    lat = np.asarray(lat, np.float64)
+    nlat = lat.shape[0]
+    lon = np.arange(nlon) * 2 * math.pi / nlon
+    x = np.cos(lat)[:, None] * np.cos(lon)[None, :]
+    y = np.cos(lat)[:, None] * np.sin(lon)[None, :]
+    z = np.sin(lat)[:, None] * np.ones(nlon)[None, :]
+    om = speed / 6371220.0
+    # V = omega x r with omega along the x axis: (0, -om z, om y) * radius
+    shape = (nlev, nlat, nlon)
+    scale = 1.0 + 0.1 * np.arange(nlev)[:, None, None] / nlev
+    vx = np.zeros(shape) + 0.5 * rng.standard_normal(shape)
+    vy = -om * z[None] * 6371220.0 * scale + 0.5 * rng.standard_normal(shape)
+    vz = om * y[None] * 6371220.0 * scale + 0.5 * rng.standard_normal(shape)
+    sv = 1.5e-3 * np.sin(2 * lon)[None, None, :] * np.cos(lat)[None, :, None] * np.ones(shape)
+    return [a.astype(dtype) for a in (vx, vy, vz, sv)]

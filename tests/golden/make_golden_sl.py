@@ -12,7 +12,9 @@ specification the reference grades its CUDA gather against -- on seeded
 departure points of a small Gaussian grid, and writes
 ``tests/golden/sl_gather_f64.npz`` and ``sl_gather_f32.npz``: the inputs,
 every table of both stencil widths and the outputs of each (order, limiter,
-deficit) case.  The departure points reach past both poles (rows next to a
+deficit) case; and ``trajectory.departure_points`` (fixed point, three
+iterations) on a solid-body rotation across both poles, with its
+diagnostics.  The departure points reach past both poles (rows next to a
 pole displaced by up to 1.5 rows) and into the half layers above the top
 and below the bottom full level.
 """
@@ -28,6 +30,7 @@ HERE = Path(__file__).resolve().parent
 sys.path.insert(0, str(HERE.parents[1]))
 
 NLAT, NLON, NLEV, SEED = 12, 24, 5, 20261203
+DT = 1800.0  # s: the rotation moves about 0.6 cells per step on this grid
 
 #: (name, order, limiter, deficit)
 CASES = [
@@ -44,9 +47,10 @@ def main(ref_root: str) -> None:
     sys.path.insert(0, str(Path(ref_root) / "src"))
     from arwen_global.semilag.interpolate import Stencil, gather_batch, gather_linear_batch
     from arwen_global.semilag.tables import SphericalGridTables
+    from arwen_global.semilag.trajectory import CartesianWind, departure_points
     from arwen_global.spectral.grid import GaussianGrid
 
-    from oracle.sl_gather import departure_sample
+    from oracle.sl_gather import departure_sample, rotation_wind
 
     grid = GaussianGrid.create(7, nlat=NLAT, nlon=NLON)
     lat = np.asarray(grid.lat_rad, dtype=np.float64)
@@ -78,6 +82,18 @@ def main(ref_root: str) -> None:
             else:
                 rec[name] = np.stack(out)
         rec["linear"] = np.stack(gather_linear_batch(src, st))
+        # the fixed-point departure search on a rotation across both poles
+        wind = rotation_wind(lat, NLON, NLEV, seed=SEED + 2, dtype=dtype)
+        ex = rotation_wind(lat, NLON, NLEV, speed=45.0, seed=SEED + 3, dtype=dtype)
+        dst, diag = departure_points(CartesianWind(*wind), tables, DT, iterations=3,
+                                     extrapolated=CartesianWind(*ex))
+        rec.update({"wind": np.stack(wind), "wind_ex": np.stack(ex), "dt": np.float64(DT),
+                    "dep_xi": np.asarray(dst.xi), "dep_phi": np.asarray(dst.phi),
+                    "dep_level": np.asarray(dst.level),
+                    "dep_diag": np.array([diag.move_max_m, diag.move_max_cells,
+                                          diag.move_max_levels, diag.displacement_max_m,
+                                          diag.displacement_max_cells,
+                                          diag.displacement_max_levels])})
         np.savez_compressed(HERE / f"sl_gather_{tag}.npz", **rec)
         print("wrote", HERE / f"sl_gather_{tag}.npz")
 

@@ -160,3 +160,82 @@ def test_errors_name_the_reason(golden):
         SphericalGridTables.create(_grid(g["lat"], 25))
     with pytest.raises(ValueError, match="strictly ascending"):
         SphericalGridTables.create(_grid(g["lat"][::-1], 24))
+
+
+@pytest.mark.parametrize("tag", ["f64", "f32"])
+def test_departure_search_matches_reference(golden, tag):
+    """The fixed-point search (3 iterations, a rotation across both poles)
+    against the reference's recorded departure points and diagnostics."""
+    from b200sht.semilag import CartesianWind, departure_points
+
+    g = golden(f"sl_gather_{tag}.npz")
+    tables, _, _ = _setup(g, tag)
+    dev = lambda a: torch.as_tensor(a, device="cuda")
+    st, diag = departure_points(CartesianWind(*[dev(w) for w in g["wind"]]), tables,
+                                float(g["dt"]), iterations=3,
+                                extrapolated=CartesianWind(*[dev(w) for w in g["wind_ex"]]))
+    tol = 1e-12 if tag == "f64" else 2e-6
+    # positions: radians of latitude, zonal index (2 pi / 24 radians each), levels
+    assert np.max(np.abs(st.phi.cpu().numpy() - g["dep_phi"])) < tol * 4
+    dxi = np.abs(st.xi.cpu().numpy() - g["dep_xi"])
+    assert np.max(np.minimum(dxi, 24 - dxi)) < tol * 24
+    assert np.max(np.abs(st.level.cpu().numpy() - g["dep_level"])) < tol * 8
+    got = np.array([diag.move_max_m, diag.move_max_cells, diag.move_max_levels,
+                    diag.displacement_max_m, diag.displacement_max_cells,
+                    diag.displacement_max_levels])
+    # the last move is a small difference of unit vectors: loose in float32
+    rel = 1e-9 if tag == "f64" else 5e-2
+    np.testing.assert_allclose(got[3:], g["dep_diag"][3:], rtol=1e-9 if tag == "f64" else 1e-5)
+    np.testing.assert_allclose(got[:3], g["dep_diag"][:3], rtol=rel)
+
+
+@pytest.mark.parametrize("tag", ["f64", "f32"])
+def test_departure_search_against_oracle_and_gather(tag):
+    """48 x 96 x 8 against the oracle, then the gather reads the result."""
+    from b200sht.semilag import (CartesianWind, SphericalGridTables, departure_points,
+                                 gather_batch)
+    from oracle import sl_gather as O
+
+    nlat, nlon, nlev = 48, 96, 8
+    lat = np.sort(np.arcsin(np.polynomial.legendre.leggauss(nlat)[0]))
+    dtype = np.float64 if tag == "f64" else np.float32
+    wind = O.rotation_wind(lat, nlon, nlev, speed=60.0, seed=4, dtype=dtype)
+    tables = SphericalGridTables.create(_grid(lat, nlon), dtype=DT[tag])
+    dev = lambda a: torch.as_tensor(a, device="cuda")
+    st, diag = departure_points(CartesianWind(*[dev(w) for w in wind]), tables, 900.0,
+                                iterations=4)
+    xi, phi, lev, _, _ = O.departure(wind, lat, nlon, 900.0, iterations=4, dtype=dtype)
+    tol = 1e-12 if tag == "f64" else 2e-6
+    assert np.max(np.abs(st.phi.cpu().numpy() - phi)) < tol * 4
+    dxi = np.abs(st.xi.cpu().numpy() - xi)
+    assert np.max(np.minimum(dxi, nlon - dxi)) < tol * nlon
+    assert np.max(np.abs(st.level.cpu().numpy() - lev)) < tol * nlev
+    assert diag.move_max_cells < 1e-3 and diag.displacement_max_cells > 0.1
+    f = torch.randn((nlev, nlat, nlon), dtype=DT[tag], device="cuda")
+    assert torch.isfinite(gather_batch([f], st)[0]).all()
+
+
+def test_departure_errors_and_rest_state():
+    from b200sht.semilag import CartesianWind, SphericalGridTables, departure_points
+
+    nlat, nlon, nlev = 16, 32, 5
+    lat = np.sort(np.arcsin(np.polynomial.legendre.leggauss(nlat)[0]))
+    tables = SphericalGridTables.create(_grid(lat, nlon), dtype=torch.float64)
+    zero = torch.zeros((nlev, nlat, nlon), dtype=torch.float64, device="cuda")
+    wind = CartesianWind(zero, zero, zero, zero)
+    st, diag = departure_points(wind, tables, 300.0)
+    # a resting atmosphere departs from its arrival point
+    assert torch.max(torch.abs(st.phi - torch.as_tensor(lat, device="cuda")[None, :, None])) < 1e-14
+    xi = st.xi.cpu().numpy() % nlon
+    dxi = np.abs(xi - np.arange(nlon)[None, None, :])
+    assert np.max(np.minimum(dxi, nlon - dxi)) < 1e-12
+    assert diag.displacement_max_m < 1e-6 and diag.move_max_m == 0.0
+    with pytest.raises(ValueError, match="at least one iteration"):
+        departure_points(wind, tables, 300.0, iterations=0)
+    with pytest.raises(ValueError, match="not built"):
+        departure_points(wind, tables, 300.0, solver="newton")
+    with pytest.raises(ValueError, match="must be one of"):
+        departure_points(wind, tables, 300.0, solver="rk4")
+    with pytest.raises(ValueError, match="must all be"):
+        departure_points(wind, tables, 300.0,
+                         extrapolated=CartesianWind(zero[:4], zero, zero, zero))

@@ -55,3 +55,13 @@ def test_deficit_marks_the_clipped_points(golden):
     assert np.isfinite(v).all() and np.isfinite(c).all()
     assert 0 < np.count_nonzero(c) < c.size
     np.testing.assert_array_equal(v[c == 0], g["cubic_qm"][0][c == 0])
+
+
+@pytest.mark.parametrize("tag,dtype", [("f64", np.float64), ("f32", np.float32)])
+def test_departure_search_matches_reference(golden, tag, dtype):
+    g = golden(f"sl_gather_{tag}.npz")
+    xi, phi, lev, _, _ = O.departure(list(g["wind"]), g["lat"], int(g["nlon"]), float(g["dt"]),
+                                     iterations=3, extrapolated=list(g["wind_ex"]), dtype=dtype)
+    np.testing.assert_array_equal(xi, g["dep_xi"])
+    np.testing.assert_array_equal(phi, g["dep_phi"])
+    np.testing.assert_array_equal(lev, g["dep_level"])
