@@ -205,6 +205,50 @@ def rotation_departures(lat, nlon, nlev, *, speed=80.0, dt=300.0, radius=6371220
             level.to(dtype).contiguous())
 
 
+def _rhs_timings(args, shape, peak):
+    """The fused RHS kernels at the gather's grid (float32; 8 tracers for
+    the flux, tendency and vertical flux divergence), with the bytes each
+    must move and the fraction of the measured HBM copy rate they reach."""
+    from . import rhs
+
+    dev = torch.device("cuda", torch.cuda.current_device())
+    g = torch.Generator(device=dev).manual_seed(7)
+    rnd = lambda *sh: torch.randn(sh, generator=g, device=dev, dtype=torch.float32)
+    nlev, nlat, nlon = shape
+    ntr = 8
+    n = nlev * nlat * nlon
+    res = {}
+
+    def rec(name, fn, nbytes):
+        ms = _time(fn, args.steps, args.warmup)
+        gbs = nbytes / (ms * 1e-3) / 1e9
+        res[name] = {"ms": ms, "gb_per_s": gbs, "frac_of_hbm": gbs / peak}
+
+    three = [rnd(*shape) for _ in range(8)]
+    two = [rnd(nlat, nlon) for _ in range(3)]
+    zeta, u, v, wu, wv, tv, pg, phi = three
+    cor, ge, gn = two
+    rec("momentum_bernoulli",
+        lambda: rhs.momentum_bernoulli(zeta, cor, u, v, wu, wv, tv, pg, ge, gn, phi, 287.04),
+        4 * n * (8 + 3))
+    del three
+    s = rnd(ntr, *shape)
+    dp = rnd(*shape).abs_() + 1.0
+    flux = torch.empty((2, ntr, *shape), device=dev)
+    rec("tracer_flux_8", lambda: rhs.tracer_flux(dp, s, u, v, out=flux), 4 * n * (3 + 3 * ntr))
+    del flux
+    h, vert = rnd(ntr, *shape), rnd(ntr, *shape)
+    rec("scalar_tendency_8", lambda: rhs.scalar_tendency(h, vert, s, u, dp),
+        4 * n * (2 + 4 * ntr))
+    del h, vert
+    w = rnd(nlev + 1, nlat, nlon)
+    ph = torch.cumsum(torch.rand((nlev + 1, nlat, nlon), device=dev) + 0.5, dim=0)
+    pf = 0.5 * (ph[:-1] + ph[1:])
+    rec("vertical_flux_divergence_8", lambda: rhs.vertical_flux_divergence(s, w, pf, ph),
+        4 * n * (3 + 2 * ntr))
+    return res
+
+
 def sl_gather(args, clock_sampler):
     """The semi-Lagrangian gather of 16 fields (the reference's batch) at
     T511 L40 on the 768 x 1536 grid, float32: cubic quasi-monotone (the
@@ -272,11 +316,12 @@ def sl_gather(args, clock_sampler):
                    args.warmup)
         out["departure_search_3_iterations"] = {"ms": ms, "points_per_s": npts / (ms * 1e-3)}
         del wind, dep
+        out["rhs_kernels"] = _rhs_timings(args, (nlev, grid.nlat, grid.nlon), peak)
     head = out["cubic_quasi_monotone"]
     out["clocks"] = clocks.summary()
     out["value"] = head["point_fields_per_s"]
     out["ms_per_step"] = head["ms"]
-    out["gpu_launches"] = (len(cases) + 2) * args.steps
+    out["gpu_launches"] = (len(cases) + 2 + 4) * args.steps
     out["roofline"] = {"bound": "hbm", "achieved": head["algorithmic_gb_per_s"], "peak": peak,
                        "unit": "GB/s", "frac": head["algorithmic_gb_per_s"] / peak,
                        "traffic": None, "kernel": "sl_gather_kernel<float, 4, qm>",

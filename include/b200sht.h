@@ -341,6 +341,38 @@ int sht_sl_departure(const sht_sl_tables* tables, int nlev, const void* vx, cons
                      int iterations, double dt, double radius, void* xi, void* phi,
                      void* level, void* move_m, void* move_k, void* stream);
 
+/* Fused right-hand-side kernels of the dycore step (the reference's
+ * spectral/fused.py momentum_bernoulli_kernel, tracer_flux_kernel,
+ * scalar_tendency_kernel, vertical_flux_divergence_kernel and their numpy
+ * specifications in dynamics.py).  precision: SHT_PREC_F64 (double) or
+ * SHT_PREC_F32 (float).  Volumes are C-order (nlev, nlat, nlon), horiz =
+ * nlat * nlon; `blocks` counts leading (tracer) blocks of the scalar-side
+ * arrays, the other operands being one shared block.
+ *   momentum_bernoulli: coriolis, grad_lnps_east/north are (nlat, nlon),
+ *     broadcast over levels; mu = (zeta + f) v - wu - R Tv pg ge,
+ *     mv = -(zeta + f) u - wv - R Tv pg gn, bern = (u^2 + v^2)/2 + phi.
+ *   tracer_flux: flux_east = (dp s) u, flux_north = (dp s) v.
+ *   scalar_tendency: out = (-horizontal - vertical - s dp_t) / dp.
+ *   vertical_flux_divergence: omega_half and p_half (nlev + 1, nlat, nlon),
+ *     p_full (nlev, ...); the van Leer limited upstream flux through every
+ *     interface (zero at the top and bottom), out[k] = F[k+1] - F[k]. */
+int sht_rhs_momentum_bernoulli(int precision, int64_t nlev, int64_t horiz, const void* zeta,
+                               const void* coriolis, const void* u, const void* v, const void* wu,
+                               const void* wv, const void* tv, const void* pg,
+                               const void* grad_lnps_east, const void* grad_lnps_north,
+                               const void* geopotential, double gas_constant, void* mu, void* mv,
+                               void* bernoulli, void* stream);
+int sht_rhs_tracer_flux(int precision, int64_t blocks, int64_t nlev, int64_t horiz,
+                        const void* dp, const void* scalar, const void* u, const void* v,
+                        void* flux_east, void* flux_north, void* stream);
+int sht_rhs_scalar_tendency(int precision, int64_t blocks, int64_t nlev, int64_t horiz,
+                            const void* horizontal, const void* vertical, const void* scalar,
+                            const void* dp_t, const void* dp, void* out, void* stream);
+int sht_rhs_vertical_flux_divergence(int precision, int64_t blocks, int64_t nlev, int64_t horiz,
+                                     const void* scalar, const void* omega_half,
+                                     const void* p_full, const void* p_half, void* out,
+                                     void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,93 @@
+"""The fused RHS kernels (sht_rhs_*) against the oracle and the reference's
+recorded vertical flux divergence.  Tolerances: float64 1e-13 relative to
+the operands' scale, float32 1e-6 (FMA contraction)."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+TOL = {torch.float64: 1e-13, torch.float32: 1e-6}
+NP = {torch.float64: np.float64, torch.float32: np.float32}
+
+
+def _close(got, want, dt):
+    got = got.cpu().numpy()
+    scale = max(float(np.max(np.abs(want))), 1e-300)
+    assert float(np.max(np.abs(got - want))) <= TOL[dt] * scale * 4
+
+
+@pytest.mark.parametrize("dt", [torch.float64, torch.float32])
+@pytest.mark.parametrize("nlon", [16, 18])  # 18: horizontal size not a multiple of 4
+def test_momentum_bernoulli(dt, nlon):
+    from b200sht.rhs import momentum_bernoulli
+    from oracle import rhs as O
+
+    rng = np.random.default_rng(1)
+    nlev, nlat = 7, 5
+    three = [rng.standard_normal((nlev, nlat, nlon)).astype(NP[dt]) for _ in range(8)]
+    two = [rng.standard_normal((nlat, nlon)).astype(NP[dt]) for _ in range(3)]
+    zeta, u, v, wu, wv, tv, pg, phi = three
+    cor, ge, gn = two
+    want = O.momentum_bernoulli(zeta, cor, u, v, wu, wv, tv, pg, ge, gn, phi, NP[dt](287.04))
+    dev = lambda a: torch.as_tensor(a, device="cuda")
+    got = momentum_bernoulli(dev(zeta), dev(cor), dev(u), dev(v), dev(wu), dev(wv), dev(tv),
+                             dev(pg), dev(ge), dev(gn), dev(phi), 287.04)
+    for a, b in zip(got, want):
+        _close(a, b, dt)
+
+
+@pytest.mark.parametrize("dt", [torch.float64, torch.float32])
+@pytest.mark.parametrize("lead", [(), (3,), (2, 2)])
+def test_tracer_flux_and_tendency(dt, lead):
+    from b200sht.rhs import scalar_tendency, tracer_flux
+    from oracle import rhs as O
+
+    rng = np.random.default_rng(2)
+    shape = (6, 4, 12)
+    dp = (rng.random(shape) + 0.5).astype(NP[dt])
+    u, v, dpt = [rng.standard_normal(shape).astype(NP[dt]) for _ in range(3)]
+    s, h, vert = [rng.standard_normal(lead + shape).astype(NP[dt]) for _ in range(3)]
+    dev = lambda a: torch.as_tensor(a, device="cuda")
+    fl = tracer_flux(dev(dp), dev(s), dev(u), dev(v))
+    fx, fy = O.tracer_flux(dp, s, u, v)
+    _close(fl[0], fx, dt)
+    _close(fl[1], fy, dt)
+    _close(scalar_tendency(dev(h), dev(vert), dev(s), dev(dpt), dev(dp)),
+           O.scalar_tendency(h, vert, s, dpt, dp), dt)
+
+
+@pytest.mark.parametrize("dt", [torch.float64, torch.float32])
+def test_vertical_flux_divergence_matches_reference(golden, dt):
+    from b200sht.rhs import vertical_flux_divergence
+
+    tag = "f64" if dt == torch.float64 else "f32"
+    g = golden("rhs_vertical_flux.npz")
+    dev = lambda a: torch.as_tensor(a, device="cuda")
+    got = vertical_flux_divergence(dev(g[f"s_{tag}"]), dev(g[f"w_{tag}"]), dev(g[f"pf_{tag}"]),
+                                   dev(g[f"ph_{tag}"]))
+    _close(got, g[f"out_{tag}"], dt)
+
+
+@pytest.mark.parametrize("dt", [torch.float64, torch.float32])
+@pytest.mark.parametrize("nlev", [1, 2, 3, 40])
+def test_vertical_flux_divergence_against_oracle(dt, nlev):
+    from b200sht.rhs import vertical_flux_divergence
+    from oracle import rhs as O
+
+    s, w, pf, ph = O.column_state(nlev, 7, 9, 2, nlev, dtype=NP[dt])
+    dev = lambda a: torch.as_tensor(a, device="cuda")
+    got = vertical_flux_divergence(dev(s), dev(w), dev(pf), dev(ph))
+    _close(got, O.vertical_flux_divergence(s, w, pf, ph), dt)
+
+
+def test_errors():
+    from b200sht.rhs import tracer_flux, vertical_flux_divergence
+
+    x = torch.zeros((4, 3, 8), dtype=torch.float32, device="cuda")
+    with pytest.raises(ValueError, match="mixed dtypes"):
+        tracer_flux(x, x.double(), x, x)
+    with pytest.raises(ValueError, match="nlev \\+ 1"):
+        vertical_flux_divergence(x, x, x, x)
