@@ -101,6 +101,9 @@ SIGNATURES = {
     "sht_rhs_scalar_tendency": (ctypes.c_int, [ctypes.c_int, _I64, _I64, _I64] + [_P] * 7),
     "sht_rhs_vertical_flux_divergence": (ctypes.c_int, [ctypes.c_int, _I64, _I64, _I64]
                                          + [_P] * 6),
+    "sht_sampler_create": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(_P)]),
+    "sht_sampler_destroy": (ctypes.c_int, [_P]),
+    "sht_sample": (ctypes.c_int, [_P, _P, _I64, _I64, _P, _P, ctypes.c_int, _D, _P, _P, _P]),
 }
 
 _lib = None

@@ -249,6 +249,29 @@ def _rhs_timings(args, shape, peak):
     return res
 
 
+def _sampling_timings(args):
+    """Point sampling at T511 in FP64: 4 fields at 16 384 random points,
+    scalar and gradient (the verification harness's regular-grid export)."""
+    from .sampling import sample_into
+
+    dev = torch.device("cuda", torch.cuda.current_device())
+    g = torch.Generator(device=dev).manual_seed(9)
+    T, nf, npts = 511, 4, 16384
+    c = torch.randn((nf, T + 1, T + 1), generator=g, device=dev, dtype=torch.complex128)
+    lat = (torch.rand(npts, generator=g, device=dev, dtype=torch.float64) - 0.5) * 3.0
+    lon = torch.rand(npts, generator=g, device=dev, dtype=torch.float64) * 6.283
+    o0 = torch.empty((nf, npts), dtype=torch.float64, device=dev)
+    o1 = torch.empty_like(o0)
+    steps, warm = max(2, args.steps // 10), max(1, args.warmup // 3)
+    ms_s = _time(lambda: sample_into(T, c, lat, lon, 6371220.0, o0), steps, warm)
+    ms_g = _time(lambda: sample_into(T, c, lat, lon, 6371220.0, o0, o1), steps, warm)
+    terms = nf * npts * (T + 1) * (T + 2) / 2
+    return {"truncation": T, "fields": nf, "points": npts,
+            "scalar_ms": ms_s, "gradient_ms": ms_g,
+            "scalar_point_fields_per_s": nf * npts / (ms_s * 1e-3),
+            "scalar_terms_per_s": terms / (ms_s * 1e-3)}
+
+
 def sl_gather(args, clock_sampler):
     """The semi-Lagrangian gather of 16 fields (the reference's batch) at
     T511 L40 on the 768 x 1536 grid, float32: cubic quasi-monotone (the
@@ -317,6 +340,7 @@ def sl_gather(args, clock_sampler):
         out["departure_search_3_iterations"] = {"ms": ms, "points_per_s": npts / (ms * 1e-3)}
         del wind, dep
         out["rhs_kernels"] = _rhs_timings(args, (nlev, grid.nlat, grid.nlon), peak)
+        out["point_sampling"] = _sampling_timings(args)
     head = out["cubic_quasi_monotone"]
     out["clocks"] = clocks.summary()
     out["value"] = head["point_fields_per_s"]

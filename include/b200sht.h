@@ -373,6 +373,22 @@ int sht_rhs_vertical_flux_divergence(int precision, int64_t blocks, int64_t nlev
                                      const void* p_full, const void* p_half, void* out,
                                      void* stream);
 
+/* Spectral fields at arbitrary points (the reference's spectral/sampling.py
+ * sample_scalar / sample_gradient; sample_wind is the gradient of the
+ * inverse Laplacians).  sht_sampler_create builds the x-independent
+ * recurrence factors of truncation T once.  sht_sample: coeff_mn is
+ * complex128 [fields][m][n] (the [n, m] coefficients transposed), lat/lon
+ * in radians [npoints]; gradient == 0: out0[fields][npoints] = the field;
+ * gradient != 0: out0 = eastward, out1 = northward gradient (physical,
+ * 1 / (radius cos phi) and 1 / radius applied; points off the poles).
+ * FP64 throughout, device pointers. */
+typedef struct sht_sampler sht_sampler;
+int sht_sampler_create(int truncation, sht_sampler** out);
+int sht_sampler_destroy(sht_sampler* sampler);
+int sht_sample(sht_sampler* sampler, const void* coeff_mn, int64_t fields, int64_t npoints,
+               const double* lat_rad, const double* lon_rad, int gradient, double radius,
+               double* out0, double* out1, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
