@@ -245,9 +245,10 @@ __device__ __forceinline__ T interface_flux(T wj, T phj, T sa, T ga, T pa, T sb,
 // One thread marches one column down the levels for NT tracers at once:
 // the pressures and the interface velocity of a level are loaded once for
 // all of them, and the NT recurrences are independent work between loads.
-// (Splitting a column into chunks marched by separate threads, each
-// forming its top interface's flux from the four layers around it,
-// measured slower: 2.81 against 2.40 ms at T511 L40 x 8 tracers.)
+// (Without the one-level prefetch: 2.40 ms at T511 L40 x 8 tracers, against
+// 1.16 with it; splitting a column into chunks marched by separate threads,
+// each forming its top interface's flux from the four layers around it,
+// measured 2.81.)
 template <typename T, int NT>
 __global__ void __launch_bounds__(256) vertical_flux_divergence_kernel(const VfdArgs<T> a) {
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
@@ -264,33 +265,45 @@ __global__ void __launch_bounds__(256) vertical_flux_divergence_kernel(const Vfd
     const T* pf = a.pf + col;
     const T* w = a.w + col;
     const T* ph = a.ph + col;
-    T s0[NT], sp[NT], g0[NT], fa[NT];
+    T s0[NT], sp[NT], g0[NT], fa[NT], s_pre[NT];
     T p_0 = __ldg(pf), p_p = nlev > 1 ? __ldg(pf + H) : T(0);
+    // One level of loads in flight ahead of the arithmetic: the values of
+    // level k + 2 (interface k + 1) are loaded during iteration k - 1.
+    T p_pre = nlev > 2 ? __ldg(pf + 2 * H) : T(0);
+    T w_pre = nlev > 1 ? __ldg(w + H) : T(0);
+    T ph_pre = nlev > 1 ? __ldg(ph + H) : T(0);
 #pragma unroll
     for (int t = 0; t < NT; ++t) {
       s0[t] = __ldcs(s[t]);
       sp[t] = nlev > 1 ? __ldcs(s[t] + H) : T(0);
+      s_pre[t] = nlev > 2 ? __ldcs(s[t] + 2 * H) : T(0);
       g0[t] = nlev > 1 ? layer_gradient(0, nlev, T(0), s0[t], sp[t], T(0), p_0, p_p) : T(0);
       fa[t] = T(0);  // no flux through the top
     }
     for (int k = 0; k < nlev; ++k) {
       const bool inner = k + 1 < nlev;
-      const bool next = k + 2 < nlev;
-      const T p_next = next ? __ldg(pf + (int64_t)(k + 2) * H) : T(0);
-      const T wj = inner ? __ldg(w + (int64_t)(k + 1) * H) : T(0);
-      const T phj = inner ? __ldg(ph + (int64_t)(k + 1) * H) : T(0);
+      const T p_next = p_pre, wj = w_pre, phj = ph_pre;
+      T s_next[NT];
+#pragma unroll
+      for (int t = 0; t < NT; ++t) s_next[t] = s_pre[t];
+      // prefetch level k + 3 and interface k + 2
+      p_pre = k + 3 < nlev ? __ldg(pf + (int64_t)(k + 3) * H) : T(0);
+      w_pre = k + 2 < nlev ? __ldg(w + (int64_t)(k + 2) * H) : T(0);
+      ph_pre = k + 2 < nlev ? __ldg(ph + (int64_t)(k + 2) * H) : T(0);
+#pragma unroll
+      for (int t = 0; t < NT; ++t)
+        s_pre[t] = k + 3 < nlev ? __ldcs(s[t] + (int64_t)(k + 3) * H) : T(0);
 #pragma unroll
       for (int t = 0; t < NT; ++t) {
-        const T s_next = next ? __ldcs(s[t] + (int64_t)(k + 2) * H) : T(0);
         T fb = T(0), g_next = T(0);
         if (inner) {
-          g_next = layer_gradient(k + 1, nlev, s0[t], sp[t], s_next, p_0, p_p, p_next);
+          g_next = layer_gradient(k + 1, nlev, s0[t], sp[t], s_next[t], p_0, p_p, p_next);
           fb = interface_flux(wj, phj, s0[t], g0[t], p_0, sp[t], g_next, p_p);
         }
         __stcs(out[t] + (int64_t)k * H, fb - fa[t]);
         fa[t] = fb;
         s0[t] = sp[t];
-        sp[t] = s_next;
+        sp[t] = s_next[t];
         g0[t] = g_next;
       }
       p_0 = p_p;
