@@ -51,7 +51,7 @@ def parse():
     ap.add_argument("--profile-only", action="store_true",
                     help="one plan, warmup + steps of the pair, no checks (small ncu case)")
     ap.add_argument("--precision", default="split16", choices=["split16", "float32", "float64"])
-    ap.add_argument("--workload", default="pair", choices=["pair", "ensemble", "step", "sl_gather"],
+    ap.add_argument("--workload", default="pair", choices=["pair", "ensemble", "step", "sl_gather", "native"],
                     help="pair: the T511 L40 transform pair (default); ensemble: 32 members "
                          "at T126 + the T255 control as one batch; step: the full T511 "
                          "dycore-step transform set as one CUDA graph, with the "

@@ -12,6 +12,9 @@ as one CUDA graph per 300 s step, split16 and float32, with the
 Rossby-Haurwitz wave-4 state plus 1 % red noise iterated for ``drift_steps``
 steps and the wave's spectral energy drift reported against the FP64 path.
 
+``native``: forward + inverse at T767 and T1534 on their native grids with
+resident tables (plan build time, memory, pair time, round-trip error).
+
 ``sl_gather``: the semi-Lagrangian gather of 16 fields at T511 L40 (cubic
 quasi-monotone headline, cubic and quintic unlimited, trilinear) at the
 departure points of a solid-body rotation across both poles.
@@ -353,7 +356,56 @@ def sl_gather(args, clock_sampler):
     return out
 
 
+def native_grids(args, clock_sampler):
+    """Analysis and synthesis on the verification harness's native grids,
+    T767 (1152 x 2304) and T1534 (1536 x 3072, the GFS grid), with every
+    table resident (the reference streams them from the recurrence because
+    a 16 GB card cannot hold them): plan build time, device memory, the
+    split16 pair's time at 8 planes and the round-trip error of a seeded
+    red spectrum."""
+    import time as _t
+
+    out = {"metric": "Native-grid transform pair (T767 and T1534, split16), ms per 8-plane pair",
+           "unit": "ms", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+           "higher_is_better": False, "data": "synthetic seeded red spectrum", "cases": []}
+    dev = torch.device("cuda", torch.cuda.current_device())
+    with clock_sampler(torch.cuda.current_device()) as clocks:
+        # T767 on its quadratic grid, T1534 on the linear GFS grid
+        for T, nl, no, dealias in ((767, 1152, 2304, 1.5), (1534, 1536, 3072, 1.0)):
+            torch.cuda.synchronize()
+            free0 = torch.cuda.mem_get_info()[0]
+            t0 = _t.perf_counter()
+            t = SphericalHarmonicTransform.create(T, nlat=nl, nlon=no, dealias_factor=dealias,
+                                                  precision="split16")
+            c = torch.as_tensor(red_spectrum(T, 8, CONTROL_SEED), device=dev)
+            c = c.to(t.backend.complex_dtype)
+            t.inverse(c)
+            torch.cuda.synchronize()
+            build_s = _t.perf_counter() - t0
+            used = (free0 - torch.cuda.mem_get_info()[0]) / 2**30
+            state = {}
+
+            def pair():
+                state["c"] = t.forward(t.inverse(c))
+
+            ms = _time(pair, max(2, args.steps // 20), max(1, args.warmup))
+            c2 = t.forward(t.inverse(c)).to(torch.complex128)
+            c1 = c.to(torch.complex128)
+            err = _rel_l2(c2, c1)
+            err_max = float((c2 - c1).abs().max() / c1.abs().max())
+            out["cases"].append({"truncation": T, "grid": [nl, no], "precision": "split16",
+                                 "plan_build_s": build_s, "device_gib": used,
+                                 "ms_per_pair_8_planes": ms, "roundtrip_rel_spectral_l2": err,
+                                 "roundtrip_rel_max": err_max})
+            del t, c, state
+            torch.cuda.empty_cache()
+    out["clocks"] = clocks.summary()
+    out["value"] = out["cases"][-1]["ms_per_pair_8_planes"]
+    out["ms_per_step"] = out["value"]
+    return out
+
+
 def run_workload(args, clock_sampler):
     torch.cuda.set_device(0)
-    return {"ensemble": ensemble, "step": step,
-            "sl_gather": sl_gather}[args.workload](args, clock_sampler)
+    return {"ensemble": ensemble, "step": step, "sl_gather": sl_gather,
+            "native": native_grids}[args.workload](args, clock_sampler)
