@@ -95,6 +95,8 @@ SIGNATURES = {
     "sht_sl_gather_linear": (ctypes.c_int, [_P, _P, _I64, ctypes.c_int, _P, _P, _P, _P, _P]),
     "sht_sl_departure": (ctypes.c_int, [_P, ctypes.c_int, _P, _P, _P, _P, _P, _P, _P, _P,
                                         ctypes.c_int, _D, _D, _P, _P, _P, _P, _P, _P]),
+    "sht_sl_departure_newton": (ctypes.c_int, [_P, ctypes.c_int, _P, _P, _P, _P, _P, _P, _P, _P,
+                                               ctypes.c_int, _D, _D, _P, _P, _P, _P, _P, _P]),
     "sht_rhs_momentum_bernoulli": (ctypes.c_int, [ctypes.c_int, _I64, _I64] + [_P] * 11
                                    + [_D, _P, _P, _P, _P]),
     "sht_rhs_tracer_flux": (ctypes.c_int, [ctypes.c_int, _I64, _I64, _I64] + [_P] * 7),

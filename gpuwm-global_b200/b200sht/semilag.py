@@ -296,8 +296,9 @@ def gather_linear_batch(fields: Sequence[torch.Tensor], stencil: Stencil, *,
 # local_wind, TrajectoryDiagnostics, meridional_grid_length_m and
 # departure_points (trajectory.py:50-120, 158-358, 440-490).
 
-#: Solvers of the departure-point equation.  Only the fixed-point pass (the
-#: reference's default and its numpy specification) is built here.
+#: Solvers of the departure-point equation: the fixed-point pass (the
+#: reference's default and its numpy specification) and Newton's method on
+#: the same equation; the line-search form is not built here.
 TRAJECTORY_SOLVERS = ("fixed_point", "newton", "newton_ls")
 
 
@@ -401,12 +402,13 @@ def _diagnostics(stencil: Stencil, move_m, move_k, tables, dt_s, iterations):
 
 
 def search_into(tables: SphericalGridTables, fields: Sequence[torch.Tensor], iterations: int,
-                dt_s: float, outs: Sequence[torch.Tensor]) -> None:
+                dt_s: float, outs: Sequence[torch.Tensor], newton: bool = False) -> None:
     """The search kernel alone: ``fields`` = (vx, vy, vz, level_rate) of the
     advecting wind then of the extrapolated one, contiguous; ``outs`` = xi,
     phi, level, move_m, move_k.  No checks beyond the library's."""
     nlev = int(fields[0].shape[0])
-    _lib.call("sht_sl_departure", tables._handle, nlev, *[_ptr(t) for t in fields],
+    name = "sht_sl_departure_newton" if newton else "sht_sl_departure"
+    _lib.call(name, tables._handle, nlev, *[_ptr(t) for t in fields],
               int(iterations), float(dt_s), float(tables.radius_m), *[_ptr(t) for t in outs],
               _stream())
 
@@ -429,9 +431,9 @@ def departure_points(wind: CartesianWind, tables: SphericalGridTables, dt_s: flo
             "explicit first guess, which is first order in dt and is not a trajectory")
     if solver not in TRAJECTORY_SOLVERS:
         raise ValueError(f"trajectory solver must be one of {TRAJECTORY_SOLVERS}, got {solver!r}")
-    if solver != "fixed_point":
+    if solver == "newton_ls":
         raise ValueError(f"trajectory solver {solver!r} is not built in this engine; the "
-                         "fixed-point pass is")
+                         "fixed-point pass and 'newton' are")
     ex = wind if extrapolated is None else extrapolated
     for name, arr in (("wind", wind), ("extrapolated", ex)):
         for field in arr.arrays():
@@ -444,7 +446,7 @@ def departure_points(wind: CartesianWind, tables: SphericalGridTables, dt_s: flo
                 raise ValueError(f"{name} fields must be CUDA tensors")
     ins = [f.contiguous() for f in wind.arrays()] + [f.contiguous() for f in ex.arrays()]
     outs = [torch.empty(shape, dtype=tables.dtype, device=ins[0].device) for _ in range(5)]
-    search_into(tables, ins, int(iterations), float(dt_s), outs)
+    search_into(tables, ins, int(iterations), float(dt_s), outs, newton=solver == "newton")
     xi, phi, lev, move_m, move_k = outs
     stencil = Stencil(xi=xi, phi=phi, level=lev, tables=tables)
     return stencil, _diagnostics(stencil, move_m, move_k, tables, dt_s, iterations)

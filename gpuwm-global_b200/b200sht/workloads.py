@@ -341,6 +341,9 @@ def sl_gather(args, clock_sampler):
         ms = _time(lambda: search_into(tables, wind + wind, 3, 300.0, dep), args.steps,
                    args.warmup)
         out["departure_search_3_iterations"] = {"ms": ms, "points_per_s": npts / (ms * 1e-3)}
+        ms = _time(lambda: search_into(tables, wind + wind, 3, 300.0, dep, newton=True),
+                   args.steps, args.warmup)
+        out["departure_newton_3_iterations"] = {"ms": ms, "points_per_s": npts / (ms * 1e-3)}
         del wind, dep
         out["rhs_kernels"] = _rhs_timings(args, (nlev, grid.nlat, grid.nlon), peak)
         out["point_sampling"] = _sampling_timings(args)
@@ -348,7 +351,7 @@ def sl_gather(args, clock_sampler):
     out["clocks"] = clocks.summary()
     out["value"] = head["point_fields_per_s"]
     out["ms_per_step"] = head["ms"]
-    out["gpu_launches"] = (len(cases) + 2 + 4) * args.steps
+    out["gpu_launches"] = (len(cases) + 3 + 4) * args.steps
     out["roofline"] = {"bound": "hbm", "achieved": head["algorithmic_gb_per_s"], "peak": peak,
                        "unit": "GB/s", "frac": head["algorithmic_gb_per_s"] / peak,
                        "traffic": None, "kernel": "sl_gather_kernel<float, 4, qm>",

@@ -484,6 +484,164 @@ __global__ void __launch_bounds__(256) sl_departure_kernel(const SlDepArgs<T> a)
   a.move_k[gid] = last_k;
 }
 
+// ------------------------------------------------ Newton departure search
+// The same departure equation solved by Newton's method (the reference's
+// opt-in "newton" solver, semilag/trajectory.py TRAJECTORY_SOLVERS): with
+// the fixed-point map G(q, k) above, find q, k with G(q, k) = (q, k).  At
+// the current point the residual r = G - (q, k) is taken in the local
+// east / north / level frame, the Jacobian M of G in that frame comes from
+// the trilinear interpolant's own derivatives (dV/d(east) = dV/dlambda /
+// cos phi, dV/d(north) = dV/dphi, dV/dk; the normalisation's projection is
+// dropped, exact at the solution), and (I - M) d = r is solved by Cramer's
+// rule.  A step is taken only where det(I - M) > 0.05 and cos phi > 1e-6
+// and it is at most five times the plain step; otherwise, and where the
+// residual did not shrink, the plain fixed-point step d = r is taken.  Both
+// solvers share one fixed point.
+template <typename T>
+__device__ __forceinline__ void trilinear4_grad(const SlDepArgs<T>& a, T lam, T phid, T xkd,
+                                                T (&w)[4], T (&dl)[4], T (&dp)[4], T (&dk)[4]) {
+  const T p = min(max(phid, T(-kHalfPi)), T(kHalfPi));
+  const bool kclamp = xkd <= T(0) || xkd >= T(a.nk - 1);
+  const T xk = min(max(xkd, T(0)), T(a.nk - 1));
+  const T x = lam * a.inv_dlam;
+  const T fi = floor(x);
+  const T ax = x - fi;
+  int c0 = ((int)fi) % a.ni;
+  if (c0 < 0) c0 += a.ni;
+  const int c1 = c0 + 1 == a.ni ? 0 : c0 + 1;
+  const int half = a.ni >> 1;
+  const int h0 = c0 >= a.ni - half ? c0 + half - a.ni : c0 + half;
+  const int h1 = c1 >= a.ni - half ? c1 + half - a.ni : c1 + half;
+  const int m0 = bracket<T>(p, a.lat_ext, a.mlut, a.nb, a.nj, 1, a.lut_scale);
+  const T la = __ldg(a.lat_ext + m0), lb = __ldg(a.lat_ext + m0 + 1);
+  const T inv_dphi = T(1) / (lb - la);
+  const T ay = (p - la) * inv_dphi;
+  const int r0 = __ldg(a.rowoff + m0), r1 = __ldg(a.rowoff + m0 + 1);
+  const bool s0 = __ldg(a.rowshift + m0) != 0, s1 = __ldg(a.rowshift + m0 + 1) != 0;
+  const int i00 = r0 + (s0 ? h0 : c0), i01 = r0 + (s0 ? h1 : c1);
+  const int i10 = r1 + (s1 ? h0 : c0), i11 = r1 + (s1 ? h1 : c1);
+  const int k0 = min(max((int)floor(xk), 0), a.nk - 2);
+  const T az = xk - T(k0);
+  const int64_t plane = (int64_t)a.nj * a.ni;
+  const int64_t o0 = (int64_t)k0 * plane, o1 = o0 + plane;
+  const T bx = T(1) - ax, by = T(1) - ay, bz = T(1) - az;
+  const T* f[4] = {a.vx, a.vy, a.vz, a.sv};
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const T* u = f[q] + o0;
+    const T* v = f[q] + o1;
+    const T u00 = __ldg(u + i00), u01 = __ldg(u + i01), u10 = __ldg(u + i10), u11 = __ldg(u + i11);
+    const T v00 = __ldg(v + i00), v01 = __ldg(v + i01), v10 = __ldg(v + i10), v11 = __ldg(v + i11);
+    const T t0 = by * (bx * u00 + ax * u01) + ay * (bx * u10 + ax * u11);
+    const T t1 = by * (bx * v00 + ax * v01) + ay * (bx * v10 + ax * v11);
+    w[q] = bz * t0 + az * t1;
+    const T gx0 = by * (u01 - u00) + ay * (u11 - u10), gx1 = by * (v01 - v00) + ay * (v11 - v10);
+    const T gy0 = (bx * u10 + ax * u11) - (bx * u00 + ax * u01);
+    const T gy1 = (bx * v10 + ax * v11) - (bx * v00 + ax * v01);
+    dl[q] = (bz * gx0 + az * gx1) * a.inv_dlam;
+    dp[q] = (bz * gy0 + az * gy1) * inv_dphi;
+    dk[q] = kclamp ? T(0) : t1 - t0;
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) sl_departure_newton_kernel(const SlDepArgs<T> a) {
+  const int64_t n = (int64_t)a.nk * a.nj * a.ni;
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const int64_t gid = point_index(t, a.nk, a.nj, a.ni);
+  const int plane = a.nj * a.ni;
+  const int k = (int)(gid / plane);
+  const int rem = (int)(gid - (int64_t)k * plane);
+  const int j = rem / a.ni, i = rem - j * a.ni;
+  const T lat = __ldg(a.lat_ext + j + 2);
+  const T lon = T((double)i * a.dlam);
+  const T ax = cos(lat) * cos(lon), ay = cos(lat) * sin(lon), az = sin(lat);
+  const T inv_r = T(1) / a.radius;
+  const T dt = a.dt, hdt = T(0.5) * a.dt, c = hdt * inv_r;
+  // the fixed-point search's first guess
+  T qx = ax - dt * a.vx[gid] * inv_r, qy = ay - dt * a.vy[gid] * inv_r,
+    qz = az - dt * a.vz[gid] * inv_r;
+  T nrm = sqrt(qx * qx + qy * qy + qz * qz);
+  qx /= nrm; qy /= nrm; qz /= nrm;
+  const T klo = T(-0.5), khi = T(a.nk) - T(0.5);
+  T qk = min(max(T(k) - dt * a.sv[gid], klo), khi);
+  const T ex = a.vxe[gid], ey = a.vye[gid], ez = a.vze[gid], es = a.sve[gid];
+  const T cells = T(a.nj) / T(2 * kHalfPi);  // meridional grid lengths per radian
+  T last_m = T(0), last_k = T(0), res_prev = T(-1);
+  for (int it = 0; it < a.iters; ++it) {
+    const T lam = atan2(qy, qx);
+    const T rho = sqrt(qx * qx + qy * qy);
+    const T phid = atan2(qz, rho);
+    T w[4], dl[4], dp[4], dk[4];
+    trilinear4_grad<T>(a, lam, phid, qk, w, dl, dp, dk);
+    const T ux = ax - c * (ex + w[0]), uy = ay - c * (ey + w[1]), uz = az - c * (ez + w[2]);
+    const T un = sqrt(ux * ux + uy * uy + uz * uz);
+    const T px = ux / un, py = uy / un, pz = uz / un;
+    const T pk = min(max(T(k) - hdt * (es + w[3]), klo), khi);
+    const bool kheld = pk <= klo || pk >= khi;
+    // local frame at q: east e, north nv
+    const T cl = rho > T(0) ? qx / rho : T(1), sl = rho > T(0) ? qy / rho : T(0);
+    const T cp = rho, sp = qz;
+    const T e0 = -sl, e1 = cl;
+    const T n0 = -sp * cl, n1 = -sp * sl, n2 = cp;
+    const T dx = px - qx, dy = py - qy, dz = pz - qz;
+    const T re = e0 * dx + e1 * dy, rn = n0 * dx + n1 * dy + n2 * dz, rk = pk - qk;
+    T de = re, dn = rn, dkk = rk;
+    const T res = sqrt((re * re + rn * rn) * cells * cells + rk * rk);
+    const bool shrinking = res_prev < T(0) || res <= T(0.9) * res_prev;
+    res_prev = res;
+    if (shrinking && cp > T(1e-6)) {
+      const T g = -c / un;
+      const T icp = T(1) / cp;
+      // M[r][col]: rows east, north, level; columns d(east), d(north), d(level)
+      const T m00 = g * (e0 * dl[0] + e1 * dl[1]) * icp;
+      const T m01 = g * (e0 * dp[0] + e1 * dp[1]);
+      const T m02 = g * (e0 * dk[0] + e1 * dk[1]);
+      const T m10 = g * (n0 * dl[0] + n1 * dl[1] + n2 * dl[2]) * icp;
+      const T m11 = g * (n0 * dp[0] + n1 * dp[1] + n2 * dp[2]);
+      const T m12 = g * (n0 * dk[0] + n1 * dk[1] + n2 * dk[2]);
+      const T m20 = kheld ? T(0) : -hdt * dl[3] * icp;
+      const T m21 = kheld ? T(0) : -hdt * dp[3];
+      const T m22 = kheld ? T(0) : -hdt * dk[3];
+      const T a00 = T(1) - m00, a01 = -m01, a02 = -m02;
+      const T a10 = -m10, a11 = T(1) - m11, a12 = -m12;
+      const T a20 = -m20, a21 = -m21, a22 = T(1) - m22;
+      const T det = a00 * (a11 * a22 - a12 * a21) - a01 * (a10 * a22 - a12 * a20) +
+                    a02 * (a10 * a21 - a11 * a20);
+      if (isfinite(det) && det > T(0.05)) {
+        const T id = T(1) / det;
+        const T s0 = (re * (a11 * a22 - a12 * a21) - a01 * (rn * a22 - a12 * rk) +
+                      a02 * (rn * a21 - a11 * rk)) * id;
+        const T s1 = (a00 * (rn * a22 - a12 * rk) - re * (a10 * a22 - a12 * a20) +
+                      a02 * (a10 * rk - rn * a20)) * id;
+        const T s2 = (a00 * (a11 * rk - rn * a21) - a01 * (a10 * rk - rn * a20) +
+                      re * (a10 * a21 - a11 * a20)) * id;
+        const T step = sqrt((s0 * s0 + s1 * s1) * cells * cells + s2 * s2);
+        if (isfinite(step) && step <= T(5) * res + T(1e-30)) {
+          de = s0;
+          dn = s1;
+          dkk = s2;
+        }
+      }
+    }
+    T nx = qx + de * e0 + dn * n0, ny = qy + de * e1 + dn * n1, nz = qz + dn * n2;
+    nrm = sqrt(nx * nx + ny * ny + nz * nz);
+    nx /= nrm; ny /= nrm; nz /= nrm;
+    const T nk = min(max(qk + dkk, klo), khi);
+    const T cx = nx - qx, cy = ny - qy, cz = nz - qz;
+    const T chord = sqrt(cx * cx + cy * cy + cz * cz);
+    last_m = a.radius * T(2) * asin(min(max(T(0.5) * chord, T(0)), T(1)));
+    last_k = fabs(nk - qk);
+    qx = nx; qy = ny; qz = nz; qk = nk;
+  }
+  a.xi[gid] = atan2(qy, qx) * a.inv_dlam;
+  a.phi[gid] = atan2(qz, sqrt(qx * qx + qy * qy));
+  a.lev[gid] = qk;
+  a.move_m[gid] = last_m;
+  a.move_k[gid] = last_k;
+}
+
 // ----------------------------------------------------------- tables
 // The pole-extended table of one stencil width (semilag/tables.py:51-95,
 // 164-217): G reflected rows each side, the data row and zonal shift each
@@ -756,11 +914,12 @@ int sht_sl_gather_linear(const sht_sl_tables* tables, const void* src, int64_t f
   });
 }
 
-int sht_sl_departure(const sht_sl_tables* tables, int nlev, const void* vx, const void* vy,
-                     const void* vz, const void* level_rate, const void* vx_ex,
-                     const void* vy_ex, const void* vz_ex, const void* level_rate_ex,
-                     int iterations, double dt, double radius, void* xi, void* phi,
-                     void* level, void* move_m, void* move_k, void* stream) {
+static int departure_entry(bool newton, const sht_sl_tables* tables, int nlev, const void* vx,
+                           const void* vy, const void* vz, const void* level_rate,
+                           const void* vx_ex, const void* vy_ex, const void* vz_ex,
+                           const void* level_rate_ex, int iterations, double dt, double radius,
+                           void* xi, void* phi, void* level, void* move_m, void* move_k,
+                           void* stream) {
   return guarded([&] {
     check_call(tables, vx, 1, nlev, vy, vz, level_rate, xi);
     SHT_REQUIRE(vx_ex && vy_ex && vz_ex && level_rate_ex && phi && level && move_m && move_k,
@@ -793,14 +952,37 @@ int sht_sl_departure(const sht_sl_tables* tables, int nlev, const void* vx, cons
     if (tables->prec == SHT_PREC_F64) {
       SlDepArgs<double> a;
       fill(&a);
-      sl_departure_kernel<double><<<blocks, 256, 0, s>>>(a);
+      if (newton) sl_departure_newton_kernel<double><<<blocks, 256, 0, s>>>(a);
+      else sl_departure_kernel<double><<<blocks, 256, 0, s>>>(a);
     } else {
       SlDepArgs<float> a;
       fill(&a);
-      sl_departure_kernel<float><<<blocks, 256, 0, s>>>(a);
+      if (newton) sl_departure_newton_kernel<float><<<blocks, 256, 0, s>>>(a);
+      else sl_departure_kernel<float><<<blocks, 256, 0, s>>>(a);
     }
     SHT_CUDA_OR_THROW(cudaGetLastError());
   });
+}
+
+int sht_sl_departure(const sht_sl_tables* tables, int nlev, const void* vx, const void* vy,
+                     const void* vz, const void* level_rate, const void* vx_ex,
+                     const void* vy_ex, const void* vz_ex, const void* level_rate_ex,
+                     int iterations, double dt, double radius, void* xi, void* phi,
+                     void* level, void* move_m, void* move_k, void* stream) {
+  return departure_entry(false, tables, nlev, vx, vy, vz, level_rate, vx_ex, vy_ex, vz_ex,
+                         level_rate_ex, iterations, dt, radius, xi, phi, level, move_m, move_k,
+                         stream);
+}
+
+int sht_sl_departure_newton(const sht_sl_tables* tables, int nlev, const void* vx,
+                            const void* vy, const void* vz, const void* level_rate,
+                            const void* vx_ex, const void* vy_ex, const void* vz_ex,
+                            const void* level_rate_ex, int iterations, double dt, double radius,
+                            void* xi, void* phi, void* level, void* move_m, void* move_k,
+                            void* stream) {
+  return departure_entry(true, tables, nlev, vx, vy, vz, level_rate, vx_ex, vy_ex, vz_ex,
+                         level_rate_ex, iterations, dt, radius, xi, phi, level, move_m, move_k,
+                         stream);
 }
 
 }  // extern "C"

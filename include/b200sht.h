@@ -340,6 +340,19 @@ int sht_sl_departure(const sht_sl_tables* tables, int nlev, const void* vx, cons
                      const void* vy_ex, const void* vz_ex, const void* level_rate_ex,
                      int iterations, double dt, double radius, void* xi, void* phi,
                      void* level, void* move_m, void* move_k, void* stream);
+/* The same search solved by Newton's method (the reference's opt-in
+ * "newton" solver of trajectory.departure_points): per iteration the
+ * residual of the fixed-point map in the local east / north / level frame
+ * and the trilinear interpolant's Jacobian, (I - M) d = r solved directly,
+ * the plain step where the system is near-singular, at a pole, or the
+ * residual stopped shrinking.  Same arguments and fixed point as
+ * sht_sl_departure. */
+int sht_sl_departure_newton(const sht_sl_tables* tables, int nlev, const void* vx,
+                            const void* vy, const void* vz, const void* level_rate,
+                            const void* vx_ex, const void* vy_ex, const void* vz_ex,
+                            const void* level_rate_ex, int iterations, double dt, double radius,
+                            void* xi, void* phi, void* level, void* move_m, void* move_k,
+                            void* stream);
 
 /* Fused right-hand-side kernels of the dycore step (the reference's
  * spectral/fused.py momentum_bernoulli_kernel, tracer_flux_kernel,

@@ -233,9 +233,33 @@ def test_departure_errors_and_rest_state():
     with pytest.raises(ValueError, match="at least one iteration"):
         departure_points(wind, tables, 300.0, iterations=0)
     with pytest.raises(ValueError, match="not built"):
-        departure_points(wind, tables, 300.0, solver="newton")
+        departure_points(wind, tables, 300.0, solver="newton_ls")
     with pytest.raises(ValueError, match="must be one of"):
         departure_points(wind, tables, 300.0, solver="rk4")
     with pytest.raises(ValueError, match="must all be"):
         departure_points(wind, tables, 300.0,
                          extrapolated=CartesianWind(zero[:4], zero, zero, zero))
+
+
+@pytest.mark.parametrize("tag", ["f64", "f32"])
+def test_newton_search_reaches_the_fixed_point(tag):
+    """Newton's method and the fixed-point pass solve one equation: a long
+    fixed-point run and a short Newton run on a rotation across both poles
+    (900 s steps, 48 x 96 x 8) agree, and Newton's last move is small."""
+    from b200sht.semilag import CartesianWind, SphericalGridTables, departure_points
+    from oracle import sl_gather as O
+
+    nlat, nlon, nlev = 48, 96, 8
+    lat = np.sort(np.arcsin(np.polynomial.legendre.leggauss(nlat)[0]))
+    dtype = np.float64 if tag == "f64" else np.float32
+    wind = O.rotation_wind(lat, nlon, nlev, speed=60.0, seed=4, dtype=dtype)
+    tables = SphericalGridTables.create(_grid(lat, nlon), dtype=DT[tag])
+    w = CartesianWind(*[torch.as_tensor(a, device="cuda") for a in wind])
+    fp, _ = departure_points(w, tables, 900.0, iterations=30)
+    nt, diag = departure_points(w, tables, 900.0, iterations=6, solver="newton")
+    tol = 1e-9 if tag == "f64" else 2e-5
+    assert float((nt.phi - fp.phi).abs().max()) < tol
+    dxi = (nt.xi - fp.xi).abs().cpu().numpy()
+    assert np.max(np.minimum(dxi, nlon - dxi)) < tol * nlon
+    assert float((nt.level - fp.level).abs().max()) < tol * nlev
+    assert diag.move_max_cells < (1e-6 if tag == "f64" else 1e-3)
