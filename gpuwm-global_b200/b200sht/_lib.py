@@ -97,6 +97,15 @@ SIGNATURES = {
                                         ctypes.c_int, _D, _D, _P, _P, _P, _P, _P, _P]),
     "sht_sl_departure_newton": (ctypes.c_int, [_P, ctypes.c_int, _P, _P, _P, _P, _P, _P, _P, _P,
                                                ctypes.c_int, _D, _D, _P, _P, _P, _P, _P, _P]),
+    "sht_sl_window_create": (ctypes.c_int, [_P, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                            ctypes.c_int, ctypes.POINTER(_P)]),
+    "sht_sl_window_destroy": (ctypes.c_int, [_P]),
+    "sht_sl_window_escape": (ctypes.c_int, [_P, ctypes.c_int, ctypes.POINTER(ctypes.c_int), _P]),
+    "sht_sl_gather_band": (ctypes.c_int, [_P, ctypes.c_int, ctypes.c_int, ctypes.c_int, _P, _I64,
+                                          ctypes.c_int, _P, _P, _P, _P, _P, _P]),
+    "sht_sl_departure_band": (ctypes.c_int, [_P, ctypes.c_int, ctypes.c_int, _P, _P, _P, _P, _P,
+                                             _P, _P, _P, ctypes.c_int, _D, _D, _P, _P, _P, _P,
+                                             _P, _P]),
     "sht_rhs_momentum_bernoulli": (ctypes.c_int, [ctypes.c_int, _I64, _I64] + [_P] * 11
                                    + [_D, _P, _P, _P, _P]),
     "sht_rhs_tracer_flux": (ctypes.c_int, [ctypes.c_int, _I64, _I64, _I64] + [_P] * 7),

@@ -10,9 +10,10 @@ argument meaning and the same ``ValueError`` wording; the interpolation and
 the search run in ``libb200sht.so`` (``sht_sl_gather``,
 ``sht_sl_gather_linear``, ``sht_sl_departure``).  Arrays are CUDA tensors:
 fields and departure coordinates ``(nlev, nlat, nlon)`` in the tables'
-dtype (float32 or float64).  The whole-grid form only: a latitude-band
-window (the reference's ``BandWindow``) is not part of this engine, whose
-B200 holds every level and row of a T511 state at once.
+dtype (float32 or float64).  Latitude-band windows (the reference's
+``BandWindow``, ``HaloEscape``, ``SphericalGridTables.window``) give the
+banded step's gathers and searches over a band's rows from fields that hold
+the band and its halo (``sht_sl_gather_band``, ``sht_sl_departure_band``).
 """
 from __future__ import annotations
 
@@ -103,6 +104,16 @@ class SphericalGridTables:
         """``a * 2*pi / nlon``: one zonal cell at the equator."""
         return self.radius_m * self.dlam
 
+    def window(self, source: slice, arrival: slice) -> "BandWindow":
+        """The tables of one latitude band read through its row halo
+        (cached per (held rows, band rows))."""
+        key = (int(source.start), int(source.stop), int(arrival.start), int(arrival.stop))
+        cache = self.__dict__.setdefault("_windows", {})
+        win = cache.get(key)
+        if win is None:
+            win = cache[key] = BandWindow.create(self, source, arrival)
+        return win
+
     def host_tables(self, order: int = 4) -> dict:
         """float64 host copies of one width's tables (for checks)."""
         rows, bins = ctypes.c_int(), ctypes.c_int()
@@ -123,6 +134,80 @@ class SphericalGridTables:
         return out
 
 
+class HaloEscape(ValueError):
+    """A departure point, or a trajectory iterate, read a latitude row the
+    band does not hold (the reference's tables.HaloEscape)."""
+
+    def __init__(self, window: "BandWindow", what: str):
+        self.window = window
+        super().__init__(
+            f"the semi-Lagrangian {what} of latitude rows {window.arrival.start}.."
+            f"{window.arrival.stop} read a row outside the rows {window.source.start}.."
+            f"{window.source.stop} the band holds: a departure point left the band's row "
+            "halo, and reading on would return a value from a row the band does not have")
+
+
+class BandWindow:
+    """One latitude band of the semi-Lagrangian step (``arrival`` rows) and
+    the rows its fields hold (``source``, the band plus a row halo)."""
+
+    def __init__(self, tables, source: slice, arrival: slice, handle):
+        self.tables = tables
+        self.source = source
+        self.arrival = arrival
+        self._handle = handle
+
+    @classmethod
+    def create(cls, tables: SphericalGridTables, source: slice, arrival: slice) -> "BandWindow":
+        s0, s1, a0, a1 = int(source.start), int(source.stop), int(arrival.start), int(arrival.stop)
+        handle = ctypes.c_void_p()
+        with torch.cuda.device(tables.device):
+            _lib.call("sht_sl_window_create", tables._handle, s0, s1, a0, a1, ctypes.byref(handle))
+        return cls(tables, slice(s0, s1), slice(a0, a1), handle)
+
+    def __del__(self):
+        handle = getattr(self, "_handle", None)
+        if handle is not None and handle.value and _lib._lib is not None:
+            _lib._lib.sht_sl_window_destroy(handle)
+            self._handle = None
+
+    def clear_escape(self) -> None:
+        """Lower the escape flag before a band's kernels run."""
+        _lib.call("sht_sl_window_escape", self._handle, 1, None, _stream())
+
+    def raise_if_escaped(self, what: str) -> None:
+        """Refuse by name if a band kernel since clear_escape read a row the
+        band does not hold (one device read, which waits for the stream)."""
+        flag = ctypes.c_int(0)
+        _lib.call("sht_sl_window_escape", self._handle, 0, ctypes.byref(flag), _stream())
+        if flag.value:
+            raise HaloEscape(self, what)
+
+    @property
+    def source_rows(self) -> int:
+        return int(self.source.stop - self.source.start)
+
+    @property
+    def arrival_rows(self) -> int:
+        return int(self.arrival.stop - self.arrival.start)
+
+    @property
+    def lead(self) -> int:
+        """The band's first row's index inside the held rows."""
+        return int(self.arrival.start - self.source.start)
+
+    @property
+    def local(self) -> slice:
+        """The band's rows as a slice of the held rows."""
+        return slice(self.lead, self.lead + self.arrival_rows)
+
+    def arrival_shape(self, nlev: int) -> tuple[int, int, int]:
+        return int(nlev), self.arrival_rows, int(self.tables.nlon)
+
+    def source_shape(self, nlev: int) -> tuple[int, int, int]:
+        return int(nlev), self.source_rows, int(self.tables.nlon)
+
+
 @dataclass(frozen=True)
 class Stencil:
     """Departure coordinates of every arrival point of one grid: ``xi`` in
@@ -133,6 +218,9 @@ class Stencil:
     phi: Any
     level: Any
     tables: SphericalGridTables
+    #: The latitude band these arrival points are and the rows its source
+    #: fields hold, or None for the whole grid.
+    window: "BandWindow | None" = None
 
     @property
     def shape(self) -> tuple[int, int, int]:
@@ -140,15 +228,19 @@ class Stencil:
 
     @property
     def source_shape(self) -> tuple[int, int, int]:
-        return self.shape
+        if self.window is None:
+            return self.shape
+        return self.window.source_shape(self.shape[0])
 
     def __post_init__(self) -> None:
         shape = tuple(int(s) for s in self.xi.shape)
         if len(shape) != 3:
             raise ValueError(f"departure coordinates must be (nlev, nlat, nlon), got {shape}")
-        if shape[1:] != self.tables.shape:
+        expected = (self.tables.shape if self.window is None
+                    else (self.window.arrival_rows, self.tables.nlon))
+        if shape[1:] != expected:
             raise ValueError(
-                f"departure coordinates are {shape[1:]} where {self.tables.shape} were "
+                f"departure coordinates are {shape[1:]} where {expected} were "
                 f"expected on a {self.tables.shape} grid")
         if shape[0] < 4:
             raise ValueError(f"a four-point vertical stencil needs nlev >= 4, got {shape[0]}")
@@ -228,7 +320,8 @@ def _source_block(chunk):
 
 
 def gather_batch(fields: Sequence[torch.Tensor], stencil: Stencil, *, monotone: Any = True,
-                 batch: int = DEFAULT_BATCH, deficit: bool = False, order: int = 4) -> list:
+                 batch: int = DEFAULT_BATCH, deficit: bool = False, order: int = 4,
+                 defer_escape: bool = False) -> list:
     """Read every field at the stencil's departure points (tricubic for
     ``order = 4``, quintic horizontal for 6).  ``deficit=True`` (with a
     limiter) returns ``(value, clip_deficit)`` pairs."""
@@ -246,6 +339,9 @@ def gather_batch(fields: Sequence[torch.Tensor], stencil: Stencil, *, monotone: 
             f"{stencil.tables.nlat}; the six-point tables were not built")
     nlev = stencil.shape[0]
     lim = _lib.SHT_SL_QUASI_MONOTONE if limiter == "quasi_monotone" else _lib.SHT_SL_NONE
+    window = stencil.window
+    if window is not None and not defer_escape:
+        window.clear_escape()
     out: list = []
     for start in range(0, len(fields), int(batch)):
         chunk = fields[start:start + int(batch)]
@@ -253,7 +349,9 @@ def gather_batch(fields: Sequence[torch.Tensor], stencil: Stencil, *, monotone: 
         count = len(chunk)
         dst = torch.empty((count, *stencil.shape), dtype=src.dtype, device=src.device)
         cut = torch.empty_like(dst) if deficit else None
-        _lib.call("sht_sl_gather", stencil.tables._handle, order, lim, 1 if deficit else 0,
+        name, handle = (("sht_sl_gather", stencil.tables._handle) if window is None
+                        else ("sht_sl_gather_band", window._handle))
+        _lib.call(name, handle, order, lim, 1 if deficit else 0,
                   _ptr(src), count, nlev, _ptr(stencil.xi), _ptr(stencil.phi),
                   _ptr(stencil.level), _ptr(dst), _ptr(cut) if cut is not None else None,
                   _stream())
@@ -261,6 +359,8 @@ def gather_batch(fields: Sequence[torch.Tensor], stencil: Stencil, *, monotone: 
             out.extend((dst[i], cut[i]) for i in range(count))
         else:
             out.extend(dst[i] for i in range(count))
+    if window is not None and not defer_escape:
+        window.raise_if_escaped("gather")
     return out
 
 
@@ -274,6 +374,10 @@ def gather_linear_batch(fields: Sequence[torch.Tensor], stencil: Stencil, *,
     """Every field read trilinearly inside the cubic gather's limiter cell."""
     if not fields:
         return []
+    if stencil.window is not None:
+        raise ValueError(
+            "the trilinear gather reads the whole grid's rows; assemble the whole stencil "
+            "before asking for it")
     _check_fields(fields, stencil)
     if int(batch) < 1:
         raise ValueError("batch must be >= 1")
@@ -383,11 +487,14 @@ def meridional_grid_length_m(tables: SphericalGridTables) -> np.ndarray:
 
 
 def _diagnostics(stencil: Stencil, move_m, move_k, tables, dt_s, iterations):
-    nlev, nlat, nlon = stencil.shape
+    nlev, nrows, nlon = stencil.shape
+    nlat = tables.nlat
+    rows = slice(0, nlat) if stencil.window is None else stencil.window.arrival
     dt = tables.dtype
     dev = tables.device
-    cell = torch.as_tensor(meridional_grid_length_m(tables), dtype=dt, device=dev)[None, :, None]
-    lat = torch.as_tensor(tables.host_tables(4)["lat_ext"][2:nlat + 2], dtype=dt,
+    cell = torch.as_tensor(meridional_grid_length_m(tables)[rows], dtype=dt,
+                           device=dev)[None, :, None]
+    lat = torch.as_tensor(tables.host_tables(4)["lat_ext"][2:nlat + 2][rows], dtype=dt,
                           device=dev)[None, :, None]
     index = torch.arange(nlon, dtype=dt, device=dev)[None, None, :]
     lev0 = torch.arange(nlev, dtype=dt, device=dev)[:, None, None]
@@ -415,14 +522,19 @@ def search_into(tables: SphericalGridTables, fields: Sequence[torch.Tensor], ite
 
 def departure_points(wind: CartesianWind, tables: SphericalGridTables, dt_s: float, *,
                      iterations: int = 3, extrapolated: CartesianWind | None = None,
+                     window: BandWindow | None = None, defer_escape: bool = False,
                      solver: str = "fixed_point") -> tuple[Stencil, TrajectoryDiagnostics]:
-    """The departure point of every arrival point of the grid (the
-    fixed-point search, all iterations in one launch)."""
+    """The departure point of every arrival point of the grid (all
+    iterations in one launch).  With a ``window`` the arrival points are the
+    band's rows: ``wind`` holds the band and its halo, ``extrapolated`` the
+    band's own rows (by default those rows of ``wind``); a search that reads
+    a row the band does not hold is refused by name (HaloEscape)."""
     shape = wind.shape
     nlev, nrows, nlon = shape
-    if (nrows, nlon) != tables.shape:
-        raise ValueError(f"the wind is {(nrows, nlon)} where {tables.shape} rows were expected "
-                         f"on a {tables.shape} grid")
+    held = tables.nlat if window is None else window.source_rows
+    if (nrows, nlon) != (held, tables.nlon):
+        raise ValueError(f"the wind is {(nrows, nlon)} where {(held, tables.nlon)} rows were "
+                         f"expected on a {tables.shape} grid")
     if nlev < 4:
         raise ValueError(f"nlev >= 4 is required, got {nlev}")
     if int(iterations) < 1:
@@ -434,19 +546,31 @@ def departure_points(wind: CartesianWind, tables: SphericalGridTables, dt_s: flo
     if solver == "newton_ls":
         raise ValueError(f"trajectory solver {solver!r} is not built in this engine; the "
                          "fixed-point pass and 'newton' are")
+    out_shape = shape if window is None else window.arrival_shape(nlev)
     ex = wind if extrapolated is None else extrapolated
-    for name, arr in (("wind", wind), ("extrapolated", ex)):
+    if window is not None and extrapolated is None:
+        ex = CartesianWind(*(f[:, window.local].contiguous() for f in wind.arrays()))
+    for name, arr, want in (("wind", wind, shape), ("extrapolated", ex, out_shape)):
         for field in arr.arrays():
-            if tuple(int(s) for s in field.shape) != shape:
-                raise ValueError(f"{name} fields must all be {shape}")
+            if tuple(int(s) for s in field.shape) != want:
+                raise ValueError(f"{name} fields must all be {want}")
             if field.dtype != tables.dtype:
                 raise ValueError(f"{name} is {field.dtype} where the grid tables were built for "
                                  f"{tables.dtype}")
             if not field.is_cuda:
                 raise ValueError(f"{name} fields must be CUDA tensors")
     ins = [f.contiguous() for f in wind.arrays()] + [f.contiguous() for f in ex.arrays()]
-    outs = [torch.empty(shape, dtype=tables.dtype, device=ins[0].device) for _ in range(5)]
-    search_into(tables, ins, int(iterations), float(dt_s), outs, newton=solver == "newton")
+    outs = [torch.empty(out_shape, dtype=tables.dtype, device=ins[0].device) for _ in range(5)]
+    if window is None:
+        search_into(tables, ins, int(iterations), float(dt_s), outs, newton=solver == "newton")
+    else:
+        if not defer_escape:
+            window.clear_escape()
+        _lib.call("sht_sl_departure_band", window._handle, 1 if solver == "newton" else 0, nlev,
+                  *[_ptr(t) for t in ins], int(iterations), float(dt_s), float(tables.radius_m),
+                  *[_ptr(t) for t in outs], _stream())
+        if not defer_escape:
+            window.raise_if_escaped("departure-point search")
     xi, phi, lev, move_m, move_k = outs
-    stencil = Stencil(xi=xi, phi=phi, level=lev, tables=tables)
+    stencil = Stencil(xi=xi, phi=phi, level=lev, tables=tables, window=window)
     return stencil, _diagnostics(stencil, move_m, move_k, tables, dt_s, iterations)

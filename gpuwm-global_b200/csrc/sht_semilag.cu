@@ -61,6 +61,19 @@ struct sht_sl_tables {
   SlWidth w4, w6;  // w6 empty when nlat < 6
 };
 
+// One latitude band of a semi-Lagrangian step: arrival rows [a0, a1) read
+// from fields that hold rows [s0, s1) (the band and its halo).  The row
+// offsets of both stencil widths are rebased to the held rows (-1 for a
+// row outside them); the weights and brackets stay the whole grid's, so a
+// band computes the whole-grid values bit for bit.
+struct sht_sl_window {
+  const sht_sl_tables* tables = nullptr;
+  int s0 = 0, s1 = 0, a0 = 0, a1 = 0;
+  int32_t* d_rowoff4 = nullptr;
+  int32_t* d_rowoff6 = nullptr;
+  int* d_esc = nullptr;  // escape flag
+};
+
 namespace sht {
 namespace {
 
@@ -154,26 +167,45 @@ struct SlArgs {
   const int32_t* mlut;
   const int32_t* rowoff;
   const int32_t* rowshift;
-  T* out;          // [F][nk][nj][ni]
+  T* out;          // [F][nk][nja][ni]
   T* cut;          // clip deficit (or null)
   int F, nk, nj, ni, nb;
   T lut_scale;
+  // Latitude-band form: the sources hold njs rows (the band and its halo),
+  // the coordinates and outputs the band's nja rows; rowoff then maps an
+  // extended row to its offset inside the held rows, or to -1 for a row
+  // the band does not hold (a read of it sets *esc and reads row 0).  On
+  // the whole grid njs = nja = nj and esc is null.
+  int njs, nja;
+  int* esc;
 };
+
+// The in-plane offset of extended row r: an offset of -1 (a row outside a
+// band's held rows) raises the escape flag and reads the first held row,
+// so the access stays in bounds while the caller refuses the result.
+__device__ __forceinline__ int held_row(const int32_t* __restrict__ rowoff, int r, int* esc) {
+  int ro = __ldg(rowoff + r);
+  if (ro < 0) {
+    if (esc) atomicOr(esc, 1);
+    ro = 0;
+  }
+  return ro;
+}
 
 // --------------------------------------------------------------- gather
 template <typename T, int NH, bool QM, bool DEF>
 __global__ void __launch_bounds__(256, (sizeof(T) == 4 && NH == 4) ? 3 : 2) sl_gather_kernel(const SlArgs<T> a) {
   constexpr int G = NH / 2 - 1;  // zonal lead and meridional start offset
   constexpr int MID = NH / 2 - 1;
-  const int plane = a.nj * a.ni;
-  const int64_t n = (int64_t)a.nk * plane;
+  const int plane = a.njs * a.ni;              // a held source level
+  const int64_t n = (int64_t)a.nk * a.nja * a.ni;  // arrival points
   // Threads walk the points row by row with the levels of a row together:
   // a source level plane is read by the stencils of four arrival levels,
   // which then run at the same time and find it in L2 (level-major order
   // brought every plane in from DRAM about four times).
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n) return;
-  const int64_t gid = point_index(t, a.nk, a.nj, a.ni);
+  const int64_t gid = point_index(t, a.nk, a.nja, a.ni);
 
   const T p = min(max(a.phi[gid], T(-kHalfPi)), T(kHalfPi));
   const T xk = min(max(a.lev[gid], T(-0.5)), T(a.nk) - T(0.5));
@@ -231,7 +263,7 @@ __global__ void __launch_bounds__(256, (sizeof(T) == 4 && NH == 4) ? 3 : 2) sl_g
   int adr[NH][NH];  // in-plane offsets of the stencil's taps
 #pragma unroll
   for (int m = 0; m < NH; ++m) {
-    const int ro = __ldg(a.rowoff + sst + m);
+    const int ro = held_row(a.rowoff, sst + m, a.esc);
     const bool sh = __ldg(a.rowshift + sst + m) != 0;
 #pragma unroll
     for (int q = 0; q < NH; ++q) adr[m][q] = ro + (sh ? colh[q] : col[q]);
@@ -247,7 +279,8 @@ __global__ void __launch_bounds__(256, (sizeof(T) == 4 && NH == 4) ? 3 : 2) sl_g
     for (int q = MID; q <= MID + 1; ++q)
       if (m == cy && q == cx) centre = adr[m][q];
 
-  const int64_t fstride = n;
+  const int64_t fstride = n;                          // output field stride
+  const int64_t sstride = (int64_t)a.nk * plane;       // source field stride
   const int64_t cofs = (int64_t)kn * plane + centre;
   // NB fields per pass share every address; their taps are in flight
   // together, two levels at a time (a fully unrolled level loop holds every
@@ -259,7 +292,7 @@ __global__ void __launch_bounds__(256, (sizeof(T) == 4 && NH == 4) ? 3 : 2) sl_g
     T base[NB], acc[NB], lo[NB], hi[NB], f_edge[NB], f_next[NB];
 #pragma unroll
     for (int b = 0; b < NB; ++b) {
-      s[b] = a.src + (f0 + b) * fstride;
+      s[b] = a.src + (f0 + b) * sstride;
       base[b] = __ldg(s[b] + cofs);
       acc[b] = lo[b] = hi[b] = f_edge[b] = f_next[b] = T(0);
     }
@@ -385,6 +418,12 @@ struct SlDepArgs {
   int iters, nk, nj, ni, nb;
   double dlam;  // 2 pi / nlon (the arrival longitudes are formed in double)
   T dt, radius, inv_dlam, lut_scale;
+  // Latitude-band form: the advecting wind holds njs rows starting `lead`
+  // rows above the first arrival row, grid row ja0; the extrapolated wind
+  // and the outputs hold the nja arrival rows.  Whole grid: njs = nja = nj,
+  // ja0 = lead = 0, esc null.
+  int njs, nja, ja0, lead;
+  int* esc;
 };
 
 template <typename T>
@@ -404,13 +443,13 @@ __device__ __forceinline__ void trilinear4(const SlDepArgs<T>& a, T lam, T phid,
   const int m0 = bracket<T>(p, a.lat_ext, a.mlut, a.nb, a.nj, 1, a.lut_scale);
   const T la = __ldg(a.lat_ext + m0), lb = __ldg(a.lat_ext + m0 + 1);
   const T ay = (p - la) / (lb - la);
-  const int r0 = __ldg(a.rowoff + m0), r1 = __ldg(a.rowoff + m0 + 1);
+  const int r0 = held_row(a.rowoff, m0, a.esc), r1 = held_row(a.rowoff, m0 + 1, a.esc);
   const bool s0 = __ldg(a.rowshift + m0) != 0, s1 = __ldg(a.rowshift + m0 + 1) != 0;
   const int i00 = r0 + (s0 ? h0 : c0), i01 = r0 + (s0 ? h1 : c1);
   const int i10 = r1 + (s1 ? h0 : c0), i11 = r1 + (s1 ? h1 : c1);
   const int k0 = min(max((int)floor(xk), 0), a.nk - 2);
   const T az = xk - T(k0);
-  const int64_t plane = (int64_t)a.nj * a.ni;
+  const int64_t plane = (int64_t)a.njs * a.ni;
   const int64_t o0 = (int64_t)k0 * plane, o1 = o0 + plane;
   const T bx = T(1) - ax, by = T(1) - ay, bz = T(1) - az;
   const T* f[4] = {a.vx, a.vy, a.vz, a.sv};
@@ -428,31 +467,33 @@ __device__ __forceinline__ void trilinear4(const SlDepArgs<T>& a, T lam, T phid,
 
 template <typename T>
 __global__ void __launch_bounds__(256) sl_departure_kernel(const SlDepArgs<T> a) {
-  const int64_t n = (int64_t)a.nk * a.nj * a.ni;
+  const int64_t n = (int64_t)a.nk * a.nja * a.ni;
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n) return;
-  const int64_t gid = point_index(t, a.nk, a.nj, a.ni);  // rows with their levels together
-  const int plane = a.nj * a.ni;
+  const int64_t gid = point_index(t, a.nk, a.nja, a.ni);  // rows with their levels together
+  const int plane = a.nja * a.ni;
   const int k = (int)(gid / plane);
   const int rem = (int)(gid - (int64_t)k * plane);
   const int j = rem / a.ni, i = rem - j * a.ni;
+  // the arrival point in the advecting wind's held rows
+  const int64_t here = ((int64_t)k * a.njs + (j + a.lead)) * a.ni + i;
   // the arrival point: table latitude and i * dlam (formed in double, as
   // the host computes the grid's longitudes), both in T
-  const T lat = __ldg(a.lat_ext + j + 2);
+  const T lat = __ldg(a.lat_ext + a.ja0 + j + 2);
   const T lon = T((double)i * a.dlam);
   const T sph = sin(lat), cph = cos(lat), sla = sin(lon), cla = cos(lon);
   const T ax = cph * cla, ay = cph * sla, az = sph;
   const T inv_r = T(1) / a.radius;
   const T dt = a.dt, hdt = T(0.5) * a.dt;
-  T qx = ax - dt * a.vx[gid] * inv_r;
-  T qy = ay - dt * a.vy[gid] * inv_r;
-  T qz = az - dt * a.vz[gid] * inv_r;
+  T qx = ax - dt * a.vx[here] * inv_r;
+  T qy = ay - dt * a.vy[here] * inv_r;
+  T qz = az - dt * a.vz[here] * inv_r;
   T nrm = sqrt(qx * qx + qy * qy + qz * qz);
   qx /= nrm;
   qy /= nrm;
   qz /= nrm;
   const T klo = T(-0.5), khi = T(a.nk) - T(0.5);
-  T qk = min(max(T(k) - dt * a.sv[gid], klo), khi);
+  T qk = min(max(T(k) - dt * a.sv[here], klo), khi);
   const T ex = a.vxe[gid], ey = a.vye[gid], ez = a.vze[gid], es = a.sve[gid];
   T last_m = T(0), last_k = T(0);
   for (int it = 0; it < a.iters; ++it) {
@@ -516,13 +557,13 @@ __device__ __forceinline__ void trilinear4_grad(const SlDepArgs<T>& a, T lam, T 
   const T la = __ldg(a.lat_ext + m0), lb = __ldg(a.lat_ext + m0 + 1);
   const T inv_dphi = T(1) / (lb - la);
   const T ay = (p - la) * inv_dphi;
-  const int r0 = __ldg(a.rowoff + m0), r1 = __ldg(a.rowoff + m0 + 1);
+  const int r0 = held_row(a.rowoff, m0, a.esc), r1 = held_row(a.rowoff, m0 + 1, a.esc);
   const bool s0 = __ldg(a.rowshift + m0) != 0, s1 = __ldg(a.rowshift + m0 + 1) != 0;
   const int i00 = r0 + (s0 ? h0 : c0), i01 = r0 + (s0 ? h1 : c1);
   const int i10 = r1 + (s1 ? h0 : c0), i11 = r1 + (s1 ? h1 : c1);
   const int k0 = min(max((int)floor(xk), 0), a.nk - 2);
   const T az = xk - T(k0);
-  const int64_t plane = (int64_t)a.nj * a.ni;
+  const int64_t plane = (int64_t)a.njs * a.ni;
   const int64_t o0 = (int64_t)k0 * plane, o1 = o0 + plane;
   const T bx = T(1) - ax, by = T(1) - ay, bz = T(1) - az;
   const T* f[4] = {a.vx, a.vy, a.vz, a.sv};
@@ -546,26 +587,27 @@ __device__ __forceinline__ void trilinear4_grad(const SlDepArgs<T>& a, T lam, T 
 
 template <typename T>
 __global__ void __launch_bounds__(256) sl_departure_newton_kernel(const SlDepArgs<T> a) {
-  const int64_t n = (int64_t)a.nk * a.nj * a.ni;
+  const int64_t n = (int64_t)a.nk * a.nja * a.ni;
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n) return;
-  const int64_t gid = point_index(t, a.nk, a.nj, a.ni);
-  const int plane = a.nj * a.ni;
+  const int64_t gid = point_index(t, a.nk, a.nja, a.ni);
+  const int plane = a.nja * a.ni;
   const int k = (int)(gid / plane);
   const int rem = (int)(gid - (int64_t)k * plane);
   const int j = rem / a.ni, i = rem - j * a.ni;
-  const T lat = __ldg(a.lat_ext + j + 2);
+  const int64_t here = ((int64_t)k * a.njs + (j + a.lead)) * a.ni + i;
+  const T lat = __ldg(a.lat_ext + a.ja0 + j + 2);
   const T lon = T((double)i * a.dlam);
   const T ax = cos(lat) * cos(lon), ay = cos(lat) * sin(lon), az = sin(lat);
   const T inv_r = T(1) / a.radius;
   const T dt = a.dt, hdt = T(0.5) * a.dt, c = hdt * inv_r;
   // the fixed-point search's first guess
-  T qx = ax - dt * a.vx[gid] * inv_r, qy = ay - dt * a.vy[gid] * inv_r,
-    qz = az - dt * a.vz[gid] * inv_r;
+  T qx = ax - dt * a.vx[here] * inv_r, qy = ay - dt * a.vy[here] * inv_r,
+    qz = az - dt * a.vz[here] * inv_r;
   T nrm = sqrt(qx * qx + qy * qy + qz * qz);
   qx /= nrm; qy /= nrm; qz /= nrm;
   const T klo = T(-0.5), khi = T(a.nk) - T(0.5);
-  T qk = min(max(T(k) - dt * a.sv[gid], klo), khi);
+  T qk = min(max(T(k) - dt * a.sv[here], klo), khi);
   const T ex = a.vxe[gid], ey = a.vye[gid], ez = a.vze[gid], es = a.sve[gid];
   const T cells = T(a.nj) / T(2 * kHalfPi);  // meridional grid lengths per radian
   T last_m = T(0), last_k = T(0), res_prev = T(-1);
@@ -747,6 +789,8 @@ SlArgs<T> make_args(const sht_sl_tables* t, const SlWidth& w, const void* src, i
   a.F = (int)F;
   a.nk = nlev;
   a.nj = t->nlat;
+  a.njs = a.nja = t->nlat;
+  a.esc = nullptr;
   a.ni = t->nlon;
   a.nb = w.bins;
   a.lut_scale = (T)w.lut_scale;
@@ -755,7 +799,7 @@ SlArgs<T> make_args(const sht_sl_tables* t, const SlWidth& w, const void* src, i
 
 template <typename T, int NH>
 void launch_gather(const SlArgs<T>& a, bool qm, bool def, cudaStream_t s) {
-  const int64_t n = (int64_t)a.nk * a.nj * a.ni;
+  const int64_t n = (int64_t)a.nk * a.nja * a.ni;
   const unsigned blocks = (unsigned)div_up(n, 256);
   if (qm && def)
     sl_gather_kernel<T, NH, true, true><<<blocks, 256, 0, s>>>(a);
@@ -865,9 +909,17 @@ int sht_sl_tables_read(const sht_sl_tables* tables, int order, double* lat_ext, 
   });
 }
 
-int sht_sl_gather(const sht_sl_tables* tables, int order, int limiter, int deficit,
-                  const void* src, int64_t fields, int nlev, const void* xi, const void* phi,
-                  const void* level, void* out, void* cut, void* stream) {
+static int departure_entry(bool newton, const sht_sl_window* win, const sht_sl_tables* tables,
+                           int nlev, const void* vx, const void* vy, const void* vz,
+                           const void* level_rate, const void* vx_ex, const void* vy_ex,
+                           const void* vz_ex, const void* level_rate_ex, int iterations,
+                           double dt, double radius, void* xi, void* phi, void* level,
+                           void* move_m, void* move_k, void* stream);
+
+static int gather_entry(const sht_sl_window* win, const sht_sl_tables* tables, int order,
+                        int limiter, int deficit, const void* src, int64_t fields, int nlev,
+                        const void* xi, const void* phi, const void* level, void* out, void* cut,
+                        void* stream) {
   return guarded([&] {
     check_call(tables, src, fields, nlev, xi, phi, level, out);
     SHT_REQUIRE(limiter == SHT_SL_NONE || limiter == SHT_SL_QUASI_MONOTONE,
@@ -882,16 +934,131 @@ int sht_sl_gather(const sht_sl_tables* tables, int order, int limiter, int defic
     }
     const bool qm = limiter == SHT_SL_QUASI_MONOTONE, def = deficit != 0;
     cudaStream_t s = (cudaStream_t)stream;
+    auto band = [&](auto& a) {
+      if (!win) return;
+      a.rowoff = order == 6 ? win->d_rowoff6 : win->d_rowoff4;
+      a.njs = win->s1 - win->s0;
+      a.nja = win->a1 - win->a0;
+      a.esc = win->d_esc;
+    };
     if (tables->prec == SHT_PREC_F64) {
       auto a = make_args<double>(tables, w, src, fields, nlev, xi, phi, level, out, cut);
+      band(a);
       if (order == 6) launch_gather<double, 6>(a, qm, false, s);
       else launch_gather<double, 4>(a, qm, def, s);
     } else {
       auto a = make_args<float>(tables, w, src, fields, nlev, xi, phi, level, out, cut);
+      band(a);
       if (order == 6) launch_gather<float, 6>(a, qm, false, s);
       else launch_gather<float, 4>(a, qm, def, s);
     }
   });
+}
+
+int sht_sl_gather(const sht_sl_tables* tables, int order, int limiter, int deficit,
+                  const void* src, int64_t fields, int nlev, const void* xi, const void* phi,
+                  const void* level, void* out, void* cut, void* stream) {
+  return gather_entry(nullptr, tables, order, limiter, deficit, src, fields, nlev, xi, phi, level,
+                      out, cut, stream);
+}
+
+int sht_sl_window_create(const sht_sl_tables* tables, int s0, int s1, int a0, int a1,
+                         sht_sl_window** out) {
+  return guarded([&] {
+    SHT_REQUIRE(out != nullptr, "null output handle");
+    *out = nullptr;
+    SHT_REQUIRE(tables != nullptr, "null semi-Lagrangian tables");
+    const int nlat = tables->nlat;
+    SHT_REQUIRE(0 <= s0 && s0 <= a0 && a0 < a1 && a1 <= s1 && s1 <= nlat,
+                "a band window holds rows [" + std::to_string(s0) + ", " + std::to_string(s1) +
+                    ") and computes rows [" + std::to_string(a0) + ", " + std::to_string(a1) +
+                    "); the computed rows must lie inside the held rows and both inside the " +
+                    std::to_string(nlat) + " rows of the grid");
+    int dev = 0;
+    SHT_CUDA_OR_THROW(cudaGetDevice(&dev));
+    SHT_REQUIRE(dev == tables->device, "the tables live on another device");
+    auto rebase = [&](const SlWidth& w) {
+      std::vector<int32_t> r(w.rowoff.size());
+      for (size_t e = 0; e < r.size(); ++e) {
+        const int row = w.rowoff[e] / tables->nlon;
+        r[e] = (row >= s0 && row < s1) ? (row - s0) * tables->nlon : -1;
+      }
+      return r;
+    };
+    auto* h = new sht_sl_window;
+    try {
+      h->tables = tables;
+      h->s0 = s0; h->s1 = s1; h->a0 = a0; h->a1 = a1;
+      const auto r4 = rebase(tables->w4);
+      SHT_CUDA_OR_THROW(cudaMalloc(&h->d_rowoff4, r4.size() * sizeof(int32_t)));
+      upload_now(h->d_rowoff4, r4.data(), r4.size() * sizeof(int32_t));
+      if (tables->w6.rows > 0) {
+        const auto r6 = rebase(tables->w6);
+        SHT_CUDA_OR_THROW(cudaMalloc(&h->d_rowoff6, r6.size() * sizeof(int32_t)));
+        upload_now(h->d_rowoff6, r6.data(), r6.size() * sizeof(int32_t));
+      }
+      SHT_CUDA_OR_THROW(cudaMalloc(&h->d_esc, sizeof(int)));
+      SHT_CUDA_OR_THROW(cudaMemset(h->d_esc, 0, sizeof(int)));
+      SHT_CUDA_OR_THROW(cudaDeviceSynchronize());
+    } catch (...) {
+      cudaFree(h->d_rowoff4);
+      cudaFree(h->d_rowoff6);
+      cudaFree(h->d_esc);
+      delete h;
+      throw;
+    }
+    *out = h;
+  });
+}
+
+int sht_sl_window_destroy(sht_sl_window* win) {
+  return guarded([&] {
+    if (!win) return;
+    cudaFree(win->d_rowoff4);
+    cudaFree(win->d_rowoff6);
+    cudaFree(win->d_esc);
+    delete win;
+  });
+}
+
+int sht_sl_window_escape(sht_sl_window* win, int clear, int* escaped, void* stream) {
+  return guarded([&] {
+    SHT_REQUIRE(win != nullptr, "null band window");
+    cudaStream_t s = (cudaStream_t)stream;
+    if (escaped) {
+      int flag = 0;
+      SHT_CUDA_OR_THROW(cudaMemcpyAsync(&flag, win->d_esc, sizeof(int), cudaMemcpyDeviceToHost, s));
+      SHT_CUDA_OR_THROW(cudaStreamSynchronize(s));
+      *escaped = flag;
+    }
+    if (clear) SHT_CUDA_OR_THROW(cudaMemsetAsync(win->d_esc, 0, sizeof(int), s));
+  });
+}
+
+int sht_sl_gather_band(const sht_sl_window* win, int order, int limiter, int deficit,
+                       const void* src, int64_t fields, int nlev, const void* xi,
+                       const void* phi, const void* level, void* out, void* cut, void* stream) {
+  if (win == nullptr) {
+    sht::set_error("null band window");
+    return SHT_ERR_ARG;
+  }
+  return gather_entry(win, win->tables, order, limiter, deficit, src, fields, nlev, xi, phi,
+                      level, out, cut, stream);
+}
+
+int sht_sl_departure_band(const sht_sl_window* win, int newton, int nlev, const void* vx,
+                          const void* vy, const void* vz, const void* level_rate,
+                          const void* vx_ex, const void* vy_ex, const void* vz_ex,
+                          const void* level_rate_ex, int iterations, double dt, double radius,
+                          void* xi, void* phi, void* level, void* move_m, void* move_k,
+                          void* stream) {
+  if (win == nullptr) {
+    sht::set_error("null band window");
+    return SHT_ERR_ARG;
+  }
+  return departure_entry(newton != 0, win, win->tables, nlev, vx, vy, vz, level_rate, vx_ex,
+                         vy_ex, vz_ex, level_rate_ex, iterations, dt, radius, xi, phi, level,
+                         move_m, move_k, stream);
 }
 
 int sht_sl_gather_linear(const sht_sl_tables* tables, const void* src, int64_t fields, int nlev,
@@ -914,7 +1081,8 @@ int sht_sl_gather_linear(const sht_sl_tables* tables, const void* src, int64_t f
   });
 }
 
-static int departure_entry(bool newton, const sht_sl_tables* tables, int nlev, const void* vx,
+static int departure_entry(bool newton, const sht_sl_window* win, const sht_sl_tables* tables,
+                           int nlev, const void* vx,
                            const void* vy, const void* vz, const void* level_rate,
                            const void* vx_ex, const void* vy_ex, const void* vz_ex,
                            const void* level_rate_ex, int iterations, double dt, double radius,
@@ -930,7 +1098,8 @@ static int departure_entry(bool newton, const sht_sl_tables* tables, int nlev, c
     SHT_REQUIRE(std::isfinite(dt) && std::isfinite(radius) && radius > 0.0,
                 "dt and radius must be finite, radius positive");
     const SlWidth& w = tables->w4;
-    const int64_t n = (int64_t)nlev * tables->nlat * tables->nlon;
+    const int rows_out = win ? win->a1 - win->a0 : tables->nlat;
+    const int64_t n = (int64_t)nlev * rows_out * tables->nlon;
     const unsigned blocks = (unsigned)div_up(n, 256);
     cudaStream_t s = (cudaStream_t)stream;
     auto fill = [&](auto* a) {
@@ -948,6 +1117,17 @@ static int departure_entry(bool newton, const sht_sl_tables* tables, int nlev, c
       const double dlam = 2.0 * kPi / tables->nlon;
       a->dt = (T)dt; a->radius = (T)radius; a->dlam = dlam; a->inv_dlam = (T)(1.0 / dlam);
       a->lut_scale = (T)w.lut_scale;
+      a->njs = a->nja = tables->nlat;
+      a->ja0 = a->lead = 0;
+      a->esc = nullptr;
+      if (win) {
+        a->rowoff = win->d_rowoff4;
+        a->njs = win->s1 - win->s0;
+        a->nja = win->a1 - win->a0;
+        a->ja0 = win->a0;
+        a->lead = win->a0 - win->s0;
+        a->esc = win->d_esc;
+      }
     };
     if (tables->prec == SHT_PREC_F64) {
       SlDepArgs<double> a;
@@ -969,7 +1149,7 @@ int sht_sl_departure(const sht_sl_tables* tables, int nlev, const void* vx, cons
                      const void* vy_ex, const void* vz_ex, const void* level_rate_ex,
                      int iterations, double dt, double radius, void* xi, void* phi,
                      void* level, void* move_m, void* move_k, void* stream) {
-  return departure_entry(false, tables, nlev, vx, vy, vz, level_rate, vx_ex, vy_ex, vz_ex,
+  return departure_entry(false, nullptr, tables, nlev, vx, vy, vz, level_rate, vx_ex, vy_ex, vz_ex,
                          level_rate_ex, iterations, dt, radius, xi, phi, level, move_m, move_k,
                          stream);
 }
@@ -980,7 +1160,7 @@ int sht_sl_departure_newton(const sht_sl_tables* tables, int nlev, const void* v
                             const void* level_rate_ex, int iterations, double dt, double radius,
                             void* xi, void* phi, void* level, void* move_m, void* move_k,
                             void* stream) {
-  return departure_entry(true, tables, nlev, vx, vy, vz, level_rate, vx_ex, vy_ex, vz_ex,
+  return departure_entry(true, nullptr, tables, nlev, vx, vy, vz, level_rate, vx_ex, vy_ex, vz_ex,
                          level_rate_ex, iterations, dt, radius, xi, phi, level, move_m, move_k,
                          stream);
 }

@@ -314,6 +314,29 @@ typedef struct sht_sl_tables sht_sl_tables;
 int sht_sl_tables_create(int nlat, int nlon, const double* lat_rad, const double* lon_rad,
                          int precision, sht_sl_tables** out);
 int sht_sl_tables_destroy(sht_sl_tables* tables);
+/* Latitude-band windows (the reference's semilag/tables.py BandWindow):
+ * arrival rows [a0, a1) of a step read from fields that hold only rows
+ * [s0, s1), the band and a row halo.  sht_sl_gather_band and
+ * sht_sl_departure_band take coordinates / outputs / extrapolated wind of
+ * the a1 - a0 arrival rows and sources / advecting wind of the s1 - s0 held
+ * rows; brackets and weights are the whole grid's, so the values equal the
+ * whole-grid calls' on those rows.  A read of a row outside the held rows
+ * raises the window's escape flag (and reads the first held row instead);
+ * sht_sl_window_escape reads it (synchronising `stream`) and/or clears it. */
+typedef struct sht_sl_window sht_sl_window;
+int sht_sl_window_create(const sht_sl_tables* tables, int s0, int s1, int a0, int a1,
+                         sht_sl_window** out);
+int sht_sl_window_destroy(sht_sl_window* window);
+int sht_sl_window_escape(sht_sl_window* window, int clear, int* escaped, void* stream);
+int sht_sl_gather_band(const sht_sl_window* window, int order, int limiter, int deficit,
+                       const void* src, int64_t fields, int nlev, const void* xi,
+                       const void* phi, const void* level, void* out, void* cut, void* stream);
+int sht_sl_departure_band(const sht_sl_window* window, int newton, int nlev, const void* vx,
+                          const void* vy, const void* vz, const void* level_rate,
+                          const void* vx_ex, const void* vy_ex, const void* vz_ex,
+                          const void* level_rate_ex, int iterations, double dt, double radius,
+                          void* xi, void* phi, void* level, void* move_m, void* move_k,
+                          void* stream);
 /* Host copies of one width's tables (order 4 or 6): lat_ext[rows],
  * mrden[(nlat + 1) * order], mlut[bins], rowoff[rows], rowshift[rows];
  * any pointer may be null. */

@@ -263,3 +263,87 @@ def test_newton_search_reaches_the_fixed_point(tag):
     assert np.max(np.minimum(dxi, nlon - dxi)) < tol * nlon
     assert float((nt.level - fp.level).abs().max()) < tol * nlev
     assert diag.move_max_cells < (1e-6 if tag == "f64" else 1e-3)
+
+
+def _band_case(tag, seed=5):
+    from b200sht.semilag import SphericalGridTables, Stencil
+    from oracle import sl_gather as O
+
+    nlat, nlon, nlev = 32, 64, 6
+    lat = np.sort(np.arcsin(np.polynomial.legendre.leggauss(nlat)[0]))
+    dtype = np.float64 if tag == "f64" else np.float32
+    xi, phi, level = O.departure_sample(nlev, lat, nlon, seed, cells=1.5, dtype=dtype)
+    tables = SphericalGridTables.create(_grid(lat, nlon), dtype=DT[tag])
+    dev = lambda a: torch.as_tensor(a, device="cuda")
+    whole = Stencil(xi=dev(xi), phi=dev(phi), level=dev(level), tables=tables)
+    f = [torch.randn((nlev, nlat, nlon), dtype=DT[tag], device="cuda") for _ in range(3)]
+    return tables, whole, f
+
+
+@pytest.mark.parametrize("tag", ["f64", "f32"])
+@pytest.mark.parametrize("order", [4, 6])
+@pytest.mark.parametrize("rows", [(0, 8), (12, 20), (26, 32)])
+def test_band_gather_is_the_whole_grid_gather(tag, order, rows):
+    """A band's gather from fields holding only the band and a 5-row halo
+    returns the whole-grid values of its rows bit for bit (poles included)."""
+    from b200sht.semilag import Stencil, gather_batch
+
+    tables, whole, f = _band_case(tag)
+    a0, a1 = rows
+    s0, s1 = max(0, a0 - 5), min(32, a1 + 5)
+    win = tables.window(slice(s0, s1), slice(a0, a1))
+    band = Stencil(xi=whole.xi[:, a0:a1].contiguous(), phi=whole.phi[:, a0:a1].contiguous(),
+                   level=whole.level[:, a0:a1].contiguous(), tables=tables, window=win)
+    want = gather_batch(f, whole, order=order, deficit=order == 4)
+    got = gather_batch([x[:, s0:s1].contiguous() for x in f], band, order=order,
+                       deficit=order == 4)
+    for g, w in zip(got, want):
+        if order == 4:
+            assert torch.equal(g[0], w[0][:, a0:a1]) and torch.equal(g[1], w[1][:, a0:a1])
+        else:
+            assert torch.equal(g, w[:, a0:a1])
+
+
+def test_band_escape_is_refused_by_name():
+    from b200sht.semilag import HaloEscape, Stencil, gather_batch, gather_linear_batch
+
+    tables, whole, f = _band_case("f64")
+    win = tables.window(slice(12, 20), slice(12, 20))  # no halo: stencils leave the band
+    band = Stencil(xi=whole.xi[:, 12:20].contiguous(), phi=whole.phi[:, 12:20].contiguous(),
+                   level=whole.level[:, 12:20].contiguous(), tables=tables, window=win)
+    src = [x[:, 12:20].contiguous() for x in f]
+    with pytest.raises(HaloEscape, match="outside the rows 12..20"):
+        gather_batch(src, band)
+    gather_batch(src, band, defer_escape=True)  # the flag is left for the caller
+    with pytest.raises(HaloEscape):
+        win.raise_if_escaped("gather")
+    win.clear_escape()
+    win.raise_if_escaped("gather")
+    with pytest.raises(ValueError, match="whole stencil"):
+        gather_linear_batch(src, band)
+    with pytest.raises(ValueError, match="computed rows must lie inside"):
+        tables.window(slice(4, 10), slice(2, 8))
+
+
+@pytest.mark.parametrize("tag", ["f64", "f32"])
+@pytest.mark.parametrize("solver", ["fixed_point", "newton"])
+def test_band_departure_search_is_the_whole_grid_search(tag, solver):
+    from b200sht.semilag import CartesianWind, SphericalGridTables, departure_points
+    from oracle import sl_gather as O
+
+    nlat, nlon, nlev = 32, 64, 6
+    lat = np.sort(np.arcsin(np.polynomial.legendre.leggauss(nlat)[0]))
+    dtype = np.float64 if tag == "f64" else np.float32
+    wind = [torch.as_tensor(a, device="cuda")
+            for a in O.rotation_wind(lat, nlon, nlev, speed=60.0, seed=2, dtype=dtype)]
+    tables = SphericalGridTables.create(_grid(lat, nlon), dtype=DT[tag])
+    whole, _ = departure_points(CartesianWind(*wind), tables, 900.0, solver=solver)
+    for a0, a1 in ((0, 6), (13, 19), (27, 32)):
+        s0, s1 = max(0, a0 - 4), min(nlat, a1 + 4)
+        win = tables.window(slice(s0, s1), slice(a0, a1))
+        band, diag = departure_points(CartesianWind(*[w[:, s0:s1].contiguous() for w in wind]),
+                                      tables, 900.0, window=win, solver=solver)
+        assert band.shape == (nlev, a1 - a0, nlon) and band.window is win
+        for x, y in ((band.xi, whole.xi), (band.phi, whole.phi), (band.level, whole.level)):
+            assert torch.equal(x, y[:, a0:a1])
+        assert np.isfinite(diag.displacement_max_m)
