@@ -43,3 +43,18 @@ def test_semilag_option_rules():
         _validate("none", True, 4)
     with pytest.raises(ValueError, match="cubic gather only"):
         _validate("quasi_monotone", True, 6)
+
+
+def test_band_window_geometry_and_escape_text():
+    import types
+
+    from b200sht.semilag import BandWindow, HaloEscape
+
+    tables = types.SimpleNamespace(nlon=64)
+    win = BandWindow(tables, slice(8, 24), slice(12, 20), None)
+    assert (win.source_rows, win.arrival_rows, win.lead) == (16, 8, 4)
+    assert win.local == slice(4, 12)
+    assert win.arrival_shape(5) == (5, 8, 64) and win.source_shape(5) == (5, 16, 64)
+    err = HaloEscape(win, "gather")
+    assert isinstance(err, ValueError)
+    assert "rows 12..20" in str(err) and "rows 8..24" in str(err)
