@@ -149,7 +149,13 @@ class HaloEscape(ValueError):
 
 class BandWindow:
     """One latitude band of the semi-Lagrangian step (``arrival`` rows) and
-    the rows its fields hold (``source``, the band plus a row halo)."""
+    the rows its fields hold (``source``, the band plus a row halo).
+
+    A window has one escape flag on the device.  Its band calls (each a
+    ``clear_escape`` .. kernels .. ``raise_if_escaped`` sequence) must run on
+    one stream, one after another: two calls of the same window in flight on
+    different streams would lower and read each other's flag.  The reference's
+    band windows share the same rule."""
 
     def __init__(self, tables, source: slice, arrival: slice, handle):
         self.tables = tables

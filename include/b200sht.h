@@ -120,8 +120,11 @@ int sht_forward(sht_plan* plan, const void* grid, int64_t planes, void* coeff, v
  * scratch, and it allocates nothing; a call that needs more (too many
  * planes) is rejected with SHT_ERR_ARG and the per-call plane limit in the
  * message.  FP32 and FP64 plans only.  The first call on a device looks the
- * buffer's address up (make it before any stream capture); every call shares
- * the buffer, so calls that overlap on the GPU race on it. */
+ * buffer's address up (make it before any stream capture) and caches it per
+ * device ordinal for the life of the process, so the cache assumes one
+ * primary context per device: after cudaDeviceReset the cached address is
+ * stale and the call must not be used again in that process.  Every call
+ * shares the buffer, so calls that overlap on the GPU race on it. */
 int sht_forward_static_scratch(sht_plan* plan, const void* grid, int64_t planes, void* coeff,
                                void* stream);
 
@@ -322,7 +325,16 @@ int sht_sl_tables_destroy(sht_sl_tables* tables);
  * rows; brackets and weights are the whole grid's, so the values equal the
  * whole-grid calls' on those rows.  A read of a row outside the held rows
  * raises the window's escape flag (and reads the first held row instead);
- * sht_sl_window_escape reads it (synchronising `stream`) and/or clears it. */
+ * sht_sl_window_escape reads it (synchronising `stream`) and/or clears it.
+ * Buffer shapes of the band calls (nothing in the C layer can check them):
+ * src (fields, nlev, s1 - s0, nlon); vx, vy, vz, level_rate (nlev, s1 - s0,
+ * nlon); xi, phi, level, out, cut, the *_ex winds, move_m and move_k
+ * (.., nlev, a1 - a0, nlon).
+ * A window borrows `tables` (it keeps the pointer and reads the tables on
+ * every band call): destroy every window of a tables object before
+ * sht_sl_tables_destroy.  A window holds one escape flag, so the band calls
+ * of one window are serialised on one stream; calls on different streams
+ * would set and clear each other's flag. */
 typedef struct sht_sl_window sht_sl_window;
 int sht_sl_window_create(const sht_sl_tables* tables, int s0, int s1, int a0, int a1,
                          sht_sl_window** out);

@@ -2,7 +2,7 @@
 
 Run in the build container, where the reference source tree is mounted:
 
-    python tests/golden/make_golden.py /root/reference
+    python tests/golden/make_golden.py <reference checkout>
 
 It imports the reference's own numpy float64 transform
 (``arwen_global.spectral.transform.SphericalHarmonicTransform`` and
@@ -235,7 +235,9 @@ def record_fp32_errors() -> None:
 
 
 def main() -> None:
-    ref_root = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit(f"usage: python {sys.argv[0]} <path to the reference checkout>")
+    ref_root = Path(sys.argv[1])
     os.environ.setdefault("ARWEN_GLOBAL_LEGENDRE_CACHE", "off")
     sys.path[:0] = [str(ref_root / "src"), str(ref_root / "tests")]
     record_transforms(ref_root)

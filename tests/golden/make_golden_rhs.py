@@ -3,7 +3,7 @@ reference.
 
 Run in the build container, where the reference source tree is mounted:
 
-    python tests/golden/make_golden_rhs.py /root/reference
+    python tests/golden/make_golden_rhs.py <reference checkout>
 
 It calls the reference's own numpy specification,
 ``arwen_global.dynamics.MoistHybridModel._vertical_scalar_flux_divergence``
@@ -46,4 +46,6 @@ def main(ref_root: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit(f"usage: python {sys.argv[0]} <path to the reference checkout>")
+    main(sys.argv[1])

@@ -2,7 +2,7 @@
 
 Run in the build container, where the reference source tree is mounted:
 
-    python tests/golden/make_golden_sampling.py /root/reference
+    python tests/golden/make_golden_sampling.py <reference checkout>
 
 It builds the reference's numpy T21 transform and runs its own
 ``sample_scalar``, ``sample_gradient`` and ``sample_wind``
@@ -47,4 +47,6 @@ def main(ref_root: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit(f"usage: python {sys.argv[0]} <path to the reference checkout>")
+    main(sys.argv[1])

@@ -2,7 +2,7 @@
 
 Run in the build container, where the reference source tree is mounted:
 
-    python tests/golden/make_golden_sl.py /root/reference
+    python tests/golden/make_golden_sl.py <reference checkout>
 
 It builds the reference's own grid tables
 (``arwen_global.semilag.tables.SphericalGridTables``) and runs its
@@ -99,4 +99,6 @@ def main(ref_root: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit(f"usage: python {sys.argv[0]} <path to the reference checkout>")
+    main(sys.argv[1])
