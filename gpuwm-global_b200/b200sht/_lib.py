@@ -31,6 +31,9 @@ SHT_ERR_DEVICE = 3
 SHT_ERR_STATE = 4
 SHT_SL_NONE = 0
 SHT_SL_QUASI_MONOTONE = 1
+SHT_SEMI_SOLVE_SHIFTED = 0
+SHT_SEMI_APPLY = 1
+SHT_SEMI_HALF_APPLY = 2
 #: Kernel kinds of sht_plan_read_timing, in order.
 KERNEL_KINDS = ("fft_forward", "fft_inverse", "legendre_analysis", "legendre_synthesis", "pack",
                 "unpack", "elementwise", "helmholtz")
@@ -64,6 +67,14 @@ SIGNATURES = {
     "sht_gradient": (ctypes.c_int, [_P, _P, _I64, _P, _P, _P]),
     "sht_wind_from_vordiv": (ctypes.c_int, [_P, _P, _P, _I64, _P, _P, _P]),
     "sht_vordiv_from_wind": (ctypes.c_int, [_P, _P, _P, _I64, _P, _P, _P]),
+    "sht_vordiv_from_waist": (ctypes.c_int, [_P, _P, _I64, _P, _P, _P]),
+    "sht_vertical_create_modes": (ctypes.c_int, [_P, ctypes.c_int] + [_DP] * 8
+                                  + [ctypes.POINTER(_P)]),
+    "sht_semi_implicit_map": (ctypes.c_int, [_P, _P, ctypes.c_int, ctypes.c_double,
+                                             ctypes.c_double] + [_P] * 7),
+    "sht_semi_implicit_metric": (ctypes.c_int, [_P, _DP, _P]),
+    "sht_helmholtz_synthesis": (ctypes.c_int, [_P, _P, ctypes.c_double] + [_P] * 8),
+    "sht_divergence_from_waist": (ctypes.c_int, [_P, _P, _I64, _P, _P]),
     "sht_project": (ctypes.c_int, [_P, _P, _I64, _P, _P]),
     "sht_laplacian": (ctypes.c_int, [_P, _P, _I64, _P, _P]),
     "sht_inverse_laplacian": (ctypes.c_int, [_P, _P, _I64, _P, _P]),

@@ -9,10 +9,11 @@ holds every buffer of that call set on the device and issues it as:
 
 1. ``forward``: ``n_scalar x nlev`` scalar planes (temperature first) and ln ps;
 2. ``vordiv_from_wind``: (u, v) -> (zeta, D), ``nlev`` levels;
-3. ``sht_helmholtz_apply``: (D, theta, ln ps) -> (D', theta', ln ps');
+3. ``sht_helmholtz_synthesis``: (D, theta, ln ps) -> (D', theta', ln ps') and
+   the grid divergence, the solve writing D' straight into the synthesis
+   operand (the Helmholtz solve fused into the synthesis prologue);
 4. ``wind_from_vordiv``: (zeta, D') -> (u, v), written back into the input wind;
-5. ``gradient``: of theta' (``nlev`` planes) and ln ps' (one plane);
-6. ``inverse``: D' -> grid divergence.
+5. ``gradient``: of theta' (``nlev`` planes) and ln ps' (one plane).
 
 Step 4 overwrites the wind the next step starts from, so replaying the graph
 iterates the step.  Nothing in it allocates, copies from the host or
@@ -88,16 +89,16 @@ class DycoreTransformStep:
         _lib.call("sht_forward", h, _ptr(self.lnps), 1, _ptr(self.lnps_coeff), st)
         _lib.call("sht_vordiv_from_wind", h, _ptr(self.u), _ptr(self.v), L, _ptr(self.vorticity),
                   _ptr(self.divergence), st)
-        self.solver.solve_into(t, self.vertical, self.tau_s, self.divergence,
-                               self.scalar_coeff[0], self.lnps_coeff, self.div_solved,
-                               self.theta_solved, self.lnps_solved)
+        self.solver.solve_and_synthesize_into(t, self.vertical, self.tau_s, self.divergence,
+                                              self.scalar_coeff[0], self.lnps_coeff,
+                                              self.div_solved, self.theta_solved,
+                                              self.lnps_solved, self.div_grid)
         _lib.call("sht_wind_from_vordiv", h, _ptr(self.vorticity), _ptr(self.div_solved), L,
                   _ptr(self.u), _ptr(self.v), st)
         _lib.call("sht_gradient", h, _ptr(self.theta_solved), L, _ptr(self.grad_theta[0]),
                   _ptr(self.grad_theta[1]), st)
         _lib.call("sht_gradient", h, _ptr(self.lnps_solved), 1, _ptr(self.grad_lnps[0]),
                   _ptr(self.grad_lnps[1]), st)
-        _lib.call("sht_inverse", h, _ptr(self.div_solved), L, _ptr(self.div_grid), st)
 
     def capture(self) -> torch.cuda.CUDAGraph:
         """Record ``run`` in a CUDA graph (``prepare`` first)."""

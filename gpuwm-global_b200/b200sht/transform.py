@@ -22,6 +22,7 @@ tables are resident in HBM and the contraction walks the triangle directly.
 """
 from __future__ import annotations
 
+import contextlib
 import ctypes
 import hashlib
 import json
@@ -95,8 +96,66 @@ def _stream():
     return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
 
 
+class _FusedJob:
+    """One fused library call that performs several Legendre contractions
+    (and the FFTs and layout passes around them); run once, on first demand."""
+
+    def __init__(self, run):
+        self._run = run
+        self._out = None
+
+    def output(self, index: int):
+        if self._out is None:
+            self._out = self._run()
+            self._run = None
+        return self._out[index]
+
+
+class FusedOperand:
+    """The operand of one Legendre contraction that runs inside a fused
+    library call.
+
+    The reference routes every contraction through
+    ``SphericalHarmonicTransform._batched_contract`` (transform.py:1178-1274),
+    and its census tool (tools/arwen_global_transform_census.py:64-140)
+    counts the calls by replacing that method and reading
+    ``values.shape[:-2]``.  Here a contraction runs inside one C-ABI call
+    together with its FFT and layout passes, so each public method hands the
+    seam one ``FusedOperand`` per contraction the reference performs, shaped
+    like the reference's operand (``(*lead, nlat, T+1)`` for an analysis,
+    ``(*lead, T+1, T+1)`` for a synthesis).  The first operand of a call
+    runs the library call; each returns its own output of it."""
+
+    def __init__(self, shape, job: _FusedJob, index: int = 0):
+        self.shape = tuple(int(v) for v in shape)
+        self.ndim = len(self.shape)
+        self._job = job
+        self._index = int(index)
+
+    def result(self):
+        return self._job.output(self._index)
+
+
+def fused_operands(shapes, run):
+    """``FusedOperand`` objects of the given shapes over one call ``run()``
+    (which returns a tuple of as many outputs)."""
+    job = _FusedJob(run)
+    return [FusedOperand(sh, job, i) for i, sh in enumerate(shapes)]
+
+
 @dataclass
 class SphericalHarmonicTransform:
+    #: The multi-card row exchange, or None (transform.py:632-640).  Not a
+    #: dataclass field and in no identity.  The reference sets it at run
+    #: start on a multi-card run; its ``agree_once`` hook is called on each
+    #: contraction output here as there (``_agree_across_cards``) and its
+    #: ``fill_rows`` completes a band-filled waist (``FourierWaist.close``).
+    row_exchange = None
+    #: The multi-card order exchange, or None (transform.py:641-647).  The
+    #: order-partitioned contraction it serves is not built: a transform with
+    #: an exchange of more than one rank refuses to run forward or inverse.
+    order_exchange = None
+
     grid: GaussianGrid
     backend: Backend
     plan: Plan = field(repr=False)
@@ -104,8 +163,7 @@ class SphericalHarmonicTransform:
     legendre_band: int = 32
     streaming: bool = False
     latitude_bands: int = 1
-    #: Number of Legendre contractions issued (the reference's census seam,
-    #: tools/arwen_global_transform_census.py counts ``_batched_contract``).
+    #: Legendre contractions issued through ``_batched_contract``.
     contraction_count: int = 0
 
     @classmethod
@@ -231,24 +289,112 @@ class SphericalHarmonicTransform:
         return torch.empty((*lead, *self.spectral_shape), dtype=self.backend.complex_dtype,
                            device=self.backend.device)
 
+    # ------------------------------------------------------ contraction seam
+    def _contraction_scope(self):
+        """The reference scopes its TF32 compute type around each contraction
+        (transform.py:1146-1176) because CuPy's compute type is process-global.
+        Here the arithmetic is a property of the plan, so there is nothing to
+        scope."""
+        return contextlib.nullcontext()
+
+    def _batched_contract(self, values, table, *, transposed=False, realify=False):
+        """The Legendre contraction seam (transform.py:1178-1274): every
+        contraction of this transform passes through here, once per
+        contraction the reference performs, so a caller that replaces this
+        method (the reference's census tool) counts the same calls and planes.
+
+        ``values`` is a ``FusedOperand`` (the contraction runs inside a fused
+        library call; its output is returned) or a device array:
+        ``table`` analysis with ``(*lead, nlat, T+1)`` waist values gives the
+        ``(*lead, T+1, T+1)`` coefficients (``sht_contract_waist``; the m = 0
+        imaginary parts are stored 0, what the reference's callers store after
+        it with ``realify``); ``table`` basis or derivative basis with
+        ``(*lead, T+1, T+1)`` coefficients gives the ``(*lead, nlat, T+1)``
+        waist (``sht_contract_to_waist``).  A transposed contraction of an
+        arbitrary weighted waist is not a library operation: the vector
+        analysis runs it fused (``VorticityDivergenceOperator``)."""
+        self.contraction_count += 1
+        if isinstance(values, FusedOperand):
+            return values.result()
+        from .waist import ANALYSIS, BASIS, DERIVATIVE_BASIS
+
+        if transposed:
+            raise NotImplementedError(
+                "a transposed contraction of caller-weighted waist values is not a library "
+                "operation here; VorticityDivergenceOperator runs the vector analysis fused")
+        if table == ANALYSIS:
+            v = self.backend.asarray(values, dtype=self.backend.complex_dtype).contiguous()
+            if tuple(v.shape[-2:]) != (self.grid.nlat, self.truncation + 1):
+                raise ValueError(f"waist values have trailing shape {tuple(v.shape[-2:])}, "
+                                 f"expected {(self.grid.nlat, self.truncation + 1)}")
+            out = self._empty_spec(v.shape[:-2])
+            _lib.call("sht_contract_waist", self.plan.handle, _ptr(v), self._planes(v),
+                      _ptr(out), _stream())
+            return out
+        if table in (BASIS, DERIVATIVE_BASIS):
+            c = self._spec_in(values)
+            out = torch.empty((*c.shape[:-2], self.grid.nlat, self.truncation + 1),
+                              dtype=self.backend.complex_dtype, device=self.backend.device)
+            code = _lib.SHT_WAIST_DBASIS if table == DERIVATIVE_BASIS else _lib.SHT_WAIST_BASIS
+            _lib.call("sht_contract_to_waist", self.plan.handle, _ptr(c), self._planes(c),
+                      int(code), _ptr(out), _stream())
+            return out
+        raise ValueError(f"unknown table {table!r}: expected the transform's _analysis, _basis "
+                         "or _derivative_basis")
+
+    def _agree_across_cards(self, direction: str, table, array) -> None:
+        """Hand a contraction's output to the row exchange's ``agree_once``
+        hook (transform.py:1405-1433); one attribute read on a one-card run."""
+        exchange = self.row_exchange
+        hook = getattr(exchange, "agree_once", None)
+        if hook is None or int(getattr(exchange, "world", 1)) <= 1:
+            return
+        name = table if isinstance(table, str) else getattr(table, "name", None) or f"table@{id(table):x}"
+        hook(self.backend.xp,
+             (direction, name, tuple(int(v) for v in array.shape), str(array.dtype)), array)
+
+    def _refuse_order_exchange(self, what: str) -> None:
+        exchange = self.order_exchange
+        if exchange is not None and int(getattr(exchange, "world", 1)) > 1:
+            raise NotImplementedError(
+                f"{what}: the order-partitioned contraction of a multi-card order exchange is "
+                "not built by the B200 engine (one GPU holds every order's table)")
+
     # ---------------------------------------------------------- transforms
     def forward(self, field):
         """grid -> spectral (transform.py:1486)."""
+        self._refuse_order_exchange("forward")
         f = self._grid_in(field)
-        out = self._empty_spec(f.shape[:-2])
-        self.contraction_count += 1
-        _lib.call("sht_forward", self.plan.handle, _ptr(f), self._planes(f), _ptr(out), _stream())
+        lead = tuple(f.shape[:-2])
+
+        def run():
+            out = self._empty_spec(lead)
+            _lib.call("sht_forward", self.plan.handle, _ptr(f), self._planes(f), _ptr(out),
+                      _stream())
+            return (out,)
+
+        (op,) = fused_operands([(*lead, self.grid.nlat, self.truncation + 1)], run)
+        with self._contraction_scope():
+            out = self._batched_contract(op, self._analysis, realify=True)
+        self._agree_across_cards("analysis", self._analysis, out)
         return out
 
-    def _synth(self, name, coeff):
+    def _synth(self, name, coeff, table=None):
         c = self._spec_in(coeff)
-        out = self._empty_grid(c.shape[:-2])
-        self.contraction_count += 1
-        _lib.call(name, self.plan.handle, _ptr(c), self._planes(c), _ptr(out), _stream())
-        return out
+        lead = tuple(c.shape[:-2])
+
+        def run():
+            out = self._empty_grid(lead)
+            _lib.call(name, self.plan.handle, _ptr(c), self._planes(c), _ptr(out), _stream())
+            return (out,)
+
+        (op,) = fused_operands([tuple(c.shape)], run)
+        with self._contraction_scope():
+            return self._batched_contract(op, self._basis if table is None else table)
 
     def inverse(self, coeff):
         """spectral -> grid (transform.py:1742)."""
+        self._refuse_order_exchange("inverse")
         return self._synth("sht_inverse", coeff)
 
     # ------------------------------------------------- host-resident batches
@@ -269,7 +415,6 @@ class SphericalHarmonicTransform:
               or tuple(out.shape) != (*lead, *out_tail)):
             raise ValueError("out must be a contiguous host tensor of shape "
                              f"{(*lead, *out_tail)} and dtype {out_dtype}")
-        self.contraction_count += 1
         _lib.call(name, self.plan.handle, x.data_ptr(), self._planes(x), out.data_ptr(), int(chunk))
         return out
 
@@ -296,20 +441,29 @@ class SphericalHarmonicTransform:
 
     def inverse_meridional_derivative(self, coeff):
         """d field / d latitude in grid space (transform.py:1748)."""
-        return self._synth("sht_inverse_meridional_derivative", coeff)
+        return self._synth("sht_inverse_meridional_derivative", coeff, self._derivative_basis)
 
     def inverse_zonal_derivative(self, coeff):
         """d field / d longitude in grid space (transform.py:1752)."""
         return self._synth("sht_inverse_zonal_derivative", coeff)
 
     def gradient(self, coeff):
-        """Physical (east, north) derivatives per metre (transform.py:1762)."""
+        """Physical (east, north) derivatives per metre (transform.py:1762):
+        both syntheses in one library call, two contractions at the seam."""
         c = self._spec_in(coeff)
-        east = self._empty_grid(c.shape[:-2])
-        north = self._empty_grid(c.shape[:-2])
-        self.contraction_count += 2
-        _lib.call("sht_gradient", self.plan.handle, _ptr(c), self._planes(c), _ptr(east),
-                  _ptr(north), _stream())
+        lead = tuple(c.shape[:-2])
+
+        def run():
+            east = self._empty_grid(lead)
+            north = self._empty_grid(lead)
+            _lib.call("sht_gradient", self.plan.handle, _ptr(c), self._planes(c), _ptr(east),
+                      _ptr(north), _stream())
+            return east, north
+
+        op_e, op_n = fused_operands([tuple(c.shape)] * 2, run)
+        with self._contraction_scope():
+            east = self._batched_contract(op_e, self._basis)
+            north = self._batched_contract(op_n, self._derivative_basis)
         return east, north
 
     def _elementwise(self, name, coeff):

@@ -25,10 +25,10 @@ from __future__ import annotations
 import torch
 
 from . import _lib
-from .transform import SphericalHarmonicTransform, _ptr, _stream
+from .transform import SphericalHarmonicTransform, _ptr, _stream, fused_operands
 
 BASIS = "basis"
-DERIVATIVE_BASIS = "derivative"
+DERIVATIVE_BASIS = "derivative_basis"
 ANALYSIS = "analysis"
 _TABLE_CODE = {None: _lib.SHT_WAIST_BASIS, BASIS: _lib.SHT_WAIST_BASIS,
                DERIVATIVE_BASIS: _lib.SHT_WAIST_DBASIS}
@@ -118,8 +118,16 @@ class FourierWaist:
     def close(self) -> "FourierWaist":
         """Refuse a waist with an unwritten row, then transform it."""
         if self._open:
-            self._filled.require_complete()
             t = self.transform
+            exchange = getattr(t, "row_exchange", None)
+            if (exchange is not None and int(getattr(exchange, "world", 1)) > 1
+                    and not bool(self._filled.rows.all())):
+                # The rows other cards hold arrive through the card layer
+                # (transform.py:547-563); the staged band rows are grid rows.
+                exchange.fill_rows(t.backend.xp, self._staging, self._staging.ndim - 2,
+                                   name="waist")
+                self._filled.rows[:] = True
+            self._filled.require_complete()
             out = torch.empty(self.shape, dtype=t.backend.complex_dtype, device=t.backend.device)
             _lib.call("sht_fourier_waist", t.plan.handle, _ptr(self._staging),
                       t._planes(self._staging), _ptr(out), _stream())
@@ -167,16 +175,13 @@ def fourier_waist(self, field, *, bands: int | None = None) -> FourierWaist:
 
 
 def contract_values(self, values, table=None):
+    """The analysis tail on a waist's buffer or a leading slice of it
+    (transform.py:1455-1472): one contraction at the seam."""
     if table not in (None, ANALYSIS):
         raise ValueError("the analysis contraction reads the Gram-solved analysis table")
-    v = self.backend.asarray(values, dtype=self.backend.complex_dtype).contiguous()
-    if tuple(v.shape[-2:]) != (self.grid.nlat, self.truncation + 1):
-        raise ValueError(f"waist values have trailing shape {tuple(v.shape[-2:])}, expected "
-                         f"{(self.grid.nlat, self.truncation + 1)}")
-    out = self._empty_spec(v.shape[:-2])
-    self.contraction_count += 1
-    _lib.call("sht_contract_waist", self.plan.handle, _ptr(v), self._planes(v), _ptr(out),
-              _stream())
+    with self._contraction_scope():
+        out = self._batched_contract(values, ANALYSIS, realify=True)
+    self._agree_across_cards("analysis", ANALYSIS, out)
     return out
 
 
@@ -191,12 +196,25 @@ def contract_to_waist(self, coeff, table=None, *, bands: int | None = None) -> F
 
 
 def _contract_to_waist(self, coeff, code, bands):
+    """One synthesis contraction at the seam (transform.py:1629-1652); the
+    zonal form (basis times i m, which the reference applies to the
+    coefficients first) runs fused."""
     c = self._spec_in(coeff)
-    out = torch.empty((*c.shape[:-2], self.grid.nlat, self.truncation + 1),
-                      dtype=self.backend.complex_dtype, device=self.backend.device)
-    self.contraction_count += 1
-    _lib.call("sht_contract_to_waist", self.plan.handle, _ptr(c), self._planes(c), int(code),
-              _ptr(out), _stream())
+    table = DERIVATIVE_BASIS if code == _lib.SHT_WAIST_DBASIS else BASIS
+    if code == _lib.SHT_WAIST_ZONAL:
+        def run():
+            out = torch.empty((*c.shape[:-2], self.grid.nlat, self.truncation + 1),
+                              dtype=self.backend.complex_dtype, device=self.backend.device)
+            _lib.call("sht_contract_to_waist", self.plan.handle, _ptr(c), self._planes(c),
+                      int(code), _ptr(out), _stream())
+            return (out,)
+
+        (values,) = fused_operands([tuple(c.shape)], run)
+    else:
+        values = c
+    with self._contraction_scope():
+        out = self._batched_contract(values, table)
+    self._agree_across_cards("synthesis", table, out)
     return FourierWaist(self, out, latitude_band_edges(
         self.grid.nlat, self.latitude_bands if bands is None else bands))
 

@@ -23,7 +23,9 @@ struct sht_vertical {
   int device = 0;
   int prec = 0;
   int nlev = 0;
+  bool thermo = false;  // W, W^-1 and mu follow (half maps)
   void* mats = nullptr;
+  void* metric = nullptr;  // one value of the plan's type: max |D' - D| of the last map
 };
 
 namespace sht {
@@ -181,6 +183,27 @@ void contract2(sht_plan* p, int kind0, T* out0, int kind1, T* out1, const T* dat
   contract<T>(p, kind1, data, out1, R, s);
 }
 
+// Two contractions of different operands, each with its own row maxima (the
+// rotational table on the u rows and the shear table on the v rows of a
+// divergence-only analysis): one tensor-core launch with two groups on the
+// split path.
+template <typename T>
+void contract_pair(sht_plan* p, int kind0, const T* data0, const float* rm0, T* out0, int kind1,
+                   const T* data1, const float* rm1, T* out1, int64_t R, cudaStream_t s) {
+  if constexpr (sizeof(T) == 4) {
+    if (uses_tc(p)) {
+      const int dir = table_dir(kind0);
+      KernelScope scope(p, dir == 0 ? SHT_KIND_LEGENDRE_SYNTHESIS : SHT_KIND_LEGENDRE_ANALYSIS, s);
+      TcGroupSpec g[2] = {{p, dir, table_flip(kind0), kind0, data0, rm0, out0, R},
+                          {p, table_dir(kind1), table_flip(kind1), kind1, data1, rm1, out1, R}};
+      launch_gemm_tc_groups(g, 2, tc_plan_cache(p), s);
+      return;
+    }
+  }
+  contract<T>(p, kind0, data0, out0, R, s);
+  contract<T>(p, kind1, data1, out1, R, s);
+}
+
 template <typename T>
 void do_forward(sht_plan* p, const T* grid, int64_t planes, T* coeff, cudaStream_t s) {
   const int64_t R = 2 * planes;
@@ -278,6 +301,81 @@ void do_vordiv(sht_plan* p, const T* u, const T* v, int64_t planes, T* vort, T* 
   }
 }
 
+// Vorticity and divergence from the reference-layout Fourier waist of a
+// stacked (u, v) pair, (2, planes, nlat, T+1): the contraction half of
+// vordiv_from_wind (vector.py:113-134).  The import interleaves the two
+// fields per plane, the layout the rotational/shear contractions and the
+// vordiv epilogue of do_vordiv read.
+template <typename T>
+void do_vordiv_waist(sht_plan* p, const T* waist, int64_t planes, T* vort, T* div,
+                     cudaStream_t s) {
+  const int64_t R = 4 * planes;
+  ensure_scratch(p, R);
+  T* w = static_cast<T*>(p->wfold[0]);
+  T* c0 = static_cast<T*>(p->cfold[0]);
+  T* c1 = static_cast<T*>(p->cfold[1]);
+  {
+    float* rm = rowmax_for(p, R, s);
+    KernelScope k(p, SHT_KIND_PACK, s);
+    launch_waist_import<T>(p, waist, 2 * planes, 1.0, w, rm, s, 2);
+  }
+  contract2<T>(p, kRot, c0, kShear, c1, w, R, s);
+  {
+    KernelScope k(p, SHT_KIND_UNPACK, s);
+    launch_unpack<T>(p, kUnpackVorDiv, c0, c1, planes, vort, div, s);
+  }
+}
+
+// Divergence alone from the same stacked waist (divergence_from_fourier,
+// vector.py:136-166): the rotational table on the u half and the shear table
+// on the v half only, each contraction at half the rows of the full pair.
+template <typename T>
+void do_divergence_waist(sht_plan* p, const T* waist, int64_t planes, T* div, cudaStream_t s) {
+  const int64_t R = 2 * planes;
+  ensure_scratch(p, 2 * R);
+  T* wu = static_cast<T*>(p->wfold[0]);
+  T* wv = static_cast<T*>(p->wfold[1]);
+  T* c0 = static_cast<T*>(p->cfold[0]);
+  T* c1 = static_cast<T*>(p->cfold[1]);
+  const int64_t per_field = (int64_t)p->nlat * (p->T + 1) * planes;  // complex values
+  {
+    float* rm = rowmax_for(p, 2 * R, s);
+    KernelScope k(p, SHT_KIND_PACK, s);
+    launch_waist_import<T>(p, waist, planes, 1.0, wu, rm, s);
+    launch_waist_import<T>(p, waist + 2 * per_field, planes, 1.0, wv, rm ? rm + R : nullptr, s);
+  }
+  const float* rm = uses_tc(p) ? p->rowmax : nullptr;
+  contract_pair<T>(p, kRot, wu, rm, c0, kShear, wv, rm ? rm + R : nullptr, c1, R, s);
+  {
+    KernelScope k(p, SHT_KIND_UNPACK, s);
+    launch_unpack<T>(p, kUnpackDiv, c0, c1, planes, div, nullptr, s);
+  }
+}
+
+// The stage solve with the divergence synthesis fused onto it: the kernel
+// writes D' into the plan's folded synthesis operand (and its row maxima),
+// then the Legendre synthesis and the inverse FFT of D' follow.
+template <typename T>
+void do_helmholtz_synthesis(sht_plan* p, const sht_vertical* op, double tau_w, const T* div,
+                            const T* theta, const T* lnps, T* odiv, T* otheta, T* olnps,
+                            T* grid, cudaStream_t s) {
+  const int64_t planes = op->nlev, R = 2 * planes;
+  ensure_scratch(p, R);
+  T* c = static_cast<T*>(p->cfold[0]);
+  T* w = static_cast<T*>(p->wfold[0]);
+  {
+    float* rm = rowmax_for(p, R, s);
+    KernelScope k(p, SHT_KIND_HELMHOLTZ, s);
+    launch_semi_implicit<T>(p, op->nlev, static_cast<const T*>(op->mats), op->thermo, kSemiSolve,
+                            tau_w, 1.0, div, theta, lnps, odiv, otheta, olnps, nullptr, c, rm, s);
+  }
+  contract<T>(p, kBasis, c, w, R, s);
+  {
+    KernelScope k(p, SHT_KIND_FFT_INVERSE, s);
+    launch_inverse_unfold<T>(p, kUnfoldScalar, w, nullptr, planes, grid, nullptr, s);
+  }
+}
+
 // ------------------------------------------------------------------ batches
 // A batch of plans (different truncations, or the same truncation under
 // separate plans) run as one transform: per-plan FFT, pack and unpack
@@ -353,30 +451,45 @@ void do_batch_inverse(sht_batch* b, const void* const* coeffs, void* const* grid
 }
 
 // ------------------------------------------------------- vertical operators
+// Packs B, C, V, V^-1, lambda and (when w is given) W, W^-1, mu in the
+// plan's type, in the order the semi-implicit kernel reads them.
 sht_vertical* vertical_upload(const sht_plan* plan, int nlev, const double* b, const double* c,
                               const double* eigvec, const double* eigvec_inv,
-                              const double* eigenvalues) {
+                              const double* eigenvalues, const double* w = nullptr,
+                              const double* w_inv = nullptr, const double* x_eigenvalues = nullptr) {
   SHT_REQUIRE(nlev >= 1 && nlev <= 96, "nlev must be in [1, 96]");
   for (const void* q : {(const void*)b, (const void*)c, (const void*)eigvec,
                         (const void*)eigvec_inv, (const void*)eigenvalues})
     check_ptr(q, "vertical operator matrix");
+  const bool thermo = w != nullptr;
+  if (thermo) {
+    check_ptr(w_inv, "thermodynamic modes' inverse");
+    check_ptr(x_eigenvalues, "thermodynamic eigenvalues");
+  }
   const int L1 = nlev + 1;
-  const size_t nm = (size_t)nlev * L1 * 2 + (size_t)nlev * nlev * 2 + nlev;
+  const size_t nm = (size_t)nlev * L1 * 2 + (size_t)nlev * nlev * 2 + nlev +
+                    (thermo ? (size_t)L1 * L1 * 2 + L1 : 0);
   std::vector<double> host(nm);
   size_t o = 0;
-  std::copy(b, b + nlev * L1, host.begin() + o);
-  o += nlev * L1;
-  std::copy(c, c + L1 * nlev, host.begin() + o);
-  o += L1 * nlev;
-  std::copy(eigvec, eigvec + nlev * nlev, host.begin() + o);
-  o += nlev * nlev;
-  std::copy(eigvec_inv, eigvec_inv + nlev * nlev, host.begin() + o);
-  o += nlev * nlev;
-  std::copy(eigenvalues, eigenvalues + nlev, host.begin() + o);
+  auto put = [&](const double* src, size_t n) {
+    std::copy(src, src + n, host.begin() + o);
+    o += n;
+  };
+  put(b, (size_t)nlev * L1);
+  put(c, (size_t)L1 * nlev);
+  put(eigvec, (size_t)nlev * nlev);
+  put(eigvec_inv, (size_t)nlev * nlev);
+  put(eigenvalues, nlev);
+  if (thermo) {
+    put(w, (size_t)L1 * L1);
+    put(w_inv, (size_t)L1 * L1);
+    put(x_eigenvalues, L1);
+  }
   auto* op = new sht_vertical;
   op->device = plan->device;
   op->prec = plan->prec;
   op->nlev = nlev;
+  op->thermo = thermo;
   try {
     if (plan->prec == SHT_PREC_F64) {
       SHT_CUDA_OR_THROW(cudaMalloc(&op->mats, sizeof(double) * nm));
@@ -386,8 +499,10 @@ sht_vertical* vertical_upload(const sht_plan* plan, int nlev, const double* b, c
       SHT_CUDA_OR_THROW(cudaMalloc(&op->mats, sizeof(float) * nm));
       upload_now(op->mats, conv.data(), sizeof(float) * nm);
     }
+    SHT_CUDA_OR_THROW(cudaMalloc(&op->metric, sizeof(double)));
   } catch (...) {
     if (op->mats) cudaFree(op->mats);
+    if (op->metric) cudaFree(op->metric);
     delete op;
     throw;
   }
@@ -397,6 +512,7 @@ sht_vertical* vertical_upload(const sht_plan* plan, int nlev, const double* b, c
 void vertical_free(sht_vertical* op) {
   if (!op) return;
   if (op->mats) cudaFree(op->mats);
+  if (op->metric) cudaFree(op->metric);
   delete op;
 }
 
@@ -790,6 +906,27 @@ int sht_vordiv_from_wind(sht_plan* plan, const void* u, const void* v, int64_t p
   });
 }
 
+int sht_vordiv_from_waist(sht_plan* plan, const void* waist, int64_t planes, void* vorticity,
+                          void* divergence, void* stream) {
+  return guarded([&] {
+    SHT_CHECK_CALL(plan, planes);
+    check_ptr(waist, "waist");
+    check_ptr(vorticity, "vorticity");
+    check_ptr(divergence, "divergence");
+    SHT_TYPED(plan, do_vordiv_waist<T>(plan, CP(waist), planes, MP(vorticity), MP(divergence), s));
+  });
+}
+
+int sht_divergence_from_waist(sht_plan* plan, const void* waist, int64_t planes, void* divergence,
+                              void* stream) {
+  return guarded([&] {
+    SHT_CHECK_CALL(plan, planes);
+    check_ptr(waist, "waist");
+    check_ptr(divergence, "divergence");
+    SHT_TYPED(plan, do_divergence_waist<T>(plan, CP(waist), planes, MP(divergence), s));
+  });
+}
+
 static int elementwise_entry(sht_plan* plan, int mode, const void* in, int64_t planes, void* out,
                              void* stream) {
   return guarded([&] {
@@ -824,6 +961,80 @@ static void vertical_apply(sht_plan* plan, const sht_vertical* op, double tau_w,
   SHT_TYPED(plan, launch_helmholtz<T>(plan, op->nlev, static_cast<const T*>(op->mats), tau_w,
                                       CP(divergence), CP(theta), CP(lnps), MP(out_divergence),
                                       MP(out_theta), MP(out_lnps), s));
+}
+
+static void check_vertical(const sht_plan* plan, const sht_vertical* op) {
+  check_transform_plan(plan);
+  check_ptr(op, "vertical operator");
+  SHT_REQUIRE(op->device == plan->device && op->prec == plan->prec,
+              "the vertical operator was created for another plan's device or precision");
+}
+
+int sht_semi_implicit_map(sht_plan* plan, const sht_vertical* op, int mode, double dt_w,
+                          double alpha, const void* divergence, const void* theta,
+                          const void* lnps, void* out_divergence, void* out_theta,
+                          void* out_lnps, void* stream) {
+  return guarded([&] {
+    check_vertical(plan, op);
+    for (const void* q : {divergence, theta, lnps, (const void*)out_divergence,
+                          (const void*)out_theta, (const void*)out_lnps})
+      check_ptr(q, "semi-implicit argument");
+    SHT_REQUIRE(mode == SHT_SEMI_SOLVE_SHIFTED || mode == SHT_SEMI_APPLY ||
+                    mode == SHT_SEMI_HALF_APPLY,
+                "mode must be SHT_SEMI_SOLVE_SHIFTED, SHT_SEMI_APPLY or SHT_SEMI_HALF_APPLY");
+    SHT_REQUIRE(mode == SHT_SEMI_SOLVE_SHIFTED || (alpha >= 0.5 && alpha <= 1.0),
+                "off_centring_weight must lie in [0.5, 1]");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    plan->last_stream = s;
+    const int kmode = mode == SHT_SEMI_APPLY ? kSemiApply
+                      : mode == SHT_SEMI_HALF_APPLY ? kSemiHalf : kSemiSolve;
+    SHT_CUDA_OR_THROW(cudaMemsetAsync(op->metric, 0, sizeof(double), s));
+    KernelScope k(plan, SHT_KIND_HELMHOLTZ, s);
+    SHT_TYPED(plan, launch_semi_implicit<T>(plan, op->nlev, static_cast<const T*>(op->mats),
+                                            op->thermo, kmode, dt_w,
+                                            mode == SHT_SEMI_SOLVE_SHIFTED ? 1.0 : alpha,
+                                            CP(divergence), CP(theta), CP(lnps),
+                                            MP(out_divergence), MP(out_theta), MP(out_lnps),
+                                            static_cast<T*>(op->metric), nullptr, nullptr, s));
+  });
+}
+
+int sht_semi_implicit_metric(const sht_vertical* op, double* max_divergence_increment,
+                             void* stream) {
+  return guarded([&] {
+    check_ptr(op, "vertical operator");
+    check_ptr(max_divergence_increment, "max_divergence_increment");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    double v = 0.0;
+    if (op->prec == SHT_PREC_F64) {
+      SHT_CUDA_OR_THROW(cudaMemcpyAsync(&v, op->metric, sizeof(double), cudaMemcpyDeviceToHost, s));
+      SHT_CUDA_OR_THROW(cudaStreamSynchronize(s));
+    } else {
+      float f = 0.f;
+      SHT_CUDA_OR_THROW(cudaMemcpyAsync(&f, op->metric, sizeof(float), cudaMemcpyDeviceToHost, s));
+      SHT_CUDA_OR_THROW(cudaStreamSynchronize(s));
+      v = f;
+    }
+    *max_divergence_increment = v;
+  });
+}
+
+int sht_helmholtz_synthesis(sht_plan* plan, const sht_vertical* op, double tau_w,
+                            const void* divergence, const void* theta, const void* lnps,
+                            void* out_divergence, void* out_theta, void* out_lnps,
+                            void* divergence_grid, void* stream) {
+  return guarded([&] {
+    check_vertical(plan, op);
+    for (const void* q : {divergence, theta, lnps, (const void*)out_divergence,
+                          (const void*)out_theta, (const void*)out_lnps,
+                          (const void*)divergence_grid})
+      check_ptr(q, "helmholtz_synthesis argument");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    plan->last_stream = s;
+    SHT_TYPED(plan, do_helmholtz_synthesis<T>(plan, op, tau_w, CP(divergence), CP(theta),
+                                              CP(lnps), MP(out_divergence), MP(out_theta),
+                                              MP(out_lnps), MP(divergence_grid), s));
+  });
 }
 
 int sht_helmholtz_solve(sht_plan* plan, int nlev, const double* b, const double* c,
@@ -862,6 +1073,24 @@ int sht_vertical_create(sht_plan* plan, int nlev, const double* b, const double*
   });
 }
 
+int sht_vertical_create_modes(sht_plan* plan, int nlev, const double* b, const double* c,
+                              const double* eigvec, const double* eigvec_inv,
+                              const double* eigenvalues, const double* x_eigvec,
+                              const double* x_eigvec_inv, const double* x_eigenvalues,
+                              sht_vertical** out) {
+  return guarded([&] {
+    check_ptr(out, "out");
+    *out = nullptr;
+    check_transform_plan(plan);
+    check_ptr(x_eigvec, "x_eigvec");
+    int device = 0;
+    SHT_CUDA_OR_THROW(cudaGetDevice(&device));
+    SHT_REQUIRE(device == plan->device, "the current device is not the plan's device");
+    *out = vertical_upload(plan, nlev, b, c, eigvec, eigvec_inv, eigenvalues, x_eigvec,
+                           x_eigvec_inv, x_eigenvalues);
+  });
+}
+
 int sht_vertical_destroy(sht_vertical* op) {
   return guarded([&] { vertical_free(op); });
 }
@@ -870,10 +1099,7 @@ int sht_helmholtz_apply(sht_plan* plan, const sht_vertical* op, double tau_w,
                         const void* divergence, const void* theta, const void* lnps,
                         void* out_divergence, void* out_theta, void* out_lnps, void* stream) {
   return guarded([&] {
-    check_transform_plan(plan);
-    check_ptr(op, "vertical operator");
-    SHT_REQUIRE(op->device == plan->device && op->prec == plan->prec,
-                "the vertical operator was created for another plan's device or precision");
+    check_vertical(plan, op);
     vertical_apply(plan, op, tau_w, divergence, theta, lnps, out_divergence, out_theta, out_lnps,
                    static_cast<cudaStream_t>(stream));
   });

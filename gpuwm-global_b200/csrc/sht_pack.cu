@@ -117,7 +117,7 @@ __global__ void __launch_bounds__(256) pack_kernel(int Tn, double radius,
 // One CTA: 32 orders x NB degrees x 32 planes, every load issued before the
 // CTA's one barrier; a CTA wholly above the triangle writes zeros only.
 template <typename T, int MODE> struct UnpackCfg {
-  static constexpr int NO = MODE == kUnpackScalar ? 1 : 2;  // output fields
+  static constexpr int NO = MODE == kUnpackVorDiv ? 2 : 1;  // output fields
   static constexpr int NB = sizeof(T) == 4 ? 2 : 1;
 };
 
@@ -169,6 +169,11 @@ __global__ void __launch_bounds__(256) unpack_kernel(int Tn, const V2<T>* __rest
           const int64_t row = base + (q ? size0 : 0) + i;
           if constexpr (MODE == kUnpackScalar) {
             va[nb][k] = __ldcs(cf0 + row * Rc + p);
+          } else if constexpr (MODE == kUnpackDiv) {
+            // cf0: rotational rows of u, cf1: shear rows of v (one column per plane).
+            const V2<T> ru = __ldcs(cf0 + row * Rc + p), sv = __ldcs(cf1 + row * Rc + p);
+            const T mf = T(m);
+            va[nb][k] = mk2<T>(-mf * ru.y - sv.x, mf * ru.x - sv.y);
           } else {
             // rot/shear rows hold (u, v) per plane: columns 2p (u), 2p+1 (v).
             const V2<T> ru = __ldcs(cf0 + row * Rc + 2 * p), rv = __ldcs(cf0 + row * Rc + 2 * p + 1);
@@ -271,6 +276,8 @@ void launch_unpack(const sht_plan* p, int mode, const T* cf0, const T* cf1, int6
   if (planes == 0) return;
   if (mode == kUnpackVorDiv)
     launch_unpack_mode<T, kUnpackVorDiv>(p, cf0, cf1, planes, out0, out1, s);
+  else if (mode == kUnpackDiv)
+    launch_unpack_mode<T, kUnpackDiv>(p, cf0, cf1, planes, out0, out1, s);
   else
     launch_unpack_mode<T, kUnpackScalar>(p, cf0, cf1, planes, out0, out1, s);
 }

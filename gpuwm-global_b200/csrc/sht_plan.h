@@ -169,7 +169,9 @@ __device__ __forceinline__ void rowmax_merge(float* rowmax, int64_t col, bool va
     atomicMax(reinterpret_cast<int*>(rowmax + 2 * col + 1), __float_as_int(mim));
   }
 }
-enum UnpackMode { kUnpackScalar = 0, kUnpackVorDiv = 1 };
+// kUnpackDiv: divergence alone, D = i m rot[u] - shear[v], from single-field
+// rotational (cf0, u) and shear (cf1, v) outputs.
+enum UnpackMode { kUnpackScalar = 0, kUnpackVorDiv = 1, kUnpackDiv = 2 };
 template <typename T>
 void launch_unpack(const sht_plan* p, int mode, const T* cf0, const T* cf1, int64_t planes,
                    T* out0, T* out1, cudaStream_t s);
@@ -178,7 +180,14 @@ template <typename T>
 void launch_elementwise(const sht_plan* p, int mode, const T* in, int64_t planes, T* out,
                         cudaStream_t s);
 
-// Helmholtz (sht_helmholtz.cu).
+// Semi-implicit maps (sht_helmholtz.cu).  `mats` packs B, C, V, V^-1,
+// lambda and, when has_thermo, W, W^-1, mu (the thermodynamic block's modes).
+enum SemiMode { kSemiSolve = 0, kSemiApply = 1, kSemiHalf = 2 };
+template <typename T>
+void launch_semi_implicit(const sht_plan* p, int nlev, const T* mats, bool has_thermo, int mode,
+                          double dt, double alpha, const T* div, const T* theta, const T* lnps,
+                          T* odiv, T* otheta, T* olnps, T* metric, T* cfold, float* rowmax,
+                          cudaStream_t s);
 template <typename T>
 void launch_helmholtz(const sht_plan* p, int nlev, const T* mats, double tau_w,
                       const T* div, const T* theta, const T* lnps, T* odiv, T* otheta,
@@ -190,7 +199,7 @@ void launch_waist_export(const sht_plan* p, const T* wfold, int64_t planes, doub
                          T* waist, cudaStream_t s);
 template <typename T>
 void launch_waist_import(const sht_plan* p, const T* waist, int64_t planes, double c, T* wfold,
-                         float* rowmax, cudaStream_t s);
+                         float* rowmax, cudaStream_t s, int fields = 1);
 
 // Split-precision tensor-core path (sht_gemm_tc.cu).
 void build_tc_tables(sht_plan* p, const double* basis64, const double* dbasis64,

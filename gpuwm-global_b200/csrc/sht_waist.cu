@@ -70,10 +70,15 @@ __global__ void __launch_bounds__(256) waist_export_kernel(int Tn, int H, int nl
   }
 }
 
+// `fields` F > 1: the input is a stack of F fields of planes / F planes each
+// (field-major, the reference's stacked (u, v) waist), written with the
+// fields interleaved per plane (column plane * F + field), the layout the
+// multi-field contractions and their epilogues read.
 template <typename T>
 __global__ void __launch_bounds__(256) waist_import_kernel(int Tn, int H, int nlat, int nlat_odd,
                                                            double c, const V2<T>* __restrict__ in,
-                                                           int64_t planes, V2<T>* __restrict__ wf,
+                                                           int64_t planes, int fields,
+                                                           V2<T>* __restrict__ wf,
                                                            float* __restrict__ rowmax) {
   __shared__ V2<T> tile[2][32][33];  // [S/D][plane][order]
   __shared__ float red[2][8][32];
@@ -104,12 +109,14 @@ __global__ void __launch_bounds__(256) waist_import_kernel(int Tn, int H, int nl
   __syncthreads();
   float mre = 0.f, mim = 0.f;
   const int64_t p = p0 + tx;
+  const int64_t per_field = planes / fields;
+  const int64_t col = fields == 1 ? p : (p % per_field) * fields + p / per_field;
   for (int mm = ty; mm < 32; mm += 8) {
     const int m = m0 + mm;
     if (m >= t1 || p >= planes) continue;
     const V2<T> S = tile[0][tx][mm], D = tile[1][tx][mm];
-    wf[((int64_t)(m * 2 + 0) * H + h) * planes + p] = S;
-    wf[((int64_t)(m * 2 + 1) * H + h) * planes + p] = D;
+    wf[((int64_t)(m * 2 + 0) * H + h) * planes + col] = S;
+    wf[((int64_t)(m * 2 + 1) * H + h) * planes + col] = D;
     mre = fmaxf(mre, fmaxf((float)fabs(S.x), (float)fabs(D.x)));
     mim = fmaxf(mim, fmaxf((float)fabs(S.y), (float)fabs(D.y)));
   }
@@ -123,8 +130,8 @@ __global__ void __launch_bounds__(256) waist_import_kernel(int Tn, int H, int nl
         ra = fmaxf(ra, red[0][k][tx]);
         rb = fmaxf(rb, red[1][k][tx]);
       }
-      atomicMax(reinterpret_cast<int*>(rowmax + 2 * p), __float_as_int(ra));
-      atomicMax(reinterpret_cast<int*>(rowmax + 2 * p + 1), __float_as_int(rb));
+      atomicMax(reinterpret_cast<int*>(rowmax + 2 * col), __float_as_int(ra));
+      atomicMax(reinterpret_cast<int*>(rowmax + 2 * col + 1), __float_as_int(rb));
     }
   }
 }
@@ -145,13 +152,14 @@ void launch_waist_export(const sht_plan* p, const T* wfold, int64_t planes, doub
 
 template <typename T>
 void launch_waist_import(const sht_plan* p, const T* waist, int64_t planes, double c, T* wfold,
-                         float* rowmax, cudaStream_t s) {
+                         float* rowmax, cudaStream_t s, int fields) {
   if (planes == 0) return;
+  SHT_REQUIRE(fields >= 1 && planes % fields == 0, "waist import: planes not a multiple of fields");
   dim3 grid((unsigned)div_up(p->T + 1, 32), (unsigned)p->H, (unsigned)div_up(planes, 32));
   SHT_REQUIRE(grid.z <= 65535, "too many planes for one waist launch");
   waist_import_kernel<T><<<grid, dim3(32, 8), 0, s>>>(p->T, p->H, p->nlat, p->nlat_odd ? 1 : 0, c,
-                                                      (const V2<T>*)waist, planes, (V2<T>*)wfold,
-                                                      rowmax);
+                                                      (const V2<T>*)waist, planes, fields,
+                                                      (V2<T>*)wfold, rowmax);
   SHT_CUDA_OR_THROW(cudaGetLastError());
 }
 
@@ -159,7 +167,7 @@ void launch_waist_import(const sht_plan* p, const T* waist, int64_t planes, doub
   template void launch_waist_export<T>(const sht_plan*, const T*, int64_t, double, int, T*,     \
                                        cudaStream_t);                                           \
   template void launch_waist_import<T>(const sht_plan*, const T*, int64_t, double, T*, float*,  \
-                                       cudaStream_t);
+                                       cudaStream_t, int);
 INST(float)
 INST(double)
 #undef INST

@@ -171,6 +171,21 @@ int sht_wind_from_vordiv(sht_plan* plan, const void* vorticity, const void* dive
 int sht_vordiv_from_wind(sht_plan* plan, const void* u, const void* v, int64_t planes,
                          void* vorticity, void* divergence, void* stream);
 
+/* Vorticity/divergence from the Fourier waist of a stacked (u, v) pair,
+ * `waist` = (2, planes, nlat, T+1) complex in the layout of
+ * sht_fourier_waist (u first): the contraction half of vordiv_from_wind,
+ * for a waist a band pipeline filled.
+ * VorticityDivergenceOperator.vordiv_from_wind_waist / _vordiv_from_fourier
+ * (vector.py:75-82, 113-134). */
+int sht_vordiv_from_waist(sht_plan* plan, const void* waist, int64_t planes, void* vorticity,
+                          void* divergence, void* stream);
+
+/* The divergence alone from the same stacked (u, v) waist:
+ * D = i m rot[u] - shear[v], each contraction over one field's rows.
+ * VorticityDivergenceOperator.divergence_from_fourier (vector.py:136-166). */
+int sht_divergence_from_waist(sht_plan* plan, const void* waist, int64_t planes,
+                              void* divergence, void* stream);
+
 /* Triangle mask and Imag(c[n,0]) = 0.  project (transform.py:1124-1144).
  * in and out may alias. */
 int sht_project(sht_plan* plan, const void* in, int64_t planes, void* out, void* stream);
@@ -214,6 +229,48 @@ int sht_vertical_destroy(sht_vertical* op);
 int sht_helmholtz_apply(sht_plan* plan, const sht_vertical* op, double tau_w,
                         const void* divergence, const void* theta, const void* lnps,
                         void* out_divergence, void* out_theta, void* out_lnps, void* stream);
+
+/* An operator that also carries the modes of the thermodynamic block C B
+ * (x_eigvec W, its inverse, and x_eigenvalues mu, (nlev+1) x (nlev+1) and
+ * nlev+1, row-major; VerticalStructureOperator._build,
+ * semi_implicit.py:551-577), which half_apply needs. */
+int sht_vertical_create_modes(sht_plan* plan, int nlev, const double* b, const double* c,
+                              const double* eigvec, const double* eigvec_inv,
+                              const double* eigenvalues, const double* x_eigvec,
+                              const double* x_eigvec_inv, const double* x_eigenvalues,
+                              sht_vertical** out);
+
+/* The three maps of VerticalModeSemiImplicit on (D, theta, ln ps), with
+ * dt_w = dt (or tau) times the divergence weight:
+ *   SHT_SEMI_SOLVE_SHIFTED  the IMEX stage solve (I - tau w L) y = r
+ *                           (solve_shifted, semi_implicit.py:921-953; alpha ignored);
+ *   SHT_SEMI_APPLY          the off-centred Crank-Nicolson step with weight
+ *                           alpha (apply, semi_implicit.py:887-919);
+ *   SHT_SEMI_HALF_APPLY     its square root (half_apply, semi_implicit.py:845-877;
+ *                           needs sht_vertical_create_modes).
+ * Degree zero passes through and the outputs are projected (_finish,
+ * semi_implicit.py:815-843).  The largest |D' - D| of the call is kept on
+ * the device in the operator; sht_semi_implicit_metric reads it
+ * (synchronising `stream`). */
+#define SHT_SEMI_SOLVE_SHIFTED 0
+#define SHT_SEMI_APPLY 1
+#define SHT_SEMI_HALF_APPLY 2
+int sht_semi_implicit_map(sht_plan* plan, const sht_vertical* op, int mode, double dt_w,
+                          double alpha, const void* divergence, const void* theta,
+                          const void* lnps, void* out_divergence, void* out_theta,
+                          void* out_lnps, void* stream);
+int sht_semi_implicit_metric(const sht_vertical* op, double* max_divergence_increment,
+                             void* stream);
+
+/* solve_shifted fused with the synthesis of the solved divergence: the
+ * solve writes D' straight into the folded synthesis operand, then the
+ * Legendre synthesis and inverse FFT give divergence_grid
+ * (nlev, nlat, nlon).  Equal to sht_helmholtz_apply followed by
+ * sht_inverse of out_divergence, without the pack pass between them. */
+int sht_helmholtz_synthesis(sht_plan* plan, const sht_vertical* op, double tau_w,
+                            const void* divergence, const void* theta, const void* lnps,
+                            void* out_divergence, void* out_theta, void* out_lnps,
+                            void* divergence_grid, void* stream);
 
 /* Autotuner settings of a plan (no counterpart call in the reference, whose
  * tile shapes and band splits are fixed in code; b200sht/autotune.py times

@@ -232,12 +232,25 @@ class DenseSHT:
         return -north[0] + east[1], east[0] + north[1]
 
     def vordiv_from_wind(self, u, v):
-        fm = self.fourier(np.stack([np.asarray(u, np.float64), np.asarray(v, np.float64)]))
+        return self.vordiv_from_fourier(
+            self.fourier(np.stack([np.asarray(u, np.float64), np.asarray(v, np.float64)])))
+
+    def vordiv_from_fourier(self, fourier):
+        """The contraction half of the vector analysis on a stacked (u, v)
+        waist, or on a wider zonal spectrum cut here (vector.py:113-134)."""
+        fm = np.asarray(fourier, dtype=np.complex128)[..., : self.truncation + 1]
         basis_mjn = self.basis_mnj.transpose(0, 2, 1)
         dbasis_mjn = self.dbasis_mnj.transpose(0, 2, 1)
         rot = self._contract(fm * self.rotation_weight, basis_mjn)
         shear = self._contract(fm * self.shear_weight, dbasis_mjn)
         return self.project(rot[1] + shear[0]), self.project(rot[0] - shear[1])
+
+    def divergence_from_fourier(self, fourier):
+        """D = i m rot[u] - shear[v] alone (vector.py:136-166)."""
+        fm = np.asarray(fourier, dtype=np.complex128)[..., : self.truncation + 1]
+        rot = self._contract(fm[0] * self.rotation_weight, self.basis_mnj.transpose(0, 2, 1))
+        shear = self._contract(fm[1] * self.shear_weight, self.dbasis_mnj.transpose(0, 2, 1))
+        return self.project(rot - shear)
 
     # -- diagnostics (transform.py:1813-1863)
     def spectral_weights(self):
@@ -305,3 +318,83 @@ def solve_shifted(divergence, theta, lnps, b_matrix, c_matrix, eigenvalues,
         return c
 
     return proj(d_new), proj(x_new[:-1]), proj(x_new[-1])
+
+
+def _finish(divergence, x, d_new, x_new):
+    """Degree zero passes through, the max divergence increment, projection
+    (semi_implicit.py:815-843)."""
+    t1 = divergence.shape[-1]
+    d_new = np.array(d_new)
+    x_new = np.array(x_new)
+    d_new[:, 0, 0] = divergence[:, 0, 0]
+    x_new[:, 0, 0] = x[:, 0, 0]
+    metric = float(np.max(np.abs(d_new - divergence)))
+    tri = np.tri(t1, dtype=bool)
+
+    def proj(c):
+        c = c * tri
+        c[..., :, 0] = c[..., :, 0].real
+        return c
+
+    return proj(d_new), proj(x_new[:-1]), proj(x_new[-1]), metric
+
+
+def _wave_k2(t1, radius_m):
+    n = np.arange(t1, dtype=np.float64)
+    return n * (n + 1.0) / radius_m ** 2
+
+
+def apply_crank_nicolson(divergence, theta, lnps, b_matrix, c_matrix, eigenvalues, eigenvectors,
+                         dt_w, alpha, radius_m=EARTH_RADIUS_M):
+    """The off-centred Crank-Nicolson step of the subtracted operator
+    (semi_implicit.py:887-919): ``forcing = D + dt k^2 B x - a(1-a) dt^2 k^2 M D``,
+    ``D' = (I + (a dt)^2 k^2 M)^-1 forcing``, ``x' = x + dt C((1-a) D + a D')``.
+    Returns ``(divergence, theta, lnps, max |D' - D|)``."""
+    k2 = _wave_k2(divergence.shape[-1], radius_m)
+    structure = -b_matrix @ c_matrix
+    inv = helmholtz_inverse(eigenvalues, eigenvectors, k2, dt_w, alpha)
+    x = np.concatenate([theta, lnps[None]], axis=0)
+    kc = k2[None, :, None]
+    forcing = (divergence + dt_w * kc * np.einsum("ij,jnm->inm", b_matrix, x)
+               - (alpha * (1.0 - alpha) * dt_w * dt_w) * kc
+               * np.einsum("ij,jnm->inm", structure, divergence))
+    d_new = np.einsum("nij,jnm->inm", inv, forcing)
+    x_new = x + dt_w * np.einsum("ij,jnm->inm", c_matrix,
+                                 (1.0 - alpha) * divergence + alpha * d_new)
+    return _finish(divergence, x, d_new, x_new)
+
+
+def half_map_scalars(frequencies, dt_s, alpha):
+    """``(p, q)`` with ``sqrt(g) = p + i q omega`` for the off-centred
+    Crank-Nicolson factor ``g = (1 + i(1-a) omega dt) / (1 - i a omega dt)``
+    (principal root); ``omega = 0`` gives ``p = 1, q = dt/2``
+    (semi_implicit.py:611-627)."""
+    y = frequencies * float(dt_s)
+    root = np.sqrt((1.0 + 1j * (1.0 - alpha) * y) / (1.0 - 1j * alpha * y))
+    safe = np.where(frequencies > 0.0, frequencies, 1.0)
+    return root.real, np.where(frequencies > 0.0, root.imag / safe, 0.5 * float(dt_s))
+
+
+def half_apply(divergence, theta, lnps, b_matrix, c_matrix, eigenvalues, eigenvectors,
+               x_eigenvalues, x_eigenvectors, dt_w, alpha, radius_m=EARTH_RADIUS_M):
+    """The square root ``H = P + Q L`` of the Crank-Nicolson map, per block
+    and degree (semi_implicit.py:629-663, 845-877):
+    ``D' = P_D D + Q_D k^2 B x``, ``x' = P_x x + Q_x C D``, with
+    ``P_D = V diag(p) V^-1`` at frequencies ``k sqrt(lambda)`` and ``P_x``,
+    ``Q_x`` in the modes of ``C B`` at ``k sqrt(-mu)``."""
+    k2 = _wave_k2(divergence.shape[-1], radius_m)
+    k = np.sqrt(k2)
+    p_d, q_d = half_map_scalars(k[:, None] * np.sqrt(eigenvalues)[None, :], dt_w, alpha)
+    p_x, q_x = half_map_scalars(k[:, None] * np.sqrt(-np.asarray(x_eigenvalues))[None, :],
+                                dt_w, alpha)
+    v, vi = eigenvectors, np.linalg.inv(eigenvectors)
+    w, wi = x_eigenvectors, np.linalg.inv(x_eigenvectors)
+    maps = [np.einsum("ij,nj,jk->nik", a, s, b) for a, s, b in
+            ((v, p_d, vi), (v, q_d, vi), (w, p_x, wi), (w, q_x, wi))]
+    x = np.concatenate([theta, lnps[None]], axis=0)
+    l_div = k2[None, :, None] * np.einsum("ij,jnm->inm", b_matrix, x)
+    l_x = np.einsum("ij,jnm->inm", c_matrix, divergence)
+    d_new = (np.einsum("nij,jnm->inm", maps[0], divergence)
+             + np.einsum("nij,jnm->inm", maps[1], l_div))
+    x_new = np.einsum("nij,jnm->inm", maps[2], x) + np.einsum("nij,jnm->inm", maps[3], l_x)
+    return _finish(divergence, x, d_new, x_new)
