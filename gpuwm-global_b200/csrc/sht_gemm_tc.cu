@@ -58,15 +58,24 @@
 
 #include "sht_plan.h"
 
-struct ShtTcTile {
-  int group;    // index into the launch's group list
-  int problem;  // index into the direction's descriptor list
-  int n0;       // first x of the tile
-  int nsize;    // tile N (multiple of 16, <= 256); 0 for an empty problem
-  int kst;      // K stages of BK (0 for an empty problem: the tile writes zeros)
-  int r0;       // first data row
-  int img;      // index of the tile's (problem, n-tile) image block
+// One tile of a launch, self-contained: every role reads one 64-byte record
+// per tile (staged in shared memory per CTA) instead of a chain of dependent
+// global loads (tile -> descriptor -> image offset) at each tile start.
+struct alignas(16) ShtTcTile {
+  int group;      // index into the launch's group list
+  int problem;    // index into the direction's descriptor list
+  int n0;         // first x of the tile
+  int nsize;      // tile N (multiple of 16, <= 128); 0 for an empty problem
+  int kst;        // K stages of BK (0 for an empty problem: the tile writes zeros)
+  int r0;         // first data row
+  int X;          // the problem's output extent (columns past it are not stored)
+  int K;          // the problem's contraction extent
+  int64_t img;    // byte offset of the tile's table image (k-stage 0)
+  int64_t d_row;  // data row of the problem's k = 0
+  int64_t c_row;  // output row of the problem's x = 0
+  int64_t cs;     // column-scale index of the problem's x = 0
 };
+static_assert(sizeof(ShtTcTile) == 64, "tile records are 64 bytes");
 
 struct ShtTc16 {
   // Per table kind (basis, dbasis, analysis, rot, shear): the hi/lo images
@@ -94,12 +103,23 @@ constexpr int BK = 32;
 constexpr int NPARTS = 2;
 constexpr int NMAX = 128;   // tile N
 constexpr int kMaxNBuf = 2;
-constexpr int kEpiWarps = 8;                     // two per TMEM lane quarter
+// Roles: warp 0 table loader (and TMEM owner), warp 1 MMA issuer, warps 2-9
+// the epilogue (two per TMEM lane quarter), warps 10-17 the converters,
+// warp 18 the data-tile TMA loader.
+constexpr int kEpiWarp0 = 2;
+constexpr int kEpiWarps = 8;
 constexpr int kEpiThreads = kEpiWarps * 32;
 constexpr int kConvThreads = 256;
-constexpr int kConvWarp0 = 2 + kEpiWarps;
-constexpr int kThreads = kConvWarp0 * 32 + kConvThreads;  // 576
+constexpr int kConvWarp0 = kEpiWarp0 + kEpiWarps;
+constexpr int kRawWarp = kConvWarp0 + kConvThreads / 32;
+constexpr int kThreads = (kRawWarp + 1) * 32;  // 608
 constexpr long long kWaitBudget = 4000000000LL;  // clock cycles (~2 s)
+// Per-CTA staging in shared memory: the CTA's tile records (when it has at
+// most kMaxCtaTiles) and the power-of-two row scales of every group (when the
+// launch has at most kMaxRowScales data rows); larger launches read both from
+// global memory.
+constexpr int kMaxCtaTiles = 192;
+constexpr int kMaxRowScales = 2048;
 
 // Shared-memory pieces (bytes).
 constexpr int kAPart = BM * BK * 2;      // one FP16 part of the A stage: 8 KB
@@ -136,11 +156,13 @@ struct AccPlan {
   static constexpr int kOffB = kOffA + (A_TMEM ? 0 : NA * NPARTS * kAPart);   // [S][NPARTS][kBPart]
   static constexpr int kOffRaw = kOffB + S * NPARTS * kBPart;                 // [S][4 boxes], swizzled
   static constexpr int kOffBar = kOffRaw + S * kRawStage;                     // mbarriers (8 B each)
-  static constexpr int kNumBars = 3 * S + 2 * NA + 2 * kMaxNBuf + 1;
+  static constexpr int kNumBars = 4 * S + 2 * NA + 2 * kMaxNBuf + 1;
   static_assert(kOffRaw % 1024 == 0, "128-byte swizzled TMA destinations are 1024-byte aligned");
   static constexpr int kOffMisc = kOffBar + kNumBars * 8;           // tmem base, abort flag
   static constexpr int kOffCs = (kOffMisc + 16 + 127) / 128 * 128;  // [epilogue warps][NMAX] floats
-  static constexpr int kSmemBytes = kOffCs + kEpiWarps * NMAX * 4 + 1024;  // + alignment slack
+  static constexpr int kOffTiles = kOffCs + kEpiWarps * NMAX * 4;     // [kMaxCtaTiles] tile records
+  static constexpr int kOffRs = kOffTiles + kMaxCtaTiles * (int)sizeof(ShtTcTile);  // row scales
+  static constexpr int kSmemBytes = kOffRs + kMaxRowScales * 4 + 1024;  // + alignment slack
   static_assert(kSmemBytes <= 227 * 1024, "shared memory plan exceeds 227 KB");
 };
 using kAccurate = AccPlan<3, 1>;
@@ -329,21 +351,21 @@ __device__ __forceinline__ float pow2_scale(float mx) {
 struct alignas(64) TcGroup {
   CUtensorMap data_map;    // the data operand as a [rows][R] FP32 tensor (when use_tma)
   int use_tma;             // 1: the loader brings the data tiles in by TMA
-  const ShtGemmDesc* descs;
   const unsigned char* img;
-  const int64_t* img_off;  // per (problem, n-tile) block: byte offset of k-stage 0
   const float* colscale;
-  const int64_t* cs_off;   // per problem
   const float* data;
   const float* rowmax;     // per data row: max |value| (from the producer kernel)
   float* out;
   int64_t R;
+  int rs_off;              // first entry of this group's row scales in shared memory
 };
 
 struct TcArgs {
   TcGroup g[kMaxTcGroups];
   const ShtTcTile* tiles;
   int n_tiles;
+  int stage_rs;            // 1: the launch's row scales fit in shared memory
+  int rs_total;            // their count
   unsigned* err;
 };
 
@@ -351,11 +373,12 @@ struct Pipe {
   uint64_t* full_a;    // [NA] the data operand of a slot is converted
   uint64_t* full_b;    // [S]
   uint64_t* empty;     // [S] the MMAs of a shared stage are done
-  uint64_t* full_raw;  // [S] the FP32 data tile of a stage has landed (TMA)
+  uint64_t* full_raw;  // [S] the FP32 data tile of a raw stage has landed (TMA)
   uint64_t* a_empty;   // [NA] the MMAs of a TMEM data slot are done (A_TMEM)
-  uint64_t* acc_full;
-  uint64_t* acc_empty;
+  uint64_t* acc_full;   // [kMaxNBuf]
+  uint64_t* acc_empty;  // [kMaxNBuf]
   uint64_t* done;
+  uint64_t* raw_empty;  // [S] the converters have read a raw stage
   volatile int* abort;
 };
 
@@ -421,6 +444,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
           bars + 2 * NA + 3 * S,
           bars + 2 * NA + 3 * S + kMaxNBuf,
           bars + 2 * NA + 3 * S + 2 * kMaxNBuf,
+          bars + 2 * NA + 3 * S + 2 * kMaxNBuf + 1,
           abort_flag};
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -433,6 +457,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
       mbar_init(&pp.full_b[s], 1);
       mbar_init(&pp.empty[s], 1);
       mbar_init(&pp.full_raw[s], 1);
+      mbar_init(&pp.raw_empty[s], kConvThreads / 32);
     }
     for (int b = 0; b < kMaxNBuf; ++b) {
       mbar_init(&pp.acc_full[b], 1);
@@ -446,6 +471,32 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
     tmem_alloc(tmem_base_smem, 512);
     tmem_relinquish();
   }
+  // This CTA's tile records and the launch's row scales, staged once.
+  ShtTcTile* s_tiles = reinterpret_cast<ShtTcTile*>(smem + Acc::kOffTiles);
+  float* s_rs = reinterpret_cast<float*>(smem + Acc::kOffRs);
+  const int my_tiles = (int)blockIdx.x < a.n_tiles ? (a.n_tiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+  const bool staged = my_tiles <= kMaxCtaTiles;
+  if (staged) {
+    const uint4* src = reinterpret_cast<const uint4*>(a.tiles);
+    uint4* dst = reinterpret_cast<uint4*>(s_tiles);
+    for (int e = threadIdx.x; e < my_tiles * 4; e += blockDim.x)
+      dst[e] = src[((int64_t)blockIdx.x + (int64_t)(e >> 2) * gridDim.x) * 4 + (e & 3)];
+  }
+  if (a.stage_rs) {
+#pragma unroll 1
+    for (int gi = 0; gi < kMaxTcGroups; ++gi) {
+      const TcGroup& G = a.g[gi];
+      for (int64_t r = threadIdx.x; r < G.R; r += blockDim.x) s_rs[G.rs_off + r] = pow2_scale(G.rowmax[r]);
+    }
+  }
+  // The k-th tile of this CTA (tile index blockIdx.x + k * gridDim.x).
+  auto tile_k = [&](int k) -> ShtTcTile {
+    return staged ? s_tiles[k] : a.tiles[(int64_t)blockIdx.x + (int64_t)k * gridDim.x];
+  };
+  // Power-of-two scale of data row r (< R) of a group.
+  auto row_scale = [&](const TcGroup& G, int64_t r) -> float {
+    return a.stage_rs ? s_rs[G.rs_off + r] : pow2_scale(G.rowmax[r]);
+  };
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
@@ -456,16 +507,15 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
     if (lane == 0) {
       int stage = 0;
       uint32_t phase = 0;
-      int armed[S], armed_raw[S];
+      int armed[S];
 #pragma unroll
-      for (int s = 0; s < S; ++s) armed[s] = armed_raw[s] = -1;
-      for (int t = blockIdx.x; t < a.n_tiles && !*abort_flag; t += gridDim.x) {
-        const ShtTcTile tl = a.tiles[t];
+      for (int s = 0; s < S; ++s) armed[s] = -1;
+      for (int k = 0; k < my_tiles && !*abort_flag; ++k) {
+        const ShtTcTile tl = tile_k(k);
         if (reject_tile(tl, abort_flag, a.err)) break;
         const TcGroup& G = a.g[tl.group];
         const int part = tl.nsize * BK * 2;  // bytes of one FP16 part of one stage
-        const unsigned char* src = G.img + G.img_off[tl.img];
-        const int64_t d_row = G.use_tma ? G.descs[tl.problem].d_row : 0;
+        const unsigned char* src = G.img + tl.img;
         bool ok = true;
         for (int ks = 0; ks < tl.kst; ++ks) {
           if (!wait_bar(&pp.empty[stage], phase ^ 1, pp, a.err, 1)) {
@@ -479,17 +529,6 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
             bulk_g2s(dst + pt * kBPart, src + ((int64_t)ks * NPARTS + pt) * part, part,
                      &pp.full_b[stage]);
           armed[stage] = (int)phase;
-          if (G.use_tma) {
-            // The stage's FP32 data tile: rows r0 .. r0+127 as four 32-row
-            // boxes, contraction rows d_row + ks*BK .. +BK-1.
-            mbar_arrive_expect_tx(&pp.full_raw[stage], kRawStage);
-            unsigned char* raw = sRaw + stage * kRawStage;
-#pragma unroll
-            for (int q = 0; q < BM / 32; ++q)
-              tma_load_2d(raw + q * kRawBox, &G.data_map, tl.r0 + 32 * q,
-                          (int)(d_row + (int64_t)ks * BK), &pp.full_raw[stage]);
-            armed_raw[stage] = (int)phase;
-          }
           if (++stage == S) { stage = 0; phase ^= 1; }
         }
         if (!ok) break;
@@ -502,10 +541,50 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
         if (armed[s] >= 0)
           while (!mbar_try_wait(&pp.full_b[s], (uint32_t)armed[s]) && clock64() - t0 < kWaitBudget) {
           }
-        t0 = clock64();
-        if (armed_raw[s] >= 0)
-          while (!mbar_try_wait(&pp.full_raw[s], (uint32_t)armed_raw[s]) &&
-                 clock64() - t0 < kWaitBudget) {
+      }
+    }
+  } else if (warp == kRawWarp) {
+    // ---------------------------------------------------- data-tile loader
+    // The FP32 data tiles by TMA into their own ring of S raw stages, each
+    // refilled as soon as the converters have read it (not when the MMAs of
+    // its stage finish): the data runs up to S stages ahead of the converted
+    // operand ring, which is what keeps the tensor pipe fed across the
+    // memory latency.
+    if (lane == 0 && a.g[0].use_tma) {
+      int stage = 0;
+      uint32_t phase = 0;
+      int armed[S];
+#pragma unroll
+      for (int s = 0; s < S; ++s) armed[s] = -1;
+      for (int k = 0; k < my_tiles && !*abort_flag; ++k) {
+        const ShtTcTile tl = tile_k(k);
+        if (reject_tile(tl, abort_flag, a.err)) break;
+        const TcGroup& G = a.g[tl.group];
+        bool ok = true;
+        for (int ks = 0; ks < tl.kst; ++ks) {
+          if (!wait_bar(&pp.raw_empty[stage], phase ^ 1, pp, a.err, 9)) {
+            ok = false;
+            break;
+          }
+          // Rows r0 .. r0+127 as four 32-row boxes, contraction rows
+          // d_row + ks*BK .. +BK-1.
+          mbar_arrive_expect_tx(&pp.full_raw[stage], kRawStage);
+          unsigned char* raw = sRaw + stage * kRawStage;
+#pragma unroll
+          for (int q = 0; q < BM / 32; ++q)
+            tma_load_2d(raw + q * kRawBox, &G.data_map, tl.r0 + 32 * q,
+                        (int)(tl.d_row + (int64_t)ks * BK), &pp.full_raw[stage]);
+          armed[stage] = (int)phase;
+          if (++stage == S) { stage = 0; phase ^= 1; }
+        }
+        if (!ok) break;
+      }
+      // Drain: every armed copy lands before the CTA exits (after an abort
+      // this wait keeps a late copy from writing freed shared memory).
+      for (int s = 0; s < S; ++s) {
+        long long t0 = clock64();
+        if (armed[s] >= 0)
+          while (!mbar_try_wait(&pp.full_raw[s], (uint32_t)armed[s]) && clock64() - t0 < kWaitBudget) {
           }
       }
     }
@@ -518,8 +597,8 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
       uint32_t aphase = 0;
       uint32_t acc_it = 0;  // accumulator set = acc_it % NBUF, parity = (acc_it / NBUF) & 1
       bool issued = false;
-      for (int t = blockIdx.x; t < a.n_tiles && !*abort_flag; t += gridDim.x) {
-        const ShtTcTile tl = a.tiles[t];
+      for (int k = 0; k < my_tiles && !*abort_flag; ++k) {
+        const ShtTcTile tl = tile_k(k);
         if (reject_tile(tl, abort_flag, a.err)) break;
         if (tl.kst == 0) continue;
         const uint32_t buf = acc_it % NBUF, acc_phase = (acc_it / NBUF) & 1;
@@ -602,41 +681,39 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
     // consecutive r (one 128-byte line per store), so no staging through
     // shared memory is needed (the tensor core's operand reads have its whole
     // bandwidth).  The accumulator goes back to the MMA warp once its last
-    // chunk is in registers.  Every decision that steers the epilogue's named
-    // barrier is reduced over its eight warps (epi_bar_or), so all 256 threads
-    // take the same path, and the warp-collective tcgen05.ld is entered
-    // warp-uniformly.
+    // chunk is in registers.  Every decision that steers the epilogue's named barrier is reduced over
+    // its eight warps (epi_bar_or), so all 256 threads take the same path,
+    // and the warp-collective tcgen05.ld is entered warp-uniformly.
     const int eg = warp & 3;  // TMEM lane group accessible to this warp
-    const int half = (warp - 2) / 4;
+    const int half = (warp - kEpiWarp0) / 4;
     const int row = eg * 32 + lane;
-    float* cs_s = reinterpret_cast<float*>(smem + Acc::kOffCs) + (warp - 2) * NMAX;  // this warp's copy
+    float* cs_s = reinterpret_cast<float*>(smem + Acc::kOffCs) + (warp - kEpiWarp0) * NMAX;  // this warp's copy
     uint32_t acc_it = 0;
-    for (int t = blockIdx.x; t < a.n_tiles; t += gridDim.x) {
-      const ShtTcTile tl = a.tiles[t];
+    for (int k = 0; k < my_tiles; ++k) {
+      const ShtTcTile tl = tile_k(k);
       if (reject_tile(tl, abort_flag, a.err)) break;  // the same tile for all 256 threads
       const TcGroup& G = a.g[tl.group];
-      const ShtGemmDesc d = G.descs[tl.problem];
       const int64_t R = G.R;
       const int64_t r = tl.r0 + row;
-      float* outb = G.out + d.c_row * R;
+      float* outb = G.out + tl.c_row * R;
       const int cbeg = half * (NMAX / 2), cend = min(tl.nsize, cbeg + NMAX / 2);
       if (tl.kst == 0) {
         // empty contraction (K = 0): the output block is zero
         if (r < R)
-          for (int x = tl.n0 + cbeg; x < min(tl.n0 + cend, d.X); ++x) outb[(int64_t)x * R + r] = 0.f;
+          for (int x = tl.n0 + cbeg; x < min(tl.n0 + cend, tl.X); ++x) outb[(int64_t)x * R + r] = 0.f;
         continue;
       }
       // The tile's row and column scales are fetched while the MMAs run: the
       // column scales into this warp's shared copy (one L2 round trip per
       // tile instead of one per 16-column chunk).
-      const float rs = r < R ? 1.f / pow2_scale(G.rowmax[r]) : 0.f;
+      const float rs = r < R ? __frcp_rn(row_scale(G, r)) : 0.f;  // exact: a power of two
       {
-        const float* cs = G.colscale + G.cs_off[tl.problem];
+        const float* cs = G.colscale + tl.cs;
         __syncwarp();  // the previous tile's reads of cs_s are done
 #pragma unroll
         for (int j = 0; j < NMAX / 32; ++j) {
           const int c = j * 32 + lane;
-          cs_s[c] = (c < tl.nsize && tl.n0 + c < d.X) ? cs[tl.n0 + c] : 0.f;
+          cs_s[c] = (c < tl.nsize && tl.n0 + c < tl.X) ? cs[tl.n0 + c] : 0.f;
         }
         __syncwarp();
       }
@@ -650,7 +727,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
       const int nsteps = tl.kst * (BK / 16);
       const int nseg = nsteps < NMAIN ? nsteps : NMAIN;
       // Columns past the problem's extent are not stored.
-      const int ncols = min(tl.nsize, d.X - tl.n0);
+      const int ncols = min(tl.nsize, tl.X - tl.n0);
       float* dst = outb + (int64_t)tl.n0 * R + r;
       bool released = false;
       for (int c0 = cbeg; c0 < cend; c0 += 16) {
@@ -716,26 +793,22 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
     const int q4 = warp & 3, kh = (warp - kConvWarp0) >> 2;
     const int rowi = q4 * 32 + lane;
     const uint32_t lane_base = tmem_base + ((uint32_t)(q4 * 32) << 16);
-    int stage = 0;  // shared stage of the raw data (TMA)
+    int stage = 0;  // raw stage of the data (TMA)
     uint32_t phase = 0;
     int aslot = 0;  // TMEM data slot
     uint32_t aphase = 0;
-    for (int t = blockIdx.x; t < a.n_tiles; t += gridDim.x) {
-      const ShtTcTile tl = a.tiles[t];
+    for (int k = 0; k < my_tiles; ++k) {
+      const ShtTcTile tl = tile_k(k);
       if (reject_tile(tl, abort_flag, a.err)) break;
       if (tl.kst == 0) continue;
       const TcGroup& G = a.g[tl.group];
-      const ShtGemmDesc d = G.descs[tl.problem];
       const int64_t R = G.R;
       const int64_t r = tl.r0 + rowi;
-      const float sc = r < R ? pow2_scale(G.rowmax[r]) : 1.f;
-      const float* Db = G.data + d.d_row * R;
+      const float sc = r < R ? row_scale(G, r) : 1.f;
+      const float* Db = G.data + tl.d_row * R;
       bool ok = true;
       for (int ks = 0; ks < tl.kst; ++ks) {
         float v[16];
-        // The TMEM slot's previous MMAs are done.
-        ok = wait_bar(&pp.a_empty[aslot], aphase ^ 1, pp, a.err, 7);
-        if (!ok) break;
         if (G.use_tma) {
           // Box q4 of the stage holds rows q4*32 .. +31 as 128-byte k rows,
           // 16-byte chunks swizzled by k % 8.
@@ -747,15 +820,21 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
             const int kl = kh * 16 + i;
             const float x = *reinterpret_cast<const float*>(
                 box + kl * 128 + ((((lane >> 2) ^ (kl & 7))) << 4) + (lane & 3) * 4);
-            v[i] = ks * BK + kl < d.K ? x : 0.f;  // rows past K belong to the next problem
+            v[i] = ks * BK + kl < tl.K ? x : 0.f;  // rows past K belong to the next problem
           }
+          __syncwarp();  // the warp's reads of the raw stage are done
+          if (lane == 0) mbar_arrive(&pp.raw_empty[stage]);
+          if (++stage == S) { stage = 0; phase ^= 1; }
         } else {
 #pragma unroll
           for (int i = 0; i < 16; ++i) {
             const int k = ks * BK + kh * 16 + i;
-            v[i] = (k < d.K && r < R) ? __ldg(Db + (int64_t)k * R + r) : 0.f;
+            v[i] = (k < tl.K && r < R) ? __ldg(Db + (int64_t)k * R + r) : 0.f;
           }
         }
+        // The TMEM slot's previous MMAs are done.
+        ok = wait_bar(&pp.a_empty[aslot], aphase ^ 1, pp, a.err, 7);
+        if (!ok) break;
         uint32_t hi[8], lo[8];
 #pragma unroll
         for (int c = 0; c < 8; ++c) {
@@ -773,7 +852,6 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
         tc_fence_before();
         mbar_arrive(&pp.full_a[aslot]);
         if (++aslot == NA) { aslot = 0; aphase ^= 1; }
-        if (++stage == S) { stage = 0; phase ^= 1; }
       }
       if (!ok) break;
     }
@@ -784,20 +862,21 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
     // and a warp's 32 stores cover 512 contiguous bytes (no bank conflicts).
     const int ct = threadIdx.x - kConvWarp0 * 32;  // 0..255
     const int kk = ct & 7, mg = (ct >> 3) & 15, kgs = ct >> 7;
-    int stage = 0;
+    int stage = 0;  // converted-operand stage (shared with the table stage and the MMA)
     uint32_t phase = 0;
-    for (int t = blockIdx.x; t < a.n_tiles; t += gridDim.x) {
-      const ShtTcTile tl = a.tiles[t];
+    int rstage = 0;  // raw stage of the data (TMA)
+    uint32_t rphase = 0;
+    for (int k = 0; k < my_tiles; ++k) {
+      const ShtTcTile tl = tile_k(k);
       if (reject_tile(tl, abort_flag, a.err)) break;
       if (tl.kst == 0) continue;
       const TcGroup& G = a.g[tl.group];
-      const ShtGemmDesc d = G.descs[tl.problem];
       const int64_t R = G.R;
-      const float* Db = G.data + d.d_row * R;
+      const float* Db = G.data + tl.d_row * R;
       const int64_t rbase = tl.r0 + mg * 8;
       float sc[8];
 #pragma unroll
-      for (int i = 0; i < 8; ++i) sc[i] = rbase + i < R ? pow2_scale(G.rowmax[rbase + i]) : 1.f;
+      for (int i = 0; i < 8; ++i) sc[i] = rbase + i < R ? row_scale(G, rbase + i) : 1.f;
       const bool full_rows = rbase + 8 <= R && (R % 4) == 0;
       // Stage ks + 1 is loaded while stage ks waits for its slot and is
       // converted (two register buffers, swapped by a 2x unrolled loop).
@@ -805,7 +884,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
 #pragma unroll
         for (int j = 0; j < BK / 16; ++j) {
           const int k = ks * BK + (kgs + 2 * j) * 8 + kk;
-          if (k < d.K) {
+          if (k < tl.K) {
             const float* p = Db + (int64_t)k * R + rbase;
             if (full_rows) {
               const float4 u0 = __ldg(reinterpret_cast<const float4*>(p));
@@ -827,7 +906,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
       // by (k mod 8), which makes this warp's reads (8 consecutive k of one
       // 8-row group per quarter warp) bank-conflict free.
       auto fetch_raw = [&](int ks, float (&v)[BK / 16][8]) {
-        const unsigned char* raw = sRaw + stage * kRawStage + (mg >> 2) * kRawBox;
+        const unsigned char* raw = sRaw + rstage * kRawStage + (mg >> 2) * kRawBox;
 #pragma unroll
         for (int j = 0; j < BK / 16; ++j) {
           const int kl = (kgs + 2 * j) * 8 + kk;  // k within the stage
@@ -835,7 +914,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
           const int c0 = (mg & 3) * 2;
           const float4 u0 = *reinterpret_cast<const float4*>(row + ((c0 ^ (kl & 7)) << 4));
           const float4 u1 = *reinterpret_cast<const float4*>(row + (((c0 + 1) ^ (kl & 7)) << 4));
-          const bool live = ks * BK + kl < d.K;  // rows past K belong to the next problem
+          const bool live = ks * BK + kl < tl.K;  // rows past K belong to the next problem
           v[j][0] = live ? u0.x : 0.f; v[j][1] = live ? u0.y : 0.f;
           v[j][2] = live ? u0.z : 0.f; v[j][3] = live ? u0.w : 0.f;
           v[j][4] = live ? u1.x : 0.f; v[j][5] = live ? u1.y : 0.f;
@@ -869,13 +948,16 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
       bool ok = true;
       float va[BK / 16][8], vb[BK / 16][8];
       if (G.use_tma) {
-        // The loader issued this stage's data after the slot was freed, so
-        // the data's arrival is also the slot's.
+        // Read the raw stage into registers and hand it back at once, then
+        // wait for the converted-operand slot.
         for (int ks = 0; ks < tl.kst && ok; ++ks) {
-          ok = wait_bar(&pp.full_raw[stage], phase, pp, a.err, 8);
+          ok = wait_bar(&pp.full_raw[rstage], rphase, pp, a.err, 8);
           if (!ok) break;
           fetch_raw(ks, va);
-          ok = convert_stage(va, false);
+          __syncwarp();  // the warp's reads of the raw stage are done
+          if ((threadIdx.x & 31) == 0) mbar_arrive(&pp.raw_empty[rstage]);
+          if (++rstage == S) { rstage = 0; rphase ^= 1; }
+          ok = convert_stage(va, true);
         }
       } else {
         load_stage(0, va);
@@ -1185,7 +1267,10 @@ void launch_gemm_tc_groups(const TcGroupSpec* g, int ngroups, TcTileCache* cache
   for (int i = 0; i < ngroups; ++i) {
     SHT_REQUIRE(g[i].plan->tc != nullptr, "tensor-core tables not built");
     SHT_REQUIRE(g[i].R < ((int64_t)1 << 26), "tensor-core launch: too many data rows");
+    // Plans of one cache differ in their descriptors: the key names the plan.
+    key.push_back((int64_t)(uintptr_t)g[i].plan);
     key.push_back(g[i].direction);
+    key.push_back(g[i].flip);
     key.push_back(g[i].R);
     rows += g[i].R;
   }
@@ -1206,6 +1291,7 @@ void launch_gemm_tc_groups(const TcGroupSpec* g, int ngroups, TcTileCache* cache
         for (int i = 0; i < np; ++i) {
           const int nt = tc->nt_of[dir][i], ns = tc->nsize_of[dir][i], kst = tc->kst_of[dir][i];
           if (p->h_desc[dir][0][i].X == 0) continue;
+          const ShtGemmDesc& d = p->h_desc[dir][g[gi].flip][i];
           // Order 0: a column tile's row blocks are adjacent (they share its
           // table image); order 1: a row block's column tiles are adjacent
           // (they share its converted data rows).
@@ -1213,7 +1299,19 @@ void launch_gemm_tc_groups(const TcGroupSpec* g, int ngroups, TcTileCache* cache
           for (int64_t o = 0; o < nt * nr; ++o) {
             const int j = order == 0 ? (int)(o / nr) : (int)(o % nt);
             const int64_t r0 = BM * (order == 0 ? o % nr : o / nt);
-            ShtTcTile t{gi, i, j * ns, ns, kst, (int)r0, tc->img_base[dir][i] + j};
+            ShtTcTile t{};
+            t.group = gi;
+            t.problem = i;
+            t.n0 = j * ns;
+            t.nsize = ns;
+            t.kst = kst;
+            t.r0 = (int)r0;
+            t.X = d.X;
+            t.K = d.K;
+            t.img = tc->img_off[dir][tc->img_base[dir][i] + j];
+            t.d_row = d.d_row;
+            t.c_row = d.c_row;
+            t.cs = tc->cs_off[dir][i];
             v.push_back({(int64_t)ns * kst * BK + 4096, t});
           }
         }
@@ -1251,22 +1349,23 @@ void launch_gemm_tc_groups(const TcGroupSpec* g, int ngroups, TcTileCache* cache
       tma = data_map(cache, g[gi].data, g[gi].R, rows, &a.g[gi].data_map);
     }
   }
+  int rs_off = 0;
   for (int gi = 0; gi < ngroups; ++gi) {
     const sht_plan* p = g[gi].plan;
     const ShtTc16* tc = p->tc;
-    const int dir = g[gi].direction;
     TcGroup& G = a.g[gi];
     G.use_tma = tma ? 1 : 0;
-    G.descs = p->d_desc[dir][g[gi].flip];
     G.img = (const unsigned char*)tc->img[g[gi].table_kind];
-    G.img_off = tc->d_img_off[dir];
     G.colscale = tc->colscale[g[gi].table_kind];
-    G.cs_off = tc->d_cs_off[dir];
     G.data = g[gi].data;
     G.rowmax = g[gi].rowmax;
     G.out = g[gi].out;
     G.R = g[gi].R;
+    G.rs_off = rs_off;
+    rs_off += (int)std::min<int64_t>(g[gi].R, kMaxRowScales + 1);
   }
+  a.stage_rs = rs_off <= kMaxRowScales ? 1 : 0;
+  a.rs_total = rs_off;
   a.tiles = list.d;
   a.n_tiles = list.n;
   a.err = g[0].plan->d_err;
