@@ -56,6 +56,7 @@ SIGNATURES = {
     "sht_plan_set_timing": (ctypes.c_int, [_P, ctypes.c_int]),
     "sht_plan_read_timing": (ctypes.c_int, [_P, _DP, ctypes.POINTER(_I64), ctypes.POINTER(_I64),
                                             ctypes.c_int, ctypes.c_int]),
+    "sht_measure_fp32_peak": (ctypes.c_int, [_P, _DP]),
     "sht_forward": (ctypes.c_int, [_P, _P, _I64, _P, _P]),
     "sht_forward_static_scratch": (ctypes.c_int, [_P, _P, _I64, _P, _P]),
     "sht_forward_host": (ctypes.c_int, [_P, _P, _I64, _P, _I64]),

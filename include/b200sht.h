@@ -105,6 +105,14 @@ int sht_plan_set_timing(sht_plan* plan, int enable);
 int sht_plan_read_timing(sht_plan* plan, double* ms, int64_t* launches, int64_t* timed,
                          int n, int reset);
 
+/* Measured FP32 FFMA rate of the current device in TFLOP/s: register-only
+ * fmaf chains on two 512-thread CTAs per SM, timed with CUDA events on
+ * `stream` after a warm-up launch (about 10 ms of GPU time; synchronises on
+ * the stream).  The denominator of the plain FP32 contraction's roofline.
+ * A measurement helper of this engine; the reference has no counterpart
+ * (its profiler, src/arwen_global/profile.py, times whole steps only). */
+int sht_measure_fp32_peak(void* stream, double* tflops);
+
 /* grid -> spectral.  SphericalHarmonicTransform.forward (transform.py:1486). */
 int sht_forward(sht_plan* plan, const void* grid, int64_t planes, void* coeff, void* stream);
 
