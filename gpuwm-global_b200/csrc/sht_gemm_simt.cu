@@ -24,7 +24,7 @@ template <> struct SimtCfg<double> {
 };
 
 template <typename T>
-__global__ void __launch_bounds__(256) gemm_simt_kernel(const ShtGemmDesc* __restrict__ descs,
+__global__ void __launch_bounds__(256, 2) gemm_simt_kernel(const ShtGemmDesc* __restrict__ descs,
                                                         const ShtGemmItem* __restrict__ items,
                                                         const T* __restrict__ table,
                                                         const T* __restrict__ data,
@@ -47,8 +47,17 @@ __global__ void __launch_bounds__(256) gemm_simt_kernel(const ShtGemmDesc* __res
   __shared__ __align__(16) T Bs[2][BK][BR];
 
   const int tid = threadIdx.x;
-  const int tx = tid % NTR;  // r direction
-  const int ty = tid / NTR;  // x direction
+  // Thread -> a TMX x TMR block of contiguous x and r.  Warp w covers the
+  // rows wr * BR/4 .. +BR/4 (wr = w % 4) and the columns wx * BX/2 .. +BX/2
+  // (wx = w / 4); lane -> (lr = lane % 4, lx = lane / 4) within it.  A warp
+  // whose rows or columns lie wholly past the problem's extent (the ragged x
+  // tail of an analysis block, the last partial row block) skips its FFMAs:
+  // the issue slots go to the other warps and CTAs of the SM.
+  const int warp = tid >> 5, lane = tid & 31;
+  const int r_base = (warp & 3) * (BR / 4) + (lane & 3) * TMR;
+  const int x_base = (warp >> 2) * (BX / 2) + (lane >> 2) * TMX;
+  static_assert(4 * TMR * 4 == BR && 8 * TMX * 2 == BX, "warp tiling covers the block");
+  const bool busy = x0 + (warp >> 2) * (BX / 2) < d.X && r0 + (warp & 3) * (BR / 4) < R;
 
   // Global-load mapping: each tile is BK x B{X,R} = 8 x 128 (or 8 x 64);
   // thread loads LPT consecutive elements of one k-row.
@@ -91,27 +100,29 @@ __global__ void __launch_bounds__(256) gemm_simt_kernel(const ShtGemmDesc* __res
   for (int kt = 0; kt < nk; ++kt) {
     const int buf = kt & 1;
     if (kt + 1 < nk) load_global((kt + 1) * BK);
+    if (busy) {
 #pragma unroll
-    for (int kk = 0; kk < BK; ++kk) {
-      T a[TMX], b[TMR];
+      for (int kk = 0; kk < BK; ++kk) {
+        T a[TMX], b[TMR];
 #pragma unroll
-      for (int g = 0; g < GX; ++g) {
-        typename C::V v = *reinterpret_cast<const typename C::V*>(&As[buf][kk][g * (BX / GX) + ty * VW]);
-        const T* pv = reinterpret_cast<const T*>(&v);
+        for (int g = 0; g < GX; ++g) {
+          typename C::V v = *reinterpret_cast<const typename C::V*>(&As[buf][kk][x_base + g * VW]);
+          const T* pv = reinterpret_cast<const T*>(&v);
 #pragma unroll
-        for (int u = 0; u < VW; ++u) a[g * VW + u] = pv[u];
+          for (int u = 0; u < VW; ++u) a[g * VW + u] = pv[u];
+        }
+#pragma unroll
+        for (int g = 0; g < GR; ++g) {
+          typename C::V v = *reinterpret_cast<const typename C::V*>(&Bs[buf][kk][r_base + g * VW]);
+          const T* pv = reinterpret_cast<const T*>(&v);
+#pragma unroll
+          for (int u = 0; u < VW; ++u) b[g * VW + u] = pv[u];
+        }
+#pragma unroll
+        for (int i = 0; i < TMX; ++i)
+#pragma unroll
+          for (int j = 0; j < TMR; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
       }
-#pragma unroll
-      for (int g = 0; g < GR; ++g) {
-        typename C::V v = *reinterpret_cast<const typename C::V*>(&Bs[buf][kk][g * (BR / GR) + tx * VW]);
-        const T* pv = reinterpret_cast<const T*>(&v);
-#pragma unroll
-        for (int u = 0; u < VW; ++u) b[g * VW + u] = pv[u];
-      }
-#pragma unroll
-      for (int i = 0; i < TMX; ++i)
-#pragma unroll
-        for (int j = 0; j < TMR; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
     }
     if (kt + 1 < nk) {
       store_shared(buf ^ 1);
@@ -121,16 +132,14 @@ __global__ void __launch_bounds__(256) gemm_simt_kernel(const ShtGemmDesc* __res
 
   // Epilogue: C[x][r], r innermost.
 #pragma unroll
-  for (int g = 0; g < GX; ++g)
-#pragma unroll
-    for (int u = 0; u < VW; ++u) {
-      int x = x0 + g * (BX / GX) + ty * VW + u;
+  for (int i = 0; i < TMX; ++i) {
+      int x = x0 + x_base + i;
       if (x >= d.X) continue;
       T* crow = Cb + (int64_t)x * R;
 #pragma unroll
       for (int gr = 0; gr < GR; ++gr) {
-        int64_t r = r0 + gr * (BR / GR) + tx * VW;
-        const T* av = &acc[g * VW + u][gr * VW];
+        int64_t r = r0 + r_base + gr * VW;
+        const T* av = &acc[i][gr * VW];
         if (r + VW <= R && (R % VW) == 0) {
           typename C::V v;
           T* pv = reinterpret_cast<T*>(&v);
