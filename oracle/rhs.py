@@ -10,10 +10,13 @@ replace, in their association:
 * the van Leer limited vertical flux divergence (dynamics.py:1355-1434).
 
 The vertical flux divergence is pinned to the reference's own numpy method
-run on seeded columns (``tests/golden/rhs_vertical_flux.npz``, recorded by
-``tests/golden/make_golden_rhs.py``); the three elementwise chains are
-one-line formulas checked against the reference's source by reading
-(parity unpinned by fixtures for those three).
+run on seeded columns (``tests/golden/rhs_vertical_flux.npz``); the three
+elementwise chains are pinned, bit for bit, to the reference's numpy
+specifications of its fused kernels (``tools/gpu_selftest_rhs.py``:
+``momentum_bernoulli_reference``, ``tracer_flux_reference``,
+``scalar_tendency_reference``) run on seeded fields
+(``tests/golden/rhs_elementwise.npz``).  Both fixtures are recorded by
+``tests/golden/make_golden_rhs.py``.
 """
 from __future__ import annotations
 

@@ -60,6 +60,28 @@ def test_tracer_flux_and_tendency(dt, lead):
 
 
 @pytest.mark.parametrize("dt", [torch.float64, torch.float32])
+def test_elementwise_chains_match_reference(golden, dt):
+    """The three elementwise kernels against outputs of the reference's own
+    numpy specifications (tests/golden/rhs_elementwise.npz)."""
+    from b200sht.rhs import momentum_bernoulli, scalar_tendency, tracer_flux
+
+    tag = "f64" if dt == torch.float64 else "f32"
+    g = golden("rhs_elementwise.npz")
+    f = {k[: -len(tag) - 1]: g[k] for k in g if k.endswith(tag)}
+    dev = lambda a: torch.as_tensor(np.ascontiguousarray(a), device="cuda")
+    got = momentum_bernoulli(dev(f["zeta"]), dev(f["cor"]), dev(f["u"]), dev(f["v"]), dev(f["wu"]),
+                             dev(f["wv"]), dev(f["tv"]), dev(f["pg"]), dev(f["ge"]), dev(f["gn"]),
+                             dev(f["phi"]), 287.0528)
+    for a, k in zip(got, ("mu", "mv", "bern")):
+        _close(a, f[k], dt)
+    fx, fy = tracer_flux(dev(f["dp"]), dev(f["s"]), dev(f["u"]), dev(f["v"]))
+    _close(fx, f["fx"], dt)
+    _close(fy, f["fy"], dt)
+    _close(scalar_tendency(dev(f["h"]), dev(f["vert"]), dev(f["s"]), dev(f["dpt"]), dev(f["dp"])),
+           f["st"], dt)
+
+
+@pytest.mark.parametrize("dt", [torch.float64, torch.float32])
 def test_vertical_flux_divergence_matches_reference(golden, dt):
     from b200sht.rhs import vertical_flux_divergence
 
