@@ -60,3 +60,42 @@ def test_batch_argument_errors():
     batch = TransformBatch([a, b], [2, 2])
     with pytest.raises(ValueError, match="does not hold"):
         batch.inverse([np.zeros((3, 22, 22), complex), np.zeros((2, 63, 63), complex)])
+
+
+@pytest.mark.parametrize("precision", ["split16", "float32"])
+def test_ensemble_configuration_against_oracle(precision):
+    """The ensemble configuration's shapes -- 32 members at T126 on 192 x 384
+    plus the control at T255 on 384 x 768, one batch -- with two planes per
+    member (64 at T126) and two at T255: sampled planes of every plan
+    against the CPU oracle within 2e-6."""
+    import torch
+
+    from b200sht import SphericalHarmonicTransform, TransformBatch
+    from b200sht.synthetic import CONTROL_SEED, ensemble_member, red_spectrum
+    from oracle.dense_sht import DenseSHT
+
+    members, per = 32, 2
+    specs = [(126, 192, 384), (255, 384, 768)]
+    plans = [SphericalHarmonicTransform.create(T, nlat=nl, nlon=no, precision=precision)
+             for T, nl, no in specs]
+    c126 = np.concatenate([ensemble_member(red_spectrum(126, per, CONTROL_SEED), k)
+                           for k in range(members)])
+    c255 = red_spectrum(255, per, CONTROL_SEED)
+    batch = TransformBatch(plans, [members * per, per])
+    np_ = plans[0].backend.to_numpy
+    grids = batch.inverse([c126, c255])
+    coeffs = batch.forward([g.contiguous() for g in grids])
+    for (T, nl, no), c, g, f, sample in ((specs[0], c126, grids[0], coeffs[0], [0, 37, 63]),
+                                         (specs[1], c255, grids[1], coeffs[1], [0, 1])):
+        ora = DenseSHT(T, nlat=nl, nlon=no)
+        want_g = ora.inverse(c[sample])
+        got_g = np_(g)[sample]
+        assert np.max(np.abs(got_g - want_g)) / np.max(np.abs(want_g)) < 2e-6, (T, "inverse")
+        want_c = ora.forward(got_g.astype(np.float64))
+        got_c = np_(f)[sample]
+        w = np.where(np.arange(T + 1) == 0, 1.0, 2.0)
+        rel = np.sqrt(np.sum(w * np.abs(got_c - want_c) ** 2) / np.sum(w * np.abs(want_c) ** 2))
+        assert rel < 2e-6, (T, "forward", rel)
+    for p in plans:
+        p.check_device()
+    torch.cuda.synchronize()

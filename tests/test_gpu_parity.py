@@ -321,3 +321,24 @@ def test_fp64_roundtrip_t511():
     back = sht.backend.to_numpy(sht.forward(sht.inverse(coeff)))
     assert rel_l2(back, coeff) < 1e-12
     assert rel_max(back, coeff) < 1e-11
+
+
+def test_t511_against_oracle_two_planes():
+    """The benchmark's grid (T511, 768 x 1536) against the CPU oracle itself
+    on two planes: FP64 within 1e-12, FP32 and split16 within 2e-6
+    (forward: relative spectral L2; inverse: max grid error)."""
+    from b200sht import SphericalHarmonicTransform
+    from b200sht.synthetic import red_spectrum
+    from oracle.dense_sht import DenseSHT
+
+    ora = DenseSHT(511)
+    coeff = red_spectrum(511, 2, seed=11)
+    want_g = ora.inverse(coeff)
+    want_c = ora.forward(want_g)
+    for precision, tol in (("float64", 1e-12), ("float32", 2e-6), ("split16", 2e-6)):
+        sht = SphericalHarmonicTransform.create(511, precision=precision)
+        np_ = sht.backend.to_numpy
+        g = want_g if precision == "float64" else want_g.astype(np.float32)
+        assert rel_l2(np_(sht.forward(g)), want_c) < tol, precision
+        assert rel_max(np_(sht.inverse(coeff)), want_g) < tol, precision
+        sht.check_device()
