@@ -407,8 +407,9 @@ def gather_linear_batch(fields: Sequence[torch.Tensor], stencil: Stencil, *,
 # departure_points (trajectory.py:50-120, 158-358, 440-490).
 
 #: Solvers of the departure-point equation: the fixed-point pass (the
-#: reference's default and its numpy specification) and Newton's method on
-#: the same equation; the line-search form is not built here.
+#: reference's default and its numpy specification), Newton's method on the
+#: same equation, and Newton with a backtracking line search on the residual
+#: (the form that converges where (dt/2)|J| nears one).
 TRAJECTORY_SOLVERS = ("fixed_point", "newton", "newton_ls")
 
 
@@ -514,13 +515,17 @@ def _diagnostics(stencil: Stencil, move_m, move_k, tables, dt_s, iterations):
     return TrajectoryDiagnostics(int(iterations), float(dt_s), *[float(x) for x in maxima])
 
 
+_SOLVER_CALLS = {"fixed_point": "sht_sl_departure", "newton": "sht_sl_departure_newton",
+                 "newton_ls": "sht_sl_departure_newton_ls"}
+
+
 def search_into(tables: SphericalGridTables, fields: Sequence[torch.Tensor], iterations: int,
-                dt_s: float, outs: Sequence[torch.Tensor], newton: bool = False) -> None:
+                dt_s: float, outs: Sequence[torch.Tensor], solver: str = "fixed_point") -> None:
     """The search kernel alone: ``fields`` = (vx, vy, vz, level_rate) of the
     advecting wind then of the extrapolated one, contiguous; ``outs`` = xi,
     phi, level, move_m, move_k.  No checks beyond the library's."""
     nlev = int(fields[0].shape[0])
-    name = "sht_sl_departure_newton" if newton else "sht_sl_departure"
+    name = _SOLVER_CALLS[solver]
     _lib.call(name, tables._handle, nlev, *[_ptr(t) for t in fields],
               int(iterations), float(dt_s), float(tables.radius_m), *[_ptr(t) for t in outs],
               _stream())
@@ -549,9 +554,6 @@ def departure_points(wind: CartesianWind, tables: SphericalGridTables, dt_s: flo
             "explicit first guess, which is first order in dt and is not a trajectory")
     if solver not in TRAJECTORY_SOLVERS:
         raise ValueError(f"trajectory solver must be one of {TRAJECTORY_SOLVERS}, got {solver!r}")
-    if solver == "newton_ls":
-        raise ValueError(f"trajectory solver {solver!r} is not built in this engine; the "
-                         "fixed-point pass and 'newton' are")
     out_shape = shape if window is None else window.arrival_shape(nlev)
     ex = wind if extrapolated is None else extrapolated
     if window is not None and extrapolated is None:
@@ -568,11 +570,11 @@ def departure_points(wind: CartesianWind, tables: SphericalGridTables, dt_s: flo
     ins = [f.contiguous() for f in wind.arrays()] + [f.contiguous() for f in ex.arrays()]
     outs = [torch.empty(out_shape, dtype=tables.dtype, device=ins[0].device) for _ in range(5)]
     if window is None:
-        search_into(tables, ins, int(iterations), float(dt_s), outs, newton=solver == "newton")
+        search_into(tables, ins, int(iterations), float(dt_s), outs, solver=solver)
     else:
         if not defer_escape:
             window.clear_escape()
-        _lib.call("sht_sl_departure_band", window._handle, 1 if solver == "newton" else 0, nlev,
+        _lib.call("sht_sl_departure_band", window._handle, TRAJECTORY_SOLVERS.index(solver), nlev,
                   *[_ptr(t) for t in ins], int(iterations), float(dt_s), float(tables.radius_m),
                   *[_ptr(t) for t in outs], _stream())
         if not defer_escape:

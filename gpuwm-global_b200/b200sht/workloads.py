@@ -341,9 +341,12 @@ def sl_gather(args, clock_sampler):
         ms = _time(lambda: search_into(tables, wind + wind, 3, 300.0, dep), args.steps,
                    args.warmup)
         out["departure_search_3_iterations"] = {"ms": ms, "points_per_s": npts / (ms * 1e-3)}
-        ms = _time(lambda: search_into(tables, wind + wind, 3, 300.0, dep, newton=True),
+        ms = _time(lambda: search_into(tables, wind + wind, 3, 300.0, dep, solver="newton"),
                    args.steps, args.warmup)
         out["departure_newton_3_iterations"] = {"ms": ms, "points_per_s": npts / (ms * 1e-3)}
+        ms = _time(lambda: search_into(tables, wind + wind, 3, 300.0, dep, solver="newton_ls"),
+                   args.steps, args.warmup)
+        out["departure_newton_ls_3_iterations"] = {"ms": ms, "points_per_s": npts / (ms * 1e-3)}
         del wind, dep
         out["rhs_kernels"] = _rhs_timings(args, (nlev, grid.nlat, grid.nlon), peak)
         out["point_sampling"] = _sampling_timings(args)

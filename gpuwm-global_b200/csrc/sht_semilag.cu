@@ -93,6 +93,10 @@ int guarded(F&& f) {
 }
 
 constexpr double kHalfPi = 1.57079632679489661923;
+// Departure-point solvers (the reference's TRAJECTORY_SOLVERS, in order).
+constexpr int kSolverFixedPoint = 0;
+constexpr int kSolverNewton = 1;
+constexpr int kSolverNewtonLs = 2;
 
 // ------------------------------------------------------------- weights
 
@@ -684,6 +688,150 @@ __global__ void __launch_bounds__(256) sl_departure_newton_kernel(const SlDepArg
   a.move_k[gid] = last_k;
 }
 
+// ------------------------------------- line-search Newton departure search
+// The reference's opt-in "newton_ls" solver (semilag/trajectory.py
+// TRAJECTORY_SOLVERS, kernels.cu sl_departure_newton_ls_body): the same
+// equation, gather and interpolant Jacobian, with each step accepted by a
+// backtracking line search on the residual.  The interpolant is piecewise
+// trilinear, so its Jacobian jumps at cell faces; where (dt/2)|J| nears one
+// a full Newton step from one cell lands in the next, whose step points
+// back, and the point cycles.  Here every iteration takes the Newton
+// direction (or the residual itself where the 3 x 3 system is not solved:
+// det(I - M) <= 0.05 or a pole) and halves it, at most four times, until
+// the residual in grid cells falls by the Armijo factor 1 - 1e-4 alpha; the
+// Newton step is capped at 20 times the residual.  A point whose residual
+// is below 1e-4 cells stops.  The accepted trial point has been evaluated
+// already, so an accepted full step costs one gather.  The reported move is
+// the step AT THE RETURNED POINT (the linearised distance to the root, or
+// the residual where the system was not solved), not the last move taken.
+template <typename T>
+struct NewtonEval {
+  T res;           // |G(q) - q| in meridional grid cells (levels as they are)
+  T de, dn, dk;    // the direction: Newton solve, or the residual itself
+};
+
+template <typename T>
+__device__ __forceinline__ NewtonEval<T> newton_eval(const SlDepArgs<T>& a, T qx, T qy, T qz,
+                                                     T qk, T ax, T ay, T az, int k, T ex, T ey,
+                                                     T ez, T es, T c, T hdt, T klo, T khi,
+                                                     T cells) {
+  const T lam = atan2(qy, qx);
+  const T rho = sqrt(qx * qx + qy * qy);
+  const T phid = atan2(qz, rho);
+  T w[4], dl[4], dp[4], dk[4];
+  trilinear4_grad<T>(a, lam, phid, qk, w, dl, dp, dk);
+  const T ux = ax - c * (ex + w[0]), uy = ay - c * (ey + w[1]), uz = az - c * (ez + w[2]);
+  const T un = sqrt(ux * ux + uy * uy + uz * uz);
+  const T px = ux / un, py = uy / un, pz = uz / un;
+  const T pk_free = T(k) - hdt * (es + w[3]);
+  const bool kheld = pk_free <= klo || pk_free >= khi;
+  const T pk = min(max(pk_free, klo), khi);
+  // local frame at q: east e, north nv
+  const T cl = rho > T(0) ? qx / rho : T(1), sl = rho > T(0) ? qy / rho : T(0);
+  const T cp = rho, sp = qz;
+  const T e0 = -sl, e1 = cl;
+  const T n0 = -sp * cl, n1 = -sp * sl, n2 = cp;
+  const T dx = px - qx, dy = py - qy, dz = pz - qz;
+  const T re = e0 * dx + e1 * dy, rn = n0 * dx + n1 * dy + n2 * dz, rk = pk - qk;
+  NewtonEval<T> out{sqrt((re * re + rn * rn) * cells * cells + rk * rk), re, rn, rk};
+  if (cp > T(1e-6)) {
+    const T g = -c / un;
+    const T icp = T(1) / cp;
+    const T m00 = g * (e0 * dl[0] + e1 * dl[1]) * icp;
+    const T m01 = g * (e0 * dp[0] + e1 * dp[1]);
+    const T m02 = g * (e0 * dk[0] + e1 * dk[1]);
+    const T m10 = g * (n0 * dl[0] + n1 * dl[1] + n2 * dl[2]) * icp;
+    const T m11 = g * (n0 * dp[0] + n1 * dp[1] + n2 * dp[2]);
+    const T m12 = g * (n0 * dk[0] + n1 * dk[1] + n2 * dk[2]);
+    const T m20 = kheld ? T(0) : -hdt * dl[3] * icp;
+    const T m21 = kheld ? T(0) : -hdt * dp[3];
+    const T m22 = kheld ? T(0) : -hdt * dk[3];
+    const T a00 = T(1) - m00, a01 = -m01, a02 = -m02;
+    const T a10 = -m10, a11 = T(1) - m11, a12 = -m12;
+    const T a20 = -m20, a21 = -m21, a22 = T(1) - m22;
+    const T det = a00 * (a11 * a22 - a12 * a21) - a01 * (a10 * a22 - a12 * a20) +
+                  a02 * (a10 * a21 - a11 * a20);
+    if (isfinite(det) && det > T(0.05)) {
+      const T id = T(1) / det;
+      const T s0 = (re * (a11 * a22 - a12 * a21) - a01 * (rn * a22 - a12 * rk) +
+                    a02 * (rn * a21 - a11 * rk)) * id;
+      const T s1 = (a00 * (rn * a22 - a12 * rk) - re * (a10 * a22 - a12 * a20) +
+                    a02 * (a10 * rk - rn * a20)) * id;
+      const T s2 = (a00 * (a11 * rk - rn * a21) - a01 * (a10 * rk - rn * a20) +
+                    re * (a10 * a21 - a11 * a20)) * id;
+      if (isfinite(s0) && isfinite(s1) && isfinite(s2)) {
+        const T step = sqrt((s0 * s0 + s1 * s1) * cells * cells + s2 * s2);
+        const T ratio = step / (out.res + T(1e-30));
+        const T shrink = ratio > T(20) ? T(20) / ratio : T(1);
+        out.de = s0 * shrink;
+        out.dn = s1 * shrink;
+        out.dk = s2 * shrink;
+      }
+    }
+  }
+  return out;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) sl_departure_newton_ls_kernel(const SlDepArgs<T> a) {
+  const int64_t n = (int64_t)a.nk * a.nja * a.ni;
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const int64_t gid = point_index(t, a.nk, a.nja, a.ni);
+  const int plane = a.nja * a.ni;
+  const int k = (int)(gid / plane);
+  const int rem = (int)(gid - (int64_t)k * plane);
+  const int j = rem / a.ni, i = rem - j * a.ni;
+  const int64_t here = ((int64_t)k * a.njs + (j + a.lead)) * a.ni + i;
+  const T lat = __ldg(a.lat_ext + a.ja0 + j + 2);
+  const T lon = T((double)i * a.dlam);
+  const T ax = cos(lat) * cos(lon), ay = cos(lat) * sin(lon), az = sin(lat);
+  const T inv_r = T(1) / a.radius;
+  const T dt = a.dt, hdt = T(0.5) * a.dt, c = hdt * inv_r;
+  // the fixed-point search's first guess
+  T qx = ax - dt * a.vx[here] * inv_r, qy = ay - dt * a.vy[here] * inv_r,
+    qz = az - dt * a.vz[here] * inv_r;
+  T nrm = sqrt(qx * qx + qy * qy + qz * qz);
+  qx /= nrm; qy /= nrm; qz /= nrm;
+  const T klo = T(-0.5), khi = T(a.nk) - T(0.5);
+  T qk = min(max(T(k) - dt * a.sv[here], klo), khi);
+  const T ex = a.vxe[gid], ey = a.vye[gid], ez = a.vze[gid], es = a.sve[gid];
+  const T cells = T(a.nj) / T(2 * kHalfPi);  // meridional grid lengths per radian
+  NewtonEval<T> cur = newton_eval<T>(a, qx, qy, qz, qk, ax, ay, az, k, ex, ey, ez, es, c, hdt,
+                                     klo, khi, cells);
+  for (int it = 0; it < a.iters && cur.res >= T(1e-4); ++it) {
+    // q's local frame, in which the direction is expressed
+    const T rho = sqrt(qx * qx + qy * qy);
+    const T cl = rho > T(0) ? qx / rho : T(1), sl = rho > T(0) ? qy / rho : T(0);
+    const T e0 = -sl, e1 = cl;
+    const T n0 = -qz * cl, n1 = -qz * sl, n2 = rho;
+    T alpha = T(1);
+    T tx, ty, tz, tk;
+    NewtonEval<T> trial;
+    for (int ls = 0;; ++ls) {  // at most four halvings
+      const T se = alpha * cur.de, sn = alpha * cur.dn;
+      tx = qx + se * e0 + sn * n0;
+      ty = qy + se * e1 + sn * n1;
+      tz = qz + sn * n2;
+      nrm = sqrt(tx * tx + ty * ty + tz * tz);
+      tx /= nrm; ty /= nrm; tz /= nrm;
+      tk = min(max(qk + alpha * cur.dk, klo), khi);
+      trial = newton_eval<T>(a, tx, ty, tz, tk, ax, ay, az, k, ex, ey, ez, es, c, hdt, klo, khi,
+                             cells);
+      if (trial.res <= (T(1) - T(1e-4) * alpha) * cur.res || ls >= 4) break;
+      alpha *= T(0.5);
+    }
+    qx = tx; qy = ty; qz = tz; qk = tk;
+    cur = trial;
+  }
+  a.xi[gid] = atan2(qy, qx) * a.inv_dlam;
+  a.phi[gid] = atan2(qz, sqrt(qx * qx + qy * qy));
+  a.lev[gid] = qk;
+  // the distance from the returned point to the root, linearised there
+  a.move_m[gid] = a.radius * sqrt(cur.de * cur.de + cur.dn * cur.dn);
+  a.move_k[gid] = fabs(cur.dk);
+}
+
 // ----------------------------------------------------------- tables
 // The pole-extended table of one stencil width (semilag/tables.py:51-95,
 // 164-217): G reflected rows each side, the data row and zonal shift each
@@ -909,7 +1057,7 @@ int sht_sl_tables_read(const sht_sl_tables* tables, int order, double* lat_ext, 
   });
 }
 
-static int departure_entry(bool newton, const sht_sl_window* win, const sht_sl_tables* tables,
+static int departure_entry(int solver, const sht_sl_window* win, const sht_sl_tables* tables,
                            int nlev, const void* vx, const void* vy, const void* vz,
                            const void* level_rate, const void* vx_ex, const void* vy_ex,
                            const void* vz_ex, const void* level_rate_ex, int iterations,
@@ -1046,7 +1194,7 @@ int sht_sl_gather_band(const sht_sl_window* win, int order, int limiter, int def
                       level, out, cut, stream);
 }
 
-int sht_sl_departure_band(const sht_sl_window* win, int newton, int nlev, const void* vx,
+int sht_sl_departure_band(const sht_sl_window* win, int solver, int nlev, const void* vx,
                           const void* vy, const void* vz, const void* level_rate,
                           const void* vx_ex, const void* vy_ex, const void* vz_ex,
                           const void* level_rate_ex, int iterations, double dt, double radius,
@@ -1056,7 +1204,7 @@ int sht_sl_departure_band(const sht_sl_window* win, int newton, int nlev, const 
     sht::set_error("null band window");
     return SHT_ERR_ARG;
   }
-  return departure_entry(newton != 0, win, win->tables, nlev, vx, vy, vz, level_rate, vx_ex,
+  return departure_entry(solver, win, win->tables, nlev, vx, vy, vz, level_rate, vx_ex,
                          vy_ex, vz_ex, level_rate_ex, iterations, dt, radius, xi, phi, level,
                          move_m, move_k, stream);
 }
@@ -1081,7 +1229,7 @@ int sht_sl_gather_linear(const sht_sl_tables* tables, const void* src, int64_t f
   });
 }
 
-static int departure_entry(bool newton, const sht_sl_window* win, const sht_sl_tables* tables,
+static int departure_entry(int solver, const sht_sl_window* win, const sht_sl_tables* tables,
                            int nlev, const void* vx,
                            const void* vy, const void* vz, const void* level_rate,
                            const void* vx_ex, const void* vy_ex, const void* vz_ex,
@@ -1129,15 +1277,19 @@ static int departure_entry(bool newton, const sht_sl_window* win, const sht_sl_t
         a->esc = win->d_esc;
       }
     };
+    SHT_REQUIRE(solver >= kSolverFixedPoint && solver <= kSolverNewtonLs,
+                "departure solver is 0 (fixed point), 1 (Newton) or 2 (line-search Newton)");
     if (tables->prec == SHT_PREC_F64) {
       SlDepArgs<double> a;
       fill(&a);
-      if (newton) sl_departure_newton_kernel<double><<<blocks, 256, 0, s>>>(a);
+      if (solver == kSolverNewton) sl_departure_newton_kernel<double><<<blocks, 256, 0, s>>>(a);
+      else if (solver == kSolverNewtonLs) sl_departure_newton_ls_kernel<double><<<blocks, 256, 0, s>>>(a);
       else sl_departure_kernel<double><<<blocks, 256, 0, s>>>(a);
     } else {
       SlDepArgs<float> a;
       fill(&a);
-      if (newton) sl_departure_newton_kernel<float><<<blocks, 256, 0, s>>>(a);
+      if (solver == kSolverNewton) sl_departure_newton_kernel<float><<<blocks, 256, 0, s>>>(a);
+      else if (solver == kSolverNewtonLs) sl_departure_newton_ls_kernel<float><<<blocks, 256, 0, s>>>(a);
       else sl_departure_kernel<float><<<blocks, 256, 0, s>>>(a);
     }
     SHT_CUDA_OR_THROW(cudaGetLastError());
@@ -1149,7 +1301,7 @@ int sht_sl_departure(const sht_sl_tables* tables, int nlev, const void* vx, cons
                      const void* vy_ex, const void* vz_ex, const void* level_rate_ex,
                      int iterations, double dt, double radius, void* xi, void* phi,
                      void* level, void* move_m, void* move_k, void* stream) {
-  return departure_entry(false, nullptr, tables, nlev, vx, vy, vz, level_rate, vx_ex, vy_ex, vz_ex,
+  return departure_entry(kSolverFixedPoint, nullptr, tables, nlev, vx, vy, vz, level_rate, vx_ex, vy_ex, vz_ex,
                          level_rate_ex, iterations, dt, radius, xi, phi, level, move_m, move_k,
                          stream);
 }
@@ -1160,9 +1312,20 @@ int sht_sl_departure_newton(const sht_sl_tables* tables, int nlev, const void* v
                             const void* level_rate_ex, int iterations, double dt, double radius,
                             void* xi, void* phi, void* level, void* move_m, void* move_k,
                             void* stream) {
-  return departure_entry(true, nullptr, tables, nlev, vx, vy, vz, level_rate, vx_ex, vy_ex, vz_ex,
+  return departure_entry(kSolverNewton, nullptr, tables, nlev, vx, vy, vz, level_rate, vx_ex, vy_ex, vz_ex,
                          level_rate_ex, iterations, dt, radius, xi, phi, level, move_m, move_k,
                          stream);
+}
+
+int sht_sl_departure_newton_ls(const sht_sl_tables* tables, int nlev, const void* vx,
+                               const void* vy, const void* vz, const void* level_rate,
+                               const void* vx_ex, const void* vy_ex, const void* vz_ex,
+                               const void* level_rate_ex, int iterations, double dt,
+                               double radius, void* xi, void* phi, void* level, void* move_m,
+                               void* move_k, void* stream) {
+  return departure_entry(kSolverNewtonLs, nullptr, tables, nlev, vx, vy, vz, level_rate, vx_ex,
+                         vy_ex, vz_ex, level_rate_ex, iterations, dt, radius, xi, phi, level,
+                         move_m, move_k, stream);
 }
 
 }  // extern "C"

@@ -408,7 +408,9 @@ int sht_sl_window_escape(sht_sl_window* window, int clear, int* escaped, void* s
 int sht_sl_gather_band(const sht_sl_window* window, int order, int limiter, int deficit,
                        const void* src, int64_t fields, int nlev, const void* xi,
                        const void* phi, const void* level, void* out, void* cut, void* stream);
-int sht_sl_departure_band(const sht_sl_window* window, int newton, int nlev, const void* vx,
+/* `solver`: 0 the fixed-point search, 1 Newton, 2 line-search Newton (the
+ * three whole-grid calls below). */
+int sht_sl_departure_band(const sht_sl_window* window, int solver, int nlev, const void* vx,
                           const void* vy, const void* vz, const void* level_rate,
                           const void* vx_ex, const void* vy_ex, const void* vz_ex,
                           const void* level_rate_ex, int iterations, double dt, double radius,
@@ -453,6 +455,20 @@ int sht_sl_departure_newton(const sht_sl_tables* tables, int nlev, const void* v
                             const void* level_rate_ex, int iterations, double dt, double radius,
                             void* xi, void* phi, void* level, void* move_m, void* move_k,
                             void* stream);
+/* The line-search Newton search (the reference's opt-in "newton_ls" solver,
+ * kernels.cu sl_departure_newton_ls_*): the Newton direction (or the
+ * residual where the 3 x 3 system is near-singular or at a pole), capped at
+ * 20 residuals and halved at most four times until the residual in grid
+ * cells falls by the Armijo factor 1 - 1e-4 alpha; a point whose residual is
+ * below 1e-4 cells stops.  move_m / move_k report the step at the returned
+ * point (its linearised distance to the root), not the last move.  Same
+ * arguments and fixed point as sht_sl_departure. */
+int sht_sl_departure_newton_ls(const sht_sl_tables* tables, int nlev, const void* vx,
+                               const void* vy, const void* vz, const void* level_rate,
+                               const void* vx_ex, const void* vy_ex, const void* vz_ex,
+                               const void* level_rate_ex, int iterations, double dt,
+                               double radius, void* xi, void* phi, void* level, void* move_m,
+                               void* move_k, void* stream);
 
 /* Fused right-hand-side kernels of the dycore step (the reference's
  * spectral/fused.py momentum_bernoulli_kernel, tracer_flux_kernel,

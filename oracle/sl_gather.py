@@ -312,6 +312,40 @@ def departure(wind, lat, nlon, dt, *, iterations=3, extrapolated=None, radius=63
     return xi, phi, qk.astype(dtype), move_m.astype(dtype), move_k.astype(dtype)
 
 
+def departure_residual(wind, lat, nlon, dt, xi, phi, level, *, extrapolated=None,
+                       radius=6371220.0):
+    """How far given departure points are from solving the departure
+    equation: |G(q) - q| for the fixed-point map G of ``departure`` above,
+    in float64, the horizontal part in meridional grid lengths (the arc over
+    pi / nlat) and the level part in levels.  Returns (cells, levels)."""
+    tab = build_tables(lat, nlon, 4)
+    vx, vy, vz, sv = [np.asarray(w, np.float64) for w in wind]
+    ex = [np.asarray(w, np.float64) for w in (extrapolated or wind)]
+    nlev, nlat, _ = vx.shape
+    shape = vx.shape
+    latd = tab["lat_ext"][2:nlat + 2]
+    lon = np.arange(nlon) * (2.0 * math.pi / nlon)
+    ax = np.broadcast_to(np.cos(latd)[None, :, None] * np.cos(lon)[None, None, :], shape)
+    ay = np.broadcast_to(np.cos(latd)[None, :, None] * np.sin(lon)[None, None, :], shape)
+    az = np.broadcast_to(np.sin(latd)[None, :, None] + 0.0 * lon[None, None, :], shape)
+    ak = np.broadcast_to(np.arange(nlev, dtype=np.float64)[:, None, None], shape)
+    lam = np.asarray(xi, np.float64) * (2.0 * math.pi / nlon)
+    ph = np.asarray(phi, np.float64)
+    qk = np.asarray(level, np.float64)
+    qx, qy, qz = np.cos(ph) * np.cos(lam), np.cos(ph) * np.sin(lam), np.sin(ph)
+    w = _trilinear_at([vx, vy, vz, sv], lam, ph, qk, tab, nlat, nlon, np.dtype(np.float64))
+    hdt = 0.5 * dt
+    px = ax - hdt * (ex[0] + w[0]) / radius
+    py = ay - hdt * (ex[1] + w[1]) / radius
+    pz = az - hdt * (ex[2] + w[2]) / radius
+    nrm = np.sqrt(px * px + py * py + pz * pz)
+    px, py, pz = px / nrm, py / nrm, pz / nrm
+    pk = np.clip(ak - hdt * (ex[3] + w[3]), -0.5, nlev - 0.5)
+    chord = np.sqrt((px - qx) ** 2 + (py - qy) ** 2 + (pz - qz) ** 2)
+    arc = 2.0 * np.arcsin(np.clip(0.5 * chord, 0.0, 1.0))
+    return arc * nlat / math.pi, np.abs(pk - qk)
+
+
 def rotation_wind(lat, nlon, nlev, *, speed=40.0, seed=0, dtype=np.float64):
     """Seeded advecting flow: a solid-body rotation about the axis through
     (0 N, 0 E) (its flow crosses both poles) as Cartesian components, plus

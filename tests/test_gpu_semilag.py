@@ -232,8 +232,6 @@ def test_departure_errors_and_rest_state():
     assert diag.displacement_max_m < 1e-6 and diag.move_max_m == 0.0
     with pytest.raises(ValueError, match="at least one iteration"):
         departure_points(wind, tables, 300.0, iterations=0)
-    with pytest.raises(ValueError, match="not built"):
-        departure_points(wind, tables, 300.0, solver="newton_ls")
     with pytest.raises(ValueError, match="must be one of"):
         departure_points(wind, tables, 300.0, solver="rk4")
     with pytest.raises(ValueError, match="must all be"):
@@ -263,6 +261,69 @@ def test_newton_search_reaches_the_fixed_point(tag):
     assert np.max(np.minimum(dxi, nlon - dxi)) < tol * nlon
     assert float((nt.level - fp.level).abs().max()) < tol * nlev
     assert diag.move_max_cells < (1e-6 if tag == "f64" else 1e-3)
+
+
+@pytest.mark.parametrize("tag", ["f64", "f32"])
+def test_line_search_newton_reaches_the_fixed_point(tag):
+    """The line-search Newton form solves the same equation: on the rotation
+    across both poles (900 s, 48 x 96 x 8) six iterations land on the point
+    thirty fixed-point iterations reach, to within its own stopping gate (a
+    residual of 1e-4 meridional grid lengths), and its reported step at the
+    returned point is below the gate as well."""
+    from b200sht.semilag import CartesianWind, SphericalGridTables, departure_points
+    from oracle import sl_gather as O
+
+    nlat, nlon, nlev = 48, 96, 8
+    lat = np.sort(np.arcsin(np.polynomial.legendre.leggauss(nlat)[0]))
+    dtype = np.float64 if tag == "f64" else np.float32
+    wind = O.rotation_wind(lat, nlon, nlev, speed=60.0, seed=4, dtype=dtype)
+    tables = SphericalGridTables.create(_grid(lat, nlon), dtype=DT[tag])
+    w = CartesianWind(*[torch.as_tensor(a, device="cuda") for a in wind])
+    fp, _ = departure_points(w, tables, 900.0, iterations=30)
+    ls, diag = departure_points(w, tables, 900.0, iterations=6, solver="newton_ls")
+    gate = 1e-4 * np.pi / nlat  # the stopping residual, radians
+    tol = 2 * gate if tag == "f64" else 2 * gate + 2e-5
+    def unit(st):
+        lam = st.xi.double() * (2 * np.pi / nlon)
+        ph = st.phi.double()
+        return torch.stack([ph.cos() * lam.cos(), ph.cos() * lam.sin(), ph.sin()])
+
+    # the great-circle distance between the two answers (chord ~ arc here)
+    assert float((unit(ls) - unit(fp)).norm(dim=0).max()) < tol
+    assert float((ls.level - fp.level).abs().max()) < (2e-4 if tag == "f64" else 1e-3)
+    assert diag.move_max_cells < (2e-4 if tag == "f64" else 1e-3)
+
+
+def test_line_search_newton_on_a_strongly_deforming_flow():
+    """Where (dt/2)|J| nears one (a rough 150 m/s flow at a 3600 s step on a
+    coarse grid) the fixed-point pass stops contracting and the full Newton
+    step cycles between cells; the line-search form keeps the residual of
+    the departure equation falling.  Measured independently of the search
+    kernels (the oracle's float64 residual |G(q) - q| at the returned
+    points), after the same four iterations: the line-search form's mean
+    residual is below both others', and its 90th percentile too."""
+    from b200sht.semilag import CartesianWind, SphericalGridTables, departure_points
+    from oracle import sl_gather as O
+
+    nlat, nlon, nlev = 32, 64, 6
+    lat = np.sort(np.arcsin(np.polynomial.legendre.leggauss(nlat)[0]))
+    rng = np.random.default_rng(8)
+    base = O.rotation_wind(lat, nlon, nlev, speed=60.0, seed=3)
+    wind = [base[i] + 150.0 * rng.standard_normal(base[i].shape) for i in range(3)]
+    wind.append(base[3] + 2e-4 * rng.standard_normal(base[3].shape))
+    tables = SphericalGridTables.create(_grid(lat, nlon), dtype=torch.float64)
+    w = CartesianWind(*[torch.as_tensor(a, device="cuda") for a in wind])
+    stats = {}
+    for solver in ("fixed_point", "newton", "newton_ls"):
+        st, _ = departure_points(w, tables, 3600.0, iterations=4, solver=solver)
+        cells, levels = O.departure_residual(wind, lat, nlon, 3600.0, st.xi.cpu().numpy(),
+                                             st.phi.cpu().numpy(), st.level.cpu().numpy())
+        r = np.sqrt(cells ** 2 + levels ** 2).ravel()
+        stats[solver] = (float(np.mean(r)), float(np.percentile(r, 90)))
+    ls = stats["newton_ls"]
+    for other in ("fixed_point", "newton"):
+        assert ls[0] < stats[other][0], stats
+        assert ls[1] < stats[other][1], stats
 
 
 def _band_case(tag, seed=5):
@@ -326,7 +387,7 @@ def test_band_escape_is_refused_by_name():
 
 
 @pytest.mark.parametrize("tag", ["f64", "f32"])
-@pytest.mark.parametrize("solver", ["fixed_point", "newton"])
+@pytest.mark.parametrize("solver", ["fixed_point", "newton", "newton_ls"])
 def test_band_departure_search_is_the_whole_grid_search(tag, solver):
     from b200sht.semilag import CartesianWind, SphericalGridTables, departure_points
     from oracle import sl_gather as O
