@@ -24,6 +24,7 @@ SHT_TUNE_FFT = 1
 SHT_TUNE_TILE_ORDER = 2
 SHT_TUNE_TC_CTAS = 3
 SHT_TUNE_ACCUMULATORS = 4
+SHT_TUNE_SIMT_TILE = 5
 SHT_OK = 0
 SHT_ERR_ARG = 1
 SHT_ERR_CUDA = 2

@@ -13,6 +13,8 @@ seeded red-spectrum planes for every combination of
 * tensor-core tile order among equal-cost tiles: a column tile's row blocks
   adjacent (table-image reuse) or a row block's column tiles adjacent
   (converted-data reuse);
+* the FP32 SIMT contraction's tile shape: 128 x 128 or 64 x 128 (columns x
+  rows; the narrow shape pads the ragged analysis blocks less);
 
 keeps the fastest on the plan (``sht_plan_set_tuning``) and returns the
 timings.  Results can be cached in a JSON file keyed by device, grid,
@@ -32,7 +34,7 @@ from . import _lib
 
 KEYS = {"contraction": _lib.SHT_TUNE_CONTRACTION, "fft": _lib.SHT_TUNE_FFT,
         "tile_order": _lib.SHT_TUNE_TILE_ORDER, "tc_ctas": _lib.SHT_TUNE_TC_CTAS,
-        "accumulators": _lib.SHT_TUNE_ACCUMULATORS}
+        "accumulators": _lib.SHT_TUNE_ACCUMULATORS, "simt_tile": _lib.SHT_TUNE_SIMT_TILE}
 
 
 def get_tuning(transform) -> dict:
@@ -62,13 +64,16 @@ def _candidates(transform) -> list[dict]:
         pass
     finally:
         set_tuning(transform, fft=current["fft"])
+    fp32 = transform.precision != "float64"
     out = []
-    for contraction, fft, order in itertools.product([0, 1] if split else [0], ffts,
-                                                     [0, 1] if split else [0]):
+    for contraction, fft, order, simt_tile in itertools.product(
+            [0, 1] if split else [0], ffts, [0, 1] if split else [0], [0, 1] if fp32 else [0]):
         if contraction == 1 and order == 1:
             continue  # the tile order only steers the tensor-core kernel
+        if split and contraction == 0 and simt_tile == 1:
+            continue  # the SIMT tile shape only steers the SIMT contraction
         out.append({"contraction": contraction, "fft": fft, "tile_order": order, "tc_ctas": 0,
-                    "accumulators": current["accumulators"]})
+                    "accumulators": current["accumulators"], "simt_tile": simt_tile})
     return out
 
 

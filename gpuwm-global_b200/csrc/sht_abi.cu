@@ -540,6 +540,7 @@ void destroy(sht_plan* p) {
   for (cudaEvent_t e : p->event_pool) cudaEventDestroy(e);
   void* ptrs[] = {p->d_mu, p->d_w, p->d_coslat, p->basis, p->dbasis, p->analysis, p->rot,
                   p->shear, p->tw_l, p->tw_n, p->d_radices, p->d_items[0], p->d_items[1],
+                  p->d_items_narrow[0], p->d_items_narrow[1],
                   p->d_desc[0][0], p->d_desc[0][1], p->d_desc[1][0], p->d_desc[1][1],
                   p->wfold[0], p->wfold[1], p->cfold[0], p->cfold[1], p->rowmax, p->d_err};
   for (void* q : ptrs)
@@ -1296,6 +1297,12 @@ int sht_plan_set_tuning(sht_plan* plan, int key, int value) {
         SHT_REQUIRE(value >= 0 && value <= 2, "SHT_TUNE_ACCUMULATORS is 0, 1 or 2");
         plan->tune_accumulators = value;
         break;
+      case SHT_TUNE_SIMT_TILE:
+        SHT_REQUIRE(value == 0 || value == 1, "SHT_TUNE_SIMT_TILE is 0 or 1");
+        SHT_REQUIRE(value == 0 || plan->prec != SHT_PREC_F64,
+                    "SHT_TUNE_SIMT_TILE 1 (64-wide column tiles) is an FP32 tile shape");
+        plan->tune_simt_tile = value;
+        break;
       default:
         throw Error{SHT_ERR_ARG, "unknown tuning key"};
     }
@@ -1312,6 +1319,7 @@ int sht_plan_get_tuning(sht_plan* plan, int key, int* value) {
       case SHT_TUNE_TILE_ORDER: *value = plan->tune_tile_order; break;
       case SHT_TUNE_TC_CTAS: *value = plan->tune_tc_ctas; break;
       case SHT_TUNE_ACCUMULATORS: *value = plan->tune_accumulators; break;
+      case SHT_TUNE_SIMT_TILE: *value = plan->tune_simt_tile; break;
       default: throw Error{SHT_ERR_ARG, "unknown tuning key"};
     }
   });

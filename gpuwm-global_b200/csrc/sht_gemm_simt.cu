@@ -7,29 +7,38 @@
 // replaces the reference's per-band dense strided-batched GEMMs
 // (transform.py:1178-1274), which multiply the zeros above the triangle too.
 #include <algorithm>
+#include <type_traits>
 
 #include "sht_plan.h"
 
 namespace sht {
 namespace {
 
-template <typename T> struct SimtCfg;
-template <> struct SimtCfg<float> {
+// Tile shapes (x columns of the table x r data rows per CTA).  FP32 has two,
+// chosen at run time (SHT_TUNE_SIMT_TILE): 128 x 128, and 64 x 128, whose
+// narrower column tiles waste less on the ragged analysis blocks (X = the
+// degrees of one order and parity) at the price of more table loads.
+template <typename T, bool NARROW> struct SimtCfg;
+template <> struct SimtCfg<float, false> {
   static constexpr int BX = 128, BR = 128, BK = 8, TMX = 8, TMR = 8, VW = 4;
   using V = float4;
 };
-template <> struct SimtCfg<double> {
+template <> struct SimtCfg<float, true> {
+  static constexpr int BX = 64, BR = 128, BK = 8, TMX = 4, TMR = 8, VW = 4;
+  using V = float4;
+};
+template <> struct SimtCfg<double, false> {
   static constexpr int BX = 64, BR = 64, BK = 8, TMX = 4, TMR = 4, VW = 2;
   using V = double2;
 };
 
-template <typename T>
+template <typename T, bool NARROW>
 __global__ void __launch_bounds__(256, 2) gemm_simt_kernel(const ShtGemmDesc* __restrict__ descs,
                                                         const ShtGemmItem* __restrict__ items,
                                                         const T* __restrict__ table,
                                                         const T* __restrict__ data,
                                                         T* __restrict__ out, int64_t R) {
-  using C = SimtCfg<T>;
+  using C = SimtCfg<T, NARROW>;
   constexpr int BX = C::BX, BR = C::BR, BK = C::BK, TMX = C::TMX, TMR = C::TMR, VW = C::VW;
   constexpr int NTX = BX / TMX, NTR = BR / TMR;  // 16 x 16 threads
   constexpr int GX = TMX / VW, GR = TMR / VW;     // vector groups per thread
@@ -159,7 +168,7 @@ __global__ void __launch_bounds__(256, 2) gemm_simt_kernel(const ShtGemmDesc* __
 
 void build_gemm_items(sht_plan* p) {
   const int T = p->T;
-  const int bx = p->prec == SHT_PREC_F64 ? SimtCfg<double>::BX : SimtCfg<float>::BX;
+  const int bx = p->prec == SHT_PREC_F64 ? SimtCfg<double, false>::BX : SimtCfg<float, false>::BX;
   p->gemm_bx = bx;
   // Every (m, q) is a problem, including the empty parity-1 block of m = T:
   // its synthesis item has K = 0 and writes the zeros the inverse FFT reads
@@ -196,13 +205,15 @@ void build_gemm_items(sht_plan* p) {
       ana.push_back(b);
     }
   }
-  for (int dir = 0; dir < 2; ++dir) {
+  // Item lists: (problem, x-tile) pairs sorted by descending cost, for the
+  // plan's tile width and, on FP32 plans, for the narrow variant's.
+  auto item_list = [&](int dir, int width, ShtGemmItem** dst, int* count) {
     std::vector<std::pair<int64_t, ShtGemmItem>> items;
     const auto& descs = p->h_desc[dir][0];
     for (int i = 0; i < (int)descs.size(); ++i) {
       const auto& d = descs[i];
-      for (int x0 = 0; x0 < d.X; x0 += bx) {
-        int64_t cost = (int64_t)d.K * std::min(bx, d.X - x0);
+      for (int x0 = 0; x0 < d.X; x0 += width) {
+        int64_t cost = (int64_t)d.K * std::min(width, d.X - x0);
         items.push_back({cost, ShtGemmItem{i, x0}});
       }
     }
@@ -210,9 +221,14 @@ void build_gemm_items(sht_plan* p) {
                      [](const auto& a, const auto& b) { return a.first > b.first; });
     std::vector<ShtGemmItem> flat;
     for (auto& it : items) flat.push_back(it.second);
-    p->n_items[dir] = (int)flat.size();
-    SHT_CUDA_OR_THROW(cudaMalloc(&p->d_items[dir], sizeof(ShtGemmItem) * std::max<size_t>(flat.size(), 1)));
-    upload_now(p->d_items[dir], flat.data(), sizeof(ShtGemmItem) * flat.size());
+    *count = (int)flat.size();
+    SHT_CUDA_OR_THROW(cudaMalloc(dst, sizeof(ShtGemmItem) * std::max<size_t>(flat.size(), 1)));
+    upload_now(*dst, flat.data(), sizeof(ShtGemmItem) * flat.size());
+  };
+  for (int dir = 0; dir < 2; ++dir) {
+    item_list(dir, bx, &p->d_items[dir], &p->n_items[dir]);
+    if (p->prec != SHT_PREC_F64)
+      item_list(dir, SimtCfg<float, true>::BX, &p->d_items_narrow[dir], &p->n_items_narrow[dir]);
     for (int f = 0; f < 2; ++f) {
       auto& v = p->h_desc[dir][f];
       SHT_CUDA_OR_THROW(cudaMalloc(&p->d_desc[dir][f], sizeof(ShtGemmDesc) * std::max<size_t>(v.size(), 1)));
@@ -225,12 +241,24 @@ template <typename T>
 void launch_gemm_simt(const sht_plan* p, int direction, int flip, const T* table, const T* data,
                       T* out, int64_t R, cudaStream_t s) {
   if (p->n_items[direction] == 0 || R == 0) return;
-  constexpr int BR = SimtCfg<T>::BR;
-  SHT_REQUIRE(p->gemm_bx == SimtCfg<T>::BX, "SIMT work list built for another tile width");
-  dim3 grid((unsigned)p->n_items[direction], (unsigned)div_up(R, BR));
+  if constexpr (std::is_same<T, float>::value) {
+    if (p->tune_simt_tile == 1) {
+      SHT_REQUIRE(p->d_items_narrow[direction] != nullptr, "narrow SIMT work list not built");
+      using C = SimtCfg<float, true>;
+      dim3 grid((unsigned)p->n_items_narrow[direction], (unsigned)div_up(R, C::BR));
+      SHT_REQUIRE(grid.y <= 65535, "too many planes for one launch");
+      gemm_simt_kernel<float, true><<<grid, 256, 0, s>>>(
+          p->d_desc[direction][flip], p->d_items_narrow[direction], table, data, out, R);
+      SHT_CUDA_OR_THROW(cudaGetLastError());
+      return;
+    }
+  }
+  using C = SimtCfg<T, false>;
+  SHT_REQUIRE(p->gemm_bx == C::BX, "SIMT work list built for another tile width");
+  dim3 grid((unsigned)p->n_items[direction], (unsigned)div_up(R, C::BR));
   SHT_REQUIRE(grid.y <= 65535, "too many planes for one launch");
-  gemm_simt_kernel<T><<<grid, 256, 0, s>>>(p->d_desc[direction][flip], p->d_items[direction],
-                                           table, data, out, R);
+  gemm_simt_kernel<T, false><<<grid, 256, 0, s>>>(p->d_desc[direction][flip], p->d_items[direction],
+                                                  table, data, out, R);
   SHT_CUDA_OR_THROW(cudaGetLastError());
 }
 

@@ -66,6 +66,7 @@ struct sht_plan {
   int tune_contraction = 0;  // 1: FP32 SIMT contraction on a split16 plan
   int tune_tile_order = 0;   // tensor-core tile order (0: row blocks innermost, 1: column tiles)
   int tune_tc_ctas = 0;      // tensor-core CTAs per launch (0: one per SM)
+  int tune_simt_tile = 0;    // FP32 SIMT column tile (0: 128 wide; 1: 64 wide)
   int tune_accumulators = 0; // tensor-core accumulators (0: three K segments; 1: one, double-buffered;
                              // 2: two K segments, data operand in TMEM)
 
@@ -74,6 +75,8 @@ struct sht_plan {
   std::vector<ShtGemmDesc> h_desc[2][2];
   ShtGemmItem* d_items[2] = {nullptr, nullptr};
   int n_items[2] = {0, 0};
+  ShtGemmItem* d_items_narrow[2] = {nullptr, nullptr};  // FP32: 64-wide column tiles
+  int n_items_narrow[2] = {0, 0};
   int n_problems = 0;
   int gemm_bx = 0;  // x tile of the SIMT kernel the item lists were built for
 

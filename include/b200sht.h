@@ -298,12 +298,17 @@ int sht_helmholtz_synthesis(sht_plan* plan, const sht_vertical* op, double tau_w
  *                        ~1.2e-6, still within 2e-6); 2: two K segments with
  *                        the data operand held in tensor memory (~1 % faster,
  *                        error ~6e-7)
+ *   SHT_TUNE_SIMT_TILE   FP32 SIMT contraction tile shape (columns x rows):
+ *                        0: 128 x 128; 1: 64 x 128 (less padding on the
+ *                        ragged analysis blocks, more table loads); FP64
+ *                        plans have the one shape 64 x 64
  * Set between calls, not while a call of the plan is in flight. */
 #define SHT_TUNE_CONTRACTION 0
 #define SHT_TUNE_FFT 1
 #define SHT_TUNE_TILE_ORDER 2
 #define SHT_TUNE_TC_CTAS 3
 #define SHT_TUNE_ACCUMULATORS 4
+#define SHT_TUNE_SIMT_TILE 5
 int sht_plan_set_tuning(sht_plan* plan, int key, int value);
 int sht_plan_get_tuning(sht_plan* plan, int key, int* value);
 

@@ -26,7 +26,8 @@ def test_every_setting_meets_the_bar_and_tune_keeps_the_fastest(tmp_path):
     grid = f64.inverse(coeff)
     want = np_(f64.forward(grid))
     cands = _candidates(t)
-    assert len(cands) == 6  # {TC x 2 orders, SIMT} x {register FFT, Stockham FFT}
+    # {TC x 2 orders, SIMT x 2 tile shapes} x {register FFT, Stockham FFT}
+    assert len(cands) == 8
     for cand in cands:
         set_tuning(t, **cand)
         assert get_tuning(t) == cand
@@ -74,4 +75,31 @@ def test_accumulator_plans_meet_the_bar_at_t255(acc):
     u64, v64 = VorticityDivergenceOperator(f64).wind_from_vordiv(coeff, coeff[::-1].copy())
     u, v = VorticityDivergenceOperator(t).wind_from_vordiv(coeff, coeff[::-1].copy())
     assert np.max(np.abs(np_(u) - np_(u64))) / np.max(np.abs(np_(u64))) < 2e-6
+    t.check_device()
+
+
+@pytest.mark.parametrize("precision", ["float32", "split16"])
+def test_simt_tile_shapes_agree_bit_for_bit(precision):
+    """The two FP32 SIMT tile shapes run every output's FFMA chain in the same
+    order, so they return the same bits (on a split16 plan through the SIMT
+    contraction switch)."""
+    import torch
+
+    from b200sht import SphericalHarmonicTransform
+    from b200sht.autotune import set_tuning
+    from b200sht.synthetic import red_spectrum
+
+    t = SphericalHarmonicTransform.create(127, precision=precision)
+    if precision == "split16":
+        set_tuning(t, contraction=1)
+    coeff = red_spectrum(127, 5)
+    out = []
+    for tile in (0, 1):
+        set_tuning(t, simt_tile=tile)
+        g = t.inverse(coeff)
+        out.append((g.clone(), t.forward(g).clone()))
+    assert torch.equal(out[0][0], out[1][0]) and torch.equal(out[0][1], out[1][1])
+    f64 = SphericalHarmonicTransform.create(21, precision="float64")
+    with pytest.raises(ValueError, match="FP32 tile shape"):
+        set_tuning(f64, simt_tile=1)
     t.check_device()
