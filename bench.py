@@ -100,7 +100,7 @@ class ClockSampler:
             os.close(fd)
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.device_index}", f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "50"],
+                 "--format=csv,noheader,nounits", "-lms", "20"],
                 stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
             # nvidia-smi takes a moment to start: let its first sample land
             # before the timed work begins, so the samples cover it.
@@ -333,15 +333,7 @@ def main():
     err_plain = errors(plain)
     del f64
 
-    # The CPU oracle (rank 0, one GPU): the reported CPU baseline, and the
-    # FP64 answer of a two-plane sample for the errors named "vs_oracle".
-    ora = None
-    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
-        from oracle.dense_sht import DenseSHT
-
-        ora = DenseSHT(T)
-
-    def errors_vs_oracle(sht, n=2):
+    def errors_vs_oracle(sht, ora, n=2):
         """Relative spectral L2 of forward and max grid error of inverse
         against the oracle's float64 transforms of the first n planes."""
         g64 = grid64[:n].cpu().numpy()
@@ -359,10 +351,11 @@ def main():
     # Headline: the pair loop with no per-kernel events in it.  Kernel shares
     # and the roofline come from a second, instrumented run (CUDA events on
     # the library's stream around every launch).
+    # Clocks are sampled over both timed loops (split, then plain).
     with ClockSampler(local) as clocks:
         ms_split, _ = timed_pairs(split, args.steps, args.warmup)
+        ms_plain, _ = timed_pairs(plain, args.steps, args.warmup)
     clk = clocks.summary()
-    ms_plain, _ = timed_pairs(plain, args.steps, args.warmup)
     k_inst = max(3, min(args.steps, 10))
     ms_split_inst, kern = timed_pairs(split, k_inst, 1, record_kernels=True)
     ms_plain_inst, kern_plain = timed_pairs(plain, k_inst, 1, record_kernels=True)
@@ -445,10 +438,17 @@ def main():
     # times the headline's pairs.
     gpu_launches = sum(v["launches"] for v in kern.values()) // k_inst * args.steps
 
+    # The CPU oracle (rank 0, one GPU), built after every GPU timing (its ~10 GB
+    # of host tables are allocated only now): the reported CPU baseline, and
+    # the FP64 answer of a two-plane sample for the errors named "vs_oracle".
     cpu = None
     oracle_err = None
-    if ora is not None:
-        oracle_err = {"split16": errors_vs_oracle(split), "float32": errors_vs_oracle(plain)}
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        from oracle.dense_sht import DenseSHT
+
+        ora = DenseSHT(T)
+        oracle_err = {"split16": errors_vs_oracle(split, ora),
+                      "float32": errors_vs_oracle(plain, ora)}
         rate, sec = cpu_oracle_rate(T, args.cpu_planes, ora=ora)
         cpu = {"value": rate, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
                "sample": f"{args.cpu_planes} planes of T{T} (768x1536), forward+inverse, "
