@@ -4,16 +4,19 @@
 // dP/dphi of legendre.py, amplitudes sum_n c_nm P_nm, then
 // sum_m (m ? 2 : 1) Re(A_m e^{i m lambda})).
 //
-// B200 layout: one CTA of 128 threads per point, thread t taking the
-// orders m = t, t + 128, ... (the triangle's work spread evenly); each
-// thread carries the sectoral value P_mm along its orders by the
-// reference's product (the same multiplications in the same order), runs
-// the n recurrence with the x-independent coefficients read from tables
-// built once per truncation (layout [m][n], so a thread walks contiguous
-// memory), applies the phase and adds up to 4 fields per pass; a
-// fixed-order shared-memory tree reduces the orders.  FP64 throughout, the
-// products and sums unfused (__dmul_rn / __dadd_rn) as the reference's
-// numpy evaluates them, so each P value is the reference's rounding.
+// B200 layout: a CTA takes 32 points, one per lane, and its 12 warps split
+// the orders into contiguous bands of equal triangular cost.  Every lane of
+// a warp walks the same (m, n) sequence for its own point, so each
+// coefficient and recurrence factor is one broadcast load for the 32
+// points (a CTA per point re-read the whole spectrum per point, ~8 MB at
+// T511, and ran at ~3 % of the FP64 rate).  A warp carries the sectoral
+// value P_mm from the first order of its band by the reference's product
+// (the same multiplications in the same order, from m = 1), runs the n
+// recurrence with the x-independent factors tabulated once per truncation
+// ([m][n]), applies the phase and adds up to 4 fields per pass; the bands'
+// partial sums are added in band order.  FP64 throughout, the products and
+// sums unfused (__dmul_rn / __dadd_rn) as the reference's numpy evaluates
+// them, so each P value is the reference's rounding.
 #include <cmath>
 #include <vector>
 
@@ -25,6 +28,7 @@ struct sht_sampler {
   double* d_b = nullptr;   // [m][n] sqrt(((n-1)^2-m^2)/(4(n-1)^2-1))
   double* d_c = nullptr;   // [m][n] derivative factor sqrt((n^2-m^2)(2n+1)/(2n-1))
   double* d_s = nullptr;   // [m] sqrt((2m+1)/(2m)) of the sectoral step
+  int* d_band = nullptr;   // [kSampleWarps + 1] first order of each warp's band
 };
 
 namespace sht {
@@ -45,7 +49,8 @@ int guarded(F&& f) {
   }
 }
 
-constexpr int kSampleThreads = 128;
+constexpr int kSamplePoints = 32;  // points per CTA, one per lane
+constexpr int kSampleWarps = 12;   // order bands per CTA, one per warp
 constexpr int kMaxFieldsPerPass = 4;
 
 struct SampleArgs {
@@ -59,24 +64,25 @@ struct SampleArgs {
 };
 
 template <int NF, bool GRAD>
-__global__ void __launch_bounds__(kSampleThreads) sample_kernel(const SampleArgs g) {
-  const int64_t p = blockIdx.x;
-  if (p >= g.npoints) return;
+__global__ void __launch_bounds__(kSamplePoints * kSampleWarps) sample_kernel(const SampleArgs g,
+                                                                        const int* __restrict__ band) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int64_t p = (int64_t)blockIdx.x * kSamplePoints + lane;
+  const bool live = p < g.npoints;  // dead lanes follow along on a dummy point
   const int T = g.T, T1 = T + 1;
-  const double lat = g.lat[p], lon = g.lon[p];
+  const double lat = live ? g.lat[p] : 0.0, lon = live ? g.lon[p] : 0.0;
   const double x = sin(lat);
   const double root = __dsqrt_rn(fmax(0.0, __dsub_rn(1.0, __dmul_rn(x, x))));
   const double denom = __dsub_rn(__dmul_rn(x, x), 1.0);
   double acc0[NF], acc1[NF];
 #pragma unroll
   for (int f = 0; f < NF; ++f) acc0[f] = acc1[f] = 0.0;
-  // sectoral value P_mm, continued from this thread's previous order
+  const int m0 = band[warp], m1 = band[warp + 1];
+  // sectoral value P_mm at the band's first order, by the product from m = 1
   double diag = 1.0 / sqrt(4.0 * kPi);
-  int mdone = 0;
-  for (int m = threadIdx.x; m <= T; m += kSampleThreads) {
-    for (int k = mdone + 1; k <= m; ++k)
-      diag = __dmul_rn(__dmul_rn(-g.s[k], root), diag);
-    mdone = m;
+  for (int k = 1; k <= m0; ++k) diag = __dmul_rn(__dmul_rn(-g.s[k], root), diag);
+  for (int m = m0; m < m1; ++m) {
+    if (m > m0) diag = __dmul_rn(__dmul_rn(-g.s[m], root), diag);
     const double* arow = g.a + (int64_t)m * T1;
     const double* brow = g.b + (int64_t)m * T1;
     const double* crow = g.c + (int64_t)m * T1;
@@ -139,55 +145,69 @@ __global__ void __launch_bounds__(kSampleThreads) sample_kernel(const SampleArgs
       }
     }
   }
-  // fixed-order tree over the 128 threads
-  __shared__ double red[2][NF][kSampleThreads];
+  // the bands' partial sums, added in band order
+  __shared__ double red[kSampleWarps][2][NF][kSamplePoints];
 #pragma unroll
   for (int f = 0; f < NF; ++f) {
-    red[0][f][threadIdx.x] = acc0[f];
-    red[1][f][threadIdx.x] = acc1[f];
+    red[warp][0][f][lane] = acc0[f];
+    red[warp][1][f][lane] = acc1[f];
   }
   __syncthreads();
-  for (int w = kSampleThreads / 2; w > 0; w >>= 1) {
-    if (threadIdx.x < w) {
-#pragma unroll
-      for (int f = 0; f < NF; ++f) {
-        red[0][f][threadIdx.x] += red[0][f][threadIdx.x + w];
-        red[1][f][threadIdx.x] += red[1][f][threadIdx.x + w];
-      }
+  if (warp < NF) {
+    const int f = warp;
+    double s0 = red[0][0][f][lane], s1 = red[0][1][f][lane];
+    for (int w = 1; w < kSampleWarps; ++w) {
+      s0 += red[w][0][f][lane];
+      s1 += red[w][1][f][lane];
     }
-    __syncthreads();
-  }
-  if (threadIdx.x == 0) {
-#pragma unroll
-    for (int f = 0; f < NF; ++f) {
+    if (live) {
       const int64_t o = (int64_t)(g.f0 + f) * g.npoints + p;
       if (GRAD) {
-        g.out0[o] = red[0][f][0] / (g.radius * cos(lat));
-        g.out1[o] = red[1][f][0] / g.radius;
+        g.out0[o] = s0 / (g.radius * cos(lat));
+        g.out1[o] = s1 / g.radius;
       } else {
-        g.out0[o] = red[0][f][0];
+        g.out0[o] = s0;
       }
     }
   }
 }
 
 template <bool GRAD>
-void launch_passes(SampleArgs g, cudaStream_t s) {
-  const unsigned blocks = (unsigned)g.npoints;
+void launch_passes(SampleArgs g, const int* band, cudaStream_t s) {
+  const unsigned blocks = (unsigned)div_up(g.npoints, kSamplePoints);
+  const int threads = kSamplePoints * kSampleWarps;
   for (g.f0 = 0; g.f0 < g.F;) {
     const int left = g.F - g.f0;
     if (left >= 4) {
-      sample_kernel<4, GRAD><<<blocks, kSampleThreads, 0, s>>>(g);
+      sample_kernel<4, GRAD><<<blocks, threads, 0, s>>>(g, band);
       g.f0 += 4;
     } else if (left >= 2) {
-      sample_kernel<2, GRAD><<<blocks, kSampleThreads, 0, s>>>(g);
+      sample_kernel<2, GRAD><<<blocks, threads, 0, s>>>(g, band);
       g.f0 += 2;
     } else {
-      sample_kernel<1, GRAD><<<blocks, kSampleThreads, 0, s>>>(g);
+      sample_kernel<1, GRAD><<<blocks, threads, 0, s>>>(g, band);
       g.f0 += 1;
     }
     SHT_CUDA_OR_THROW(cudaGetLastError());
   }
+}
+
+// Order bands of equal cost: order m costs its T + 1 - m recurrence terms
+// plus a fixed share for its sectoral step, phase and set-up.
+std::vector<int> order_bands(int T) {
+  const int T1 = T + 1;
+  auto cost = [&](int m) { return (double)(T1 - m) + 24.0; };
+  double total = 0.0;
+  for (int m = 0; m <= T; ++m) total += cost(m);
+  std::vector<int> band(kSampleWarps + 1, T1);
+  band[0] = 0;
+  double run = 0.0;
+  int w = 1;
+  for (int m = 0; m <= T && w < kSampleWarps; ++m) {
+    run += cost(m);
+    while (w < kSampleWarps && run >= total * w / kSampleWarps) band[w++] = m + 1;
+  }
+  return band;
 }
 
 }  // namespace
@@ -223,6 +243,9 @@ int sht_sampler_create(int truncation, sht_sampler** out) {
       for (double** d : {&h->d_a, &h->d_b, &h->d_c})
         SHT_CUDA_OR_THROW(cudaMalloc(d, a.size() * sizeof(double)));
       SHT_CUDA_OR_THROW(cudaMalloc(&h->d_s, sv.size() * sizeof(double)));
+      const std::vector<int> band = order_bands(T);
+      SHT_CUDA_OR_THROW(cudaMalloc(&h->d_band, band.size() * sizeof(int)));
+      upload_now(h->d_band, band.data(), band.size() * sizeof(int));
       upload_now(h->d_a, a.data(), a.size() * sizeof(double));
       upload_now(h->d_b, b.data(), b.size() * sizeof(double));
       upload_now(h->d_c, c.data(), c.size() * sizeof(double));
@@ -232,6 +255,7 @@ int sht_sampler_create(int truncation, sht_sampler** out) {
       cudaFree(h->d_b);
       cudaFree(h->d_c);
       cudaFree(h->d_s);
+      cudaFree(h->d_band);
       delete h;
       throw;
     }
@@ -246,6 +270,7 @@ int sht_sampler_destroy(sht_sampler* h) {
     cudaFree(h->d_b);
     cudaFree(h->d_c);
     cudaFree(h->d_s);
+    cudaFree(h->d_band);
     delete h;
   });
 }
@@ -268,8 +293,8 @@ int sht_sample(sht_sampler* h, const void* coeff_mn, int64_t fields, int64_t npo
     SampleArgs g{h->T, (int)fields, 0, npoints, (const double2*)coeff_mn, lat_rad, lon_rad,
                  h->d_a, h->d_b, h->d_c, h->d_s, radius, out0, out1};
     cudaStream_t s = (cudaStream_t)stream;
-    if (gradient) launch_passes<true>(g, s);
-    else launch_passes<false>(g, s);
+    if (gradient) launch_passes<true>(g, h->d_band, s);
+    else launch_passes<false>(g, h->d_band, s);
   });
 }
 
