@@ -72,3 +72,25 @@ def test_sampling_errors_and_device_output(golden):
     assert isinstance(out, torch.Tensor) and out.is_cuda
     lat, lon, f = regular_latlon_scalar(t, c[0], nlat=8, nlon=16)
     assert f.shape == (8, 16) and lat.shape == (8,) and lon.shape == (16,)
+
+
+@pytest.mark.parametrize("T", [1, 3, 7])
+def test_sampling_small_truncations(T):
+    """Truncations with fewer orders than the kernel has order bands (some
+    bands empty) and point counts that are not a multiple of 32: scalar and
+    gradient against the oracle."""
+    from b200sht import SphericalHarmonicTransform
+    from b200sht.sampling import sample_gradient, sample_scalar
+    from b200sht.synthetic import red_spectrum
+    from oracle import sampling as O
+
+    t = SphericalHarmonicTransform.create(T, precision="float64")
+    c = red_spectrum(T, 3, 5 + T)
+    rng = np.random.default_rng(T)
+    lat = rng.uniform(-85, 85, 37)
+    lon = rng.uniform(0, 360, 37)
+    dc = torch.as_tensor(c, device="cuda")
+    assert _rel(sample_scalar(t, dc, lat, lon), O.sample(c, lat, lon)) < 1e-12
+    e, n = sample_gradient(t, dc, lat, lon)
+    we, wn = O.sample(c, lat, lon, gradient=True)
+    assert _rel(e, we) < 1e-12 and _rel(n, wn) < 1e-12
