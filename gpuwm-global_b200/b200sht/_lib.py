@@ -19,6 +19,11 @@ SHT_FLAG_GENERIC_FFT = 2
 SHT_WAIST_BASIS = 0
 SHT_WAIST_DBASIS = 1
 SHT_WAIST_ZONAL = 2
+SHT_TABLE_BASIS = 0
+SHT_TABLE_DBASIS = 1
+SHT_TABLE_ANALYSIS = 2
+SHT_TABLE_ROTATION = 3
+SHT_TABLE_SHEAR = 4
 SHT_TUNE_CONTRACTION = 0
 SHT_TUNE_FFT = 1
 SHT_TUNE_TILE_ORDER = 2
@@ -54,6 +59,8 @@ SIGNATURES = {
     "sht_plan_reserve": (ctypes.c_int, [_P, _I64]),
     "sht_plan_geometry": (ctypes.c_int, [_P, _DP, _DP, _DP]),
     "sht_plan_check": (ctypes.c_int, [_P]),
+    "sht_plan_table_bytes": (ctypes.c_int, [_P, ctypes.c_int, ctypes.POINTER(_I64)]),
+    "sht_plan_read_table": (ctypes.c_int, [_P, ctypes.c_int, _P]),
     "sht_plan_set_timing": (ctypes.c_int, [_P, ctypes.c_int]),
     "sht_plan_read_timing": (ctypes.c_int, [_P, _DP, ctypes.POINTER(_I64), ctypes.POINTER(_I64),
                                             ctypes.c_int, ctypes.c_int]),

@@ -27,6 +27,7 @@ import ctypes
 import hashlib
 import json
 import math
+import weakref
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -64,6 +65,17 @@ class Plan:
     def check(self):
         _lib.check(self._lib.sht_plan_check(self.handle))
 
+    def table_bytes(self, code: int) -> int:
+        out = ctypes.c_int64()
+        _lib.check(self._lib.sht_plan_table_bytes(self.handle, int(code), ctypes.byref(out)))
+        return int(out.value)
+
+    def read_table(self, code: int, shape, dtype) -> np.ndarray:
+        out = np.empty(shape, dtype=dtype)
+        _lib.check(self._lib.sht_plan_read_table(self.handle, int(code),
+                                                 ctypes.c_void_p(out.ctypes.data)))
+        return out
+
     def set_timing(self, enable: bool):
         _lib.check(self._lib.sht_plan_set_timing(self.handle, 1 if enable else 0))
 
@@ -86,6 +98,62 @@ class Plan:
             except Exception:
                 pass
             self.handle = None
+
+
+class LegendreTable(str):
+    """One of a transform's resident Legendre tables, as its contraction seam
+    names it.
+
+    Equal to (and hashing as) its name, ``"basis"``, ``"derivative_basis"`` or
+    ``"analysis"``, which is what ``_batched_contract`` dispatches on; the
+    object itself is the transform's one instance per table, so a census hook
+    that tells tables apart by identity (the reference's
+    tools/arwen_global_transform_census.py:64-140) sees three distinct
+    tables.  ``dense()`` is the reference's BandedLegendreTable.dense()
+    (src/arwen_global/spectral/transform.py:214-216): the whole table in the
+    dense layout, in host numpy, assembled from the device table
+    (``sht_plan_read_table``); tests and inspection only."""
+
+    _CODES = {"basis": _lib.SHT_TABLE_BASIS, "derivative_basis": _lib.SHT_TABLE_DBASIS,
+              "analysis": _lib.SHT_TABLE_ANALYSIS}
+
+    def __new__(cls, name: str, owner: "SphericalHarmonicTransform"):
+        table = super().__new__(cls, name)
+        table.name = name
+        table.layout = "jn" if name == "analysis" else "nj"
+        table._owner_ref = weakref.ref(owner)
+        return table
+
+    @property
+    def _owner(self) -> "SphericalHarmonicTransform":
+        owner = self._owner_ref()
+        if owner is None:
+            raise RuntimeError(f"the transform that held the {self.name} table is gone")
+        return owner
+
+    @property
+    def code(self) -> int:
+        return self._CODES[self.name]
+
+    @property
+    def nbytes(self) -> int:
+        """Resident device bytes (the folded table; on a split16 transform
+        also its FP16 hi/lo tile image)."""
+        return self._owner.plan.table_bytes(self.code)
+
+    def dense(self) -> np.ndarray:
+        """``(T+1, T+1, nlat)`` indexed ``[m, n, j]`` (basis, derivative
+        basis) or ``(T+1, nlat, T+1)`` indexed ``[m, j, n]`` (analysis), in the
+        transform's float dtype, latitude row 0 southernmost, zero above the
+        triangle."""
+        t = self._owner
+        t1, nlat = t.truncation + 1, t.grid.nlat
+        shape = (t1, nlat, t1) if self.layout == "jn" else (t1, t1, nlat)
+        dtype = np.float64 if t.precision == "float64" else np.float32
+        return t.plan.read_table(self.code, shape, dtype)
+
+    def __reduce__(self):
+        return (str, (str(self),))
 
 
 def _ptr(t: torch.Tensor):
@@ -250,6 +318,52 @@ class SphericalHarmonicTransform:
     def identity_hash(self) -> str:
         raw = json.dumps(self.identity, sort_keys=True, separators=(",", ":")).encode()
         return hashlib.sha256(raw).hexdigest()
+
+    # ------------------------------------------------------------ tables
+    def _table(self, name: str) -> LegendreTable:
+        tables = self.__dict__.setdefault("_legendre_tables", {})
+        if name not in tables:
+            tables[name] = LegendreTable(name, self)
+        return tables[name]
+
+    @property
+    def _basis(self) -> LegendreTable:
+        """P_nm (transform.py:888-899)."""
+        return self._table("basis")
+
+    @property
+    def _analysis(self) -> LegendreTable:
+        """The Gram-corrected analysis rows (transform.py:97-119)."""
+        return self._table("analysis")
+
+    @property
+    def _derivative_basis(self) -> LegendreTable:
+        """dP_nm/dphi (transform.py:901-933)."""
+        return self._table("derivative_basis")
+
+    @property
+    def _dbasis(self) -> LegendreTable:
+        """The derivative table.  The reference builds it on the first
+        gradient and holds None until then (transform.py:905-933); the plan
+        here computes dP/dphi in the same recurrence pass as P when it is
+        created, so the table is always resident."""
+        return self._derivative_basis
+
+    @property
+    def legendre_table_nbytes(self) -> dict[str, int]:
+        """Resident table bytes by name (transform.py:936-954).  ``rotation``
+        and ``shear`` are the vector analysis's weighted tables, which the
+        reference forms per call; ``scratch`` is 0: the contraction reads the
+        folded tables directly and expands nothing."""
+        plan = self.plan
+        return {
+            "basis": plan.table_bytes(_lib.SHT_TABLE_BASIS),
+            "analysis": plan.table_bytes(_lib.SHT_TABLE_ANALYSIS),
+            "derivative": plan.table_bytes(_lib.SHT_TABLE_DBASIS),
+            "rotation": plan.table_bytes(_lib.SHT_TABLE_ROTATION),
+            "shear": plan.table_bytes(_lib.SHT_TABLE_SHEAR),
+            "scratch": 0,
+        }
 
     def zeros(self, *leading):
         return torch.zeros((*leading, *self.spectral_shape), dtype=self.backend.complex_dtype,

@@ -269,7 +269,3 @@ for _name, _fn in (("open_waist", open_waist), ("fourier_waist", fourier_waist),
                    ("waist_band_to_grid", waist_band_to_grid), ("waist_to_grid", waist_to_grid),
                    ("gradient_waists", gradient_waists), ("gradient_band", gradient_band)):
     setattr(SphericalHarmonicTransform, _name, _fn)
-# The reference passes its table objects; these names select the same tables.
-SphericalHarmonicTransform._basis = BASIS
-SphericalHarmonicTransform._derivative_basis = DERIVATIVE_BASIS
-SphericalHarmonicTransform._analysis = ANALYSIS

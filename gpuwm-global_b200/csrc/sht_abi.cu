@@ -649,6 +649,49 @@ void host_streamed(sht_plan* p, int op, const void* hin, int64_t planes, void* h
 
 using namespace sht;
 
+namespace {
+
+// The folded table of one kind: device pointer, and whether it is held in the
+// synthesis layout [m][q][i][h] (ld Hx) or the analysis layout [m][q][h][i]
+// (ld ex).
+const void* folded_table(const sht_plan* p, int table, bool* synthesis_layout) {
+  SHT_REQUIRE(table >= SHT_TABLE_BASIS && table <= SHT_TABLE_SHEAR,
+              "table must be one of SHT_TABLE_BASIS .. SHT_TABLE_SHEAR");
+  SHT_REQUIRE(!p->geometry_only, "a geometry-only plan holds no Legendre tables");
+  const void* t[5] = {p->basis, p->dbasis, p->analysis, p->rot, p->shear};
+  *synthesis_layout = table <= SHT_TABLE_DBASIS;
+  return t[table];
+}
+
+// Dense expansion of a folded table (host copy `f`) into `out`.  Row j < H is
+// the folded row h = j; row j >= H mirrors h = nlat - 1 - j with the sign
+// (-1)^(n-m) of P_nm under mu -> -mu, negated for the tables built from
+// dP/dphi.
+template <typename T>
+void expand_dense(const sht_plan* p, int table, bool syn, const T* f, T* out) {
+  const int T1 = p->T + 1, nlat = p->nlat, H = p->H;
+  const bool odd_in_lat = table == SHT_TABLE_DBASIS || table == SHT_TABLE_SHEAR;
+  std::fill(out, out + (int64_t)T1 * T1 * nlat, T(0));
+  for (int m = 0; m < T1; ++m)
+    for (int n = m; n < T1; ++n) {
+      const int q = (n - m) & 1, i = (n - m) >> 1, idx = m * 2 + q;
+      const bool flip = (q == 1) != odd_in_lat;
+      for (int j = 0; j < nlat; ++j) {
+        const bool north = j >= H;
+        const int h = north ? nlat - 1 - j : j;
+        T v = syn ? f[p->syn_off[idx] + (int64_t)i * p->Hx + h]
+                  : f[p->ana_off[idx] + (int64_t)h * p->ex[idx] + i];
+        if (north && flip) v = -v;
+        if (syn)
+          out[((int64_t)m * T1 + n) * nlat + j] = v;
+        else
+          out[((int64_t)m * nlat + j) * T1 + n] = v;
+      }
+    }
+}
+
+}  // namespace
+
 extern "C" {
 
 int sht_abi_version(void) { return SHT_ABI_VERSION; }
@@ -722,6 +765,36 @@ int sht_plan_geometry(const sht_plan* plan, double* mu, double* weights, double*
     if (mu) std::copy(plan->h_mu.begin(), plan->h_mu.begin() + n, mu);
     if (weights) std::copy(plan->h_w.begin(), plan->h_w.begin() + n, weights);
     if (coslat) std::copy(plan->h_coslat.begin(), plan->h_coslat.begin() + n, coslat);
+  });
+}
+
+int sht_plan_table_bytes(const sht_plan* plan, int table, int64_t* bytes) {
+  return guarded([&] {
+    check_plan(plan);
+    SHT_REQUIRE(bytes != nullptr, "bytes must not be NULL");
+    bool syn = false;
+    folded_table(plan, table, &syn);
+    const int64_t elems = syn ? plan->syn_total : plan->ana_total;
+    *bytes = elems * (int64_t)plan->elem() + sht::tc_table_bytes(plan, table);
+  });
+}
+
+int sht_plan_read_table(const sht_plan* plan, int table, void* host_out) {
+  return guarded([&] {
+    check_plan(plan);
+    SHT_REQUIRE(host_out != nullptr, "host_out must not be NULL");
+    bool syn = false;
+    const void* d = folded_table(plan, table, &syn);
+    const int64_t elems = syn ? plan->syn_total : plan->ana_total;
+    if (plan->prec == SHT_PREC_F64) {
+      std::vector<double> f((size_t)std::max<int64_t>(elems, 1));
+      SHT_CUDA_OR_THROW(cudaMemcpy(f.data(), d, 8 * elems, cudaMemcpyDeviceToHost));
+      expand_dense(plan, table, syn, f.data(), static_cast<double*>(host_out));
+    } else {
+      std::vector<float> f((size_t)std::max<int64_t>(elems, 1));
+      SHT_CUDA_OR_THROW(cudaMemcpy(f.data(), d, 4 * elems, cudaMemcpyDeviceToHost));
+      expand_dense(plan, table, syn, f.data(), static_cast<float*>(host_out));
+    }
   });
 }
 

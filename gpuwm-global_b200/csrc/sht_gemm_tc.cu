@@ -1186,6 +1186,13 @@ void destroy_tc_tables(sht_plan* p) {
   p->tc = nullptr;
 }
 
+int64_t tc_table_bytes(const sht_plan* p, int kind) {
+  const ShtTc16* tc = p->tc;
+  if (!tc || kind < 0 || kind >= 5) return 0;
+  const int dir = kind == 0 || kind == 1 ? 0 : 1;
+  return tc->img_bytes[dir] + 4 * tc->cs_elems[dir];
+}
+
 struct TcTileCache {
   struct List {
     ShtTcTile* d = nullptr;

@@ -209,6 +209,8 @@ void build_tc_tables(sht_plan* p, const double* basis64, const double* dbasis64,
                      const double* analysis64, const double* rot64, const double* shear64,
                      cudaStream_t s);
 void destroy_tc_tables(sht_plan* p);
+// Device bytes of one table kind's FP16 hi/lo image and column scales.
+int64_t tc_table_bytes(const sht_plan* p, int kind);
 void launch_gemm_tc(const sht_plan* p, int direction, int flip, int table_kind,
                     const float* data, const float* rowmax, float* out, int64_t R,
                     cudaStream_t s);

@@ -77,6 +77,34 @@ int sht_plan_reserve(sht_plan* plan, int64_t planes);
 /* Copy the FP64 geometry to host arrays of nlat doubles (any may be NULL). */
 int sht_plan_geometry(const sht_plan* plan, double* mu, double* weights, double* coslat);
 
+/* The plan's Legendre tables.  BASIS is P_nm, DBASIS dP_nm/dphi, ANALYSIS the
+ * Gram-corrected 2 pi w P_nm rows, ROTATION (2 pi w / (a cos phi)) P_nm and
+ * SHEAR (2 pi w / a) dP_nm/dphi (the vector analysis's weighted tables). */
+#define SHT_TABLE_BASIS 0
+#define SHT_TABLE_DBASIS 1
+#define SHT_TABLE_ANALYSIS 2
+#define SHT_TABLE_ROTATION 3
+#define SHT_TABLE_SHEAR 4
+
+/* Resident device bytes of one table: the equator-folded table in the plan's
+ * element type plus, on a SPLIT16 plan, its FP16 hi/lo tile image and column
+ * scales.  The reference's legendre_table_nbytes
+ * (src/arwen_global/spectral/transform.py:936-954) reports the same per-table
+ * figure for its banded tables. */
+int sht_plan_table_bytes(const sht_plan* plan, int table, int64_t* bytes);
+
+/* One table copied to host memory in the reference's dense layout, in the
+ * plan's element type (double for F64, float for F32 and SPLIT16): BASIS and
+ * DBASIS as [m][n][j] ((T+1) x (T+1) x nlat), ANALYSIS, ROTATION and SHEAR as
+ * [m][j][n] ((T+1) x nlat x (T+1)), latitude row 0 southernmost, zero above
+ * the triangle (n < m).  The northern rows are the folded table's southern
+ * rows times the degree-parity sign (-1)^(n-m) (negated for DBASIS and SHEAR,
+ * odd in latitude).  Replaces BandedLegendreTable.dense()
+ * (src/arwen_global/spectral/transform.py:214-216), which the reference's
+ * tests compare with its dense tables.  Synchronous; for tests and
+ * inspection, not for a hot path. */
+int sht_plan_read_table(const sht_plan* plan, int table, void* host_out);
+
 /* Read and clear the plan's device error word (synchronises the plan's last
  * stream).  Returns SHT_ERR_DEVICE with a message if a kernel gave up on a
  * bounded wait. */
