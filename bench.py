@@ -183,6 +183,45 @@ def cpu_oracle_rate(T, planes, reps=2, ora=None):
     return planes / best, best
 
 
+def copy_floor(host_in, host_out, steps):
+    """Milliseconds per step of the end-to-end leg's copies alone: the pinned
+    grid host-to-device, the grid device-to-host, and both at once on two
+    streams (the floor a host-streamed round trip can approach)."""
+    import torch
+
+    dev_in = torch.empty(host_in.shape, dtype=host_in.dtype, device="cuda")
+    dev_out = torch.zeros_like(dev_in)
+    cur = torch.cuda.current_stream()
+    s_in, s_out = torch.cuda.Stream(), torch.cuda.Stream()
+
+    def one(h2d, d2h):
+        s_in.wait_stream(cur)
+        s_out.wait_stream(cur)
+        if h2d:
+            with torch.cuda.stream(s_in):
+                dev_in.copy_(host_in, non_blocking=True)
+        if d2h:
+            with torch.cuda.stream(s_out):
+                host_out.copy_(dev_out, non_blocking=True)
+        cur.wait_stream(s_in)
+        cur.wait_stream(s_out)
+
+    out = {}
+    for name, h2d, d2h in (("h2d_only_ms", True, False), ("d2h_only_ms", False, True),
+                           ("both_directions_ms", True, True)):
+        one(h2d, d2h)
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(steps):
+            one(h2d, d2h)
+        b.record()
+        torch.cuda.synchronize()
+        out[name] = a.elapsed_time(b) / steps
+    del dev_in, dev_out
+    return out
+
+
 def cpu_sl_gather_rate():
     """Point-fields/s of the CPU oracle's cubic quasi-monotone gather on a
     bounded sample: one field of 4 levels on the 768 x 1536 grid."""
@@ -444,6 +483,8 @@ def main():
     e2e_ms = max_over_ranks(a.elapsed_time(b) / e2e_steps)
     e2e_err = float((host_out - g_split_dev_ref).abs().max() / g_split_dev_ref.abs().max())
     nbytes = grid32.numel() * 4
+    del g_split_dev_ref
+    copies = copy_floor(host_in, host_out, e2e_steps)
     # Launches of the headline loop: the instrumented run's count per pair
     # times the headline's pairs.
     gpu_launches = sum(v["launches"] for v in kern.values()) // k_inst * args.steps
@@ -499,7 +540,10 @@ def main():
             "e2e": {"value": ws * P / (e2e_ms * 1e-3), "unit": UNIT,
                     "api": "SphericalHarmonicTransform.round_trip_host (sht_round_trip_host)",
                     "rel_diff_vs_device_calls": e2e_err,
-                    "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes},
+                    "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
+                    "ms_per_step": e2e_ms,
+                    "copies_alone": copies,
+                    "copies_alone_over_e2e": copies["both_directions_ms"] / e2e_ms},
             "gpu_launches": gpu_launches,
             "clocks": clk,
         }

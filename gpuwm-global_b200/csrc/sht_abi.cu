@@ -575,6 +575,39 @@ void host_stream_prepare(sht_plan* p, const size_t (&bytes)[3]) {
 
 enum HostOp { kHostForward = 0, kHostInverse = 1, kHostRoundTrip = 2 };
 
+// Plane counts of the chunks of a host-streamed call, each <= chunk.
+// Uniform: chunk planes each, the remainder last.  Ramped (the default
+// schedule): 2, 4, 8, ... planes below `chunk` at both ends and near-equal
+// even chunks of at most `chunk` planes between, so the first copy-out
+// starts after a short copy-in and the last copy-out after the end of the
+// copy-in is short; the pipeline's fill and drain then cost a few planes'
+// copies instead of two whole chunks'.
+std::vector<int64_t> chunk_schedule(int64_t planes, int64_t chunk, bool ramped) {
+  std::vector<int64_t> ramp;
+  if (ramped) {
+    int64_t sum = 0;
+    for (int64_t c = 2; c < chunk; c *= 2) {
+      ramp.push_back(c);
+      sum += c;
+    }
+    if (planes < 2 * sum + 2 * chunk) ramp.clear();  // too short a batch to ramp
+  }
+  std::vector<int64_t> sizes(ramp);
+  int64_t middle = planes;
+  for (int64_t c : ramp) middle -= 2 * c;
+  if (!ramped) {
+    for (int64_t p0 = 0; p0 < middle; p0 += chunk) sizes.push_back(std::min(chunk, middle - p0));
+  } else {
+    // near-equal chunks in units of two planes; an odd plane goes last
+    const int64_t pairs = middle / 2, n_mid = std::max<int64_t>(1, div_up(middle, chunk));
+    for (int64_t i = 0; i < n_mid; ++i)
+      sizes.push_back(2 * (pairs / n_mid + (i < pairs % n_mid ? 1 : 0)));
+    sizes.back() += middle % 2;
+  }
+  for (auto it = ramp.rbegin(); it != ramp.rend(); ++it) sizes.push_back(*it);
+  return sizes;
+}
+
 // Host in, host out, in chunks of `chunk` planes: chunk k's copy in (stream
 // s_in), transforms (s_comp) and copy out (s_out) run in slot k % 3, so the
 // copies of neighbouring chunks overlap each other and the transforms.  A
@@ -590,8 +623,18 @@ void host_streamed(sht_plan* p, int op, const void* hin, int64_t planes, void* h
   // Default: about a sixteenth of the planes, even (the register FFTs' pair
   // kernel wants even plane counts); at T511 x 200 planes chunks of 8-26
   // planes time alike, within 2 %, and whole-batch copies 60 % slower.
+  const bool ramped = chunk <= 0;
   if (chunk <= 0) chunk = std::max<int64_t>(2, (div_up(planes, 16) + 1) / 2 * 2);
   chunk = std::min(chunk, planes);
+  const std::vector<int64_t> sizes = chunk_schedule(planes, chunk, ramped);
+  {
+    int64_t sum = 0;
+    for (int64_t n : sizes) {
+      SHT_REQUIRE(n >= 1 && n <= chunk, "internal: a chunk outside [1, chunk] planes");
+      sum += n;
+    }
+    SHT_REQUIRE(sum == planes, "internal: the chunks do not cover the planes");
+  }
   const size_t bytes[3] = {(size_t)(chunk * in_e) * es,
                            op == kHostRoundTrip ? (size_t)(chunk * ce) * es : 0,
                            (size_t)(chunk * out_e) * es};
@@ -600,10 +643,11 @@ void host_streamed(sht_plan* p, int op, const void* hin, int64_t planes, void* h
   auto& h = p->hs;
   p->last_stream = h.s_comp;
   try {
-    const int64_t n_chunks = div_up(planes, chunk);
-    for (int64_t k = 0; k < n_chunks; ++k) {
+    const int64_t n_chunks = (int64_t)sizes.size();
+    int64_t p0 = 0;
+    for (int64_t k = 0; k < n_chunks; p0 += sizes[k], ++k) {
       const int sl = (int)(k % sht_plan::kHostSlots);
-      const int64_t p0 = k * chunk, n = std::min(chunk, planes - p0);
+      const int64_t n = sizes[k];
       if (k >= sht_plan::kHostSlots) SHT_CUDA_OR_THROW(cudaStreamWaitEvent(h.s_in, h.comp[sl], 0));
       SHT_CUDA_OR_THROW(cudaMemcpyAsync(h.buf[sl][0], static_cast<const char*>(hin) + p0 * in_e * es,
                                         (size_t)(n * in_e) * es, cudaMemcpyHostToDevice, h.s_in));

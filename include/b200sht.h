@@ -170,9 +170,11 @@ int sht_inverse(sht_plan* plan, const void* coeff, int64_t planes, void* grid, v
 /* Host-resident fields.  The reference accepts host (numpy) arrays and
  * moves them to its backend's device inside forward/inverse
  * (transform.py:1486, 1742); these are that path for whole batches: planes
- * move host -> device -> host in chunks of `chunk` planes (0: about a
- * sixteenth of the planes, even) on three internal streams, so the copies of
- * neighbouring chunks overlap each other and the transforms.  Host buffers
+ * move host -> device -> host in chunks of `chunk` planes on three internal
+ * streams, so the copies of neighbouring chunks overlap each other and the
+ * transforms.  chunk = 0 selects the library's schedule: chunks of about a
+ * sixteenth of the planes (even), ramped 2, 4, 8, ... planes at both ends of
+ * the batch so the pipeline fills and drains in a few planes' copies.  Host buffers
  * should be page-locked (cudaHostAlloc / cudaHostRegister) for the copies to
  * run asynchronously; pageable memory works, without the overlap.  The
  * calls return when the output is on the host.  sht_round_trip_host is the
