@@ -17,8 +17,11 @@ reference's ``tensor_core_contractions=True`` (its TF32 opt-in) selects
 
 The reference's memory-layout knobs (``legendre_band``, ``streaming``,
 ``latitude_bands``) are accepted and validated but change nothing here: the
-tables are resident in HBM and the contraction walks the triangle directly.
-``order_partition`` (the multi-card order axis) is out of scope and refused.
+tables are resident in HBM and the contraction walks the triangle directly
+(``forward_streaming`` / ``inverse_streaming`` return the resident bits).
+``order_partition`` (a table built for some orders only) is refused: every
+order's table is resident; an order exchange's collective is honoured
+(``forward_orders`` / ``inverse_orders``).
 """
 from __future__ import annotations
 
@@ -219,9 +222,11 @@ class SphericalHarmonicTransform:
     #: contraction output here as there (``_agree_across_cards``) and its
     #: ``fill_rows`` completes a band-filled waist (``FourierWaist.close``).
     row_exchange = None
-    #: The multi-card order exchange, or None (transform.py:641-647).  The
-    #: order-partitioned contraction it serves is not built: a transform with
-    #: an exchange of more than one rank refuses to run forward or inverse.
+    #: The multi-card order exchange, or None (transform.py:641-647).  With
+    #: more than one rank, forward and inverse run on the order axis
+    #: (``forward_orders`` / ``inverse_orders``): the whole contraction on this
+    #: GPU, this rank's order columns gathered with the others' through the
+    #: exchange's ``gather_columns``.
     order_exchange = None
 
     grid: GaussianGrid
@@ -467,17 +472,123 @@ class SphericalHarmonicTransform:
         hook(self.backend.xp,
              (direction, name, tuple(int(v) for v in array.shape), str(array.dtype)), array)
 
-    def _refuse_order_exchange(self, what: str) -> None:
-        exchange = self.order_exchange
-        if exchange is not None and int(getattr(exchange, "world", 1)) > 1:
-            raise NotImplementedError(
-                f"{what}: the order-partitioned contraction of a multi-card order exchange is "
-                "not built by the B200 engine (one GPU holds every order's table)")
+    # ------------------------------------------------- the order axis
+    @property
+    def owned_order_range(self) -> tuple[int, int]:
+        """``(m_lo, m_hi)`` orders this transform holds a table for
+        (transform.py:828-836): every order, since one GPU holds the whole
+        table (``order_partition`` is refused at ``create``)."""
+        return (0, self.truncation + 1)
+
+    def _exchange_range(self, exchange) -> tuple[int, int]:
+        """The order range this rank owns, from the exchange or the table
+        (transform.py:1580-1584)."""
+        if exchange is not None and hasattr(exchange, "owned_order_range"):
+            m_lo, m_hi = (int(v) for v in exchange.owned_order_range)
+            if not 0 <= m_lo < m_hi <= self.truncation + 1:
+                raise ValueError(f"the exchange's owned_order_range {(m_lo, m_hi)} is not a "
+                                 f"non-empty range of orders in [0, {self.truncation + 1}]")
+            return m_lo, m_hi
+        return self.owned_order_range
+
+    def _gather_order_columns(self, exchange, compact, width, *, name):
+        """The whole ``(*lead, X, width)`` from every rank's columns through
+        the exchange's ``gather_columns`` (transform.py:1586-1599); with no
+        exchange, or a world of one, the columns are already whole."""
+        if exchange is None or int(getattr(exchange, "world", 1)) <= 1:
+            return compact
+        full = exchange.gather_columns(self.backend.xp, compact, int(width), name=name)
+        full = self.backend.asarray(full, dtype=self.backend.complex_dtype).contiguous()
+        if tuple(full.shape) != (*compact.shape[:-1], int(width)):
+            raise ValueError(f"gather_columns returned shape {tuple(full.shape)}, expected "
+                             f"{(*compact.shape[:-1], int(width))}")
+        return full
+
+    @staticmethod
+    def _multi_card(exchange) -> bool:
+        return exchange is not None and int(getattr(exchange, "world", 1)) > 1
+
+    def forward_orders(self, field, exchange=None):
+        """Analysis on the order axis (transform.py:1532-1557).
+
+        The reference's rank contracts only its own orders and the ranks
+        all-gather the coefficient columns.  Here every order's table is
+        resident, so the contraction runs whole on this GPU; this rank's
+        owned columns still go through the exchange's ``gather_columns`` (so
+        every rank takes the reference's collective step, named
+        ``"analysis_orders"``) and the gathered spectrum, disjoint column
+        ranges placed side by side, is the single-card spectrum bit for bit.
+        With no exchange, or a world of one, this is :meth:`forward`."""
+        exchange = self.order_exchange if exchange is None else exchange
+        whole = self._analyze_whole(field)
+        if not self._multi_card(exchange):
+            return whole
+        m_lo, m_hi = self._exchange_range(exchange)
+        full = self._gather_order_columns(exchange, whole[..., m_lo:m_hi].contiguous(),
+                                          self.truncation + 1, name="analysis_orders")
+        full[..., :, 0].imag.zero_()
+        return full
+
+    def inverse_orders(self, coeff, exchange=None):
+        """Synthesis on the order axis (transform.py:1559-1578): the waist
+        columns of this rank's orders are gathered with every rank's
+        (``"synthesis_orders"``), then the whole waist goes through the
+        inverse FFT.  The contraction runs whole on this GPU (every order's
+        table is resident), so the result is this engine's waist-path
+        synthesis (``waist_to_grid(contract_to_waist(c))``) bit for bit.
+        With no exchange, or a world of one, this is :meth:`inverse`."""
+        exchange = self.order_exchange if exchange is None else exchange
+        if not self._multi_card(exchange):
+            return self._synth("sht_inverse", coeff)
+        from .waist import FourierWaist, latitude_band_edges
+
+        m_lo, m_hi = self._exchange_range(exchange)
+        values = self.contract_to_waist(coeff).take()
+        full = self._gather_order_columns(exchange, values[..., m_lo:m_hi].contiguous(),
+                                          self.truncation + 1, name="synthesis_orders")
+        waist = FourierWaist(self, full, latitude_band_edges(self.grid.nlat,
+                                                             self.latitude_bands))
+        return self.waist_to_grid(waist)
+
+    # ------------------------------------------------- the streamed forms
+    @staticmethod
+    def _check_order_chunk(order_chunk) -> None:
+        if order_chunk is not None and int(order_chunk) < 1:
+            raise ValueError(f"order_chunk must be >= 1, got {order_chunk}")
+
+    def forward_streaming(self, field, *, order_chunk: int | None = None):
+        """:meth:`forward` without a resident table in the reference
+        (transform.py:1603-1618), whose contract is the resident table's
+        bits in O(order_chunk x (T+1) x nlat) host memory.  The plan here
+        keeps its tables resident in HBM (T1534's few GB on a 180 GB part),
+        so the streamed form is the resident contraction: the same bits,
+        and no per-chunk table."""
+        self._check_order_chunk(order_chunk)
+        return self.forward(field)
+
+    def inverse_streaming(self, coeff, *, order_chunk: int | None = None):
+        """:meth:`inverse`; see :meth:`forward_streaming`
+        (transform.py:1620-1627)."""
+        self._check_order_chunk(order_chunk)
+        return self.inverse(coeff)
+
+    def streaming_working_bytes(self, order_chunk: int | None = None) -> dict[str, int]:
+        """Bytes one streamed contraction holds for a chunk of orders
+        (transform.py:1025-1045): none here, since the streamed forms run on
+        the resident tables (``legendre_table_nbytes``) and allocate no
+        per-chunk block."""
+        self._check_order_chunk(order_chunk)
+        return {"recurrence": 0, "analysis": 0, "device": 0, "scratch": 0}
 
     # ---------------------------------------------------------- transforms
     def forward(self, field):
-        """grid -> spectral (transform.py:1486)."""
-        self._refuse_order_exchange("forward")
+        """grid -> spectral (transform.py:1486); on the order axis
+        (:meth:`forward_orders`) when a multi-card order exchange is set."""
+        if self._multi_card(self.order_exchange):
+            return self.forward_orders(field)
+        return self._analyze_whole(field)
+
+    def _analyze_whole(self, field):
         f = self._grid_in(field)
         lead = tuple(f.shape[:-2])
 
@@ -507,8 +618,10 @@ class SphericalHarmonicTransform:
             return self._batched_contract(op, self._basis if table is None else table)
 
     def inverse(self, coeff):
-        """spectral -> grid (transform.py:1742)."""
-        self._refuse_order_exchange("inverse")
+        """spectral -> grid (transform.py:1742); on the order axis
+        (:meth:`inverse_orders`) when a multi-card order exchange is set."""
+        if self._multi_card(self.order_exchange):
+            return self.inverse_orders(coeff)
         return self._synth("sht_inverse", coeff)
 
     # ------------------------------------------------- host-resident batches
