@@ -40,6 +40,7 @@ SHT_SL_QUASI_MONOTONE = 1
 SHT_SEMI_SOLVE_SHIFTED = 0
 SHT_SEMI_APPLY = 1
 SHT_SEMI_HALF_APPLY = 2
+SHT_SEMI_LINEAR_TENDENCIES = 3
 #: Kernel kinds of sht_plan_read_timing, in order.
 KERNEL_KINDS = ("fft_forward", "fft_inverse", "legendre_analysis", "legendre_synthesis", "pack",
                 "unpack", "elementwise", "helmholtz")

@@ -181,3 +181,9 @@ class GaussianGrid:
     def rms(self, field) -> float:
         arr = np.asarray(field, dtype=np.float64)
         return math.sqrt(max(0.0, self.global_mean(arr * arr)))
+
+    def degree_length_m(self, degree: int) -> float:
+        """The wavelength of total degree ``degree`` along a great circle,
+        2 pi a / n (infinite at n = 0; grid.py:229-231)."""
+        n = int(degree)
+        return math.inf if n == 0 else 2.0 * math.pi * self.radius_m / n

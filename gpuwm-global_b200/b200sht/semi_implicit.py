@@ -23,6 +23,7 @@ import ctypes
 import dataclasses
 import math
 from dataclasses import dataclass
+from typing import NamedTuple
 
 import numpy as np
 import torch
@@ -84,6 +85,26 @@ class VerticalModeOperator:
         self.x_eigenvalues = np.ascontiguousarray(x_eigenvalues, dtype=np.float64)
         self.x_eigenvectors = np.ascontiguousarray(x_eigenvectors, dtype=np.float64)
         self.x_eigenvectors_inv = np.ascontiguousarray(np.linalg.inv(self.x_eigenvectors))
+        # The reference state (set by from_coordinate; None for an operator
+        # built from ready matrices) and the modes as the reference reports
+        # them (semi_implicit.py:551-570).
+        self.reference_temperature_k = None
+        self.reference_surface_pressure_pa = None
+        self.phase_speeds_m_s = np.sqrt(self.eigenvalues)
+        self.equivalent_depths_m = self.eigenvalues / GRAVITY_M_S2
+
+    @property
+    def fastest_mode_m_s(self) -> float:
+        return float(self.phase_speeds_m_s[0])
+
+    def describe(self) -> dict:
+        return {
+            "reference_temperature_k": self.reference_temperature_k,
+            "reference_surface_pressure_pa": self.reference_surface_pressure_pa,
+            "nlev": self.nlev,
+            "phase_speeds_m_s": [float(v) for v in self.phase_speeds_m_s],
+            "equivalent_depths_m": [float(v) for v in self.equivalent_depths_m],
+        }
 
     @classmethod
     def from_coordinate(cls, vertical, reference_temperature_k: float,
@@ -155,7 +176,10 @@ class VerticalModeOperator:
         c = np.empty((nlev + 1, nlev))
         c[:nlev] = -gamma
         c[nlev] = -(dp / ps)
-        return cls(b, c)
+        op = cls(b, c)
+        op.reference_temperature_k = t_ref
+        op.reference_surface_pressure_pa = ps
+        return op
 
     @property
     def nlev(self) -> int:
@@ -237,6 +261,16 @@ class SpectralState:
 _METRIC = "semi_implicit_max_divergence_increment_s1"
 
 
+class LinearTendencies(NamedTuple):
+    """The weighted linear triple the explicit right-hand side must not
+    integrate (semi_implicit.py:205-215): ``(nlev, T+1, T+1)`` divergence
+    and theta tendencies and the ``(T+1, T+1)`` ln ps tendency."""
+
+    divergence: object
+    theta: object
+    log_surface_pressure: object
+
+
 @dataclass(frozen=True)
 class VerticalModeSemiImplicit:
     """Every vertical gravity-wave mode implicit; the reference's fields,
@@ -280,6 +314,37 @@ class VerticalModeSemiImplicit:
             return vertical
         return vertical_structure_operator(vertical, self.reference_temperature_k,
                                            self.reference_surface_pressure_pa)
+
+    def explicit_wave_speed_m_s(self, vertical) -> float:
+        """The fastest mode speed times the fraction left explicit
+        (semi_implicit.py:776-781)."""
+        fastest = self.operator(vertical).fastest_mode_m_s
+        if self.active:
+            return (1.0 - self.divergence_weight) * fastest
+        return fastest
+
+    def describe(self, vertical) -> dict:
+        """semi_implicit.py:783-790."""
+        return {
+            "scheme": self.scheme,
+            "enabled": bool(self.enabled),
+            "off_centring_weight": float(self.off_centring_weight),
+            "weight": float(self.divergence_weight),
+            **self.operator(vertical).describe(),
+        }
+
+    def linear_tendencies(self, state, transform, vertical):
+        """``w L y``: the divergence, theta and ln ps tendencies of the
+        weighted linear operator at the state, ``D_t = w k^2 (B x)`` and
+        ``x_t = w (C D)`` with ``x = (theta, ln ps)``, projected
+        (semi_implicit.py:796-813): one library call
+        (``SHT_SEMI_LINEAR_TENDENCIES``).  None when inactive."""
+        if not self.active:
+            return None
+        (d, th, lp), _ = self._map(transform, self.operator(vertical),
+                                   _lib.SHT_SEMI_LINEAR_TENDENCIES, self.divergence_weight,
+                                   state.divergence, state.theta, state.log_surface_pressure)
+        return LinearTendencies(d, th, lp)
 
     # ----------------------------------------------------------- arrays
     def _map(self, transform, operator, mode, dt_w, divergence, theta, lnps, outs=None):

@@ -157,6 +157,17 @@ class FourierWaist:
         """The waist rows of one latitude band, a view."""
         return self.values[..., int(r0):int(r1), :]
 
+    def drain_scratch(self, rows: int):
+        """A zero ``(*lead, rows, nlon//2 + 1)`` half spectrum on the device
+        for one band (transform.py:608-630): the orders above T stay the
+        zeros an inverse real FFT reads as the spectrum's vanishing tail.
+        A fresh buffer per call.  The engine's own drains
+        (``waist_band_to_grid``) run the FFT in the library and need none;
+        this is for a caller that drains a band itself."""
+        t = self.transform
+        return torch.zeros((*self.lead, int(rows), t.grid.nlon // 2 + 1),
+                           dtype=t.backend.complex_dtype, device=t.backend.device)
+
 
 # ----------------------------------------------------------------- methods
 def open_waist(self, lead, *, bands: int | None = None) -> FourierWaist:

@@ -1098,19 +1098,21 @@ int sht_semi_implicit_map(sht_plan* plan, const sht_vertical* op, int mode, doub
                           (const void*)out_theta, (const void*)out_lnps})
       check_ptr(q, "semi-implicit argument");
     SHT_REQUIRE(mode == SHT_SEMI_SOLVE_SHIFTED || mode == SHT_SEMI_APPLY ||
-                    mode == SHT_SEMI_HALF_APPLY,
-                "mode must be SHT_SEMI_SOLVE_SHIFTED, SHT_SEMI_APPLY or SHT_SEMI_HALF_APPLY");
-    SHT_REQUIRE(mode == SHT_SEMI_SOLVE_SHIFTED || (alpha >= 0.5 && alpha <= 1.0),
+                    mode == SHT_SEMI_HALF_APPLY || mode == SHT_SEMI_LINEAR_TENDENCIES,
+                "mode must be SHT_SEMI_SOLVE_SHIFTED, SHT_SEMI_APPLY, SHT_SEMI_HALF_APPLY or "
+                "SHT_SEMI_LINEAR_TENDENCIES");
+    const bool uses_alpha = mode == SHT_SEMI_APPLY || mode == SHT_SEMI_HALF_APPLY;
+    SHT_REQUIRE(!uses_alpha || (alpha >= 0.5 && alpha <= 1.0),
                 "off_centring_weight must lie in [0.5, 1]");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     plan->last_stream = s;
     const int kmode = mode == SHT_SEMI_APPLY ? kSemiApply
-                      : mode == SHT_SEMI_HALF_APPLY ? kSemiHalf : kSemiSolve;
+                      : mode == SHT_SEMI_HALF_APPLY ? kSemiHalf
+                      : mode == SHT_SEMI_LINEAR_TENDENCIES ? kSemiLinear : kSemiSolve;
     SHT_CUDA_OR_THROW(cudaMemsetAsync(op->metric, 0, sizeof(double), s));
     KernelScope k(plan, SHT_KIND_HELMHOLTZ, s);
     SHT_TYPED(plan, launch_semi_implicit<T>(plan, op->nlev, static_cast<const T*>(op->mats),
-                                            op->thermo, kmode, dt_w,
-                                            mode == SHT_SEMI_SOLVE_SHIFTED ? 1.0 : alpha,
+                                            op->thermo, kmode, dt_w, uses_alpha ? alpha : 1.0,
                                             CP(divergence), CP(theta), CP(lnps),
                                             MP(out_divergence), MP(out_theta), MP(out_lnps),
                                             static_cast<T*>(op->metric), nullptr, nullptr, s));

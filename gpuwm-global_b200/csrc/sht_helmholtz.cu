@@ -13,6 +13,10 @@
 //             = D + dt k^2 B (x + alpha (1-alpha) dt C D)
 //     D'      = V diag(1/(1 + (alpha dt)^2 k^2 lambda)) V^-1 forcing
 //     x'      = x + dt C ((1-alpha) D + alpha D')
+//   linear_tendencies, the weighted linear operator itself (kLinear, 796-813):
+//     D_t = w k^2 (B x),   x_t = w (C D)
+//     (projected like the maps, without the degree-zero pass-through: the
+//     tendency of degree zero is w k_0^2 B x = 0 for D and w C D for x)
 //   half_apply, the square root of that map (kHalf, 845-877 with
 //   symmetric_half_maps, 611-663):
 //     D' = V [diag(p_D) V^-1 D + diag(q_D) V^-1 (k^2 B x)]
@@ -375,6 +379,28 @@ __global__ void __launch_bounds__(256) semi_implicit_kernel(
       });
       continue;
     }
+    if (mode == kSemiLinear) {
+      // dt carries the weight w; the outputs are projected only.
+      const T wk2 = dt * k2;
+      matvec<T>(sB, nlev, L1, xs, tx, ty, [&](int i, T ar, T ai) {
+        V2<T> v = mk2<T>(wk2 * ar, wk2 * ai);
+        if (m == 0) v.y = T(0);
+        if (!live) v = mk2<T>(T(0), T(0));
+        if (m <= Tn) odiv[i * lev + cidx] = v;
+      });
+      matvec<T>(sC, L1, nlev, ds, tx, ty, [&](int i, T ar, T ai) {
+        V2<T> v = mk2<T>(dt * ar, dt * ai);
+        if (m == 0) v.y = T(0);
+        if (!live) v = mk2<T>(T(0), T(0));
+        if (m <= Tn) {
+          if (i < nlev)
+            otheta[i * lev + cidx] = v;
+          else
+            olnps[cidx] = v;
+        }
+      });
+      continue;
+    }
     const V2<T>* bx = xs;
     if (off_centred) {
       // gs = x + alpha (1-alpha) dt C D: the M D term folded into the B product
@@ -447,7 +473,8 @@ void launch_semi_implicit(const sht_plan* p, int nlev, const T* mats, bool has_t
                           T* odiv, T* otheta, T* olnps, T* metric, T* cfold, float* rowmax,
                           cudaStream_t s) {
   SHT_REQUIRE(nlev >= 1 && nlev <= kMaxLev, "nlev must be in [1, 96]");
-  SHT_REQUIRE(mode == kSemiSolve || mode == kSemiApply || mode == kSemiHalf,
+  SHT_REQUIRE(mode == kSemiSolve || mode == kSemiApply || mode == kSemiHalf ||
+                  mode == kSemiLinear,
               "unknown semi-implicit mode");
   SHT_REQUIRE(mode != kSemiHalf || has_thermo,
               "half_apply needs the thermodynamic block's modes (sht_vertical_create_modes)");

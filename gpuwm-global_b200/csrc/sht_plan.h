@@ -185,7 +185,7 @@ void launch_elementwise(const sht_plan* p, int mode, const T* in, int64_t planes
 
 // Semi-implicit maps (sht_helmholtz.cu).  `mats` packs B, C, V, V^-1,
 // lambda and, when has_thermo, W, W^-1, mu (the thermodynamic block's modes).
-enum SemiMode { kSemiSolve = 0, kSemiApply = 1, kSemiHalf = 2 };
+enum SemiMode { kSemiSolve = 0, kSemiApply = 1, kSemiHalf = 2, kSemiLinear = 3 };
 template <typename T>
 void launch_semi_implicit(const sht_plan* p, int nlev, const T* mats, bool has_thermo, int mode,
                           double dt, double alpha, const T* div, const T* theta, const T* lnps,

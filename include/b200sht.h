@@ -285,7 +285,11 @@ int sht_vertical_create_modes(sht_plan* plan, int nlev, const double* b, const d
  *   SHT_SEMI_APPLY          the off-centred Crank-Nicolson step with weight
  *                           alpha (apply, semi_implicit.py:887-919);
  *   SHT_SEMI_HALF_APPLY     its square root (half_apply, semi_implicit.py:845-877;
- *                           needs sht_vertical_create_modes).
+ *                           needs sht_vertical_create_modes);
+ *   SHT_SEMI_LINEAR_TENDENCIES  the weighted linear operator itself, dt_w = w:
+ *                           D_t = w k^2 (B x), x_t = w (C D)
+ *                           (linear_tendencies, semi_implicit.py:796-813; alpha
+ *                           ignored, no degree-zero pass-through, metric 0).
  * Degree zero passes through and the outputs are projected (_finish,
  * semi_implicit.py:815-843).  The largest |D' - D| of the call is kept on
  * the device in the operator; sht_semi_implicit_metric reads it
@@ -293,6 +297,7 @@ int sht_vertical_create_modes(sht_plan* plan, int nlev, const double* b, const d
 #define SHT_SEMI_SOLVE_SHIFTED 0
 #define SHT_SEMI_APPLY 1
 #define SHT_SEMI_HALF_APPLY 2
+#define SHT_SEMI_LINEAR_TENDENCIES 3
 int sht_semi_implicit_map(sht_plan* plan, const sht_vertical* op, int mode, double dt_w,
                           double alpha, const void* divergence, const void* theta,
                           const void* lnps, void* out_divergence, void* out_theta,

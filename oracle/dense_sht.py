@@ -375,6 +375,26 @@ def half_map_scalars(frequencies, dt_s, alpha):
     return root.real, np.where(frequencies > 0.0, root.imag / safe, 0.5 * float(dt_s))
 
 
+def linear_tendencies(divergence, theta, lnps, b_matrix, c_matrix, weight,
+                      radius_m=EARTH_RADIUS_M):
+    """``w L y`` (semi_implicit.py:796-813): ``D_t = w k^2 (B x)`` and
+    ``x_t = w (C D)`` with ``x = (theta, ln ps)``, each projected.  Returns
+    ``(divergence_t, theta_t, lnps_t)``."""
+    t1 = divergence.shape[-1]
+    k2 = _wave_k2(t1, radius_m)
+    x = np.concatenate([theta, lnps[None]], axis=0)
+    d_t = weight * k2[None, :, None] * np.einsum("ij,jnm->inm", b_matrix, x)
+    x_t = weight * np.einsum("ij,jnm->inm", c_matrix, divergence)
+    tri = np.tri(t1, dtype=bool)
+
+    def proj(c):
+        c = c * tri
+        c[..., :, 0] = c[..., :, 0].real
+        return c
+
+    return proj(d_t), proj(x_t[:-1]), proj(x_t[-1])
+
+
 def half_apply(divergence, theta, lnps, b_matrix, c_matrix, eigenvalues, eigenvectors,
                x_eigenvalues, x_eigenvectors, dt_w, alpha, radius_m=EARTH_RADIUS_M):
     """The square root ``H = P + Q L`` of the Crank-Nicolson map, per block

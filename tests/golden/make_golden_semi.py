@@ -7,7 +7,9 @@ Run in the build container, where the reference source tree is mounted:
 For two cases (T7 with 6 levels, T21 with 40) it builds the reference's
 ``HybridCoordinate.pressure_blend`` stack and its ``VerticalModeSemiImplicit``
 (default reference state; off-centring 0.5 and 0.55), runs ``solve_shifted``,
-``apply`` and ``half_apply`` on a seeded projected state, and writes
+``apply``, ``half_apply`` and ``linear_tendencies`` on a seeded projected
+state, records ``explicit_wave_speed_m_s`` and the modes ``describe`` reports,
+and writes
 ``semi_<case>.npz`` with:
 
 * the coordinate's half-level A and B and its hydrostatic geopotential
@@ -79,6 +81,8 @@ def main(ref_root: str) -> None:
         applied55, m_apply55 = semi55.apply(state, transform, vertical, dt)
         half, m_half = semi.half_apply(state, transform, vertical, dt)
         half55, m_half55 = semi55.half_apply(state, transform, vertical, dt)
+        lin = semi.linear_tendencies(state, transform, vertical)
+        lin90 = semi55.linear_tendencies(state, transform, vertical)
         np.savez_compressed(
             HERE / f"semi_{name}.npz",
             truncation=t, nlev=nlev, tau_s=tau, dt_s=dt,
@@ -106,6 +110,14 @@ def main(ref_root: str) -> None:
             half55_divergence=half55.divergence, half55_theta=half55.theta,
             half55_lnps=half55.log_surface_pressure,
             half55_metric=m_half55["semi_implicit_max_divergence_increment_s1"],
+            linear_divergence=lin.divergence, linear_theta=lin.theta,
+            linear_lnps=lin.log_surface_pressure,
+            linear90_divergence=lin90.divergence, linear90_theta=lin90.theta,
+            linear90_lnps=lin90.log_surface_pressure,
+            explicit_wave_speed_m_s=semi.explicit_wave_speed_m_s(vertical),
+            explicit90_wave_speed_m_s=semi55.explicit_wave_speed_m_s(vertical),
+            phase_speeds_m_s=np.asarray(semi.describe(vertical)["phase_speeds_m_s"]),
+            equivalent_depths_m=np.asarray(semi.describe(vertical)["equivalent_depths_m"]),
         )
         print("wrote semi", name)
 

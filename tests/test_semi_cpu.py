@@ -11,7 +11,7 @@ import numpy as np
 import pytest
 
 from conftest import load_golden
-from oracle.dense_sht import apply_crank_nicolson, half_apply, solve_shifted
+from oracle.dense_sht import apply_crank_nicolson, half_apply, linear_tendencies, solve_shifted
 from semi_fixtures import RecordedCoordinate
 
 CASES = ["semi_t7_l6.npz", "semi_t21_l40.npz"]
@@ -61,6 +61,30 @@ def test_oracle_maps_match_reference(case):
         _close(th, g[f"{key}_theta"], 1e-12)
         _close(lp, g[f"{key}_lnps"], 1e-12)
         assert abs(metric - float(g[f"{key}_metric"])) <= 1e-12 * float(g[f"{key}_metric"])
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_oracle_linear_tendencies_and_mode_report_match_reference(case):
+    from b200sht.semi_implicit import VerticalModeSemiImplicit
+
+    g = load_golden(case)
+    for key, weight in (("linear", 1.0), ("linear90", 0.9)):
+        d, th, lp = linear_tendencies(g["divergence"], g["theta"], g["lnps"], g["b_matrix"],
+                                      g["c_matrix"], weight, radius_m=float(g["radius_m"]))
+        _close(d, g[f"{key}_divergence"], 1e-13)
+        _close(th, g[f"{key}_theta"], 1e-13)
+        _close(lp, g[f"{key}_lnps"], 1e-13)
+    # the host-side report of the operator's modes and the explicit budget
+    vertical = RecordedCoordinate(g)
+    semi = VerticalModeSemiImplicit()
+    semi90 = VerticalModeSemiImplicit(off_centring_weight=0.55, divergence_weight=0.9)
+    report = semi.describe(vertical)
+    assert report["scheme"] == "vertical_modes" and report["nlev"] == int(g["nlev"])
+    assert report["reference_temperature_k"] == float(g["reference_temperature_k"])
+    _close(report["phase_speeds_m_s"], g["phase_speeds_m_s"], 1e-12)
+    _close(report["equivalent_depths_m"], g["equivalent_depths_m"], 1e-12)
+    assert semi.explicit_wave_speed_m_s(vertical) == float(g["explicit_wave_speed_m_s"]) == 0.0
+    _close(semi90.explicit_wave_speed_m_s(vertical), g["explicit90_wave_speed_m_s"], 1e-12)
 
 
 def test_semi_implicit_refusals_match_reference():
