@@ -121,6 +121,10 @@ SIGNATURES = {
     "sht_sl_departure_newton_ls": (ctypes.c_int, [_P, ctypes.c_int, _P, _P, _P, _P, _P, _P, _P,
                                                   _P, ctypes.c_int, _D, _D, _P, _P, _P, _P, _P,
                                                   _P]),
+    "sht_sl_lipschitz": (ctypes.c_int, [_P, ctypes.c_int, ctypes.c_int, ctypes.c_int, _P, _P, _P,
+                                        _P, ctypes.c_int, ctypes.c_int, _P, _P, _P, _P,
+                                        ctypes.c_int, ctypes.c_int, _D, _D, _D, _DP, _DP,
+                                        ctypes.POINTER(_I64), _P]),
     "sht_sl_window_create": (ctypes.c_int, [_P, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                             ctypes.c_int, ctypes.POINTER(_P)]),
     "sht_sl_window_destroy": (ctypes.c_int, [_P]),

@@ -14,6 +14,10 @@ dtype (float32 or float64).  Latitude-band windows (the reference's
 ``BandWindow``, ``HaloEscape``, ``SphericalGridTables.window``) give the
 banded step's gathers and searches over a band's rows from fields that hold
 the band and its halo (``sht_sl_gather_band``, ``sht_sl_departure_band``).
+The search's gate is the reference's too (trajectory.py:121-155, 755-1560):
+``lipschitz`` (the flow deformation, one kernel: ``sht_sl_lipschitz``),
+``LipschitzDiagnostics``, ``refuse_trajectory_fold``, ``convergence``,
+``converged_departure_points`` and ``level_rate_from_mass_flux``.
 """
 from __future__ import annotations
 
@@ -582,3 +586,276 @@ def departure_points(wind: CartesianWind, tables: SphericalGridTables, dt_s: flo
     xi, phi, lev, move_m, move_k = outs
     stencil = Stencil(xi=xi, phi=phi, level=lev, tables=tables, window=window)
     return stencil, _diagnostics(stencil, move_m, move_k, tables, dt_s, iterations)
+
+
+# ------------------------------------------------------- trajectory gate
+def level_rate_from_mass_flux(omega_half, *, p_full, xp=None):
+    """The vertical rate in level indices per second at full levels
+    (trajectory.py:121-155): the interface mass flux ``etadot dp/deta``
+    (Pa/s, ``nlev + 1`` interfaces, zero at both boundaries) divided by the
+    pressure distance between the neighbouring full levels, averaged onto
+    the levels.  ``p_full`` is the full-level pressure, ``(nlev, ...)``
+    broadcasting against the interfaces' trailing axes.  Works on torch
+    tensors and numpy arrays alike (``xp`` is accepted for the reference's
+    signature and not needed)."""
+    nlev = int(p_full.shape[0])
+    if int(omega_half.shape[0]) != nlev + 1:
+        raise ValueError(f"omega_half must have {nlev + 1} interfaces for {nlev} layers, "
+                         f"got {int(omega_half.shape[0])}")
+    if isinstance(omega_half, torch.Tensor):
+        s_half = torch.zeros_like(omega_half)
+        p = torch.as_tensor(p_full, dtype=omega_half.dtype, device=omega_half.device)
+    else:
+        s_half = np.zeros_like(omega_half)
+        p = p_full
+    distance = p[1:] - p[:-1]  # broadcast against omega_half[1:nlev] as given
+    s_half[1:nlev] = omega_half[1:nlev] / distance
+    return 0.5 * (s_half[:nlev] + s_half[1:nlev + 1])
+
+
+@dataclass(frozen=True)
+class LipschitzDiagnostics:
+    """The flow deformation: the fold determinants the trajectory gate reads
+    and the Jacobian norms reported beside them (the reference's
+    LipschitzDiagnostics, trajectory.py:755-952, same fields, properties
+    and receipt keys).  ``fold_determinant`` = the smaller of
+    min det(I - (dt/2) J_ex) (arrival side) and min det(I + (dt/2) J)
+    (departure side); the norms are per second (``jacobian_*``) and times dt
+    (``lipschitz_*``)."""
+
+    dt_s: float
+    reference_length_m: float
+    lipschitz: float
+    lipschitz_frobenius: float
+    lipschitz_horizontal: float
+    jacobian_spectral_s: float
+    jacobian_frobenius_s: float
+    jacobian_horizontal_s: float
+    lipschitz_vertical: float = 0.0
+    jacobian_vertical_s: float = 0.0
+    lipschitz_mixed: float = 0.0
+    lipschitz_balanced: float = 0.0
+    jacobian_balanced_s: float = 0.0
+    fold_determinant_arrival: float = 1.0
+    fold_determinant_departure: float = 1.0
+    fold_where_arrival: str = ""
+    fold_where_departure: str = ""
+
+    @property
+    def fold_determinant(self) -> float:
+        return min(self.fold_determinant_arrival, self.fold_determinant_departure)
+
+    @property
+    def fold_side(self) -> str:
+        return ("arrival" if self.fold_determinant_arrival <= self.fold_determinant_departure
+                else "departure")
+
+    @property
+    def binding_direction(self) -> str:
+        if self.lipschitz_balanced > 1.000001 * max(self.lipschitz_horizontal,
+                                                     self.lipschitz_vertical):
+            return "coupling"
+        return "vertical" if self.lipschitz_vertical > self.lipschitz_horizontal else "horizontal"
+
+    def as_dict(self) -> dict:
+        return {
+            "semilag_lipschitz": self.lipschitz,
+            "semilag_lipschitz_frobenius": self.lipschitz_frobenius,
+            "semilag_lipschitz_horizontal": self.lipschitz_horizontal,
+            "semilag_lipschitz_vertical": self.lipschitz_vertical,
+            "semilag_lipschitz_balanced": self.lipschitz_balanced,
+            "semilag_lipschitz_mixed": self.lipschitz_mixed,
+            "semilag_jacobian_balanced_s": self.jacobian_balanced_s,
+            "semilag_jacobian_spectral_s": self.jacobian_spectral_s,
+            "semilag_jacobian_frobenius_s": self.jacobian_frobenius_s,
+            "semilag_jacobian_horizontal_s": self.jacobian_horizontal_s,
+            "semilag_jacobian_vertical_s": self.jacobian_vertical_s,
+            "semilag_lipschitz_reference_length_m": self.reference_length_m,
+            "semilag_lipschitz_dt_s": self.dt_s,
+            "semilag_fold_determinant": self.fold_determinant,
+            "semilag_fold_determinant_arrival": self.fold_determinant_arrival,
+            "semilag_fold_determinant_departure": self.fold_determinant_departure,
+        }
+
+
+#: Levels per pass of the reference's diagnostic (accepted; the kernel here
+#: takes every level in one pass and holds no volume-sized temporary).
+LIPSCHITZ_LEVEL_CHUNK = 8
+#: The most iterations the departure search takes on a retry (trajectory.py).
+MAXIMUM_TRAJECTORY_ITERATIONS = 8
+#: The default floor under the fold determinant (trajectory.py).
+DEFAULT_MINIMUM_FOLD_DETERMINANT = 0.2
+
+
+def _where(flat: int, shape, lat_ext, dlam, a0: int) -> str:
+    _, nr, nl = shape
+    kk, jj, ii = flat // (nr * nl), (flat // nl) % nr, flat % nl
+    lat_d = float(np.degrees(lat_ext[jj + a0 + 2]))
+    lon_d = float(np.degrees(ii * dlam))
+    return f"level {kk}, lat {lat_d:.2f}, lon {lon_d:.2f}"
+
+
+def _flow_arrays(flow: CartesianWind, want, dtype, what):
+    out = []
+    for field in flow.arrays():
+        if tuple(int(s) for s in field.shape) != tuple(want):
+            raise ValueError(f"the {what} is {tuple(field.shape)} where {tuple(want)} was "
+                             "expected")
+        if field.dtype != dtype:
+            raise ValueError(f"the {what} is {field.dtype} where the grid tables were built "
+                             f"for {dtype}")
+        if not field.is_cuda:
+            raise ValueError(f"the {what} must be CUDA tensors")
+        out.append(field.contiguous())
+    return out
+
+
+def lipschitz(wind: CartesianWind, tables: SphericalGridTables, dt_s: float, *,
+              extrapolated: CartesianWind | None = None, reference_length_m: float | None = None,
+              level_chunk: int = LIPSCHITZ_LEVEL_CHUNK, fused_norms: bool = True,
+              window: BandWindow | None = None,
+              extrapolated_window: BandWindow | None = None) -> LipschitzDiagnostics:
+    """The flow deformation the trajectory has to stay inside
+    (trajectory.py:1174-1420): one kernel over every arrival point
+    (``sht_sl_lipschitz``) and one read of the reduced numbers.
+
+    ``extrapolated`` is the wind the search reads at the arrival point (None:
+    the wind itself).  With a ``window`` the wind holds the band and its halo
+    and the diagnostic is taken on the band's rows; a band's ``extrapolated``
+    wind holds the rows of ``extrapolated_window`` (the band's rows and one
+    row either side).  ``level_chunk`` and ``fused_norms`` are accepted for
+    the reference's signature: the kernel takes all levels in one pass."""
+    nlev, nrows, nlon = wind.shape
+    nlat = tables.nlat
+    held = nlat if window is None else window.source_rows
+    if (nrows, nlon) != (held, tables.nlon):
+        raise ValueError(f"the wind is {(nrows, nlon)} where {(held, tables.nlon)} rows were "
+                         f"expected on a {tables.shape} grid")
+    rows = slice(0, nlat) if window is None else window.arrival
+    ex_held0, ex_rows = (0, nlat) if window is None else (window.source.start, held)
+    if extrapolated is not None:
+        if window is None:
+            if tuple(extrapolated.shape) != tuple(wind.shape):
+                raise ValueError(f"the extrapolated wind is {extrapolated.shape} where the wind "
+                                 f"is {wind.shape}")
+        else:
+            if extrapolated_window is None or extrapolated_window.arrival != window.arrival:
+                raise ValueError("a band's extrapolated wind needs the window of the rows it "
+                                 "holds, computing the band's own rows")
+            want = extrapolated_window.source_shape(nlev)
+            if tuple(extrapolated.shape) != tuple(want):
+                raise ValueError(f"the band's extrapolated wind is {extrapolated.shape} where "
+                                 f"{want} was expected")
+            ex_held0, ex_rows = extrapolated_window.source.start, extrapolated_window.source_rows
+    lref = (tables.equatorial_spacing_m() if reference_length_m is None
+            else float(reference_length_m))
+    if not np.isfinite(lref) or lref <= 0.0:
+        raise ValueError("reference_length_m must be finite and positive")
+    if nlev < 2:
+        raise ValueError(f"nlev >= 2 is required, got {nlev}")
+    # the rows a derivative reads: the band's and one either side (the pole
+    # row itself beyond a pole)
+    need0 = 0 if rows.start == 0 else rows.start - 1
+    need1 = nlat if rows.stop == nlat else rows.stop + 1
+    if window is not None:
+        for h0, n in ((window.source.start, held),) + (
+                ((ex_held0, ex_rows),) if extrapolated is not None else ()):
+            if h0 > need0 or h0 + n < need1:
+                raise HaloEscape(window, "Lipschitz diagnostic")
+    ins = _flow_arrays(wind, wind.shape, tables.dtype, "wind")
+    exs = ([None] * 4 if extrapolated is None else
+           _flow_arrays(extrapolated, extrapolated.shape, tables.dtype, "extrapolated wind"))
+    maxima = (ctypes.c_double * 5)()
+    minima = (ctypes.c_double * 2)()
+    argmin = (ctypes.c_int64 * 2)()
+    src0 = 0 if window is None else window.source.start
+    _lib.call("sht_sl_lipschitz", tables._handle, int(nlev), int(rows.start), int(rows.stop),
+              *[_ptr(t) for t in ins], int(src0), int(held),
+              *[None if t is None else _ptr(t) for t in exs], int(ex_held0), int(ex_rows),
+              float(dt_s), float(tables.radius_m), float(lref), maxima, minima, argmin,
+              _stream())
+    sm, fm, hm, vm, bm = (max(0.0, float(v)) for v in maxima)
+    lat_ext = tables.host_tables(4)["lat_ext"]
+    shape = (nlev, rows.stop - rows.start, nlon)
+    folds = {}
+    for side, value, flat in (("departure", minima[0], argmin[0]),
+                              ("arrival", minima[1], argmin[1])):
+        value = float(value)
+        text = _where(int(flat), shape, lat_ext, tables.dlam, rows.start) if value < 2.0 else ""
+        folds[side] = (min(1.0, value), text)
+    dt = float(dt_s)
+    return LipschitzDiagnostics(
+        dt_s=dt, reference_length_m=lref, lipschitz=dt * max(hm, vm, bm),
+        lipschitz_frobenius=dt * fm, lipschitz_horizontal=dt * hm,
+        jacobian_spectral_s=sm, jacobian_frobenius_s=fm, jacobian_horizontal_s=hm,
+        lipschitz_vertical=dt * vm, jacobian_vertical_s=vm, lipschitz_mixed=dt * sm,
+        lipschitz_balanced=dt * bm, jacobian_balanced_s=bm,
+        fold_determinant_arrival=folds["arrival"][0],
+        fold_determinant_departure=folds["departure"][0],
+        fold_where_arrival=folds["arrival"][1], fold_where_departure=folds["departure"][1])
+
+
+def convergence(diagnostics: TrajectoryDiagnostics, limit_cells: float) -> None:
+    """Refuse a trajectory whose last iteration still moved more than
+    ``limit_cells`` of the local meridional grid length
+    (trajectory.py:1423-1441)."""
+    if diagnostics.move_max_cells > float(limit_cells):
+        raise ValueError(
+            "the departure-point search did not converge: the last of "
+            f"{diagnostics.iterations} iterations still moved a point by "
+            f"{diagnostics.move_max_m:.3f} m, which is "
+            f"{diagnostics.move_max_cells:.4f} of the local meridional grid "
+            f"length against a limit of {float(limit_cells):.4f}; an "
+            "unconverged trajectory mislocates the flow and shows no other symptom")
+
+
+def converged_departure_points(wind: CartesianWind, tables: SphericalGridTables, dt_s: float,
+                               *, iterations: int, limit_cells: float,
+                               extrapolated: CartesianWind | None = None,
+                               window: BandWindow | None = None, defer_escape: bool = False,
+                               solver: str = "fixed_point"):
+    """The departure points, converged or refused (trajectory.py:1454-1490):
+    a search whose last iteration still moved more than ``limit_cells`` is
+    run again from the start at ``MAXIMUM_TRAJECTORY_ITERATIONS`` before
+    ``convergence`` refuses it; a search that converges at the configured
+    count returns its own bits."""
+    stencil, diagnostics = departure_points(
+        wind, tables, dt_s, iterations=int(iterations), extrapolated=extrapolated,
+        window=window, defer_escape=defer_escape, solver=solver)
+    if (diagnostics.move_max_cells > float(limit_cells)
+            and int(iterations) < MAXIMUM_TRAJECTORY_ITERATIONS):
+        del stencil
+        stencil, diagnostics = departure_points(
+            wind, tables, dt_s, iterations=MAXIMUM_TRAJECTORY_ITERATIONS,
+            extrapolated=extrapolated, window=window, defer_escape=defer_escape, solver=solver)
+    convergence(diagnostics, limit_cells)
+    return stencil, diagnostics
+
+
+def refuse_trajectory_fold(diagnostics: LipschitzDiagnostics, minimum: float) -> None:
+    """Refuse a time step whose trajectory map folds: the fold determinant
+    below ``minimum`` (trajectory.py:1511-1560; the same message)."""
+    floor = float(minimum)
+    if not (0.0 <= floor < 1.0):
+        raise ValueError(
+            "the minimum fold determinant must lie in [0, 1): zero is the fold itself, and one "
+            "would refuse every flow with any divergence or strain at all")
+    value = diagnostics.fold_determinant
+    if not np.isfinite(value) or value < floor:
+        where = (diagnostics.fold_where_departure if diagnostics.fold_side == "departure"
+                 else diagnostics.fold_where_arrival)
+        raise ValueError(
+            f"the trajectory map folds: min det(I - (dt/2) J) over the grid "
+            f"reads {diagnostics.fold_determinant_arrival:.4f} on the "
+            f"arrival side and det(I + (dt/2) J) "
+            f"{diagnostics.fold_determinant_departure:.4f} on the departure "
+            f"side at dt = {diagnostics.dt_s:g} s, against a floor of "
+            f"{floor:.4f} (binding: {diagnostics.fold_side}, at {where}); at zero two "
+            "arrival points share a departure point and the interpolation "
+            "samples a folded field, which mislocates the flow silently.  "
+            f"The deformation norms, reported and not gated, read "
+            f"{diagnostics.lipschitz:.4f} (horizontal "
+            f"{diagnostics.lipschitz_horizontal:.4f}, vertical "
+            f"{diagnostics.lipschitz_vertical:.4f}, balanced "
+            f"{diagnostics.lipschitz_balanced:.4f}).  A shorter [time] dt_s "
+            "moves the determinant toward one")

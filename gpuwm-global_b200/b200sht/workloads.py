@@ -281,8 +281,8 @@ def sl_gather(args, clock_sampler):
     limited species, headline), cubic unlimited, quintic unlimited (the
     dynamical bundle) and the trilinear value."""
     from .grid import GaussianGrid
-    from .semilag import (SphericalGridTables, Stencil, gather_batch, gather_linear_batch,
-                          search_into)
+    from .semilag import (CartesianWind, SphericalGridTables, Stencil, gather_batch,
+                          gather_linear_batch, lipschitz, search_into)
 
     nlev, nfield = getattr(args, "sl_levels", 40), getattr(args, "sl_fields", 16)
     grid = GaussianGrid.create(511, nlat=768, nlon=1536)
@@ -347,14 +347,23 @@ def sl_gather(args, clock_sampler):
         ms = _time(lambda: search_into(tables, wind + wind, 3, 300.0, dep, solver="newton_ls"),
                    args.steps, args.warmup)
         out["departure_newton_ls_3_iterations"] = {"ms": ms, "points_per_s": npts / (ms * 1e-3)}
-        del wind, dep
+        # the trajectory gate's deformation diagnostic on the same wind, the
+        # arrival side reading an extrapolated wind (the same arrays): norms
+        # and both fold determinants, reduced to the host each call
+        flow = CartesianWind(*wind)
+        ms = _time(lambda: lipschitz(flow, tables, 300.0, extrapolated=flow), args.steps,
+                   args.warmup)
+        out["deformation_diagnostic"] = {"ms": ms, "points_per_s": npts / (ms * 1e-3),
+                                         "algorithmic_gb_per_s": npts * 32 / (ms * 1e-3) / 1e9,
+                                         "algorithmic_bytes_per_point": 32}
+        del wind, dep, flow
         out["rhs_kernels"] = _rhs_timings(args, (nlev, grid.nlat, grid.nlon), peak)
         out["point_sampling"] = _sampling_timings(args)
     head = out["cubic_quasi_monotone"]
     out["clocks"] = clocks.summary()
     out["value"] = head["point_fields_per_s"]
     out["ms_per_step"] = head["ms"]
-    out["gpu_launches"] = (len(cases) + 3 + 4) * args.steps
+    out["gpu_launches"] = (len(cases) + 3 + 4 + 2) * args.steps
     out["roofline"] = {"bound": "hbm", "achieved": head["algorithmic_gb_per_s"], "peak": peak,
                        "unit": "GB/s", "frac": head["algorithmic_gb_per_s"] / peak,
                        "traffic": None, "kernel": "sl_gather_kernel<float, 4, qm>",

@@ -40,6 +40,7 @@
 #include <type_traits>
 
 #include "sht_common.cuh"
+#include "sht_lipschitz.h"
 
 struct SlWidth {
   int ghost = 0;                // reflected rows beyond each pole
@@ -59,6 +60,7 @@ struct SlWidth {
 struct sht_sl_tables {
   int nlat = 0, nlon = 0, prec = 0, device = 0;
   SlWidth w4, w6;  // w6 empty when nlat < 6
+  void* d_lip = nullptr;  // scratch of the deformation diagnostic, made on first use
 };
 
 // One latitude band of a semi-Lagrangian step: arrival rows [a0, a1) read
@@ -1036,6 +1038,7 @@ int sht_sl_tables_destroy(sht_sl_tables* tables) {
     if (!tables) return;
     free_width(tables->w4);
     free_width(tables->w6);
+    if (tables->d_lip) cudaFree(tables->d_lip);
     delete tables;
   });
 }
@@ -1315,6 +1318,68 @@ int sht_sl_departure_newton(const sht_sl_tables* tables, int nlev, const void* v
   return departure_entry(kSolverNewton, nullptr, tables, nlev, vx, vy, vz, level_rate, vx_ex, vy_ex, vz_ex,
                          level_rate_ex, iterations, dt, radius, xi, phi, level, move_m, move_k,
                          stream);
+}
+
+int sht_sl_lipschitz(const sht_sl_tables* tables, int nlev, int a0, int a1, const void* vx,
+                     const void* vy, const void* vz, const void* level_rate, int held0,
+                     int held_rows, const void* vx_ex, const void* vy_ex, const void* vz_ex,
+                     const void* level_rate_ex, int ex_held0, int ex_held_rows, double dt,
+                     double radius, double reference_length, double* maxima, double* minima,
+                     int64_t* argmin, void* stream) {
+  return guarded([&] {
+    SHT_REQUIRE(tables != nullptr, "null semi-Lagrangian tables");
+    SHT_REQUIRE(vx && vy && vz && level_rate, "null wind array");
+    SHT_REQUIRE(maxima && minima && argmin, "null result array");
+    const bool has_ex = vx_ex != nullptr;
+    SHT_REQUIRE(!has_ex || (vy_ex && vz_ex && level_rate_ex),
+                "the extrapolated wind needs all four arrays (or none)");
+    const int nlat = tables->nlat;
+    SHT_REQUIRE(nlev >= 2, "the deformation diagnostic needs nlev >= 2");
+    SHT_REQUIRE(0 <= a0 && a0 < a1 && a1 <= nlat, "arrival rows out of range");
+    SHT_REQUIRE(std::isfinite(dt) && std::isfinite(radius) && radius > 0.0,
+                "dt and radius must be finite, radius positive");
+    SHT_REQUIRE(std::isfinite(reference_length) && reference_length > 0.0,
+                "reference_length_m must be finite and positive");
+    // Every row a derivative reads: the arrival rows and one neighbour each
+    // side (the pole row itself beyond a pole).
+    const int need0 = a0 == 0 ? 0 : a0 - 1, need1 = a1 == nlat ? nlat : a1 + 1;
+    auto covers = [&](int h0, int rows) {
+      return h0 >= 0 && rows >= 1 && h0 + rows <= nlat && h0 <= need0 && need1 <= h0 + rows;
+    };
+    SHT_REQUIRE(covers(held0, held_rows),
+                "the deformation diagnostic reads a row the band's wind does not hold (halo "
+                "escape)");
+    SHT_REQUIRE(!has_ex || covers(ex_held0, ex_held_rows),
+                "the deformation diagnostic reads a row the band's extrapolated wind does not "
+                "hold (halo escape)");
+    cudaStream_t s = (cudaStream_t)stream;
+    if (!tables->d_lip) {
+      void* p = nullptr;
+      SHT_CUDA_OR_THROW(cudaMalloc(&p, lipschitz_scratch_bytes()));
+      const_cast<sht_sl_tables*>(tables)->d_lip = p;
+    }
+    LipResult r{};
+    auto run = [&](auto zero) {
+      using T = decltype(zero);
+      LipFlow<T> w{{(const T*)vx, (const T*)vy, (const T*)vz, (const T*)level_rate}, held0,
+                   held_rows};
+      LipFlow<T> e{{nullptr, nullptr, nullptr, nullptr}, 0, 0};
+      if (has_ex)
+        e = LipFlow<T>{{(const T*)vx_ex, (const T*)vy_ex, (const T*)vz_ex, (const T*)level_rate_ex},
+                       ex_held0, ex_held_rows};
+      launch_lipschitz<T>(nlev, nlat, tables->nlon, a0, a1, (const T*)tables->w4.d_lat_ext, w, e,
+                          dt, radius, reference_length, tables->d_lip, &r, s);
+    };
+    if (tables->prec == SHT_PREC_F64)
+      run(0.0);
+    else
+      run(0.0f);
+    for (int q = 0; q < 5; ++q) maxima[q] = r.maxima[q];
+    minima[0] = r.minima[0];
+    minima[1] = r.minima[1];
+    argmin[0] = r.argmin[0];
+    argmin[1] = r.argmin[1];
+  });
 }
 
 int sht_sl_departure_newton_ls(const sht_sl_tables* tables, int nlev, const void* vx,

@@ -510,6 +510,34 @@ int sht_sl_departure_newton_ls(const sht_sl_tables* tables, int nlev, const void
                                double radius, void* xi, void* phi, void* level, void* move_m,
                                void* move_k, void* stream);
 
+/* The flow deformation the trajectory must stay inside (the reference's
+ * semilag/trajectory.py lipschitz, 1174-1420): at every point of the arrival
+ * rows [a0, a1), the Jacobian of (vx, vy, vz, level_rate) -- zonal centred
+ * differences, the three-point formula on the Gauss latitudes with the pole
+ * row read half a turn round beyond a pole, centred level differences with
+ * one-sided ends -- projected on the local east/north basis; out
+ *   maxima[5]  = max over the points of the spectral norm of the mixed-unit
+ *                3 x 3 (vertical entries scaled by reference_length), its
+ *                Frobenius norm, the spectral norm of the horizontal 2 x 2,
+ *                |d(level rate)/dk| and the spectral norm of the balanced
+ *                3 x 3 (per second);
+ *   minima[2]  = min det(I + (dt/2) J) (departure side, the wind) and
+ *                min det(I - (dt/2) J_ex) (arrival side, the extrapolated
+ *                wind, or the wind when vx_ex is NULL);
+ *   argmin[2]  = where each minimum sits, flat (level, arrival row, lon),
+ *                the first in that order among equal values.
+ * The wind holds rows [held0, held0 + held_rows) of the grid, the
+ * extrapolated wind [ex_held0, ex_held0 + ex_held_rows); both must hold the
+ * arrival rows and one row either side (the pole row at a pole), else
+ * SHT_ERR_ARG (a halo escape).  nlev >= 2.  Synchronises `stream`.  The
+ * tables' element type is the arrays'. */
+int sht_sl_lipschitz(const sht_sl_tables* tables, int nlev, int a0, int a1, const void* vx,
+                     const void* vy, const void* vz, const void* level_rate, int held0,
+                     int held_rows, const void* vx_ex, const void* vy_ex, const void* vz_ex,
+                     const void* level_rate_ex, int ex_held0, int ex_held_rows, double dt,
+                     double radius, double reference_length, double* maxima, double* minima,
+                     int64_t* argmin, void* stream);
+
 /* Fused right-hand-side kernels of the dycore step (the reference's
  * spectral/fused.py momentum_bernoulli_kernel, tracer_flux_kernel,
  * scalar_tendency_kernel, vertical_flux_divergence_kernel and their numpy
