@@ -143,6 +143,8 @@ SIGNATURES = {
     "sht_sampler_create": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(_P)]),
     "sht_sampler_destroy": (ctypes.c_int, [_P]),
     "sht_sample": (ctypes.c_int, [_P, _P, _I64, _I64, _P, _P, ctypes.c_int, _D, _P, _P, _P]),
+    "sht_sample_packed_basis": (ctypes.c_int, [_P, _I64, _P, _P, ctypes.c_int, ctypes.c_int, _P,
+                                               _P, _P]),
 }
 
 _lib = None

@@ -156,3 +156,79 @@ def regular_latlon_scalar(transform, coeff, *, nlat: int, nlon: int, include_pol
     lat, lon = regular_latlon_coordinates(nlat, nlon, include_poles=include_poles)
     lon2, lat2 = np.meshgrid(lon, lat)
     return lat, lon, sample_scalar(transform, coeff, lat2, lon2, chunk_points=chunk_points)
+
+
+# ------------------------------------------------- the packed basis form
+def triangle_index(truncation: int) -> tuple[np.ndarray, np.ndarray]:
+    """``(n, m)`` of every coefficient inside the triangle, order-major
+    (``m = 0..T``, ``n = m..T`` inside each order): the packed order of
+    ``packed_basis`` and ``packed_coefficients`` (sampling.py:72-80)."""
+    t = int(truncation)
+    ms = np.concatenate([np.full(t + 1 - m, m, dtype=np.int64) for m in range(t + 1)])
+    ns = np.concatenate([np.arange(m, t + 1, dtype=np.int64) for m in range(t + 1)])
+    return ns, ms
+
+
+def _torch_dtype(dtype) -> torch.dtype:
+    if dtype in (torch.float64, torch.float32):
+        return dtype
+    d = np.dtype(dtype)
+    if d == np.float64:
+        return torch.float64
+    if d == np.float32:
+        return torch.float32
+    raise ValueError(f"dtype must be float64 or float32, got {dtype!r}")
+
+
+def packed_basis(xp, truncation: int, lat_rad, lon_rad, *, gradient: bool, dtype=np.float64,
+                 device=None):
+    """The packed real basis blocks of a point chunk on the device
+    (sampling.py:198-237): scalar, one ``(2K, p)`` block ``B`` with
+    ``[Re c | Im c] @ B`` the field (``B[k] = mult P cos(m lam)``,
+    ``B[K + k] = -mult P sin(m lam)``); gradient, the zonal and meridional
+    blocks, whose products over ``a cos(phi)`` and ``a`` are the eastward
+    and northward derivatives.  ``K = (T+1)(T+2)/2`` in the order of
+    ``triangle_index``; one kernel (``sht_sample_packed_basis``).  ``xp`` is
+    accepted for the reference's signature; the blocks are CUDA tensors."""
+    t = int(truncation)
+    dev = torch.device(device) if device is not None else torch.device(
+        "cuda", torch.cuda.current_device())
+    lat = torch.as_tensor(np.asarray(lat_rad, dtype=np.float64).ravel(), device=dev)
+    lon = torch.as_tensor(np.asarray(lon_rad, dtype=np.float64).ravel(), device=dev)
+    if lat.numel() != lon.numel():
+        raise ValueError("lat_rad and lon_rad must hold the same number of points")
+    npts = int(lat.numel())
+    ktri = (t + 1) * (t + 2) // 2
+    tdt = _torch_dtype(dtype)
+    code = _lib.SHT_PREC_F64 if tdt == torch.float64 else _lib.SHT_PREC_F32
+    b0 = torch.empty((2 * ktri, npts), dtype=tdt, device=dev)
+    b1 = torch.empty_like(b0) if gradient else None
+    ptr = lambda x: ctypes.c_void_p(x.data_ptr()) if x is not None else None
+    with torch.cuda.device(dev):
+        _lib.call("sht_sample_packed_basis", _sampler(t, dev), npts, ptr(lat), ptr(lon),
+                  1 if gradient else 0, code, ptr(b0), ptr(b1),
+                  ctypes.c_void_p(torch.cuda.current_stream().cuda_stream))
+    return (b0, b1) if gradient else b0
+
+
+def packed_coefficients(xp, coeff, truncation: int, dtype=np.float64):
+    """``[Re c | Im c]`` of ``coeff (..., T+1, T+1)`` over the packed
+    triangle, ``(fields, 2K)`` in ``dtype`` with the leading dimensions
+    flattened, and the leading shape (sampling.py:240-254).  A CUDA tensor
+    stays on its device; anything else is read as host data."""
+    t = int(truncation)
+    c = coeff if isinstance(coeff, torch.Tensor) else torch.as_tensor(np.asarray(coeff))
+    lead = tuple(c.shape[:-2])
+    fields = int(np.prod(lead)) if lead else 1
+    n_idx, m_idx = triangle_index(t)
+    tri = torch.as_tensor(n_idx * (t + 1) + m_idx, device=c.device)
+    flat = c.reshape(fields, (t + 1) * (t + 1))[:, tri]
+    tdt = _torch_dtype(dtype)
+    packed = torch.empty((fields, 2 * int(tri.numel())), dtype=tdt, device=c.device)
+    if torch.is_complex(flat):
+        packed[:, :tri.numel()] = flat.real
+        packed[:, tri.numel():] = flat.imag
+    else:
+        packed[:, :tri.numel()] = flat
+        packed[:, tri.numel():] = 0
+    return packed, lead

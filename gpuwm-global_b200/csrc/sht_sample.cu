@@ -172,6 +172,71 @@ __global__ void __launch_bounds__(kSamplePoints * kSampleWarps) sample_kernel(co
   }
 }
 
+// The packed real basis blocks the reference's device sampler contracts
+// (spectral/sampling.py:198-237): one thread per (order m, point p), the
+// point fastest.  For the packed (n, m) row k (orders below m fill
+// T + 1 - m' rows each, n fastest) the scalar block holds
+// mult P cos(m lam) in row k and -mult P sin(m lam) in row K + k; the
+// gradient blocks hold -m mult P sin / -m mult P cos (zonal) and
+// mult dP cos / -mult dP sin (meridional), mult = 1 at m = 0 and 2 above.
+// The P and dP values are the sampler's recurrence, unfused.
+struct BasisArgs {
+  int T;
+  int64_t npoints, ktri;
+  const double *lat, *lon;
+  const double *a, *b, *c, *s;
+  void *out0, *out1;  // [2 K][npoints] of OUT
+};
+
+template <typename OUT, bool GRAD>
+__global__ void __launch_bounds__(256) packed_basis_kernel(const BasisArgs g) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (int64_t)(g.T + 1) * g.npoints) return;
+  const int64_t p = i % g.npoints;
+  const int m = (int)(i / g.npoints);
+  const int T = g.T, T1 = T + 1;
+  const double x = sin(g.lat[p]);
+  const double root = __dsqrt_rn(fmax(0.0, __dsub_rn(1.0, __dmul_rn(x, x))));
+  const double denom = __dsub_rn(__dmul_rn(x, x), 1.0);
+  double diag = 1.0 / sqrt(4.0 * kPi);
+  for (int k = 1; k <= m; ++k) diag = __dmul_rn(__dmul_rn(-g.s[k], root), diag);
+  double sn, cs;
+  sincos((double)m * g.lon[p], &sn, &cs);
+  const double mult = m == 0 ? 1.0 : 2.0;
+  const double mm = mult * (double)m;
+  OUT* b0 = static_cast<OUT*>(g.out0);
+  OUT* b1 = static_cast<OUT*>(g.out1);
+  const int64_t np = g.npoints, kk = g.ktri;
+  auto emit = [&](int64_t k, double P, double dP) {
+    if (GRAD) {
+      b0[k * np + p] = (OUT)(-__dmul_rn(__dmul_rn(mm, P), sn));
+      b0[(k + kk) * np + p] = (OUT)(-__dmul_rn(__dmul_rn(mm, P), cs));
+      b1[k * np + p] = (OUT)__dmul_rn(__dmul_rn(mult, dP), cs);
+      b1[(k + kk) * np + p] = (OUT)(-__dmul_rn(__dmul_rn(mult, dP), sn));
+    } else {
+      b0[k * np + p] = (OUT)__dmul_rn(__dmul_rn(mult, P), cs);
+      b0[(k + kk) * np + p] = (OUT)(-__dmul_rn(__dmul_rn(mult, P), sn));
+    }
+  };
+  int64_t k = (int64_t)m * T1 - (int64_t)m * (m - 1) / 2;
+  const double d0 =
+      m >= 1 ? __ddiv_rn(__dmul_rn(root, __dmul_rn(__dmul_rn((double)m, x), diag)), denom) : 0.0;
+  emit(k++, diag, d0);
+  const double* arow = g.a + (int64_t)m * T1;
+  const double* brow = g.b + (int64_t)m * T1;
+  const double* crow = g.c + (int64_t)m * T1;
+  double p2 = 0.0, p1 = diag;
+  for (int n = m + 1; n <= T; ++n) {
+    const double pn = n == m + 1
+                          ? __dmul_rn(__dmul_rn(__dsqrt_rn((double)(2 * m + 3)), x), diag)
+                          : __dmul_rn(arow[n], __dsub_rn(__dmul_rn(x, p1), __dmul_rn(brow[n], p2)));
+    const double num = __dsub_rn(__dmul_rn(__dmul_rn((double)n, x), pn), __dmul_rn(crow[n], p1));
+    emit(k++, pn, __ddiv_rn(__dmul_rn(root, num), denom));
+    p2 = p1;
+    p1 = pn;
+  }
+}
+
 template <bool GRAD>
 void launch_passes(SampleArgs g, const int* band, cudaStream_t s) {
   const unsigned blocks = (unsigned)div_up(g.npoints, kSamplePoints);
@@ -295,6 +360,36 @@ int sht_sample(sht_sampler* h, const void* coeff_mn, int64_t fields, int64_t npo
     cudaStream_t s = (cudaStream_t)stream;
     if (gradient) launch_passes<true>(g, h->d_band, s);
     else launch_passes<false>(g, h->d_band, s);
+  });
+}
+
+int sht_sample_packed_basis(sht_sampler* h, int64_t npoints, const double* lat_rad,
+                            const double* lon_rad, int gradient, int out_precision, void* out0,
+                            void* out1, void* stream) {
+  return guarded([&] {
+    SHT_REQUIRE(h != nullptr, "null sampler");
+    SHT_REQUIRE(lat_rad && lon_rad && out0, "null array pointer");
+    SHT_REQUIRE(!gradient || out1 != nullptr, "null meridional block");
+    SHT_REQUIRE(npoints >= 1 && npoints < (1LL << 31), "npoints must be in [1, 2^31)");
+    SHT_REQUIRE(out_precision == SHT_PREC_F64 || out_precision == SHT_PREC_F32,
+                "out_precision must be SHT_PREC_F64 or SHT_PREC_F32");
+    int dev = 0;
+    SHT_CUDA_OR_THROW(cudaGetDevice(&dev));
+    SHT_REQUIRE(dev == h->device, "the sampler lives on another device");
+    const int64_t ktri = (int64_t)(h->T + 1) * (h->T + 2) / 2;
+    BasisArgs g{h->T, npoints, ktri, lat_rad, lon_rad, h->d_a, h->d_b, h->d_c, h->d_s, out0,
+                out1};
+    const int64_t threads = (int64_t)(h->T + 1) * npoints;
+    const unsigned blocks = (unsigned)div_up(threads, 256);
+    cudaStream_t s = (cudaStream_t)stream;
+    if (out_precision == SHT_PREC_F64) {
+      if (gradient) packed_basis_kernel<double, true><<<blocks, 256, 0, s>>>(g);
+      else packed_basis_kernel<double, false><<<blocks, 256, 0, s>>>(g);
+    } else {
+      if (gradient) packed_basis_kernel<float, true><<<blocks, 256, 0, s>>>(g);
+      else packed_basis_kernel<float, false><<<blocks, 256, 0, s>>>(g);
+    }
+    SHT_CUDA_OR_THROW(cudaGetLastError());
   });
 }
 

@@ -585,6 +585,18 @@ int sht_sampler_destroy(sht_sampler* sampler);
 int sht_sample(sht_sampler* sampler, const void* coeff_mn, int64_t fields, int64_t npoints,
                const double* lat_rad, const double* lon_rad, int gradient, double radius,
                double* out0, double* out1, void* stream);
+/* The packed real basis blocks of the reference's device sampler
+ * (spectral/sampling.py packed_basis, 198-237) at npoints points (device
+ * lat/lon in radians), each block [2 K][npoints], K = (T+1)(T+2)/2, rows in
+ * the packed order of triangle_index (order-major, n fastest), in FP64 or
+ * FP32 (out_precision SHT_PREC_F64 / SHT_PREC_F32).  gradient == 0: out0 =
+ * [mult P cos(m lam); -mult P sin(m lam)], so that [Re c | Im c] @ out0 is
+ * the field; gradient != 0: out0 = [-m mult P sin; -m mult P cos] (zonal),
+ * out1 = [mult dP/dphi cos; -mult dP/dphi sin] (meridional); mult = 1 at
+ * m = 0, 2 above.  The values are sht_sample's recurrence. */
+int sht_sample_packed_basis(sht_sampler* sampler, int64_t npoints, const double* lat_rad,
+                            const double* lon_rad, int gradient, int out_precision, void* out0,
+                            void* out1, void* stream);
 
 #ifdef __cplusplus
 }

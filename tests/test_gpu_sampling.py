@@ -94,3 +94,54 @@ def test_sampling_small_truncations(T):
     e, n = sample_gradient(t, dc, lat, lon)
     we, wn = O.sample(c, lat, lon, gradient=True)
     assert _rel(e, we) < 1e-12 and _rel(n, wn) < 1e-12
+
+
+@pytest.mark.parametrize("T", [7, 21])
+def test_packed_basis_blocks(T):
+    """The reference's packed-basis form (sampling.py:198-254): the blocks
+    against the oracle's recurrence entry by entry, [Re c | Im c] @ B against
+    the sampled field and gradient, and the FP32 blocks as the FP64 ones
+    rounded once."""
+    from b200sht import SphericalHarmonicTransform
+    from b200sht.sampling import (packed_basis, packed_coefficients, sample_gradient,
+                                  sample_scalar, triangle_index)
+    from b200sht.synthetic import red_spectrum
+    from oracle import sampling as O
+    from oracle.dense_sht import legendre_derivative_table, legendre_table
+
+    t = SphericalHarmonicTransform.create(T, precision="float64")
+    rng = np.random.default_rng(100 + T)
+    lat_d = rng.uniform(-85, 85, 45)
+    lon_d = rng.uniform(0, 360, 45)
+    lat, lon = np.deg2rad(lat_d), np.deg2rad(lon_d)
+    b = packed_basis(torch, T, lat, lon, gradient=False).cpu().numpy()
+    bz, bm = (x.cpu().numpy() for x in packed_basis(torch, T, lat, lon, gradient=True))
+    k = (T + 1) * (T + 2) // 2
+    assert b.shape == bz.shape == bm.shape == (2 * k, lat.size)
+    n_idx, m_idx = triangle_index(T)
+    mu = np.sin(lat)
+    p = legendre_table(T, mu)[n_idx, m_idx]            # (K, points)
+    dp = legendre_derivative_table(T, mu, legendre_table(T, mu))[n_idx, m_idx]
+    mult = np.where(m_idx == 0, 1.0, 2.0)[:, None]
+    ang = m_idx[:, None] * lon[None, :]
+    want = np.concatenate([mult * p * np.cos(ang), -(mult * p * np.sin(ang))])
+    assert np.max(np.abs(b - want)) <= 1e-13 * np.max(np.abs(want))
+    mm = mult * m_idx[:, None]
+    want_z = np.concatenate([-(mm * p * np.sin(ang)), -(mm * p * np.cos(ang))])
+    want_m = np.concatenate([mult * dp * np.cos(ang), -(mult * dp * np.sin(ang))])
+    assert np.max(np.abs(bz - want_z)) <= 1e-13 * np.max(np.abs(want_z))
+    assert np.max(np.abs(bm - want_m)) <= 1e-13 * np.max(np.abs(want_m))
+    # the contraction of the packed spectrum with the blocks is the sample
+    c = red_spectrum(T, 3, 7 + T)
+    pc, lead = packed_coefficients(torch, c, T)
+    assert lead == (3,) and tuple(pc.shape) == (3, 2 * k)
+    pc = pc.cpu().numpy()
+    dc = torch.as_tensor(c, device="cuda")
+    assert _rel(pc @ b, sample_scalar(t, dc, lat_d, lon_d)) < 1e-12
+    assert _rel(pc @ b, O.sample(c, lat_d, lon_d)) < 1e-12
+    a = t.grid.radius_m
+    e, nrt = sample_gradient(t, dc, lat_d, lon_d)
+    assert _rel(pc @ bz / (a * np.cos(lat)), e) < 1e-12 and _rel(pc @ bm / a, nrt) < 1e-12
+    # FP32 blocks: the FP64 values rounded once
+    b32 = packed_basis(torch, T, lat, lon, gradient=False, dtype=np.float32).cpu().numpy()
+    assert b32.dtype == np.float32 and np.array_equal(b32, b.astype(np.float32))
