@@ -59,7 +59,15 @@ struct LipArgs {
   T two_dlam, radius, inv_y, lref, half;
   T* part;              // [gridDim.x][7]
   long long* part_idx;  // [gridDim.x][2]
+  // Per arrival row: sin phi, cos phi, 1 / (a max(cos phi, 1e-12)) and the
+  // three-point latitude formula's numerators and denominators n0, d0, n1,
+  // d1, n2, d2; per longitude: sin lam, cos lam.  Filled once per launch by
+  // lipschitz_tables_kernel with the very operations a point would do.
+  T* rows;  // [nrows][kRowVals]
+  T* cols;  // [nlon][2]
 };
+
+constexpr int kRowVals = 9;
 
 // The twelve derivatives of one flow at one point: d/dx, d/dy, d/dk of the
 // three Cartesian components, then of the level rate.
@@ -76,8 +84,34 @@ __device__ __forceinline__ T at(const LipFlow<T>& F, int c, int nlon, int nheld,
 }
 
 template <typename T>
+__global__ void lipschitz_tables_kernel(LipArgs<T> a) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < a.nrows) {
+    const int j = a.a0 + t;
+    const T lat = __ldg(a.lat_ext + j + 2);
+    const T sph = sin(lat), cph = cos(lat);
+    const T x0 = __ldg(a.lat_ext + j + 1), x1 = lat, x2 = __ldg(a.lat_ext + j + 3);
+    T* r = a.rows + (int64_t)t * kRowVals;
+    r[0] = sph;
+    r[1] = cph;
+    r[2] = T(1) / mul(a.radius, fmax(cph, T(1e-12)));
+    r[3] = sub(x1, x2);
+    r[4] = mul(sub(x0, x1), sub(x0, x2));
+    r[5] = sub(sub(mul(T(2), x1), x0), x2);
+    r[6] = mul(sub(x1, x0), sub(x1, x2));
+    r[7] = sub(x1, x0);
+    r[8] = mul(sub(x2, x0), sub(x2, x1));
+  }
+  if (t < a.nlon) {
+    const T lon = (T)((double)t * a.dlam);
+    a.cols[2 * t] = sin(lon);
+    a.cols[2 * t + 1] = cos(lon);
+  }
+}
+
+template <typename T>
 __device__ void gradient(const LipArgs<T>& a, const LipFlow<T>& F, int k, int j, int i, T inv_x,
-                         Grad<T>& g) {
+                         const T* __restrict__ row, Grad<T>& g) {
   const int nlon = a.nlon, nh = F.held;
   const int ip = i + 1 == nlon ? 0 : i + 1;
   const int im = i == 0 ? nlon - 1 : i - 1;
@@ -85,10 +119,7 @@ __device__ void gradient(const LipArgs<T>& a, const LipFlow<T>& F, int k, int j,
   const int half_turn = (i - nlon / 2 + nlon) % nlon;
   const int ju = j == 0 ? 0 : j - 1, iu = j == 0 ? half_turn : i;
   const int jd = j == a.nlat - 1 ? j : j + 1, id = j == a.nlat - 1 ? half_turn : i;
-  const T x0 = __ldg(a.lat_ext + j + 1), x1 = __ldg(a.lat_ext + j + 2), x2 = __ldg(a.lat_ext + j + 3);
-  const T n0 = sub(x1, x2), d0 = mul(sub(x0, x1), sub(x0, x2));
-  const T n1 = sub(sub(mul(T(2), x1), x0), x2), d1 = mul(sub(x1, x0), sub(x1, x2));
-  const T n2 = sub(x1, x0), d2 = mul(sub(x2, x0), sub(x2, x1));
+  const T n0 = row[3], d0 = row[4], n1 = row[5], d1 = row[6], n2 = row[7], d2 = row[8];
   const int kd = k == 0 ? 0 : k - 1, ku = k == a.nlev - 1 ? k : k + 1;
   const bool centred = k > 0 && k < a.nlev - 1;
 #pragma unroll
@@ -234,13 +265,12 @@ __global__ void __launch_bounds__(kLipThreads) lipschitz_kernel(LipArgs<T> a) {
     const long long kr = p / a.nlon;
     const int r = (int)(kr % a.nrows), k = (int)(kr / a.nrows);
     const int j = a.a0 + r;
-    const T lat = __ldg(a.lat_ext + j + 2);
-    const T lon = (T)((double)i * a.dlam);
-    const T sph = sin(lat), cph = cos(lat), sla = sin(lon), cla = cos(lon);
-    const T inv_x = T(1) / mul(a.radius, fmax(cph, T(1e-12)));
+    const T* row = a.rows + (int64_t)r * kRowVals;
+    const T sph = row[0], cph = row[1], inv_x = row[2];
+    const T sla = a.cols[2 * i], cla = a.cols[2 * i + 1];
     const Basis<T> b{-sla, cla, mul(-sph, cla), mul(-sph, sla), cph};
     Grad<T> g;
-    gradient<T>(a, a.wind, k, j, i, inv_x, g);
+    gradient<T>(a, a.wind, k, j, i, inv_x, row, g);
     T nr[4];
     jacobian_norms<T>(b, g, a.lref, nr);
     const T vert = fabs(g.sk);
@@ -248,7 +278,7 @@ __global__ void __launch_bounds__(kLipThreads) lipschitz_kernel(LipArgs<T> a) {
 #pragma unroll
     for (int q = 0; q < 5; ++q) mx[q] = v5[q] > mx[q] ? v5[q] : mx[q];
     take_min(fold_det<T>(b, g, cplus), p, mn[0], at_mn[0]);
-    if (a.ex.f[0] != nullptr) gradient<T>(a, a.ex, k, j, i, inv_x, g);
+    if (a.ex.f[0] != nullptr) gradient<T>(a, a.ex, k, j, i, inv_x, row, g);
     take_min(fold_det<T>(b, g, cminus), p, mn[1], at_mn[1]);
   }
   // CTA reduction through shared memory, then one partial record per CTA.
@@ -324,10 +354,13 @@ __global__ void __launch_bounds__(kLipThreads) lipschitz_combine_kernel(const T*
 
 }  // namespace
 
-size_t lipschitz_scratch_bytes() {
-  // partials (7 doubles + 2 indices per CTA) and the result record
-  return (size_t)kLipMaxBlocks * (7 * sizeof(double) + 2 * sizeof(long long)) +
-         7 * sizeof(double) + 2 * sizeof(long long) + 64;
+// Scratch layout: partials (7 doubles + 2 indices per CTA), the result
+// record (7 doubles, 2 indices), then the row and column tables in doubles.
+constexpr size_t kPartBytes = (size_t)kLipMaxBlocks * (7 * sizeof(double) + 2 * sizeof(long long));
+constexpr size_t kResultBytes = 7 * sizeof(double) + 2 * sizeof(long long);
+
+size_t lipschitz_scratch_bytes(int nlat, int nlon) {
+  return kPartBytes + kResultBytes + sizeof(double) * ((size_t)nlat * kRowVals + 2 * (size_t)nlon);
 }
 
 template <typename T>
@@ -362,9 +395,13 @@ void launch_lipschitz(int nlev, int nlat, int nlon, int a0, int a1, const T* lat
   char* base = static_cast<char*>(scratch);
   a.part = reinterpret_cast<T*>(base);
   a.part_idx = reinterpret_cast<long long*>(base + (size_t)kLipMaxBlocks * 7 * sizeof(double));
-  double* res = reinterpret_cast<double*>(base + (size_t)kLipMaxBlocks * (7 * sizeof(double) +
-                                                                          2 * sizeof(long long)));
+  double* res = reinterpret_cast<double*>(base + kPartBytes);
   long long* res_idx = reinterpret_cast<long long*>(res + 7);
+  a.rows = reinterpret_cast<T*>(base + kPartBytes + kResultBytes);
+  a.cols = a.rows + (size_t)a.nrows * kRowVals;
+  const int nt = std::max(a.nrows, nlon);
+  lipschitz_tables_kernel<T><<<(nt + 255) / 256, 256, 0, s>>>(a);
+  SHT_CUDA_OR_THROW(cudaGetLastError());
   lipschitz_kernel<T><<<blocks, kLipThreads, 0, s>>>(a);
   SHT_CUDA_OR_THROW(cudaGetLastError());
   lipschitz_combine_kernel<T><<<1, kLipThreads, 0, s>>>(a.part, a.part_idx, blocks, res, res_idx);

@@ -25,9 +25,9 @@ struct LipResult {
   long long argmin[2];
 };
 
-// Bytes of device scratch the launcher needs (per-block partials and the
-// reduced result).
-size_t lipschitz_scratch_bytes();
+// Bytes of device scratch the launcher needs on an nlat x nlon grid
+// (per-block partials, the reduced result, the row and column tables).
+size_t lipschitz_scratch_bytes(int nlat, int nlon);
 
 // The diagnostics of the arrival rows [a0, a1) of an nlat x nlon grid
 // (lat_ext: the extended latitudes in T, row j at j + 2; the rows beyond a

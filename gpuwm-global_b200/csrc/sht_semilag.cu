@@ -1355,7 +1355,7 @@ int sht_sl_lipschitz(const sht_sl_tables* tables, int nlev, int a0, int a1, cons
     cudaStream_t s = (cudaStream_t)stream;
     if (!tables->d_lip) {
       void* p = nullptr;
-      SHT_CUDA_OR_THROW(cudaMalloc(&p, lipschitz_scratch_bytes()));
+      SHT_CUDA_OR_THROW(cudaMalloc(&p, lipschitz_scratch_bytes(nlat, tables->nlon)));
       const_cast<sht_sl_tables*>(tables)->d_lip = p;
     }
     LipResult r{};

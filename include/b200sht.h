@@ -530,7 +530,9 @@ int sht_sl_departure_newton_ls(const sht_sl_tables* tables, int nlev, const void
  * extrapolated wind [ex_held0, ex_held0 + ex_held_rows); both must hold the
  * arrival rows and one row either side (the pole row at a pole), else
  * SHT_ERR_ARG (a halo escape).  nlev >= 2.  Synchronises `stream`.  The
- * tables' element type is the arrays'. */
+ * tables' element type is the arrays'.  The call's scratch (per-CTA
+ * partials, row and column tables) belongs to the tables object: one call
+ * at a time per tables object. */
 int sht_sl_lipschitz(const sht_sl_tables* tables, int nlev, int a0, int a1, const void* vx,
                      const void* vy, const void* vz, const void* level_rate, int held0,
                      int held_rows, const void* vx_ex, const void* vy_ex, const void* vz_ex,

@@ -113,3 +113,46 @@ def test_errors():
         tracer_flux(x, x.double(), x, x)
     with pytest.raises(ValueError, match="nlev \\+ 1"):
         vertical_flux_divergence(x, x, x, x)
+
+
+@pytest.mark.parametrize("dt", [torch.float64, torch.float32])
+def test_reference_kernel_factories(dt):
+    """The reference's ``*_kernel(xp)(...)`` calling forms (fused.py:233-386,
+    as dynamics.py calls them): the same bits as the functions, outputs
+    written in place when passed."""
+    from b200sht import rhs as R
+
+    rng = np.random.default_rng(9)
+    nlev, nlat, nlon = 6, 5, 12
+    dev = lambda a: torch.as_tensor(a.astype(NP[dt]), device="cuda")
+    three = [dev(rng.standard_normal((nlev, nlat, nlon))) for _ in range(8)]
+    two = [dev(rng.standard_normal((nlat, nlon))) for _ in range(3)]
+    zeta, u, v, wu, wv, tv, pg, phi = three
+    cor, ge, gn = two
+    want = R.momentum_bernoulli(zeta, cor, u, v, wu, wv, tv, pg, ge, gn, phi, 287.04)
+    got = R.momentum_bernoulli_kernel(torch)(zeta, cor, u, v, wu, wv, tv, pg, ge, gn, phi,
+                                             NP[dt](287.04))
+    outs = [torch.empty_like(zeta) for _ in range(3)]
+    R.momentum_bernoulli_kernel(torch)(zeta, cor, u, v, wu, wv, tv, pg, ge, gn, phi, 287.04,
+                                       *outs)
+    for a, b, c in zip(got, outs, want):
+        assert torch.equal(a, c) and torch.equal(b, c)
+    dp = dev(np.abs(rng.standard_normal((nlev, nlat, nlon))) + 1.0)
+    s = dev(rng.standard_normal((3, nlev, nlat, nlon)))
+    fluxes = torch.empty((2, *s.shape), dtype=dt, device="cuda")
+    R.tracer_flux_kernel(torch)(dp, s, u, v, fluxes[0], fluxes[1])
+    assert torch.equal(fluxes, R.tracer_flux(dp, s, u, v))
+    fx, fy = R.tracer_flux_kernel(torch)(dp, s, u, v)
+    assert torch.equal(fx, fluxes[0]) and torch.equal(fy, fluxes[1])
+    h, vert = (dev(rng.standard_normal(s.shape)) for _ in range(2))
+    dpt = dev(rng.standard_normal((nlev, nlat, nlon)))
+    assert torch.equal(R.scalar_tendency_kernel(torch)(h, vert, s, dpt, dp),
+                       R.scalar_tendency(h, vert, s, dpt, dp))
+    ph = dev(np.cumsum(np.abs(rng.standard_normal((nlev + 1, nlat, nlon))) + 1.0, axis=0))
+    pf = torch.sqrt(ph[:-1] * ph[1:]).contiguous()
+    w = dev(rng.standard_normal((nlev + 1, nlat, nlon)))
+    out = torch.empty_like(s)
+    R.vertical_flux_divergence_kernel(torch)(s, w, pf, ph, nlev, nlat * nlon, out)
+    assert torch.equal(out, R.vertical_flux_divergence(s, w, pf, ph))
+    with pytest.raises(ValueError, match="do not match"):
+        R.vertical_flux_divergence_kernel(torch)(s, w, pf, ph, nlev + 1, nlat * nlon, out)
