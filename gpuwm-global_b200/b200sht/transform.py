@@ -491,6 +491,30 @@ class SphericalHarmonicTransform:
             return m_lo, m_hi
         return self.owned_order_range
 
+    def _contract_orders(self, values, table, m_lo, m_hi, *, transposed=False):
+        """Only orders ``[m_lo, m_hi)`` of a contraction, compactly
+        (transform.py:1491-1530): the analysis of waist values gives
+        ``(*lead, T+1, m_hi-m_lo)`` coefficient columns, a synthesis of
+        coefficients ``(*lead, nlat, m_hi-m_lo)`` waist columns.  The whole
+        table is resident, so these are the whole contraction's columns
+        there, bit for bit."""
+        m_lo, m_hi = int(m_lo), int(m_hi)
+        if not 0 <= m_lo < m_hi <= self.truncation + 1:
+            raise ValueError(f"orders [{m_lo}, {m_hi}) are not a non-empty range in "
+                             f"[0, {self.truncation + 1}]")
+        with self._contraction_scope():
+            whole = self._batched_contract(values, table, transposed=transposed,
+                                           realify=table == "analysis")
+        return whole[..., m_lo:m_hi].contiguous()
+
+    def _analyze(self, field, table=None, *, bands=None):
+        """grid -> spectral through the waist (transform.py:1474-1484)."""
+        return self.contract_waist(self.fourier_waist(field, bands=bands), table)
+
+    def _synthesize(self, coeff, table=None, *, bands=None):
+        """spectral -> grid through the waist (transform.py:1736-1739)."""
+        return self.waist_to_grid(self.contract_to_waist(coeff, table, bands=bands))
+
     def _gather_order_columns(self, exchange, compact, width, *, name):
         """The whole ``(*lead, X, width)`` from every rank's columns through
         the exchange's ``gather_columns`` (transform.py:1586-1599); with no

@@ -114,3 +114,29 @@ def test_streamed_forms_return_the_resident_bits(precision):
         t.forward_streaming(np.zeros(t.grid.shape), order_chunk=0)
     assert t.streaming_working_bytes(32) == {"recurrence": 0, "analysis": 0, "device": 0,
                                             "scratch": 0}
+
+
+@pytest.mark.parametrize("precision", ["float64", "float32"])
+def test_compact_order_contractions(precision):
+    """``_contract_orders`` (the reference's rank-local contraction, which its
+    multi-card tests call) returns the whole contraction's columns bit for
+    bit; ``_analyze`` / ``_synthesize`` are the waist-path transforms."""
+    from b200sht import SphericalHarmonicTransform
+    from b200sht.synthetic import red_spectrum
+
+    T = 21
+    t = SphericalHarmonicTransform.create(T, precision=precision)
+    coeff = torch.as_tensor(red_spectrum(T, 2), device="cuda").to(t.backend.complex_dtype)
+    field = t.inverse(coeff)
+    spec = t.contract_waist(t.fourier_waist(field))
+    waist = t.contract_to_waist(coeff).take()
+    for lo, hi in ((0, 5), (5, 22), (11, 12)):
+        got = t._contract_orders(t.fourier_waist(field).take(), t._analysis, lo, hi)
+        assert tuple(got.shape) == (2, T + 1, hi - lo) and torch.equal(got, spec[..., lo:hi])
+        got = t._contract_orders(coeff, t._basis, lo, hi)
+        assert tuple(got.shape) == (2, t.grid.nlat, hi - lo)
+        assert torch.equal(got, waist[..., lo:hi])
+    with pytest.raises(ValueError, match="non-empty range"):
+        t._contract_orders(coeff, t._basis, 4, 4)
+    assert torch.equal(t._analyze(field), spec)
+    assert torch.equal(t._synthesize(coeff), t.waist_to_grid(t.contract_to_waist(coeff)))
