@@ -21,10 +21,12 @@
 // without fused multiply-adds (every product and sum rounded on its own), so
 // the only differences from the reference are the last bits of sin, cos and
 // acos.  One thread per point, consecutive threads along a latitude row (the
-// neighbour loads of a warp share cache lines), a grid of a few CTAs per SM;
-// each CTA reduces its points to partial maxima/minima in shared memory and
-// one CTA combines the partials.  HBM-bound: every field is read from DRAM
-// about once.
+// neighbour loads of a warp share cache lines), one resident wave of CTAs
+// (three per SM in FP32 at 78 registers, two in FP64); each CTA reduces its
+// points to partial maxima/minima in shared memory and one CTA combines the
+// partials.  Every field is read from DRAM about once, but the kernel is
+// bound by its arithmetic (some 45 correctly rounded divisions, 10 square
+// roots and two arccosines per point), not by those 32 bytes per point.
 #include <algorithm>
 #include <cfloat>
 #include <climits>
@@ -253,7 +255,7 @@ __device__ __forceinline__ void take_min(T v, long long idx, T& cur, long long& 
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kLipThreads) lipschitz_kernel(LipArgs<T> a) {
+__global__ void __launch_bounds__(kLipThreads, sizeof(T) == 4 ? 3 : 2) lipschitz_kernel(LipArgs<T> a) {
   T mx[5] = {T(0), T(0), T(0), T(0), T(0)};
   T mn[2] = {T(INFINITY), T(INFINITY)};
   long long at_mn[2] = {LLONG_MAX, LLONG_MAX};
@@ -371,10 +373,14 @@ void launch_lipschitz(int nlev, int nlat, int nlon, int a0, int a1, const T* lat
   int dev = 0, sms = 0;
   SHT_CUDA_OR_THROW(cudaGetDevice(&dev));
   SHT_CUDA_OR_THROW(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  int per_sm = 0;
+  SHT_CUDA_OR_THROW(
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lipschitz_kernel<T>, kLipThreads, 0));
+  per_sm = std::max(1, std::min(per_sm, kLipBlocksPerSm));
   const long long npts = (long long)nlev * (a1 - a0) * nlon;
   const int blocks = (int)std::max<long long>(
-      1, std::min<long long>({(npts + kLipThreads - 1) / kLipThreads,
-                              (long long)sms * kLipBlocksPerSm, (long long)kLipMaxBlocks}));
+      1, std::min<long long>({(npts + kLipThreads - 1) / kLipThreads, (long long)sms * per_sm,
+                              (long long)kLipMaxBlocks}));
   LipArgs<T> a;
   a.nlev = nlev;
   a.nlat = nlat;

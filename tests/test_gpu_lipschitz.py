@@ -183,3 +183,42 @@ def test_converged_departure_points_retries_then_refuses():
     assert d3.iterations == 1 and torch.equal(st3.phi, one.phi)
     with pytest.raises(ValueError, match="did not converge"):
         converged_departure_points(wind, tables, 3600.0, iterations=1, limit_cells=0.0)
+
+
+@pytest.mark.parametrize("tag", TAGS)
+def test_north_pole_band_against_the_oracle(tag):
+    """A band that ends at the north pole (its rows beyond the pole are the
+    pole row half a turn round), with an extrapolated band window, against
+    the oracle; and a whole-grid call with a two-level grid (the vertical
+    differences one-sided at both ends)."""
+    from b200sht.semilag import lipschitz
+    from oracle import sl_lipschitz as O
+
+    g, tables, dtype = _setup(tag)
+    nlat, nlon = tables.nlat, tables.nlon
+    lat_ext = tables.host_tables(4)["lat_ext"]
+    tol = 1e-12 if tag == "f64" else 2e-6
+    src, arr, ex_rows = (21, nlat), (24, nlat), (23, nlat)
+    wind = [f[:, src[0]:src[1]] for f in g["wind"]]
+    ex = [f[:, ex_rows[0]:ex_rows[1]] for f in g["wind_ex"]]
+    want = O.lipschitz(wind, lat_ext, nlon, float(g["radius_m"]), float(g["dt_long"]),
+                       extrapolated=ex, held=src, arrival=arr, extrapolated_held=ex_rows)
+    d = lipschitz(_flow(g["wind"], src, dtype), tables, float(g["dt_long"]),
+                  window=tables.window(slice(*src), slice(*arr)),
+                  extrapolated=_flow(g["wind_ex"], ex_rows, dtype),
+                  extrapolated_window=tables.window(slice(*ex_rows), slice(*arr)))
+    assert _rel(d.jacobian_spectral_s, want["spectral"]) <= tol
+    assert _rel(d.jacobian_balanced_s, want["balanced"]) <= tol
+    assert _rel(d.jacobian_vertical_s, want["vertical"]) <= tol
+    assert _rel(d.fold_determinant_departure, min(1.0, want["fold_departure"])) <= tol
+    assert _rel(d.fold_determinant_arrival, min(1.0, want["fold_arrival"])) <= tol
+    assert d.fold_where_arrival == O.where_text(want["where_arrival"], want["shape"], lat_ext,
+                                                nlon, arr[0])
+    two = [f[:2] for f in g["wind"]]
+    want2 = O.lipschitz(two, lat_ext, nlon, float(g["radius_m"]), 600.0)
+    from b200sht.semilag import CartesianWind
+
+    d2 = lipschitz(CartesianWind(*(torch.as_tensor(np.ascontiguousarray(f), dtype=dtype,
+                                                   device="cuda") for f in two)), tables, 600.0)
+    assert _rel(d2.jacobian_vertical_s, want2["vertical"]) <= tol
+    assert _rel(d2.fold_determinant_departure, min(1.0, want2["fold_departure"])) <= tol
