@@ -261,11 +261,18 @@ __global__ void __launch_bounds__(kLipThreads, sizeof(T) == 4 ? 3 : 2) lipschitz
   long long at_mn[2] = {LLONG_MAX, LLONG_MAX};
   const long long npts = (long long)a.nlev * a.nrows * a.nlon;
   const T cplus = a.half, cminus = -a.half;
-  for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < npts;
-       p += (long long)gridDim.x * blockDim.x) {
-    const int i = (int)(p % a.nlon);
-    const long long kr = p / a.nlon;
-    const int r = (int)(kr % a.nrows), k = (int)(kr / a.nrows);
+  // The grid stride and the first point decomposed into (level, row, lon)
+  // once; each step then carries the lon and row components by one
+  // subtraction at most (the stride's own components are below nlon and
+  // nrows), so the loop does no integer division per point.
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  const long long plane = (long long)a.nrows * a.nlon;
+  const int step_i = (int)(stride % a.nlon), step_r = (int)((stride / a.nlon) % a.nrows);
+  const int step_k = (int)(stride / plane);
+  long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  int i = (int)(p % a.nlon), r = (int)((p / a.nlon) % a.nrows);
+  int k = (int)(p / plane);
+  for (; p < npts; p += stride) {
     const int j = a.a0 + r;
     const T* row = a.rows + (int64_t)r * kRowVals;
     const T sph = row[0], cph = row[1], inv_x = row[2];
@@ -282,6 +289,19 @@ __global__ void __launch_bounds__(kLipThreads, sizeof(T) == 4 ? 3 : 2) lipschitz
     take_min(fold_det<T>(b, g, cplus), p, mn[0], at_mn[0]);
     if (a.ex.f[0] != nullptr) gradient<T>(a, a.ex, k, j, i, inv_x, row, g);
     take_min(fold_det<T>(b, g, cminus), p, mn[1], at_mn[1]);
+    i += step_i;
+    int carry = 0;
+    if (i >= a.nlon) {
+      i -= a.nlon;
+      carry = 1;
+    }
+    r += step_r + carry;
+    carry = 0;
+    if (r >= a.nrows) {
+      r -= a.nrows;
+      carry = 1;
+    }
+    k += step_k + carry;
   }
   // CTA reduction through shared memory, then one partial record per CTA.
   __shared__ T s_v[7][kLipThreads];
