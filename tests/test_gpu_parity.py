@@ -342,3 +342,37 @@ def test_t511_against_oracle_two_planes():
         assert rel_l2(np_(sht.forward(g)), want_c) < tol, precision
         assert rel_max(np_(sht.inverse(coeff)), want_g) < tol, precision
         sht.check_device()
+
+
+def test_baseline_configs_at_full_plane_counts():
+    """The first two benchmark configurations at their full plane counts
+    (40 levels x 4 fields + ln ps = 161 planes): T62 on the 94 x 192 grid in
+    FP64 against the oracle on every plane (forward, inverse, and u, v from
+    vorticity/divergence on the 40 levels), and T255 on 384 x 768 in FP32
+    against the FP64 plan on every plane."""
+    from b200sht import SphericalHarmonicTransform, VorticityDivergenceOperator
+    from b200sht.synthetic import red_spectrum
+    from oracle.dense_sht import DenseSHT
+
+    planes = 40 * 4 + 1
+    sht = SphericalHarmonicTransform.create(62, nlat=94, nlon=192, dealias_factor=1.49,
+                                            precision="float64")
+    ora = DenseSHT(62, 94, 192, dealias_factor=1.49)
+    np_ = sht.backend.to_numpy
+    coeff = red_spectrum(62, planes, seed=11)
+    grid = ora.inverse(coeff)
+    assert rel_max(np_(sht.inverse(coeff)), grid) < 1e-12
+    assert rel_l2(np_(sht.forward(grid)), ora.forward(grid)) < 1e-12
+    vec = VorticityDivergenceOperator(sht)
+    u, v = (np_(x) for x in vec.wind_from_vordiv(coeff[:40], coeff[40:80]))
+    uo, vo = ora.wind_from_vordiv(coeff[:40], coeff[40:80])
+    assert rel_max(u, uo) < 1e-12 and rel_max(v, vo) < 1e-12
+
+    t64 = SphericalHarmonicTransform.create(255, precision="float64")
+    t32 = SphericalHarmonicTransform.create(255, precision="float32")
+    c = red_spectrum(255, planes, seed=12)
+    g64 = t64.inverse(c)
+    assert rel_max(np_(t32.inverse(c)), np_(g64)) < 2e-6
+    assert rel_l2(t32.backend.to_numpy(t32.forward(g64.float())),
+                  np_(t64.forward(g64))) < 2e-6
+    t32.check_device()
