@@ -453,6 +453,15 @@ def main():
             ach = flops_per_plane(T, nlat) * P / (ms_l * 1e-3) / 1e12
             plain_leg[k] = {"ms_per_launch": ms_l, "achieved_tflops": ach,
                             "frac_of_ffma_peak": ach / ffma.value}
+    # The split path's Legendre kernels against the tensor-core peak: the
+    # three FP16 products of the folded triangle, 3 nlat (T+1)(T+2) flops
+    # per plane per direction.
+    split_leg = {}
+    for k in ("legendre_analysis", "legendre_synthesis"):
+        if k in per_launch:
+            ach = 3 * flops_per_plane(T, nlat) * P / (per_launch[k] * 1e-3) / 1e12
+            split_leg[k] = {"ms_per_launch": per_launch[k], "achieved_tflops": ach,
+                            "frac_of_bf16_peak_sustained": ach / peaks["bf16_tflops_sustained"]}
     traffic = ncu_traffic(dom, T)
     roof["traffic"] = None if traffic is None else traffic * P
     roof["kernel"] = dom
@@ -523,6 +532,7 @@ def main():
                                "ffma_peak_tflops_measured": ffma.value},
                 "split16_overlapped_accumulators": {"value": ws * P / (ms_overlap * 1e-3),
                                                     "ms_per_step": ms_overlap, **err_overlap},
+                "split16_legendre": split_leg,
                 "split_over_plain": value / value_plain,
                 "split_errors": err_split,
                 "errors_measured_against": "this engine's FP64 plan on all planes (its FP64 "
