@@ -65,3 +65,24 @@ def test_round_trip_host_at_t511_meets_the_bar():
     got = t.round_trip_host(grid.float().cpu().pin_memory(), chunk=2).numpy()
     assert np.max(np.abs(got - ref)) / np.max(np.abs(ref)) < 2e-6
     t.check_device()
+
+
+@pytest.mark.parametrize("precision", ["float32", "split16"])
+@pytest.mark.parametrize("planes", [57, 200])
+def test_default_chunk_schedule_on_a_register_fft_grid(precision, planes):
+    """The default schedule (chunks ramped 2, 4, ... at both ends, an odd
+    chunk where the plane count is odd) on a grid the register-resident FFTs
+    serve (T62 on 94 x 192): the same numbers as the whole-batch device
+    calls."""
+    from b200sht import SphericalHarmonicTransform
+    from b200sht.synthetic import red_spectrum
+
+    t = SphericalHarmonicTransform.create(62, nlat=94, nlon=192, dealias_factor=1.49,
+                                          precision=precision)
+    coeff = torch.as_tensor(red_spectrum(62, planes, seed=3)).to(t.backend.complex_dtype)
+    grid_dev = t.inverse(coeff.to(t.backend.device))
+    rt_dev = t.inverse(t.forward(grid_dev)).cpu()
+    got = t.round_trip_host(grid_dev.cpu().pin_memory())
+    assert torch.equal(got, rt_dev)
+    assert torch.equal(t.forward_host(grid_dev.cpu().pin_memory()), t.forward(grid_dev).cpu())
+    t.check_device()
